@@ -1,0 +1,676 @@
+// S2 (FAST-9 + NMS + 2K pre-selection + Harris + top-K) and S3 (7x7 blur +
+// IC angle + rBRIEF-256) kernels for sm_100a.
+//
+// Every kernel reads its image and buffers from a "job". A job source is
+// either one job passed by value (the per-image stage call) or a device table
+// of jobs plus a block-prefix array (the batched chain, where one launch
+// covers every image of every pair). Results are identical either way.
+//
+// Reference semantics (file:line in the reference tree):
+//   FAST score        src/s2_s3/s2.cu:37-67   (cornerScore<16>, circle order)
+//   NMS + histogram   src/s2_s3/s2.cu:81-106
+//   2K threshold      src/s2_s3/s2.cu:108-139 (SelectParams)
+//   raster compaction src/s2_s3/s2.cu:141-235 (all above, then first ties)
+//   Harris            src/s2_s3/s2.cu:247-285 (no-FMA float formula, key)
+//   top-K order       src/s2_s3/s2.cu:287-310 (descending key)
+//   blur              src/s2_s3/s3.cu:41-73
+//   describe          src/s2_s3/s3.cu:75-157
+#pragma once
+
+#include "common.cuh"
+
+namespace stitch::b200::s2s3 {
+
+// ---------------------------------------------------------------- jobs
+
+struct SelectParams {
+    std::uint32_t threshold;  // FAST score at the 2K boundary
+    std::uint32_t above;      // maxima with score > threshold
+    std::uint32_t ties;       // maxima at the threshold that are kept
+    std::uint32_t selected;   // above + ties
+};
+
+struct DetectJob {
+    const std::uint8_t* image;
+    int width, height, pitch;
+    int threshold, max_keypoints;
+    float harris_k;
+    // workspace
+    std::uint8_t* maxima;          // width*height NMS-surviving scores
+    std::uint32_t* hist;           // [256], zeroed before the FAST launch
+    SelectParams* params;
+    std::uint32_t* chunk_counts;   // [2 * chunks] (above, tie) per chunk
+    std::uint64_t* keys;           // [candidates]
+    // output
+    float* x;
+    float* y;
+    float* response;  // may be null
+    int* count;
+    // launch bookkeeping
+    int tiles_x, tiles, chunks, candidates;
+};
+
+struct DescribeJob {
+    const std::uint8_t* image;
+    int width, height, pitch;
+    std::uint8_t* blurred;  // dense width*height
+    const float* x;
+    const float* y;
+    const int* count;
+    int capacity;
+    std::uint8_t* out;  // rows of row_stride bytes
+    int row_stride;
+    int tiles_x, tiles;  // blur tiles
+};
+
+// Per-image job passed by value.
+template <class Job> struct OneJob {
+    Job job;
+    __device__ bool find(int block, int /*kind*/, Job* j, int* local) const {
+        *j = job;
+        *local = block;
+        return true;
+    }
+};
+
+// Device table: prefix[kind * (n + 1) + i] is the first block of job i for
+// launch kind `kind`; blocks past the end are idle.
+template <class Job> struct JobTable {
+    const Job* jobs;
+    const int* prefix;
+    int n;
+    __device__ bool find(int block, int kind, Job* j, int* local) const {
+        const int* p = prefix + kind * (n + 1);
+        if (block >= p[n]) return false;
+        int lo = 0, hi = n - 1;
+        while (lo < hi) {  // largest i with p[i] <= block
+            const int mid = (lo + hi + 1) >> 1;
+            if (p[mid] <= block) lo = mid; else hi = mid - 1;
+        }
+        *j = jobs[lo];
+        *local = block - p[lo];
+        return true;
+    }
+};
+
+enum DetectKind { kFastKind = 0, kChunkKind = 1, kHarrisKind = 2, kSortKind = 3, kDetectKinds = 4 };
+enum DescribeKind { kBlurKind = 0, kDescKind = 1, kDescribeKinds = 2 };
+
+constexpr int kFastTileW = 64, kFastTileH = 32;
+constexpr int kFastInW = kFastTileW + 8, kFastInH = kFastTileH + 8;  // halo 4 = FAST 3 + NMS 1
+constexpr int kFastScW = kFastTileW + 2, kFastScH = kFastTileH + 2;
+constexpr int kChunkPx = 8192;     // pixels per compaction block (256 threads x 32)
+constexpr int kHarrisThreads = 256;
+constexpr int kSortCap = 16384;    // candidates sorted in shared memory by one block
+constexpr int kSortThreads = 1024;
+constexpr int kBlurTileW = 64, kBlurTileH = 32;
+constexpr int kDescWarps = 8;
+constexpr int kEdge = 31;
+
+// ------------------------------------------------------------- FAST + NMS
+
+// FAST-9 score of the pixel at p (row stride `stride`): for each of the 16
+// circular 9-pixel arcs take the smallest centre-minus-ring difference (arc
+// darker) and the smallest ring-minus-centre difference (arc brighter); the
+// score is the largest of these minus one when it exceeds the threshold.
+// Windowed minima are built from pairwise minima (2 -> 4 -> 8 -> 9).
+__device__ __forceinline__ int fast_score(const std::uint8_t* p, int stride, int thr) {
+    const int v = p[0];
+    const int s0 = p[3 * stride], s4 = p[3], s8 = p[-3 * stride], s12 = p[-3];
+    // A qualifying 9-arc always contains two of the four compass pixels.
+    const int hi = v + thr, lo = v - thr;
+    const int bright = (s0 > hi) + (s4 > hi) + (s8 > hi) + (s12 > hi);
+    const int dark = (s0 < lo) + (s4 < lo) + (s8 < lo) + (s12 < lo);
+    if (bright < 2 && dark < 2) return 0;
+    int d[16];
+    d[0] = v - s0;
+    d[1] = v - p[3 * stride + 1];
+    d[2] = v - p[2 * stride + 2];
+    d[3] = v - p[1 * stride + 3];
+    d[4] = v - s4;
+    d[5] = v - p[-1 * stride + 3];
+    d[6] = v - p[-2 * stride + 2];
+    d[7] = v - p[-3 * stride + 1];
+    d[8] = v - s8;
+    d[9] = v - p[-3 * stride - 1];
+    d[10] = v - p[-2 * stride - 2];
+    d[11] = v - p[-1 * stride - 3];
+    d[12] = v - s12;
+    d[13] = v - p[1 * stride - 3];
+    d[14] = v - p[2 * stride - 2];
+    d[15] = v - p[3 * stride - 1];
+    int mn2[16], mx2[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        mn2[k] = min(d[k], d[(k + 1) & 15]);
+        mx2[k] = max(d[k], d[(k + 1) & 15]);
+    }
+    int mn4[16], mx4[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        mn4[k] = min(mn2[k], mn2[(k + 2) & 15]);
+        mx4[k] = max(mx2[k], mx2[(k + 2) & 15]);
+    }
+    int best = INT_MIN;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        const int mn9 = min(min(mn4[k], mn4[(k + 4) & 15]), d[(k + 8) & 15]);
+        const int mx9 = max(max(mx4[k], mx4[(k + 4) & 15]), d[(k + 8) & 15]);
+        best = max(best, max(mn9, -mx9));
+    }
+    return best > thr ? best - 1 : 0;
+}
+
+// One block = one 64x32 output tile: stage the tile with a 4-pixel halo in
+// shared memory, score the tile plus a 1-pixel ring, keep strict 3x3 maxima
+// inside the 31-pixel edge margin, write the maxima map and add the
+// survivors' scores to the image histogram.
+template <class Src>
+__global__ __launch_bounds__(256) void fast_nms_kernel(const __grid_constant__ Src src) {
+    __shared__ std::uint8_t in[kFastInH][kFastInW];
+    __shared__ std::uint8_t sc[kFastScH][kFastScW];
+    __shared__ std::uint32_t hist[256];
+    DetectJob j;
+    int local;
+    if (!src.find(blockIdx.x, kFastKind, &j, &local)) return;
+    const int tid = threadIdx.x;
+    const int W = j.width, H = j.height;
+    const int y0 = (local / j.tiles_x) * kFastTileH;
+    const int x0 = (local % j.tiles_x) * kFastTileW;
+    hist[tid] = 0;
+    for (int i = tid; i < kFastInH * kFastInW; i += 256) {
+        const int r = i / kFastInW, c = i - r * kFastInW;
+        const int gy = y0 - 4 + r, gx = x0 - 4 + c;
+        in[r][c] = (gx >= 0 && gx < W && gy >= 0 && gy < H)
+                       ? j.image[static_cast<std::size_t>(gy) * j.pitch + gx] : 0;
+    }
+    __syncthreads();
+    for (int i = tid; i < kFastScH * kFastScW; i += 256) {
+        const int r = i / kFastScW, c = i - r * kFastScW;
+        const int gy = y0 - 1 + r, gx = x0 - 1 + c;
+        int s = 0;
+        if (gx >= 3 && gx < W - 3 && gy >= 3 && gy < H - 3)
+            s = fast_score(&in[r + 3][c + 3], kFastInW, j.threshold);
+        sc[r][c] = static_cast<std::uint8_t>(s);
+    }
+    __syncthreads();
+    for (int i = tid; i < kFastTileW * kFastTileH; i += 256) {
+        const int r = i / kFastTileW, c = i - r * kFastTileW;
+        const int gy = y0 + r, gx = x0 + c;
+        if (gx >= W || gy >= H) continue;
+        const int s = sc[r + 1][c + 1];
+        bool keep = s > 0 && gx >= kEdge && gx < W - kEdge && gy >= kEdge && gy < H - kEdge;
+        if (keep) {
+            keep = s > sc[r][c] && s > sc[r][c + 1] && s > sc[r][c + 2] && s > sc[r + 1][c] &&
+                   s > sc[r + 1][c + 2] && s > sc[r + 2][c] && s > sc[r + 2][c + 1] &&
+                   s > sc[r + 2][c + 2];
+        }
+        j.maxima[static_cast<std::size_t>(gy) * W + gx] = keep ? static_cast<std::uint8_t>(s) : 0;
+        if (keep) atomicAdd(&hist[s], 1u);
+    }
+    __syncthreads();
+    if (hist[tid]) atomicAdd(&j.hist[tid], hist[tid]);
+}
+
+// --------------------------------------------------------- 2K selection
+
+// All 256 threads: suffix[s] = number of maxima with score >= s (s >= 1),
+// then the unique threshold s with suffix[s] >= cap > suffix[s + 1]; with at
+// most cap maxima, everything is kept (threshold 1).
+__device__ __forceinline__ SelectParams select_params(const std::uint32_t* hist, std::uint32_t cap,
+                                                     std::uint32_t* suffix /*[257] shared*/,
+                                                     SelectParams* out /*shared*/) {
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    __shared__ std::uint32_t warp_total[8];
+    const std::uint32_t own = t ? hist[t] : 0u;
+    std::uint32_t v = own;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const std::uint32_t n = __shfl_down_sync(0xffffffffu, v, o);
+        if (lane + o < 32) v += n;
+    }
+    if (lane == 0) warp_total[warp] = v;
+    __syncthreads();
+    for (int w = warp + 1; w < 8; ++w) v += warp_total[w];
+    suffix[t] = v;
+    if (t == 0) suffix[256] = 0;
+    __syncthreads();
+    const std::uint32_t total = suffix[1];
+    if (total <= cap) {
+        if (t == 1) *out = SelectParams{1u, total - own, own, total};
+    } else if (t >= 1 && suffix[t] >= cap && suffix[t + 1] < cap) {
+        *out = SelectParams{static_cast<std::uint32_t>(t), suffix[t + 1], cap - suffix[t + 1], cap};
+    }
+    __syncthreads();
+    return *out;
+}
+
+// Loads 32 maxima bytes of one thread (zero past the image end).
+__device__ __forceinline__ void load32(const std::uint8_t* maxima, long long first, long long pixels,
+                                       std::uint8_t (&b)[32]) {
+    if (first + 32 <= pixels) {
+        const uint4 lo = *reinterpret_cast<const uint4*>(maxima + first);
+        const uint4 hi = *reinterpret_cast<const uint4*>(maxima + first + 16);
+        const std::uint32_t w[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
+#pragma unroll
+        for (int i = 0; i < 32; ++i) b[i] = static_cast<std::uint8_t>(w[i >> 2] >> (8 * (i & 3)));
+    } else {
+#pragma unroll
+        for (int i = 0; i < 32; ++i) b[i] = first + i < pixels ? maxima[first + i] : 0;
+    }
+}
+
+// Block-wide exclusive scan of packed (above << 16 | tie) counts (block totals
+// stay below 2^16); returns the exclusive prefix, *total gets the block sum.
+__device__ __forceinline__ std::uint32_t block_scan_packed(std::uint32_t v, std::uint32_t* total) {
+    __shared__ std::uint32_t warp_sum[8];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    std::uint32_t inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const std::uint32_t n = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += n;
+    }
+    if (lane == 31) warp_sum[warp] = inc;
+    __syncthreads();
+    std::uint32_t base = 0, all = 0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) {
+        base += w < warp ? warp_sum[w] : 0u;
+        all += warp_sum[w];
+    }
+    __syncthreads();
+    *total = all;
+    return base + inc - v;
+}
+
+// Per 8192-pixel chunk: the 2K threshold (every block derives the same
+// one), the chunk's (above, tie) counts; chunk 0 publishes the parameters and
+// the keypoint count min(selected, K).
+template <class Src>
+__global__ __launch_bounds__(256) void select_count_kernel(const __grid_constant__ Src src) {
+    __shared__ std::uint32_t suffix[257];
+    __shared__ SelectParams sp;
+    DetectJob j;
+    int chunk;
+    if (!src.find(blockIdx.x, kChunkKind, &j, &chunk)) return;
+    const SelectParams p = select_params(j.hist, static_cast<std::uint32_t>(j.candidates), suffix, &sp);
+    if (chunk == 0 && threadIdx.x == 0) {
+        *j.params = p;
+        *j.count = static_cast<int>(min(p.selected, static_cast<std::uint32_t>(j.max_keypoints)));
+    }
+    const long long pixels = static_cast<long long>(j.width) * j.height;
+    const long long first = static_cast<long long>(chunk) * kChunkPx + threadIdx.x * 32;
+    std::uint8_t b[32];
+    load32(j.maxima, first, pixels, b);
+    std::uint32_t packed = 0;
+#pragma unroll
+    for (int i = 0; i < 32; ++i) {
+        packed += (b[i] > p.threshold) ? (1u << 16) : 0u;
+        packed += (b[i] == p.threshold) ? 1u : 0u;  // threshold >= 1, so b == thr is a maximum
+    }
+    std::uint32_t total;
+    block_scan_packed(packed, &total);
+    if (threadIdx.x == 0) {
+        j.chunk_counts[2 * chunk] = total >> 16;
+        j.chunk_counts[2 * chunk + 1] = total & 0xffffu;
+    }
+}
+
+// Writes the raster index of every pre-selected maximum: slots [0, above) get
+// the maxima above the threshold in raster order, slots [above, selected) the
+// first `ties` maxima at the threshold in raster order.
+template <class Src>
+__global__ __launch_bounds__(256) void scatter_kernel(const __grid_constant__ Src src) {
+    __shared__ std::uint32_t red[2][8];
+    DetectJob j;
+    int chunk;
+    if (!src.find(blockIdx.x, kChunkKind, &j, &chunk)) return;
+    const SelectParams p = *j.params;
+    // Offsets of this chunk: totals of all earlier chunks of the image.
+    std::uint32_t pa = 0, pt = 0;
+    for (int i = threadIdx.x; i < chunk; i += 256) {
+        pa += j.chunk_counts[2 * i];
+        pt += j.chunk_counts[2 * i + 1];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        pa += __shfl_xor_sync(0xffffffffu, pa, o);
+        pt += __shfl_xor_sync(0xffffffffu, pt, o);
+    }
+    if ((threadIdx.x & 31) == 0) { red[0][threadIdx.x >> 5] = pa; red[1][threadIdx.x >> 5] = pt; }
+    __syncthreads();
+    std::uint32_t off_above = 0, off_tie = 0;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) { off_above += red[0][w]; off_tie += red[1][w]; }
+    const long long pixels = static_cast<long long>(j.width) * j.height;
+    const long long first = static_cast<long long>(chunk) * kChunkPx + threadIdx.x * 32;
+    std::uint8_t b[32];
+    load32(j.maxima, first, pixels, b);
+    std::uint32_t packed = 0;
+#pragma unroll
+    for (int i = 0; i < 32; ++i) {
+        packed += (b[i] > p.threshold) ? (1u << 16) : 0u;
+        packed += (b[i] == p.threshold) ? 1u : 0u;
+    }
+    std::uint32_t total;
+    const std::uint32_t excl = block_scan_packed(packed, &total);
+    std::uint32_t ra = off_above + (excl >> 16), rt = off_tie + (excl & 0xffffu);
+#pragma unroll
+    for (int i = 0; i < 32; ++i) {
+        const std::uint64_t px = static_cast<std::uint64_t>(first + i);
+        if (b[i] > p.threshold) {
+            j.keys[ra++] = px;
+        } else if (b[i] == p.threshold) {
+            if (rt < p.ties) j.keys[p.above + rt] = px;
+            ++rt;
+        }
+    }
+}
+
+// ------------------------------------------------------------- Harris
+
+// Monotone float -> unsigned order (never 0 for a finite input).
+__device__ __forceinline__ std::uint32_t order_bits(float v) {
+    const std::uint32_t u = __float_as_uint(v);
+    return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float from_order_bits(std::uint32_t u) {
+    return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+
+// (1 / (4 * 7 * 255))^4 evaluated in float32, as ORB's HarrisResponses does.
+constexpr float kHarrisScale4 = 0x1.bb9da2p-52f;
+
+// Harris response over the 7x7 window of 3x3 Sobel gradients centred on
+// (x, y): integer sums, then det - k * trace^2 in float32 with every product
+// and sum rounded separately.
+__device__ __forceinline__ float harris_response(const std::uint8_t* img, int pitch, int x, int y, float k) {
+    int p[9][9];
+    const std::uint8_t* base = img + static_cast<std::size_t>(y - 4) * pitch + (x - 4);
+#pragma unroll
+    for (int r = 0; r < 9; ++r)
+#pragma unroll
+        for (int c = 0; c < 9; ++c) p[r][c] = base[static_cast<std::size_t>(r) * pitch + c];
+    int a = 0, b = 0, cc = 0;
+#pragma unroll
+    for (int i = 1; i < 8; ++i)
+#pragma unroll
+        for (int jx = 1; jx < 8; ++jx) {
+            const int ix = (p[i][jx + 1] - p[i][jx - 1]) * 2 + (p[i - 1][jx + 1] - p[i - 1][jx - 1]) +
+                           (p[i + 1][jx + 1] - p[i + 1][jx - 1]);
+            const int iy = (p[i + 1][jx] - p[i - 1][jx]) * 2 + (p[i + 1][jx - 1] - p[i - 1][jx - 1]) +
+                           (p[i + 1][jx + 1] - p[i - 1][jx + 1]);
+            a += ix * ix;
+            b += iy * iy;
+            cc += ix * iy;
+        }
+    const float fa = static_cast<float>(a), fb = static_cast<float>(b), fc = static_cast<float>(cc);
+    const float trace = __fadd_rn(fa, fb);
+    const float det = __fsub_rn(__fmul_rn(fa, fb), __fmul_rn(fc, fc));
+    const float penalty = __fmul_rn(__fmul_rn(k, trace), trace);
+    return __fmul_rn(__fsub_rn(det, penalty), kHarrisScale4);
+}
+
+// Replaces each pre-selected pixel index by its sort key
+// (order_bits(response) << 32) | (0xffffffff - index): larger key = better,
+// equal responses prefer the smaller raster index.
+template <class Src>
+__global__ __launch_bounds__(kHarrisThreads) void harris_kernel(const __grid_constant__ Src src) {
+    DetectJob j;
+    int local;
+    if (!src.find(blockIdx.x, kHarrisKind, &j, &local)) return;
+    const int slot = local * kHarrisThreads + threadIdx.x;
+    if (slot >= j.candidates) return;
+    const std::uint32_t selected = j.params->selected;
+    if (static_cast<std::uint32_t>(slot) >= selected) return;
+    const auto px = static_cast<std::uint32_t>(j.keys[slot]);
+    const int x = static_cast<int>(px % static_cast<std::uint32_t>(j.width));
+    const int y = static_cast<int>(px / static_cast<std::uint32_t>(j.width));
+    const float r = harris_response(j.image, j.pitch, x, y, j.harris_k);
+    j.keys[slot] = (static_cast<std::uint64_t>(order_bits(r)) << 32) | (0xffffffffu - px);
+}
+
+// ------------------------------------------------------------- top-K
+
+__device__ __forceinline__ void write_keypoint(const DetectJob& j, int rank, std::uint64_t key) {
+    const std::uint32_t px = 0xffffffffu - static_cast<std::uint32_t>(key);
+    j.x[rank] = static_cast<float>(px % static_cast<std::uint32_t>(j.width));
+    j.y[rank] = static_cast<float>(px / static_cast<std::uint32_t>(j.width));
+    if (j.response) j.response[rank] = from_order_bits(static_cast<std::uint32_t>(key >> 32));
+}
+
+// One block per image: bitonic sort (descending) of up to kSortCap keys in
+// shared memory, then the first min(K, selected) become the keypoints.
+template <class Src>
+__global__ __launch_bounds__(kSortThreads) void sort_topk_kernel(const __grid_constant__ Src src) {
+    extern __shared__ std::uint64_t sk[];
+    DetectJob j;
+    int local;
+    if (!src.find(blockIdx.x, kSortKind, &j, &local)) return;
+    const int n = static_cast<int>(j.params->selected);
+    if (n > kSortCap || n == 0) return;
+    int N = 1;
+    while (N < n) N <<= 1;
+    for (int i = threadIdx.x; i < N; i += kSortThreads) sk[i] = i < n ? j.keys[i] : 0ull;
+    __syncthreads();
+    for (int k = 2; k <= N; k <<= 1) {
+        for (int s = k >> 1; s > 0; s >>= 1) {
+            for (int t = threadIdx.x; t < (N >> 1); t += kSortThreads) {
+                const int i = (t / s) * (s << 1) + (t % s);
+                const int q = i + s;
+                const std::uint64_t a = sk[i], b = sk[q];
+                // Blocks with (i & k) == 0 end up descending.
+                const bool descending = (i & k) == 0;
+                if (descending ? (a < b) : (a > b)) { sk[i] = b; sk[q] = a; }
+            }
+            __syncthreads();
+        }
+    }
+    const int limit = min(n, j.max_keypoints);
+    for (int i = threadIdx.x; i < limit; i += kSortThreads) write_keypoint(j, i, sk[i]);
+}
+
+// Fallback for images with more than kSortCap pre-selected points: the rank
+// of a key is the number of larger keys (keys are unique). Launched over the
+// same blocks as the Harris kernel.
+template <class Src>
+__global__ __launch_bounds__(kHarrisThreads) void rank_topk_kernel(const __grid_constant__ Src src) {
+    __shared__ std::uint64_t tile[kHarrisThreads];
+    DetectJob j;
+    int local;
+    if (!src.find(blockIdx.x, kHarrisKind, &j, &local)) return;
+    const int n = static_cast<int>(j.params->selected);
+    if (n <= kSortCap) return;
+    const int slot = local * kHarrisThreads + static_cast<int>(threadIdx.x);
+    if (local * kHarrisThreads >= n) return;  // block-uniform
+    const std::uint64_t key = slot < n ? j.keys[slot] : 0ull;
+    int rank = 0;
+    for (int b0 = 0; b0 < n; b0 += kHarrisThreads) {
+        const int q = b0 + static_cast<int>(threadIdx.x);
+        tile[threadIdx.x] = q < n ? j.keys[q] : 0ull;
+        __syncthreads();
+        const int m = min(kHarrisThreads, n - b0);
+        for (int i = 0; i < m; ++i) rank += tile[i] > key;
+        __syncthreads();
+    }
+    if (slot < n && rank < j.max_keypoints) write_keypoint(j, rank, key);
+}
+
+// ------------------------------------------------------------- S3 blur
+
+// float32 taps of a 7-tap, sigma-2 Gaussian (exp in float64, normalised,
+// rounded to float32); equal to cv::getGaussianKernel(7, 2, CV_32F).
+__device__ __forceinline__ float blur_tap(int i) {
+    switch (i) {
+        case 0: case 6: return 0x1.1f5f62p-4f;
+        case 1: case 5: return 0x1.0c70fcp-3f;
+        case 2: case 4: return 0x1.869472p-3f;
+        default: return 0x1.ba95c0p-3f;
+    }
+}
+
+// Border reflection without repeating the edge pixel (BORDER_REFLECT_101).
+__device__ __forceinline__ int reflect101(int i, int n) {
+    if (n == 1) return 0;
+    while (i < 0 || i >= n) i = i < 0 ? -i : 2 * n - 2 - i;
+    return i;
+}
+
+// One block = one 64x32 tile: rows pass into a float tile with a 3-row halo,
+// then the columns pass; per output the taps are summed first to last with
+// each product and sum rounded separately, then rounded half-to-even and
+// clamped to [0, 255].
+template <class Src>
+__global__ __launch_bounds__(256) void blur_kernel(const __grid_constant__ Src src) {
+    __shared__ std::uint8_t in[kBlurTileH + 6][kBlurTileW + 6];
+    __shared__ float rows[kBlurTileH + 6][kBlurTileW];
+    DescribeJob j;
+    int local;
+    if (!src.find(blockIdx.x, kBlurKind, &j, &local)) return;
+    const int W = j.width, H = j.height;
+    const int y0 = (local / j.tiles_x) * kBlurTileH;
+    const int x0 = (local % j.tiles_x) * kBlurTileW;
+    for (int i = threadIdx.x; i < (kBlurTileH + 6) * (kBlurTileW + 6); i += 256) {
+        const int r = i / (kBlurTileW + 6), c = i - r * (kBlurTileW + 6);
+        const int gy = reflect101(y0 - 3 + r, H), gx = reflect101(x0 - 3 + c, W);
+        in[r][c] = j.image[static_cast<std::size_t>(gy) * j.pitch + gx];
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < (kBlurTileH + 6) * kBlurTileW; i += 256) {
+        const int r = i / kBlurTileW, c = i - r * kBlurTileW;
+        float acc = 0.0f;
+#pragma unroll
+        for (int t = 0; t < 7; ++t) acc = __fadd_rn(acc, __fmul_rn(blur_tap(t), static_cast<float>(in[r][c + t])));
+        rows[r][c] = acc;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kBlurTileH * kBlurTileW; i += 256) {
+        const int r = i / kBlurTileW, c = i - r * kBlurTileW;
+        const int gy = y0 + r, gx = x0 + c;
+        if (gx >= W || gy >= H) continue;
+        float acc = 0.0f;
+#pragma unroll
+        for (int t = 0; t < 7; ++t) acc = __fadd_rn(acc, __fmul_rn(blur_tap(t), rows[r + t][c]));
+        j.blurred[static_cast<std::size_t>(gy) * W + gx] =
+            static_cast<std::uint8_t>(min(max(__float2int_rn(acc), 0), 255));
+    }
+}
+
+// ---------------------------------------------------------- S3 describe
+
+__constant__ int kOrbPattern[1024] = {
+#include "orb_pattern_31.inc"
+};
+
+// Half-widths of the rows of the radius-15 orientation disc, v = 0..15:
+// 15 15 15 15 14 14 14 13 13 12 11 10 9 8 6 3 (one byte per row).
+__device__ __forceinline__ int disc_half_width(int v) {
+    constexpr unsigned long long lo = 0x0d0e0e0e0f0f0f0full;  // rows 0..7, row 0 in the low byte
+    constexpr unsigned long long hi = 0x030608090a0b0c0dull;  // rows 8..15, row 8 in the low byte
+    return v < 8 ? static_cast<int>((lo >> (8 * v)) & 0xff)
+                 : static_cast<int>((hi >> (8 * (v - 8))) & 0xff);
+}
+
+// cv::fastAtan2 in degrees [0, 360): odd polynomial of the smaller/larger
+// magnitude ratio, every step rounded in float32.
+__device__ __forceinline__ float fast_atan2_deg(float y, float x) {
+    const float ax = fabsf(x), ay = fabsf(y);
+    const bool wide = ax >= ay;
+    const float eps = 0x1p-52f;
+    const float t = wide ? __fdiv_rn(ay, __fadd_rn(ax, eps)) : __fdiv_rn(ax, __fadd_rn(ay, eps));
+    const float t2 = __fmul_rn(t, t);
+    float p = __fadd_rn(__fmul_rn(-0x1.4515b2p+1f, t2), 0x1.1d3f7ep+3f);
+    p = __fadd_rn(__fmul_rn(p, t2), -0x1.2aaddcp+4f);
+    p = __fadd_rn(__fmul_rn(p, t2), 0x1.ca44dep+5f);
+    p = __fmul_rn(p, t);
+    float a = wide ? p : __fsub_rn(90.0f, p);
+    if (x < 0) a = __fsub_rn(180.0f, a);
+    if (y < 0) a = __fsub_rn(360.0f, a);
+    return a;
+}
+
+__device__ __forceinline__ int rotated_sample(const std::uint8_t* centre, int stride, int px, int py,
+                                              float a, float b) {
+    const float fx = static_cast<float>(px), fy = static_cast<float>(py);
+    const int ix = __float2int_rn(__fsub_rn(__fmul_rn(fx, a), __fmul_rn(fy, b)));
+    const int iy = __float2int_rn(__fadd_rn(__fmul_rn(fx, b), __fmul_rn(fy, a)));
+    return centre[iy * stride + ix];
+}
+
+// One warp per keypoint: intensity-centroid moments over the radius-15 disc
+// of the unblurred image (lane v sums rows +-v), the angle on lane 0 (float
+// fastAtan2, cos/sin evaluated in double then rounded to float), then lane l
+// packs pattern pairs 8l..8l+7 of the blurred image into descriptor byte l.
+template <class Src>
+__global__ __launch_bounds__(kDescWarps * 32) void describe_kernel(const __grid_constant__ Src src) {
+    __shared__ std::uint32_t pat[8][32];  // pat[j][l] = pair 8l + j as 4 packed int8
+    DescribeJob j;
+    int local;
+    if (!src.find(blockIdx.x, kDescKind, &j, &local)) return;
+    {
+        const int p = threadIdx.x;  // 256 threads, one pattern pair each
+        const int l = p >> 3, jj = p & 7;
+        const int* q = &kOrbPattern[4 * p];
+        pat[jj][l] = (static_cast<std::uint32_t>(q[0] & 0xff)) |
+                     (static_cast<std::uint32_t>(q[1] & 0xff) << 8) |
+                     (static_cast<std::uint32_t>(q[2] & 0xff) << 16) |
+                     (static_cast<std::uint32_t>(q[3] & 0xff) << 24);
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int index = local * kDescWarps + (threadIdx.x >> 5);
+    if (index >= j.capacity || index >= *j.count) return;
+    std::uint8_t* row = j.out + static_cast<std::size_t>(index) * j.row_stride;
+    const int x = __float2int_rn(j.x[index]);
+    const int y = __float2int_rn(j.y[index]);
+    if (x < kEdge || x >= j.width - kEdge || y < kEdge || y >= j.height - kEdge) {
+        row[lane] = 0;
+        return;
+    }
+    const int pitch = j.pitch;
+    const std::uint8_t* centre = j.image + static_cast<std::size_t>(y) * pitch + x;
+    int m10 = 0, m01 = 0;
+    if (lane == 0) {
+        for (int u = -15; u <= 15; ++u) m10 += u * centre[u];
+    } else if (lane <= 15) {
+        const int d = disc_half_width(lane);
+        int vsum = 0;
+        for (int u = -d; u <= d; ++u) {
+            const int up = centre[u + lane * pitch], down = centre[u - lane * pitch];
+            vsum += up - down;
+            m10 += u * (up + down);
+        }
+        m01 = lane * vsum;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        m10 += __shfl_xor_sync(0xffffffffu, m10, o);
+        m01 += __shfl_xor_sync(0xffffffffu, m01, o);
+    }
+    float a = 0.0f, b = 0.0f;
+    if (lane == 0) {
+        const float angle = __fmul_rn(fast_atan2_deg(static_cast<float>(m01), static_cast<float>(m10)),
+                                      0x1.1df46ap-6f);
+        a = static_cast<float>(cos(static_cast<double>(angle)));
+        b = static_cast<float>(sin(static_cast<double>(angle)));
+    }
+    a = __shfl_sync(0xffffffffu, a, 0);
+    b = __shfl_sync(0xffffffffu, b, 0);
+    const std::uint8_t* smooth = j.blurred + static_cast<std::size_t>(y) * j.width + x;
+    int value = 0;
+#pragma unroll
+    for (int jj = 0; jj < 8; ++jj) {
+        const std::uint32_t pk = pat[jj][lane];
+        const int x0 = static_cast<int>(static_cast<std::int8_t>(pk & 0xff));
+        const int y0 = static_cast<int>(static_cast<std::int8_t>((pk >> 8) & 0xff));
+        const int x1 = static_cast<int>(static_cast<std::int8_t>((pk >> 16) & 0xff));
+        const int y1 = static_cast<int>(static_cast<std::int8_t>((pk >> 24) & 0xff));
+        const int t0 = rotated_sample(smooth, j.width, x0, y0, a, b);
+        const int t1 = rotated_sample(smooth, j.width, x1, y1, a, b);
+        value |= (t0 < t1) << jj;
+    }
+    row[lane] = static_cast<std::uint8_t>(value);
+}
+
+}  // namespace stitch::b200::s2s3

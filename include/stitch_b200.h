@@ -1,0 +1,184 @@
+/* C ABI of the B200 registration chain S2 -> S3 -> S4 -> S5.
+ *
+ * Plain pointers and sizes only; every struct below has the layout of the
+ * reference's C++ stage struct it mirrors, so callers may pass either. Return
+ * values are the reference's Status codes (src/common/status.hpp:6-13):
+ *   0 OK, 1 INVALID_ARGUMENT, 2 INSUFFICIENT_WORKSPACE, 3 CUDA_ERROR,
+ *   4 NOT_ENOUGH_POINTS, 5 DEGENERATE.
+ * Contract shared by every stage call (src/common/types.hpp:2,
+ * src/s4/s4.hpp:40-51): the caller allocates every device buffer and
+ * workspace; calls never allocate or synchronise; arguments are checked before
+ * anything is enqueued and a failed check writes nothing; work is ordered on
+ * the caller's stream (a cudaStream_t passed as void*, NULL = legacy default
+ * stream); device failures surface when the caller synchronises.
+ *
+ * The same library also exports the reference's C++ entry points
+ * (stitch::s2::s2_detect, ..., stitch::s5::estimate) with identical
+ * signatures, so code compiled against the reference headers links unchanged.
+ */
+#ifndef STITCH_B200_H
+#define STITCH_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------- types */
+
+/* src/common/types.hpp:16-22. format: 0 RGB8, 1 GRAY8 (stages take GRAY8). */
+typedef struct stitch_image_view {
+    uint8_t* data;
+    int width, height, pitch_bytes;
+    int format;
+} stitch_image_view;
+
+/* src/common/types.hpp:25-30. D maps original to working coordinates. */
+typedef struct stitch_scale_info {
+    int orig_w, orig_h, work_w, work_h;
+    double sx, sy;
+    double D[9];
+} stitch_scale_info;
+
+/* src/common/types.hpp:33-39. Device SoA; *d_count lives on the device. */
+typedef struct stitch_keypoints {
+    float* x;
+    float* y;
+    float* response; /* may be NULL */
+    int capacity;
+    int* d_count;
+} stitch_keypoints;
+
+/* src/common/types.hpp:44-49. type: 0 BINARY_U8 (dim bytes), 1 FLOAT32. */
+typedef struct stitch_descriptors {
+    int type, dim, row_stride_bytes;
+    void* data;
+} stitch_descriptors;
+
+/* src/common/types.hpp:52-58. */
+typedef struct stitch_matches {
+    int32_t* idx_a;
+    int32_t* idx_b;
+    float* distance;
+    int capacity;
+    int* d_count;
+} stitch_matches;
+
+/* src/common/types.hpp:61-70. H maps B -> A in original coordinates. */
+typedef struct stitch_homography_result {
+    double H[9];
+    double H_s[9];
+    int num_matches, num_inliers;
+    double inlier_ratio, inlier_coverage, reproj_residual;
+    int status;
+} stitch_homography_result;
+
+/* src/s2_s3/s2.hpp:19-23. */
+typedef struct stitch_s2_config {
+    int fast_threshold; /* 1..254 */
+    int max_keypoints;  /* K >= 0 */
+    float harris_k;     /* finite, >= 0 */
+} stitch_s2_config;
+
+/* src/s4/s4.hpp:8-11 (bool cross_check is one byte, then padding). */
+typedef struct stitch_s4_config {
+    double ratio_threshold; /* finite, in (0, 1) */
+    uint8_t cross_check;
+    uint8_t reserved[7];
+} stitch_s4_config;
+
+/* src/s4/s4.hpp:16-21. Missing neighbour: index -1, distance +inf. */
+typedef struct stitch_s4_top2 {
+    double first_distance, second_distance;
+    int first_index, second_index;
+} stitch_s4_top2;
+
+/* src/s5/s5.hpp:11-19. */
+typedef struct stitch_s5_config {
+    int hypotheses;          /* total R, including previous_hypotheses */
+    int previous_hypotheses; /* 0 restarts; else extends the saved search */
+    int batch_size;          /* 1..65535 */
+    int refinement_steps;    /* >= 0 */
+    double threshold;        /* reprojection distance in working pixels */
+    uint64_t seed;
+    uint64_t generation;
+} stitch_s5_config;
+
+/* --------------------------------------------------------------- library */
+
+/* ABI version of this header (no reference counterpart). */
+int stitch_abi_version(void);
+/* Kernels this library has launched so far, over all calls (no reference
+ * counterpart; lets a caller attribute device work to these kernels). */
+long long stitch_launch_count(void);
+/* Name of a status code; src/common/status.hpp:15-25. */
+const char* stitch_status_name(int status);
+
+/* src/common/geometry.hpp:119-131 (make_scale_info). */
+int stitch_make_scale_info(int width, int height, double scale, stitch_scale_info* out);
+/* src/common/geometry.hpp:157-163 (to_original): H = D_A^-1 H_s D_B. */
+int stitch_to_original(const double* h_s, const double* d_a, const double* d_b, double* h_out);
+
+/* ------------------------------------------------------------------- S2 */
+
+/* src/s2_s3/s2.hpp:26-27 (stitch::s2::s2_workspace_bytes). */
+int stitch_s2_workspace_bytes(int width, int height, const stitch_s2_config* config, size_t* bytes);
+/* src/s2_s3/s2.hpp:38-39 (stitch::s2::s2_detect). Writes min(found, K)
+ * keypoints sorted by Harris response, ties by raster index, and *d_count. */
+int stitch_s2_detect(const stitch_image_view* image, const stitch_s2_config* config,
+                     const stitch_keypoints* output, void* workspace, size_t workspace_bytes,
+                     void* stream);
+/* src/s2_s3/s2_s3_marks.hpp:27-29 (s2_detect_marked): cudaEvent_t marks
+ * recorded after FAST, after the 2K selection and after Harris. */
+int stitch_s2_detect_marked(const stitch_image_view* image, const stitch_s2_config* config,
+                            const stitch_keypoints* output, void* workspace, size_t workspace_bytes,
+                            void* stream, void* after_fast, void* after_select, void* after_harris);
+
+/* ------------------------------------------------------------------- S3 */
+
+/* src/s2_s3/s3.hpp:19 (stitch::s3::s3_workspace_bytes). The blurred image
+ * sits at offset 0 of the workspace after a call. */
+int stitch_s3_workspace_bytes(int width, int height, size_t* bytes);
+/* src/s2_s3/s3.hpp:28-30 (stitch::s3::s3_describe). */
+int stitch_s3_describe(const stitch_image_view* image, const stitch_keypoints* keypoints,
+                       const stitch_descriptors* output, void* workspace, size_t workspace_bytes,
+                       void* stream);
+/* src/s2_s3/s2_s3_marks.hpp:32-34 (s3_describe_marked). */
+int stitch_s3_describe_marked(const stitch_image_view* image, const stitch_keypoints* keypoints,
+                              const stitch_descriptors* output, void* workspace, size_t workspace_bytes,
+                              void* stream, void* after_blur);
+
+/* ------------------------------------------------------------------- S4 */
+
+/* src/s4/s4.hpp:25-26 (stitch::s4::s4_workspace_bytes). */
+int stitch_s4_workspace_bytes(int capacity_a, int capacity_b, const stitch_s4_config* config,
+                              size_t* bytes);
+/* src/s4/s4.hpp:36-38 (stitch::s4::s4_knn_top2). */
+int stitch_s4_knn_top2(const stitch_keypoints* a, const stitch_descriptors* da, const stitch_keypoints* b,
+                       const stitch_descriptors* db, stitch_s4_top2* output, void* stream);
+/* src/s4/s4.hpp:52-55 (stitch::s4::s4_match). */
+int stitch_s4_match(const stitch_keypoints* a, const stitch_descriptors* da, const stitch_keypoints* b,
+                    const stitch_descriptors* db, const stitch_s4_config* config, const stitch_matches* output,
+                    void* workspace, size_t workspace_bytes, void* stream);
+/* src/s4/s4.hpp:59-60 (stitch::s4::s4_forward_neighbors). */
+int stitch_s4_forward_neighbors(int capacity_a, int capacity_b, const stitch_s4_config* config,
+                                const void* workspace, size_t workspace_bytes, const stitch_s4_top2** output);
+
+/* ------------------------------------------------------------------- S5 */
+
+/* src/s5/s5.hpp:23 (stitch::s5::s5_workspace_bytes). */
+int stitch_s5_workspace_bytes(const stitch_s5_config* config, size_t* bytes);
+/* src/s5/s5.hpp:36-39 (stitch::s5::estimate). output: pinned host memory,
+ * valid after the caller synchronises the stream. */
+int stitch_s5_estimate(const stitch_keypoints* a, const stitch_keypoints* b, const stitch_matches* matches,
+                       const stitch_scale_info* scale_a, const stitch_scale_info* scale_b,
+                       const stitch_s5_config* config, uint8_t* inlier_mask, stitch_homography_result* output,
+                       void* workspace, size_t workspace_bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* STITCH_B200_H */

@@ -1,0 +1,114 @@
+"""The native library loads without a GPU, exports every C entry point of
+include/stitch_b200.h and the reference's C++ stage symbols, and its
+host-only checks behave as the reference's (no device work is queued)."""
+import ctypes as C
+import re
+import subprocess
+from pathlib import Path
+
+import pytest
+
+from crossstage_stitch_b200 import _abi
+from crossstage_stitch_b200._abi import S2Config, S4Config, S5Config, ScaleInfo, Status
+
+ROOT = Path(__file__).resolve().parents[1]
+HEADER = ROOT / "include" / "stitch_b200.h"
+REF_STAGES = ROOT / "oracle" / "_ref" / "libref_stages.so"
+
+
+def header_functions():
+    text = HEADER.read_text()
+    return sorted(set(re.findall(r"\b(stitch_[a-z0-9_]+)\s*\(", text)))
+
+
+def exported(path):
+    out = subprocess.run(["nm", "-D", "--defined-only", str(path)], capture_output=True, text=True, check=True)
+    return {line.split()[-1] for line in out.stdout.splitlines() if " T " in line}
+
+
+def test_every_header_function_is_exported_and_bound():
+    lib = _abi.load()
+    names = header_functions()
+    assert names, "no declarations parsed"
+    syms = exported(_abi.LIB_PATH)
+    for n in names:
+        assert n in syms, n
+        assert n in _abi.PROTOTYPES, f"{n} missing from the ctypes mirror"
+        getattr(lib, n)
+
+
+def test_reference_cpp_symbols_are_exported():
+    """Code compiled against the reference headers links against this library."""
+    if not REF_STAGES.exists():
+        pytest.skip("reference stage build not present (oracle/_ref)")
+    ref = {s for s in exported(REF_STAGES) if s.startswith("_ZN6stitch2s") or s.startswith("_ZN6stitch5s2_s3")}
+    public = {s for s in ref if "detail" not in s or "marked" in s}
+    ours = exported(_abi.LIB_PATH)
+    missing = sorted(public - ours)
+    assert not missing, missing
+
+
+def test_struct_sizes():
+    assert C.sizeof(_abi.HomographyResult) == 184
+    assert C.sizeof(_abi.ScaleInfo) == 104
+    assert C.sizeof(_abi.S4Config) == 16
+    assert C.sizeof(_abi.S5Config) == 40
+    assert C.sizeof(_abi.Top2) == 24
+
+
+def test_workspace_queries():
+    L = _abi.load()
+    b = C.c_size_t(123)
+    assert L.stitch_s2_workspace_bytes(640, 480, C.byref(S2Config(20, 0, 0.04)), C.byref(b)) == 0 and b.value == 0
+    assert L.stitch_s2_workspace_bytes(640, 480, C.byref(S2Config(0, 10, 0.04)), C.byref(b)) == Status.INVALID_ARGUMENT
+    assert L.stitch_s2_workspace_bytes(640, 480, C.byref(S2Config(20, 10, -1.0)), C.byref(b)) == Status.INVALID_ARGUMENT
+    assert L.stitch_s2_workspace_bytes(640, 480, C.byref(S2Config(20, 1000, 0.04)), C.byref(b)) == 0
+    small = b.value
+    assert L.stitch_s2_workspace_bytes(677, 480, C.byref(S2Config(20, 1000, 0.04)), C.byref(b)) == 0
+    assert b.value > small   # a wider image needs more workspace
+    assert L.stitch_s3_workspace_bytes(0, 5, C.byref(b)) == Status.INVALID_ARGUMENT
+    c4 = S4Config()
+    c4.ratio_threshold = 1.0
+    assert L.stitch_s4_workspace_bytes(10, 10, C.byref(c4), C.byref(b)) == Status.INVALID_ARGUMENT
+    c4.ratio_threshold = 0.8
+    assert L.stitch_s4_workspace_bytes(0, 10, C.byref(c4), C.byref(b)) == 0 and b.value == 0
+    assert L.stitch_s4_workspace_bytes(-1, 10, C.byref(c4), C.byref(b)) == Status.INVALID_ARGUMENT
+    c5 = S5Config(129, 0, 32, 2, 3.0, 20261022, 1)
+    e = C.c_size_t()
+    assert L.stitch_s5_workspace_bytes(C.byref(c5), C.byref(b)) == 0 and b.value > 0
+    c5.hypotheses, c5.previous_hypotheses = 1000, 129
+    assert L.stitch_s5_workspace_bytes(C.byref(c5), C.byref(e)) == 0 and e.value == b.value
+    for field, value in (("previous_hypotheses", 1001), ("threshold", float("nan")), ("threshold", 0.0),
+                         ("batch_size", 65536), ("refinement_steps", -1)):
+        bad = S5Config(1000, 0, 32, 2, 3.0, 1, 1)
+        setattr(bad, field, value)
+        assert L.stitch_s5_workspace_bytes(C.byref(bad), C.byref(b)) == Status.INVALID_ARGUMENT, field
+    assert L.stitch_s5_workspace_bytes(C.byref(c5), None) == Status.INVALID_ARGUMENT
+
+
+def test_scale_info_and_to_original():
+    L = _abi.load()
+    s = ScaleInfo()
+    assert L.stitch_make_scale_info(1281, 961, 0.5, C.byref(s)) == 0
+    assert (s.work_w, s.work_h) == (641, 481)
+    assert L.stitch_make_scale_info(10, 10, 1.5, C.byref(s)) == Status.INVALID_ARGUMENT
+    import numpy as np
+    from oracle import c_oracle
+    a = c_oracle.make_scale_info(641, 479, 0.5)
+    bb = c_oracle.make_scale_info(803, 601, 0.75)
+    hs = np.array([1, 0.01, 5, -0.02, 1, 9, 0.0001, 0.0002, 1.0])
+    out = np.zeros(9)
+    dp = lambda x: x.ctypes.data_as(C.POINTER(C.c_double))
+    assert L.stitch_to_original(dp(hs), dp(a["D"]), dp(bb["D"]), dp(out)) == 0
+    rec = np.linalg.inv(np.diag([1, 1, 1.0])) @ (a["D"].reshape(3, 3) @ out.reshape(3, 3)
+                                                @ np.linalg.inv(bb["D"].reshape(3, 3)))
+    assert np.max(np.abs(rec / rec[2, 2] - hs.reshape(3, 3))) < 1e-12
+
+
+def test_host_validation_needs_no_device():
+    """Invalid arguments are rejected before any CUDA call."""
+    L = _abi.load()
+    iv = _abi.ImageView(0, 64, 64, 64, 1)
+    kp = _abi.Keypoints(0, 0, 0, 10, 0)
+    assert L.stitch_s2_detect(C.byref(iv), C.byref(S2Config(20, 10, 0.04)), C.byref(kp), None, 0, None) \
+        == Status.INVALID_ARGUMENT
