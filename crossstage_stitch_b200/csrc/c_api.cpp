@@ -6,7 +6,7 @@
 #include <cmath>
 #include <cstddef>
 
-#include "../../include/stitch_b200.h"
+#include "stitch_b200.h"
 #include "stage_api.hpp"
 
 namespace {

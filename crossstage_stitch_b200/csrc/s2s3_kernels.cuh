@@ -113,15 +113,15 @@ constexpr int kEdge = 31;
 // circular 9-pixel arcs take the smallest centre-minus-ring difference (arc
 // darker) and the smallest ring-minus-centre difference (arc brighter); the
 // score is the largest of these minus one when it exceeds the threshold.
-// Windowed minima are built from pairwise minima (2 -> 4 -> 8 -> 9).
+// Pixels that cannot reach the threshold leave after four compass loads.
 __device__ __forceinline__ int fast_score(const std::uint8_t* p, int stride, int thr) {
     const int v = p[0];
     const int s0 = p[3 * stride], s4 = p[3], s8 = p[-3 * stride], s12 = p[-3];
     // A qualifying 9-arc always contains two of the four compass pixels.
     const int hi = v + thr, lo = v - thr;
-    const int bright = (s0 > hi) + (s4 > hi) + (s8 > hi) + (s12 > hi);
-    const int dark = (s0 < lo) + (s4 < lo) + (s8 < lo) + (s12 < lo);
-    if (bright < 2 && dark < 2) return 0;
+    const int n_bright = (s0 > hi) + (s4 > hi) + (s8 > hi) + (s12 > hi);
+    const int n_dark = (s0 < lo) + (s4 < lo) + (s8 < lo) + (s12 < lo);
+    if (n_bright < 2 && n_dark < 2) return 0;
     int d[16];
     d[0] = v - s0;
     d[1] = v - p[3 * stride + 1];
@@ -139,26 +139,30 @@ __device__ __forceinline__ int fast_score(const std::uint8_t* p, int stride, int
     d[13] = v - p[1 * stride - 3];
     d[14] = v - p[2 * stride - 2];
     d[15] = v - p[3 * stride - 1];
-    int mn2[16], mx2[16];
+    // Offset to unsigned so both arc kinds are minima of non-negative values:
+    // dark arc = min over the arc of (d + 256) - 256, bright arc = min over
+    // the arc of (256 - d) - 256. (CUDA 12.9 ptxas at -O1 and above
+    // miscompiles the signed max(min(arc), -max(arc)) form of this score on
+    // sm_100; this unsigned form is exact at every optimisation level.)
+    unsigned dark[16], bright[16];
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
-        mn2[k] = min(d[k], d[(k + 1) & 15]);
-        mx2[k] = max(d[k], d[(k + 1) & 15]);
+        dark[k] = static_cast<unsigned>(d[k] + 256);
+        bright[k] = 512u - dark[k];
     }
-    int mn4[16], mx4[16];
+    unsigned best = 0;
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
-        mn4[k] = min(mn2[k], mn2[(k + 2) & 15]);
-        mx4[k] = max(mx2[k], mx2[(k + 2) & 15]);
-    }
-    int best = INT_MIN;
+        unsigned a = 0xffffffffu, b = 0xffffffffu;
 #pragma unroll
-    for (int k = 0; k < 16; ++k) {
-        const int mn9 = min(min(mn4[k], mn4[(k + 4) & 15]), d[(k + 8) & 15]);
-        const int mx9 = max(max(mx4[k], mx4[(k + 4) & 15]), d[(k + 8) & 15]);
-        best = max(best, max(mn9, -mx9));
+        for (int t = 0; t < 9; ++t) {
+            a = min(a, dark[(k + t) & 15]);
+            b = min(b, bright[(k + t) & 15]);
+        }
+        best = max(best, max(a, b));
     }
-    return best > thr ? best - 1 : 0;
+    const int score = static_cast<int>(best) - 256;
+    return score > thr ? score - 1 : 0;
 }
 
 // One block = one 64x32 output tile: stage the tile with a 4-pixel halo in
@@ -360,7 +364,8 @@ __global__ __launch_bounds__(256) void scatter_kernel(const __grid_constant__ Sr
     for (int i = 0; i < 32; ++i) {
         const std::uint64_t px = static_cast<std::uint64_t>(first + i);
         if (b[i] > p.threshold) {
-            j.keys[ra++] = px;
+            if (ra < p.above) j.keys[ra] = px;  // always true when map and histogram agree
+            ++ra;
         } else if (b[i] == p.threshold) {
             if (rt < p.ties) j.keys[p.above + rt] = px;
             ++rt;
@@ -552,8 +557,11 @@ __global__ __launch_bounds__(256) void blur_kernel(const __grid_constant__ Src s
         float acc = 0.0f;
 #pragma unroll
         for (int t = 0; t < 7; ++t) acc = __fadd_rn(acc, __fmul_rn(blur_tap(t), rows[r + t][c]));
+        // Clamping the float to [0, 255] before rounding half-to-even gives
+        // the same byte as rounding then clamping the integer, for every
+        // finite acc, and keeps signed integer min/max out of this kernel.
         j.blurred[static_cast<std::size_t>(gy) * W + gx] =
-            static_cast<std::uint8_t>(min(max(__float2int_rn(acc), 0), 255));
+            static_cast<std::uint8_t>(__float2int_rn(fminf(fmaxf(acc, 0.0f), 255.0f)));
     }
 }
 

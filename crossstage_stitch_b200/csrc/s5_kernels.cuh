@@ -417,7 +417,7 @@ __global__ __launch_bounds__(kSearchThreads, 2) void search_kernel(const __grid_
             double hm[9];
             int valid = 0;
             if (lane < hend - h0) {
-                int idx[4];
+                int idx[4] = {0, 0, 0, 0};
                 sample_four(nm, seed, h0 + lane, idx);
                 Pt f[4];
                 for (int k = 0; k < 4; ++k) {
