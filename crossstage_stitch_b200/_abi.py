@@ -111,6 +111,8 @@ PROTOTYPES: dict[str, tuple] = {
                                   P(Matches), C.c_void_p, C.c_size_t, C.c_void_p]),
     "stitch_s4_forward_neighbors": (C.c_int, [C.c_int, C.c_int, P(S4Config), C.c_void_p, C.c_size_t,
                                               P(C.c_void_p)]),
+    "stitch_s4_match_static": (C.c_int, [P(Keypoints), P(Descriptors), P(Keypoints), P(Descriptors), P(S4Config),
+                                         P(Matches), C.c_void_p]),
     "stitch_s5_workspace_bytes": (C.c_int, [P(S5Config), _size_p]),
     "stitch_s5_estimate": (C.c_int, [P(Keypoints), P(Keypoints), P(Matches), P(ScaleInfo), P(ScaleInfo),
                                      P(S5Config), C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]),

@@ -162,6 +162,19 @@ int stitch_s4_knn_top2(const stitch_keypoints* a, const stitch_descriptors* da, 
 int stitch_s4_match(const stitch_keypoints* a, const stitch_descriptors* da, const stitch_keypoints* b,
                     const stitch_descriptors* db, const stitch_s4_config* config, const stitch_matches* output,
                     void* workspace, size_t workspace_bytes, void* stream);
+/* No counterpart in the reference. stitch_s4_match without a workspace, for
+ * callers that cannot allocate device memory (a plug-in whose host owns all
+ * device allocations, or a loop that cannot afford cudaMalloc's implicit
+ * device synchronisation). The workspace is a 4 MiB array in the library's
+ * own device memory, held by every GPU that loads the library until exit;
+ * requests needing more fail with INSUFFICIENT_WORKSPACE (up to 87381 query
+ * and train rows each fit with the mutual check, 174762 without, at the
+ * current workspace layout). The first call on a device
+ * looks the array up (make it before any stream capture); all calls on a
+ * device share the array, so calls that overlap on the GPU race. */
+int stitch_s4_match_static(const stitch_keypoints* a, const stitch_descriptors* da, const stitch_keypoints* b,
+                           const stitch_descriptors* db, const stitch_s4_config* config,
+                           const stitch_matches* output, void* stream);
 /* src/s4/s4.hpp:59-60 (stitch::s4::s4_forward_neighbors). */
 int stitch_s4_forward_neighbors(int capacity_a, int capacity_b, const stitch_s4_config* config,
                                 const void* workspace, size_t workspace_bytes, const stitch_s4_top2** output);
