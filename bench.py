@@ -1,22 +1,32 @@
-"""Registration throughput benchmark: pairs/s and per-pair latency.
+"""Registration throughput benchmark: pairs/s and per-pair latency, batched
+form vs the plain per-pair form, on one B200 per rank.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--form plain|batched]
 
-Workload: 64 synthetic 512x512 pairs (the batched-registration configuration:
-blobs + rectangles + band-limited noise, warped by a random homography,
-K = 2000 keypoints per image, FAST 20, ratio 0.8, R = 2000, tau = 3 px,
-1 refinement). One step registers all 64 pairs. Inputs are smaller than L2,
-so a 512 MB buffer is written between timed steps to flush it.
+Workload: 64 synthetic 512x512 pairs, the batched-registration
+configuration. Each pair is built from blobs, rectangles and band-limited
+noise, then warped by a random homography. Knobs: K = 2000 keypoints per
+image, FAST 20, ratio 0.8, R = 2000, tau = 3 px, 1 refinement, single-level
+ORB. One step registers all 64 pairs. The inputs fit in L2, so a 512 MB
+buffer is written between timed steps to flush it (outside the timed span).
 
-`value` is device time with the images already in HBM (CUDA events on the
-launching stream, max over ranks); `e2e` is the same work through the public
-API with the images copied from pinned host memory and every pair's result
-read back inside the timed region. With N GPUs each rank registers its own
-64 pairs (pairs are independent: replicas, weak scaling).
+- value: the batched form. One captured CUDA graph runs every stage for
+  all 64 pairs, with the images resident in HBM. It is device-timed with
+  CUDA events, and the max over ranks is taken.
+- e2e: the same graph through the public API. Every step copies the 128
+  images from pinned host memory and reads the 64 results back.
+- plain_per_pair: the drop-in stages called pair by pair on one stream,
+  with a sync per pair, as the reference harness does.
+- roofline: the dominant kernel, timed from event marks recorded between
+  the batched kernels inside the timed region.
+- cpu_baseline: the CPU oracle chain (NumPy S2/S3 + C S4/S5) on the host
+  cores.
 
---impl reference times the reference's CPU path (the CPU oracle of the
-chain: NumPy S2/S3 + C S4/S5) on the host cores, on a bounded sample.
+With N GPUs each rank registers its own 64 pairs. Pairs are independent,
+so this is replicas with weak scaling and no collective on the data path.
+
+--impl reference times the reference's CPU path, restated as that oracle
+chain, on the host cores, over a bounded sample of the same workload.
 """
 from __future__ import annotations
 
@@ -36,17 +46,13 @@ N_PAIRS = 64
 SIZE = 512
 K = 2000
 R = 2000
-WORKLOAD = "batched registration, 64 pairs 512x512 u8, K=2000, FAST 20, ratio 0.8, R=2000, tau 3 px"
+WORKLOAD = "batched registration, 64 pairs 512x512 u8, K=2000, FAST 20, ratio 0.8, R=2000, tau 3 px, 1 level"
+PEAKS = ROOT / "MEASURED_PEAKS.json"
 
 
 def knobs_for(i):
     from crossstage_stitch_b200 import stages, synth
     return stages.Knobs(max_keypoints=K, hypotheses=R, seed=synth.BASE_SEED + i, threshold=3.0)
-
-
-def make_pairs(rank: int):
-    from crossstage_stitch_b200 import synth
-    return [synth.config0_pair(rank * N_PAIRS + i) for i in range(N_PAIRS)]
 
 
 class Clocks:
@@ -70,17 +76,17 @@ class Clocks:
         self.proc.terminate()
         self.proc.wait(timeout=10)
         rows = [r.split(",") for r in self.path.read_text().splitlines() if r.strip()]
-        sm = [float(r[1]) for r in rows if len(r) > 8]
-        mx = [float(r[2]) for r in rows if len(r) > 8]
+        rows = [r for r in rows if len(r) > 8]
+        sm = [float(r[1]) for r in rows]
+        mx = [float(r[2]) for r in rows]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in rows if len(r) > 8 for i in range(4)
-                          if r[5 + i].strip().lower() == "active"})
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].strip().lower() == "active"})
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
                 "reasons": reasons, "samples": len(sm)}
 
 
 def cpu_pair(args):
-    """One pair through the CPU oracle chain (runs in a worker process)."""
+    """One pair through the CPU oracle chain (runs in a spawned worker)."""
     i, rank = args
     sys.path.insert(0, str(ROOT))
     from crossstage_stitch_b200 import synth
@@ -95,38 +101,52 @@ def cpu_baseline(sample_pairs: int, workers: int) -> dict:
     import multiprocessing as mp
     ctx = mp.get_context("spawn")
     with ctx.Pool(workers) as pool:
-        pool.map(cpu_pair, [(0, 0)] * workers)  # warm the workers (imports, oracle build)
+        pool.map(cpu_pair, [(0, 0)] * workers)  # warm the workers (imports)
         t = time.perf_counter()
         lat = pool.map(cpu_pair, [(i % N_PAIRS, 0) for i in range(sample_pairs)])
         wall = time.perf_counter() - t
+    lat = sorted(lat)
     return {"value": sample_pairs / wall, "unit": "pairs/s", "cores": workers, "kind": "port",
-            "sample": f"{sample_pairs} pairs of the workload on {workers} processes (NumPy S2/S3 + C S4/S5 oracle)",
-            "p50_ms": 1e3 * statistics.median(lat), "p99_ms": 1e3 * sorted(lat)[int(0.99 * (len(lat) - 1))]}
+            "sample": f"{sample_pairs} pairs of the workload on {workers} processes "
+                      f"(NumPy S2/S3 + C S4/S5 restatement of the reference)",
+            "p50_ms": 1e3 * lat[len(lat) // 2], "p99_ms": 1e3 * lat[int(0.99 * (len(lat) - 1))]}
 
 
-def run_reference(args, rank, world):
-    if rank != 0:
-        return
+def run_reference(args):
     workers = min(os.cpu_count() or 1, 32)
-    vals = []
     for _ in range(args.warmup):
         cpu_baseline(workers, workers)
-    for _ in range(args.steps):
-        vals.append(cpu_baseline(workers, workers))
+    vals = [cpu_baseline(workers, workers) for _ in range(args.steps)]
     v = statistics.median(x["value"] for x in vals)
     line = {"impl": "reference", "metric": "pairs/s", "value": v, "unit": "pairs/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "u8/i32/f64", "data": "synthetic",
-            "config": {"workload": WORKLOAD, "pyramid_levels": 1},
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * workers / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/i32/f64",
+            "data": "synthetic", "config": {"workload": WORKLOAD, "pairs_per_step": workers},
             "cpu_baseline": {**vals[-1], "value": v},
             "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
-    print(json.dumps(line))
+    print(json.dumps(line), flush=True)
+
+
+def algorithmic_work(batch, n_pairs, counts):
+    """Per-kernel algorithmic work of one step (bytes for pixel kernels,
+    ops for matching and estimation), from the actual keypoint and match
+    counts (counts: list of (n_a, n_b, n_matches))."""
+    px = 2 * n_pairs * SIZE * SIZE
+    knn_pairs = sum(a * b for a, b, _ in counts)
+    resid = sum(R * m for _, _, m in counts)
+    return {
+        "fast_nms": ("hbm", 2.0 * px, "GB/s"),           # image read + maxima write
+        "select_scatter": ("hbm", 2.0 * px, "GB/s"),     # maxima read twice
+        "blur": ("hbm", 2.0 * px, "GB/s"),               # image read + blurred write
+        "knn_popc": ("int", 24.0 * knn_pairs, "Tops/s"),  # 8 XOR + 8 POPC + 8 ADD per row pair
+        "search": ("fp64", 25.0 * resid + 2000.0 * R * n_pairs, "TFLOP/s"),
+    }
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -135,104 +155,150 @@ def main():
     world = int(os.environ.get("WORLD_SIZE", 1))
     local = int(os.environ.get("LOCAL_RANK", 0))
     if args.impl == "reference":
-        return run_reference(args, rank, world)
+        if rank == 0:
+            run_reference(args)
+        return
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline(32, min(os.cpu_count() or 1, 32))   # before any CUDA work (spawned pool)
+        cpu = cpu_baseline(32, min(os.cpu_count() or 1, 32))   # spawned pool, before any CUDA work
 
     import torch
     import torch.distributed as dist
-    from crossstage_stitch_b200 import _abi, stages
+    from crossstage_stitch_b200 import _abi, batch, stages, synth
 
     torch.cuda.set_device(local)
     if world > 1:
         from datetime import timedelta
         dist.init_process_group("nccl", timeout=timedelta(seconds=120))
     dev = torch.device("cuda", local)
-    pairs = make_pairs(rank)
-    runner = stages.PairRunner(SIZE, SIZE, K, max_r=R, device=dev)
-    imgs = [(torch.from_numpy(p.gray_a).to(dev), torch.from_numpy(p.gray_b).to(dev)) for p in pairs]
-    host = [(torch.from_numpy(p.gray_a).pin_memory(), torch.from_numpy(p.gray_b).pin_memory()) for p in pairs]
-    flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream()
     L = _abi.load()
+    pairs = [synth.config0_pair(rank * N_PAIRS + i) for i in range(N_PAIRS)]
+    knobs = [knobs_for(rank * N_PAIRS + i) for i in range(N_PAIRS)]
+    host = [(torch.from_numpy(p.gray_a).pin_memory(), torch.from_numpy(p.gray_b).pin_memory()) for p in pairs]
+    imgs = [(a.to(dev), b.to(dev)) for a, b in host]
+    flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
 
-    def step_resident(lat=None):
-        for i in range(N_PAIRS):
-            if lat is not None:
-                e0 = torch.cuda.Event(enable_timing=True); e0.record(stream)
-            runner.enqueue(SIZE, SIZE, SIZE, SIZE, knobs_for(rank * N_PAIRS + i), stream, images=imgs[i])
-            if lat is not None:
-                e1 = torch.cuda.Event(enable_timing=True); e1.record(stream)
-                lat.append((e0, e1))
-            stream.synchronize()  # the plain form reads every pair's result before the next
+    # ---- batched form: one graph for all pairs
+    b = batch.Batch([batch.pair_desc(ia, ib, k) for (ia, ib), k in zip(imgs, knobs)], device=dev)
+    marks = [torch.cuda.Event(enable_timing=True) for _ in _abi.BATCH_MARKS]
+    b.set_marks(marks)
+    b.capture()
+    start = torch.cuda.Event(enable_timing=True)
+    stop = torch.cuda.Event(enable_timing=True)
 
-    def step_e2e():
-        out = []
-        for i in range(N_PAIRS):
-            runner.img[0].copy_(host[i][0], non_blocking=True)
-            runner.img[1].copy_(host[i][1], non_blocking=True)
-            runner.enqueue(SIZE, SIZE, SIZE, SIZE, knobs_for(rank * N_PAIRS + i), stream)
-            stream.synchronize()
-            out.append(runner.result.num_inliers)
-        return out
-
-    def timed(fn, steps):
-        total = 0.0
+    def timed_graph(steps, e2e=False):
+        total, per_kernel = 0.0, [0.0] * len(marks)
         for _ in range(steps):
             flush.zero_()
             torch.cuda.synchronize()
             if world > 1:
                 dist.barrier()
+            start.record(stream)
+            if e2e:
+                for (ha, hb), (da, db) in zip(host, imgs):
+                    da.copy_(ha, non_blocking=True)
+                    db.copy_(hb, non_blocking=True)
+            b.launch(stream)
+            stop.record(stream)
+            stop.synchronize()
+            if e2e:
+                _ = b.result(N_PAIRS - 1)["status"]   # read the step's result on the host
+            total += start.elapsed_time(stop)
+            if not e2e:
+                for i in range(1, len(marks)):
+                    per_kernel[i] += marks[i - 1].elapsed_time(marks[i])
+        return total, per_kernel
+
+    for _ in range(args.warmup):
+        timed_graph(1)
+        timed_graph(1, e2e=True)
+    clocks = Clocks(local)
+    l0 = L.stitch_launch_count()
+    t_batch, per_kernel = timed_graph(args.steps)
+    launches = L.stitch_launch_count() - l0
+    t_e2e, _ = timed_graph(args.steps, e2e=True)
+    clk = clocks.stop()
+
+    # ---- plain per-pair form (drop-in stages, one pair at a time)
+    runner = stages.PairRunner(SIZE, SIZE, K, max_r=R, device=dev)
+    lat = []
+
+    def plain_step(record):
+        for i in range(N_PAIRS):
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record(stream)
-            fn()
+            runner.enqueue(SIZE, SIZE, SIZE, SIZE, knobs[i], stream, images=imgs[i])
             e1.record(stream)
-            torch.cuda.synchronize()
-            total += e0.elapsed_time(e1)
-        return total
+            stream.synchronize()
+            if record:
+                lat.append(e0.elapsed_time(e1))
 
-    for _ in range(args.warmup):
-        step_resident()
-        step_e2e()
+    plain_step(False)
     torch.cuda.synchronize()
-    clocks = Clocks(local)
-    launches0 = L.stitch_launch_count()
-    t_res = timed(step_resident, args.steps)
-    launches = L.stitch_launch_count() - launches0
-    t_e2e = timed(step_e2e, args.steps)
-    clk = clocks.stop()
-    lat = []
-    step_resident(lat)
-    torch.cuda.synchronize()
-    lat_ms = sorted(a.elapsed_time(b) for a, b in lat)
-    tt = torch.tensor([t_res, t_e2e], dtype=torch.float64, device=dev)
+    start.record(stream)
+    plain_step(True)
+    stop.record(stream)
+    stop.synchronize()
+    t_plain = start.elapsed_time(stop)
+    lat.sort()
+
+    counts = []
+    for i in range(N_PAIRS):
+        o = b.outputs(i)
+        counts.append((len(o["kp_a"]), len(o["kp_b"]), len(o["idx_a"])))
+
+    tt = torch.tensor([t_batch, t_e2e, t_plain], dtype=torch.float64, device=dev)
     if world > 1:
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-    t_res, t_e2e = tt.tolist()
+    t_batch, t_e2e, t_plain = tt.tolist()
     pairs_total = N_PAIRS * args.steps * world
     if rank == 0:
-        line = {"metric": "pairs/s", "value": pairs_total / (t_res / 1e3), "unit": "pairs/s", "n_gpus": world,
-                "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_res / args.steps,
+        names = _abi.BATCH_MARKS
+        kern = {names[i]: per_kernel[i] / args.steps for i in range(1, len(names))}
+        ksum = sum(kern.values())
+        dominant = max(kern, key=kern.get)
+        work = algorithmic_work(b, N_PAIRS, counts)
+        peaks = json.loads(PEAKS.read_text()) if PEAKS.exists() else {}
+        roof = None
+        if dominant in work:
+            bound, amount, unit = work[dominant]
+            achieved = amount / (kern[dominant] / 1e3) / (1e9 if unit == "GB/s" else 1e12)
+            if bound == "hbm":
+                peak, src = peaks.get("hbm_gbs", 6650.0), ("measured" if "hbm_gbs" in peaks else "fallback")
+            elif bound == "fp64":
+                peak, src = 37.0, "nominal B200 FP64 (no measured FP64 peak on this pool)"
+            else:
+                peak, src = 148 * 64 * 1.965e9 * 3 / 1e12, "nominal INT32 issue rate (64 lanes x 3 ops/clk/SM)"
+            roof = {"kernel": dominant, "bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
+                    "frac": achieved / peak, "peak_source": src, "traffic": None,
+                    "ms_per_launch": kern[dominant]}
+        line = {"metric": "pairs/s", "value": pairs_total / (t_batch / 1e3), "unit": "pairs/s", "n_gpus": world,
+                "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_batch / args.steps,
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/i32/f64",
                 "data": "synthetic",
-                "config": {"workload": WORKLOAD, "form": "plain per-pair", "pairs_per_step": N_PAIRS,
-                           "pyramid_levels": 1, "l2": "512 MB flush between steps",
+                "config": {"workload": WORKLOAD, "form": "batched (CUDA graph, 1 launch per stage kernel)",
+                           "pairs_per_step": N_PAIRS, "pyramid_levels": 1,
+                           "l2": "512 MB flush between steps (inputs 33.5 MB < L2)",
                            "parallelism": f"replicas x{world}"},
-                "p50_pair_ms": lat_ms[len(lat_ms) // 2], "p99_pair_ms": lat_ms[int(0.99 * (len(lat_ms) - 1))],
+                "p50_pair_ms": t_batch / args.steps, "p99_pair_ms": t_batch / args.steps,
                 "e2e": {"value": pairs_total / (t_e2e / 1e3), "unit": "pairs/s",
                         "h2d_bytes_per_step": N_PAIRS * 2 * SIZE * SIZE,
-                        "d2h_bytes_per_step": N_PAIRS * C_RESULT_BYTES},
-                "gpu_launches": launches, "clocks": clk, "roofline": None, "cpu_baseline": cpu}
-        print(json.dumps(line))
+                        "d2h_bytes_per_step": N_PAIRS * 184},
+                "plain_per_pair": {"value": N_PAIRS / (t_plain / 1e3), "unit": "pairs/s",
+                                   "p50_ms": lat[len(lat) // 2], "p99_ms": lat[int(0.99 * (len(lat) - 1))]},
+                "batched_over_plain": (pairs_total / (t_batch / 1e3)) / (N_PAIRS / (t_plain / 1e3)),
+                "kernel_ms": {k: round(v, 5) for k, v in kern.items()}, "kernel_ms_sum": ksum,
+                "keypoints_mean": statistics.mean(a + b_ for a, b_, _ in counts) / 2,
+                "matches_mean": statistics.mean(m for _, _, m in counts),
+                "gpu_launches": launches, "clocks": clk, "roofline": roof, "cpu_baseline": cpu}
+        print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
 
-
-C_RESULT_BYTES = 184
 
 if __name__ == "__main__":
     main()

@@ -85,6 +85,12 @@ class S5Config(C.Structure):
                 ("generation", C.c_uint64)]
 
 
+class PairDesc(C.Structure):
+    """stitch_pair_desc: one pair of the batched form."""
+    _fields_ = [("image_a", ImageView), ("image_b", ImageView), ("scale_a", ScaleInfo), ("scale_b", ScaleInfo),
+                ("s2", S2Config), ("s4", S4Config), ("s5", S5Config)]
+
+
 P = C.POINTER
 _size_p = P(C.c_size_t)
 
@@ -116,7 +122,19 @@ PROTOTYPES: dict[str, tuple] = {
     "stitch_s5_workspace_bytes": (C.c_int, [P(S5Config), _size_p]),
     "stitch_s5_estimate": (C.c_int, [P(Keypoints), P(Keypoints), P(Matches), P(ScaleInfo), P(ScaleInfo),
                                      P(S5Config), C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]),
+    "stitch_batch_create": (C.c_int, [C.c_int, P(PairDesc), P(C.c_void_p), _size_p, P(C.c_int)]),
+    "stitch_batch_enqueue": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p]),
+    "stitch_batch_capture": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p]),
+    "stitch_batch_launch": (C.c_int, [C.c_void_p, C.c_void_p]),
+    "stitch_batch_pair_outputs": (C.c_int, [C.c_void_p, C.c_void_p, C.c_int, P(Keypoints), P(Keypoints),
+                                            P(Descriptors), P(Descriptors), P(Matches), P(C.c_void_p),
+                                            P(C.c_void_p)]),
+    "stitch_batch_destroy": (None, [C.c_void_p]),
+    "stitch_batch_set_marks": (C.c_int, [C.c_void_p, P(C.c_void_p), C.c_int]),
 }
+
+BATCH_MARKS = ("tables", "fast_nms", "select_scatter", "harris", "sort_topk", "blur", "describe", "knn_popc",
+               "knn_merge", "accept", "prepare", "search", "finish")
 
 _LIB: C.CDLL | None = None
 

@@ -1,0 +1,129 @@
+"""Batched form: many uneven pairs registered by one launch per stage kernel,
+optionally replayed as a captured CUDA graph (C ABI stitch_batch_*)."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _abi
+from ._abi import Descriptors, HomographyResult, ImageView, Keypoints, Matches, PairDesc, StageError
+from .stages import Knobs, result_dict
+
+
+def pair_desc(img_a: torch.Tensor, img_b: torch.Tensor, knobs: Knobs, size_a=None, size_b=None) -> PairDesc:
+    """Descriptor of one pair over device uint8 images (rows, pitch); sizes
+    default to the tensors' shapes."""
+    wa, ha = size_a if size_a else (img_a.shape[1], img_a.shape[0])
+    wb, hb = size_b if size_b else (img_b.shape[1], img_b.shape[0])
+    d = PairDesc()
+    d.image_a = ImageView(img_a.data_ptr(), wa, ha, img_a.stride(0), 1)
+    d.image_b = ImageView(img_b.data_ptr(), wb, hb, img_b.stride(0), 1)
+    d.s2, d.s4, d.s5 = knobs.s2(), knobs.s4(), knobs.s5()
+    return d
+
+
+class Batch:
+    """Plan + workspace of one batch. The images must stay alive (and at the
+    same addresses) while the plan is used."""
+
+    def __init__(self, descs: list[PairDesc], device=None):
+        self.lib = _abi.load()
+        self.n = len(descs)
+        arr = (PairDesc * self.n)(*descs)
+        plan = C.c_void_p()
+        nbytes = C.c_size_t()
+        bad = C.c_int(-1)
+        st = self.lib.stitch_batch_create(self.n, arr, C.byref(plan), C.byref(nbytes), C.byref(bad))
+        if st != 0:
+            raise StageError(f"stitch_batch_create (pair {bad.value})", st)
+        self.plan = plan
+        self.bytes = nbytes.value
+        self.device = device or torch.device("cuda", torch.cuda.current_device())
+        self.ws = torch.empty(self.bytes, dtype=torch.uint8, device=self.device)
+        self.results = torch.zeros(self.n * C.sizeof(HomographyResult), dtype=torch.uint8, pin_memory=True)
+        self.captured = False
+
+    def __del__(self):
+        if getattr(self, "plan", None):
+            self.lib.stitch_batch_destroy(self.plan)
+            self.plan = None
+
+    def _stream(self, stream):
+        s = stream if stream is not None else torch.cuda.current_stream()
+        return C.c_void_p(s.cuda_stream)
+
+    def enqueue(self, stream=None, copy_results=True) -> None:
+        st = self.lib.stitch_batch_enqueue(self.plan, C.c_void_p(self.ws.data_ptr()), self.bytes,
+                                           C.c_void_p(self.results.data_ptr() if copy_results else 0),
+                                           self._stream(stream))
+        if st != 0:
+            raise StageError("stitch_batch_enqueue", st)
+
+    def capture(self, stream=None, copy_results=True) -> None:
+        s = stream or torch.cuda.Stream()
+        with torch.cuda.stream(s):
+            st = self.lib.stitch_batch_capture(self.plan, C.c_void_p(self.ws.data_ptr()), self.bytes,
+                                               C.c_void_p(self.results.data_ptr() if copy_results else 0),
+                                               C.c_void_p(s.cuda_stream))
+        s.synchronize()
+        if st != 0:
+            raise StageError("stitch_batch_capture", st)
+        self.captured = True
+
+    def set_marks(self, events: list | None) -> None:
+        """events: one torch.cuda.Event(enable_timing=True) per name in
+        _abi.BATCH_MARKS, recorded after the matching kernel group."""
+        if events is None:
+            st = self.lib.stitch_batch_set_marks(self.plan, None, 0)
+        else:
+            for e in events:   # torch creates the CUDA event on first record
+                e.record()
+            arr = (C.c_void_p * len(events))(*[e.cuda_event for e in events])
+            st = self.lib.stitch_batch_set_marks(self.plan, arr, len(events))
+        if st != 0:
+            raise StageError("stitch_batch_set_marks", st)
+
+    def launch(self, stream=None) -> None:
+        st = self.lib.stitch_batch_launch(self.plan, self._stream(stream))
+        if st != 0:
+            raise StageError("stitch_batch_launch", st)
+
+    def result(self, i: int) -> dict:
+        size = C.sizeof(HomographyResult)
+        r = HomographyResult.from_buffer_copy(self.results.numpy()[i * size:(i + 1) * size].tobytes())
+        return result_dict(r)
+
+    def outputs(self, i: int) -> dict:
+        """Host copies of pair i's keypoints, descriptors, matches and mask."""
+        ka, kb, m = Keypoints(), Keypoints(), Matches()
+        da, db = Descriptors(), Descriptors()
+        mask = C.c_void_p()
+        res = C.c_void_p()
+        st = self.lib.stitch_batch_pair_outputs(self.plan, C.c_void_p(self.ws.data_ptr()), i, C.byref(ka),
+                                                C.byref(kb), C.byref(da), C.byref(db), C.byref(m), C.byref(mask),
+                                                C.byref(res))
+        if st != 0:
+            raise StageError("stitch_batch_pair_outputs", st)
+        base = self.ws.data_ptr()
+
+        def view(ptr, count, dtype):
+            off = ptr - base
+            itemsize = torch.empty(0, dtype=dtype).element_size()
+            return self.ws[off:off + count * itemsize].view(dtype)
+
+        out = {}
+        for tag, k, d in (("a", ka, da), ("b", kb, db)):
+            n = int(view(k.d_count, 1, torch.int32).item())
+            xs = view(k.x, n, torch.float32)
+            ys = view(k.y, n, torch.float32)
+            rs = view(k.response, n, torch.float32)
+            out[f"kp_{tag}"] = torch.stack([xs, ys, rs], 1).cpu().numpy() if n else np.zeros((0, 3), np.float32)
+            out[f"desc_{tag}"] = view(d.data, n * 32, torch.uint8).reshape(n, 32).cpu().numpy()
+        nm = int(view(m.d_count, 1, torch.int32).item())
+        out["idx_a"] = view(m.idx_a, nm, torch.int32).cpu().numpy()
+        out["idx_b"] = view(m.idx_b, nm, torch.int32).cpu().numpy()
+        out["distance"] = view(m.distance, nm, torch.float32).cpu().numpy()
+        out["mask"] = view(mask.value, nm, torch.uint8).cpu().numpy()
+        return out

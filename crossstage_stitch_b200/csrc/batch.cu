@@ -1,0 +1,535 @@
+// Batched registration of N uneven pairs: every stage kernel is launched once
+// for the whole batch; each block finds its (pair, image, tile) through a
+// device job table and a block-prefix array. The per-pair stage semantics
+// are unchanged, so results equal the per-pair calls bit for bit.
+//
+// Workspace layout (one caller allocation, 256-byte aligned regions):
+//   counts   int[3n]      keypoint counts (2 per pair) and match counts,
+//                         zeroed at the start of every run
+//   hists    u32[2n][256] FAST histograms, zeroed at the start of every run
+//   results  HomographyResult[n]
+//   tables   job tables + prefixes, copied from pinned host staging
+//   per pair: keypoints x/y/response, descriptors, S2 and S3 workspaces per
+//             image, matches, inlier mask, S4 and S5 workspaces
+#include <algorithm>
+#include <cstring>
+#include <mutex>
+
+#include "batch.hpp"
+
+namespace stitch::b200::batch {
+
+namespace {
+
+using s2s3::DescribeJob;
+using s2s3::DetectJob;
+using s4k::AcceptJob;
+using s4k::KnnJob;
+using s5k::PairIO;
+using s5k::SearchJob;
+
+template <class T> T* at(void* base, std::size_t off) { return at_offset<T>(base, off); }
+
+const ImageView& view(const stitch_image_view& v) { return *reinterpret_cast<const ImageView*>(&v); }
+
+bool small_image(const stitch_image_view& v) { return v.width <= 2 * s2::kEdge || v.height <= 2 * s2::kEdge; }
+
+// Device job tables, in this order inside the table block.
+enum Table {
+    kDetJobs, kDetPrefix, kDesJobs, kDesPrefix, kKnnJobs, kKnnPrefix, kMergePrefix, kAccJobs, kAccPrefix,
+    kPairJobs, kPairPrefix, kSearchJobs, kSearchPrefix, kTables
+};
+
+void set_attributes_once() {
+    static std::once_flag flag;
+    std::call_once(flag, [] {
+        cudaFuncSetAttribute(s2s3::sort_topk_kernel<s2s3::JobTable<DetectJob>>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             s2s3::kSortCap * static_cast<int>(sizeof(std::uint64_t)));
+        s5k::enable_search_smem_once(reinterpret_cast<const void*>(s5k::search_kernel<s5k::JobTable<SearchJob>>));
+    });
+}
+
+}  // namespace
+
+Plan::~Plan() {
+    if (graph_exec) cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(graph_exec));
+    if (graph) cudaGraphDestroy(static_cast<cudaGraph_t>(graph));
+    if (staging) cudaFreeHost(staging);
+}
+
+Status Plan::build(int n_pairs, const stitch_pair_desc* p, int* bad_pair) {
+    if (n_pairs <= 0 || !p) return Status::INVALID_ARGUMENT;
+    n = n_pairs;
+    pairs.assign(p, p + n);
+    off.assign(n, PairOffsets{});
+    // 1. validate and fill identity scales
+    for (int i = 0; i < n; ++i) {
+        auto& q = pairs[i];
+        const auto& c2 = *reinterpret_cast<const s2::Config*>(&q.s2);
+        const auto& c4 = *reinterpret_cast<const s4::Config*>(&q.s4);
+        const auto& c5 = *reinterpret_cast<const s5::Config*>(&q.s5);
+        bool ok = s2s3::valid_gray(view(q.image_a)) && s2s3::valid_gray(view(q.image_b)) &&
+                  s2s3::valid_detect_config(c2) && std::isfinite(c4.ratio_threshold) && c4.ratio_threshold > 0 &&
+                  c4.ratio_threshold < 1 && s5k::valid_config(c5) && c5.previous_hypotheses == 0;
+        for (int s = 0; s < 2 && ok; ++s) {
+            stitch_scale_info& si = s ? q.scale_b : q.scale_a;
+            const stitch_image_view& im = s ? q.image_b : q.image_a;
+            if (si.orig_w == 0) {
+                stitch_make_scale_info(im.width, im.height, 1.0, &si);
+            }
+        }
+        if (!ok) {
+            if (bad_pair) *bad_pair = i;
+            return Status::INVALID_ARGUMENT;
+        }
+    }
+    // 2. layout
+    Layout lay;
+    const std::size_t counts = lay.take(3 * static_cast<std::size_t>(n), sizeof(int));
+    const std::size_t hists = lay.take(2 * static_cast<std::size_t>(n) * 256, sizeof(std::uint32_t));
+    results = lay.take(n, sizeof(HomographyResult));
+    (void)counts;
+    (void)hists;
+    for (int i = 0; i < n; ++i) {
+        auto& o = off[i];
+        const auto& q = pairs[i];
+        const int k = q.s2.max_keypoints;
+        const std::size_t kk = static_cast<std::size_t>(std::max(k, 1));
+        for (int s = 0; s < 2; ++s) {
+            const stitch_image_view& im = s ? q.image_b : q.image_a;
+            o.kx[s] = lay.take(kk, sizeof(float));
+            o.ky[s] = lay.take(kk, sizeof(float));
+            o.kr[s] = lay.take(kk, sizeof(float));
+            o.kcount[s] = counts + (2 * static_cast<std::size_t>(i) + s) * sizeof(int);
+            o.desc[s] = lay.take(kk, 32);
+            if (!s2s3::detect_layout(im.width, im.height, k, &o.det[s]) ||
+                !s2s3::describe_layout(im.width, im.height, &o.des[s])) {
+                if (bad_pair) *bad_pair = i;
+                return Status::INVALID_ARGUMENT;
+            }
+            o.s2ws[s] = lay.take(o.det[s].total, 1);
+            o.s3ws[s] = lay.take(o.des[s].total, 1);
+        }
+        o.ia = lay.take(kk, sizeof(std::int32_t));
+        o.ib = lay.take(kk, sizeof(std::int32_t));
+        o.dist = lay.take(kk, sizeof(float));
+        o.mcount = counts + (2 * static_cast<std::size_t>(n) + i) * sizeof(int);
+        o.mask = lay.take(kk, 1);
+        s4k::match_layout(k, k, q.s4.cross_check != 0, &o.match);
+        o.s4ws = lay.take(o.match.total, 1);
+        o.s5ws = lay.take(s5k::estimate_workspace_bytes(), 1);
+    }
+    // 3. launch shapes
+    std::fill(std::begin(det_blocks), std::end(det_blocks), 0);
+    std::fill(std::begin(des_blocks), std::end(des_blocks), 0);
+    int max_cand = 0, max_cap_m = 1;
+    for (int i = 0; i < n; ++i) {
+        const auto& q = pairs[i];
+        for (int s = 0; s < 2; ++s) {
+            const stitch_image_view& im = s ? q.image_b : q.image_a;
+            const auto& d = off[i].det[s];
+            if (q.s2.max_keypoints > 0 && !small_image(im)) {
+                det_blocks[s2s3::kFastKind] += d.tiles;
+                det_blocks[s2s3::kChunkKind] += d.chunks;
+                det_blocks[s2s3::kHarrisKind] += ceil_div(d.candidates, s2s3::kHarrisThreads);
+                det_blocks[s2s3::kSortKind] += 1;
+                max_cand = std::max(max_cand, d.candidates);
+            }
+            if (q.s2.max_keypoints > 0) {
+                des_blocks[s2s3::kBlurKind] += off[i].des[s].tiles;
+                des_blocks[s2s3::kDescKind] += ceil_div(q.s2.max_keypoints, s2s3::kDescWarps);
+            }
+        }
+        max_cap_m = std::max(max_cap_m, q.s2.max_keypoints);
+    }
+    sort_smem = s2s3::sort_smem_bytes(max_cand);
+    rank_fallback = max_cand > s2s3::kSortCap;
+    search_smem = s5k::search_smem_bytes(max_cap_m);
+    // S4: one train partition per block unless the batch is too small to fill the GPU
+    n_knn = 0;
+    int qtiles_total = 0;
+    for (int i = 0; i < n; ++i) {
+        const int k = pairs[i].s2.max_keypoints;
+        const int dirs = pairs[i].s4.cross_check ? 2 : 1;
+        n_knn += dirs;
+        qtiles_total += dirs * (k > 0 ? ceil_div(k, s4k::kQueryThreads) : 0);
+    }
+    const int want_splits = std::max(1, ceil_div(2 * kSmCount, std::max(qtiles_total, 1)));
+    knn_blocks = merge_blocks = 0;
+    // S5: hypotheses per warp round, as large as still fills about two waves
+    long long rounds_at = 0;
+    hpw = 32;
+    for (int h : {32, 16, 8, 4}) {
+        hpw = h;
+        rounds_at = 0;
+        for (int i = 0; i < n; ++i) rounds_at += s5k::plan_search(pairs[i].s5.hypotheses, h);
+        if (rounds_at >= 2 * kSmCount) break;
+    }
+    search_blocks = static_cast<int>(rounds_at);
+    // 4. table block layout
+    std::size_t cur = 0;
+    auto put = [&](int t, std::size_t bytes) {
+        cur = (cur + 15) / 16 * 16;
+        offsets[t] = cur;
+        cur += bytes;
+    };
+    put(kDetJobs, 2 * n * sizeof(DetectJob));
+    put(kDetPrefix, s2s3::kDetectKinds * (2 * n + 1) * sizeof(int));
+    put(kDesJobs, 2 * n * sizeof(DescribeJob));
+    put(kDesPrefix, s2s3::kDescribeKinds * (2 * n + 1) * sizeof(int));
+    put(kKnnJobs, n_knn * sizeof(KnnJob));
+    put(kKnnPrefix, (n_knn + 1) * sizeof(int));
+    put(kMergePrefix, (n_knn + 1) * sizeof(int));
+    put(kAccJobs, n * sizeof(AcceptJob));
+    put(kAccPrefix, (n + 1) * sizeof(int));
+    put(kPairJobs, n * sizeof(PairIO));
+    put(kPairPrefix, (n + 1) * sizeof(int));
+    put(kSearchJobs, n * sizeof(SearchJob));
+    put(kSearchPrefix, (n + 1) * sizeof(int));
+    table_bytes = cur;
+    tables = lay.take(table_bytes, 1);
+    if (!lay.ok) return Status::INVALID_ARGUMENT;
+    total = lay.cursor;
+    if (cudaHostAlloc(reinterpret_cast<void**>(&staging), table_bytes, cudaHostAllocDefault) != cudaSuccess) {
+        staging = nullptr;
+        return Status::CUDA_ERROR;
+    }
+    // Block counts of every launch are final once stage_tables has run.
+    return Status::OK;
+}
+
+Status Plan::stage_tables(void* ws) {
+    if (staged_for == ws) return Status::OK;
+    auto* T = staging;
+    auto* dj = reinterpret_cast<DetectJob*>(T + offsets[kDetJobs]);
+    auto* dp = reinterpret_cast<int*>(T + offsets[kDetPrefix]);
+    auto* sj = reinterpret_cast<DescribeJob*>(T + offsets[kDesJobs]);
+    auto* sp = reinterpret_cast<int*>(T + offsets[kDesPrefix]);
+    auto* kj = reinterpret_cast<KnnJob*>(T + offsets[kKnnJobs]);
+    auto* kp = reinterpret_cast<int*>(T + offsets[kKnnPrefix]);
+    auto* mp = reinterpret_cast<int*>(T + offsets[kMergePrefix]);
+    auto* aj = reinterpret_cast<AcceptJob*>(T + offsets[kAccJobs]);
+    auto* ap = reinterpret_cast<int*>(T + offsets[kAccPrefix]);
+    auto* pj = reinterpret_cast<PairIO*>(T + offsets[kPairJobs]);
+    auto* pp = reinterpret_cast<int*>(T + offsets[kPairPrefix]);
+    auto* rj = reinterpret_cast<SearchJob*>(T + offsets[kSearchJobs]);
+    auto* rp = reinterpret_cast<int*>(T + offsets[kSearchPrefix]);
+    std::uint32_t* hists = at<std::uint32_t>(ws, hists_offset());
+    int run_det[s2s3::kDetectKinds] = {}, run_des[s2s3::kDescribeKinds] = {};
+    int qtiles_total = 0;
+    for (int i = 0; i < n; ++i) {
+        const int dirs = pairs[i].s4.cross_check ? 2 : 1;
+        const int k = pairs[i].s2.max_keypoints;
+        qtiles_total += dirs * (k > 0 ? ceil_div(k, s4k::kQueryThreads) : 0);
+    }
+    const int want_splits = std::max(1, ceil_div(2 * kSmCount, std::max(qtiles_total, 1)));
+    int knn = 0, run_knn = 0, run_merge = 0, run_search = 0;
+    for (int i = 0; i < n; ++i) {
+        const auto& q = pairs[i];
+        const auto& o = off[i];
+        const int k = q.s2.max_keypoints;
+        Keypoints kps[2];
+        Descriptors desc[2];
+        for (int s = 0; s < 2; ++s) {
+            const stitch_image_view& im = s ? q.image_b : q.image_a;
+            kps[s] = Keypoints{at<float>(ws, o.kx[s]), at<float>(ws, o.ky[s]), at<float>(ws, o.kr[s]), k,
+                               at<int>(ws, o.kcount[s])};
+            desc[s] = Descriptors{DescriptorType::BINARY_U8, 32, 32, at<std::uint8_t>(ws, o.desc[s])};
+            const int idx = 2 * i + s;
+            DetectJob d = s2s3::make_detect_job(view(im), *reinterpret_cast<const s2::Config*>(&q.s2), kps[s],
+                                                at<void>(ws, o.s2ws[s]), o.det[s]);
+            d.hist = hists + static_cast<std::size_t>(idx) * 256;
+            dj[idx] = d;
+            const bool active = k > 0 && !small_image(im);
+            const int blocks[s2s3::kDetectKinds] = {
+                active ? o.det[s].tiles : 0, active ? o.det[s].chunks : 0,
+                active ? ceil_div(o.det[s].candidates, s2s3::kHarrisThreads) : 0, active ? 1 : 0};
+            for (int kind = 0; kind < s2s3::kDetectKinds; ++kind) {
+                dp[kind * (2 * n + 1) + idx] = run_det[kind];
+                run_det[kind] += blocks[kind];
+            }
+            sj[idx] = s2s3::make_describe_job(view(im), kps[s], desc[s], at<void>(ws, o.s3ws[s]), o.des[s]);
+            const int dblocks[s2s3::kDescribeKinds] = {k > 0 ? o.des[s].tiles : 0,
+                                                       k > 0 ? ceil_div(k, s2s3::kDescWarps) : 0};
+            for (int kind = 0; kind < s2s3::kDescribeKinds; ++kind) {
+                sp[kind * (2 * n + 1) + idx] = run_des[kind];
+                run_des[kind] += dblocks[kind];
+            }
+        }
+        // S4 (forward, then reverse when the mutual check is on)
+        auto* fwd = at<s4k::Top2>(ws, o.s4ws + o.match.forward);
+        auto* rev = q.s4.cross_check ? at<s4k::Top2>(ws, o.s4ws + o.match.reverse) : nullptr;
+        const int dirs = q.s4.cross_check ? 2 : 1;
+        for (int dir = 0; dir < dirs; ++dir) {
+            const int qs = dir ? 1 : 0, ts = dir ? 0 : 1;
+            const int qt = k > 0 ? ceil_div(k, s4k::kQueryThreads) : 0;
+            const int stages = std::max(1, ceil_div(std::max(k, 1), s4k::kTrainStage));
+            const int splits = std::min(want_splits, stages);
+            const int rows = ceil_div(stages, splits) * s4k::kTrainStage;
+            const int real_splits = ceil_div(std::max(k, 1), rows);
+            // the partial buffer of the match layout holds fsplits/rsplits entries;
+            // batch splits never exceed it (both come from the same capacities)
+            uint2* partial = at<uint2>(ws, o.s4ws + (dir ? o.match.rpartial : o.match.fpartial));
+            const bool fits = real_splits <= (dir ? o.match.rsplits : o.match.fsplits) || real_splits == 1;
+            const int use_splits = fits ? real_splits : 1;
+            const int use_rows = fits ? rows : std::max(s4k::kTrainStage, stages * s4k::kTrainStage);
+            kj[knn] = s4k::make_knn_job(kps[qs], desc[qs], kps[ts], desc[ts], std::max(qt, 1), use_splits, use_rows,
+                                        partial, dir ? rev : fwd);
+            kp[knn] = run_knn;
+            mp[knn] = run_merge;
+            run_knn += qt * use_splits;
+            run_merge += (use_splits > 1 && k > 0) ? ceil_div(k, 256) : 0;
+            ++knn;
+        }
+        AcceptJob a{};
+        a.forward = fwd;
+        a.reverse = rev;
+        a.capacity = k;
+        a.l2 = 0;
+        a.ratio = q.s4.ratio_threshold;
+        a.out = Matches{at<std::int32_t>(ws, o.ia), at<std::int32_t>(ws, o.ib), at<float>(ws, o.dist), k,
+                        at<int>(ws, o.mcount)};
+        aj[i] = a;
+        ap[i] = i;
+        // S5
+        PairIO io;
+        const Status st = s5k::check_and_build(
+            kps[0], kps[1], a.out, *reinterpret_cast<const ScaleInfo*>(&q.scale_a),
+            *reinterpret_cast<const ScaleInfo*>(&q.scale_b), *reinterpret_cast<const s5::Config*>(&q.s5),
+            at<std::uint8_t>(ws, o.mask), at<void>(ws, results), at<void>(ws, o.s5ws),
+            s5k::estimate_workspace_bytes(), &io);
+        if (st != Status::OK) return st;
+        io.hpw = hpw;
+        io.search_blocks = s5k::plan_search(q.s5.hypotheses, hpw);
+        io.result_out = at<HomographyResult>(ws, results) + i;
+        pj[i] = io;
+        pp[i] = i;
+        rj[i] = SearchJob{io, 0, q.s5.hypotheses};
+        rp[i] = run_search;
+        run_search += io.search_blocks;
+    }
+    for (int kind = 0; kind < s2s3::kDetectKinds; ++kind) dp[kind * (2 * n + 1) + 2 * n] = run_det[kind];
+    for (int kind = 0; kind < s2s3::kDescribeKinds; ++kind) sp[kind * (2 * n + 1) + 2 * n] = run_des[kind];
+    kp[n_knn] = run_knn;
+    mp[n_knn] = run_merge;
+    ap[n] = n;
+    pp[n] = n;
+    rp[n] = run_search;
+    knn_blocks = run_knn;
+    merge_blocks = run_merge;
+    search_blocks = run_search;
+    for (int kind = 0; kind < s2s3::kDetectKinds; ++kind) det_blocks[kind] = run_det[kind];
+    for (int kind = 0; kind < s2s3::kDescribeKinds; ++kind) des_blocks[kind] = run_des[kind];
+    staged_for = ws;
+    return Status::OK;
+}
+
+Status Plan::enqueue(void* ws, std::size_t bytes, stitch_homography_result* host_results, cudaStream_t s) {
+    if (!ws || !aligned(ws, kWorkspaceAlign)) return Status::INVALID_ARGUMENT;
+    if (bytes < total) return Status::INSUFFICIENT_WORKSPACE;
+    set_attributes_once();
+    const Status st = stage_tables(ws);
+    if (st != Status::OK) return st;
+    unsigned char* T = at<unsigned char>(ws, tables);
+    if (cudaMemcpyAsync(T, staging, table_bytes, cudaMemcpyHostToDevice, s) != cudaSuccess) return Status::CUDA_ERROR;
+    // counts and histograms: contiguous at the start, zeroed together
+    const std::size_t hist_end = hists_offset() + 2 * static_cast<std::size_t>(n) * 256 * sizeof(std::uint32_t);
+    if (cudaMemsetAsync(ws, 0, hist_end, s) != cudaSuccess) return Status::CUDA_ERROR;
+
+    using DetSrc = s2s3::JobTable<DetectJob>;
+    using DesSrc = s2s3::JobTable<DescribeJob>;
+    const DetSrc det{reinterpret_cast<const DetectJob*>(T + offsets[kDetJobs]),
+                     reinterpret_cast<const int*>(T + offsets[kDetPrefix]), 2 * n};
+    const DesSrc des{reinterpret_cast<const DescribeJob*>(T + offsets[kDesJobs]),
+                     reinterpret_cast<const int*>(T + offsets[kDesPrefix]), 2 * n};
+    int launches = 0;
+    int next_mark = 0;
+    bool marks_ok = true;
+    auto go = [&](int blocks) { launches += blocks > 0; return blocks > 0; };
+    auto mark = [&] {
+        // External: under stream capture this becomes an event-record node,
+        // so replays of the graph record the mark too.
+        if (marked && marks[next_mark])
+            marks_ok &= cudaEventRecordWithFlags(marks[next_mark], s, cudaEventRecordExternal) == cudaSuccess;
+        ++next_mark;
+    };
+    mark();  // tables uploaded, counts cleared
+    if (go(det_blocks[s2s3::kFastKind])) s2s3::fast_nms_kernel<DetSrc><<<det_blocks[s2s3::kFastKind], 256, 0, s>>>(det);
+    mark();
+    if (go(det_blocks[s2s3::kChunkKind])) {
+        s2s3::select_count_kernel<DetSrc><<<det_blocks[s2s3::kChunkKind], 256, 0, s>>>(det);
+        s2s3::scatter_kernel<DetSrc><<<det_blocks[s2s3::kChunkKind], 256, 0, s>>>(det);
+        ++launches;
+    }
+    mark();
+    if (go(det_blocks[s2s3::kHarrisKind]))
+        s2s3::harris_kernel<DetSrc><<<det_blocks[s2s3::kHarrisKind], s2s3::kHarrisThreads, 0, s>>>(det);
+    mark();
+    if (go(det_blocks[s2s3::kSortKind]))
+        s2s3::sort_topk_kernel<DetSrc><<<det_blocks[s2s3::kSortKind], s2s3::kSortThreads, sort_smem, s>>>(det);
+    if (rank_fallback && go(det_blocks[s2s3::kHarrisKind]))
+        s2s3::rank_topk_kernel<DetSrc><<<det_blocks[s2s3::kHarrisKind], s2s3::kHarrisThreads, 0, s>>>(det);
+    mark();
+    if (go(des_blocks[s2s3::kBlurKind])) s2s3::blur_kernel<DesSrc><<<des_blocks[s2s3::kBlurKind], 256, 0, s>>>(des);
+    mark();
+    if (go(des_blocks[s2s3::kDescKind]))
+        s2s3::describe_kernel<DesSrc><<<des_blocks[s2s3::kDescKind], s2s3::kDescWarps * 32, 0, s>>>(des);
+    mark();
+
+    using KnnSrc = s4k::JobTable<KnnJob>;
+    const auto* kjobs = reinterpret_cast<const KnnJob*>(T + offsets[kKnnJobs]);
+    if (go(knn_blocks))
+        s4k::knn_popc_kernel<KnnSrc><<<knn_blocks, s4k::kQueryThreads, 0, s>>>(
+            KnnSrc{kjobs, reinterpret_cast<const int*>(T + offsets[kKnnPrefix]), n_knn});
+    mark();
+    if (go(merge_blocks))
+        s4k::knn_merge_kernel<KnnSrc><<<merge_blocks, 256, 0, s>>>(
+            KnnSrc{kjobs, reinterpret_cast<const int*>(T + offsets[kMergePrefix]), n_knn});
+    mark();
+    using AccSrc = s4k::JobTable<AcceptJob>;
+    if (go(n))
+        s4k::accept_kernel<AccSrc><<<n, 1024, 0, s>>>(AccSrc{reinterpret_cast<const AcceptJob*>(T + offsets[kAccJobs]),
+                                                              reinterpret_cast<const int*>(T + offsets[kAccPrefix]), n});
+    mark();
+
+    using PairSrc = s5k::JobTable<PairIO>;
+    using SearchSrc = s5k::JobTable<SearchJob>;
+    const PairSrc pairsrc{reinterpret_cast<const PairIO*>(T + offsets[kPairJobs]),
+                          reinterpret_cast<const int*>(T + offsets[kPairPrefix]), n};
+    if (go(n)) s5k::prepare_kernel<PairSrc><<<n, 256, 0, s>>>(pairsrc);
+    mark();
+    if (go(search_blocks))
+        s5k::search_kernel<SearchSrc><<<search_blocks, s5k::kSearchThreads, search_smem, s>>>(
+            SearchSrc{reinterpret_cast<const SearchJob*>(T + offsets[kSearchJobs]),
+                      reinterpret_cast<const int*>(T + offsets[kSearchPrefix]), n});
+    mark();
+    if (go(n)) s5k::finish_kernel<PairSrc><<<n, s5k::kFinishThreads, 0, s>>>(pairsrc);
+    mark();
+    if (!marks_ok) return Status::CUDA_ERROR;
+    note_launches(launches);
+    if (cudaGetLastError() != cudaSuccess) return Status::CUDA_ERROR;
+    if (host_results &&
+        cudaMemcpyAsync(host_results, at<void>(ws, results), n * sizeof(HomographyResult), cudaMemcpyDeviceToHost,
+                        s) != cudaSuccess)
+        return Status::CUDA_ERROR;
+    return Status::OK;
+}
+
+}  // namespace stitch::b200::batch
+
+using stitch::Status;
+using stitch::b200::batch::Plan;
+
+struct stitch_batch {
+    Plan plan;
+    int launches_per_run = 0;
+};
+
+extern "C" {
+
+int stitch_batch_create(int n_pairs, const stitch_pair_desc* pairs, stitch_batch** out, size_t* bytes,
+                        int* bad_pair) {
+    if (!out || !bytes) return static_cast<int>(Status::INVALID_ARGUMENT);
+    *out = nullptr;
+    *bytes = 0;
+    auto* b = new (std::nothrow) stitch_batch;
+    if (!b) return static_cast<int>(Status::CUDA_ERROR);
+    const Status st = b->plan.build(n_pairs, pairs, bad_pair);
+    if (st != Status::OK) {
+        delete b;
+        return static_cast<int>(st);
+    }
+    *bytes = b->plan.total;
+    *out = b;
+    return 0;
+}
+
+int stitch_batch_enqueue(stitch_batch* b, void* ws, size_t bytes, stitch_homography_result* results, void* stream) {
+    if (!b) return static_cast<int>(Status::INVALID_ARGUMENT);
+    return static_cast<int>(b->plan.enqueue(ws, bytes, results, static_cast<cudaStream_t>(stream)));
+}
+
+int stitch_batch_capture(stitch_batch* b, void* ws, size_t bytes, stitch_homography_result* results, void* stream) {
+    if (!b) return static_cast<int>(Status::INVALID_ARGUMENT);
+    auto& p = b->plan;
+    if (!ws || bytes < p.total) return static_cast<int>(Status::INSUFFICIENT_WORKSPACE);
+    const Status pre = p.stage_tables(ws);  // host work, before capture
+    if (pre != Status::OK) return static_cast<int>(pre);
+    const auto s = static_cast<cudaStream_t>(stream);
+    if (p.graph_exec) {
+        cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(p.graph_exec));
+        p.graph_exec = nullptr;
+    }
+    if (p.graph) {
+        cudaGraphDestroy(static_cast<cudaGraph_t>(p.graph));
+        p.graph = nullptr;
+    }
+    // first enqueue outside capture sets kernel attributes; it is a full run
+    const long long before = stitch_launch_count();
+    Status st = p.enqueue(ws, bytes, results, s);
+    if (st != Status::OK) return static_cast<int>(st);
+    b->launches_per_run = static_cast<int>(stitch_launch_count() - before);
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return static_cast<int>(Status::CUDA_ERROR);
+    st = p.enqueue(ws, bytes, results, s);
+    cudaGraph_t g = nullptr;
+    const cudaError_t end = cudaStreamEndCapture(s, &g);
+    if (st != Status::OK || end != cudaSuccess || !g) {
+        if (g) cudaGraphDestroy(g);
+        return static_cast<int>(st != Status::OK ? st : Status::CUDA_ERROR);
+    }
+    cudaGraphExec_t e = nullptr;
+    if (cudaGraphInstantiate(&e, g, 0) != cudaSuccess) {
+        cudaGraphDestroy(g);
+        return static_cast<int>(Status::CUDA_ERROR);
+    }
+    p.graph = g;
+    p.graph_exec = e;
+    return 0;
+}
+
+int stitch_batch_launch(stitch_batch* b, void* stream) {
+    if (!b || !b->plan.graph_exec) return static_cast<int>(Status::INVALID_ARGUMENT);
+    stitch::b200::note_launches(b->launches_per_run);
+    return cudaGraphLaunch(static_cast<cudaGraphExec_t>(b->plan.graph_exec), static_cast<cudaStream_t>(stream)) ==
+                   cudaSuccess
+               ? 0
+               : static_cast<int>(Status::CUDA_ERROR);
+}
+
+int stitch_batch_pair_outputs(const stitch_batch* b, void* ws, int i, stitch_keypoints* ka, stitch_keypoints* kb,
+                              stitch_descriptors* da, stitch_descriptors* db, stitch_matches* m, uint8_t** mask,
+                              stitch_homography_result** result) {
+    if (!b || !ws || i < 0 || i >= b->plan.n) return static_cast<int>(Status::INVALID_ARGUMENT);
+    const auto& p = b->plan;
+    const auto& o = p.off[i];
+    const int k = p.pairs[i].s2.max_keypoints;
+    auto P = [&](std::size_t off) { return static_cast<char*>(ws) + off; };
+    stitch_keypoints* ks[2] = {ka, kb};
+    stitch_descriptors* ds[2] = {da, db};
+    for (int s = 0; s < 2; ++s) {
+        if (ks[s])
+            *ks[s] = stitch_keypoints{reinterpret_cast<float*>(P(o.kx[s])), reinterpret_cast<float*>(P(o.ky[s])),
+                                      reinterpret_cast<float*>(P(o.kr[s])), k, reinterpret_cast<int*>(P(o.kcount[s]))};
+        if (ds[s]) *ds[s] = stitch_descriptors{0, 32, 32, P(o.desc[s])};
+    }
+    if (m)
+        *m = stitch_matches{reinterpret_cast<int32_t*>(P(o.ia)), reinterpret_cast<int32_t*>(P(o.ib)),
+                            reinterpret_cast<float*>(P(o.dist)), k, reinterpret_cast<int*>(P(o.mcount))};
+    if (mask) *mask = reinterpret_cast<uint8_t*>(P(o.mask));
+    if (result) *result = reinterpret_cast<stitch_homography_result*>(P(p.results)) + i;
+    return 0;
+}
+
+void stitch_batch_destroy(stitch_batch* b) { delete b; }
+
+int stitch_batch_set_marks(stitch_batch* b, void* const* events, int count) {
+    if (!b || (events && count != STITCH_BATCH_MARKS)) return static_cast<int>(Status::INVALID_ARGUMENT);
+    auto& p = b->plan;
+    p.marked = events != nullptr;
+    for (int i = 0; i < STITCH_BATCH_MARKS; ++i) p.marks[i] = events ? static_cast<cudaEvent_t>(events[i]) : nullptr;
+    return 0;
+}
+
+}  // extern "C"

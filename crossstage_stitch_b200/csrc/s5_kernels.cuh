@@ -83,6 +83,7 @@ struct PairIO {
     std::uint8_t* mask;
     double inverse_a[9];  // D_A^-1 (host)
     double d_b[9];        // D_B
+    HomographyResult* result_out;  // optional second copy of the result (batched form)
 };
 
 template <class Job> struct OneJob {
@@ -262,7 +263,7 @@ __device__ __forceinline__ bool solve_normalised(double (*m)[9], double cax, dou
 }
 
 // Minimal 4-point model (one thread).
-__device__ bool fit4(const Pt* p, double* out) {
+__device__ inline bool fit4(const Pt* p, double* out) {
     double cax = 0, cay = 0, cbx = 0, cby = 0;
     for (int i = 0; i < 4; ++i) { cax += p[i].ax; cay += p[i].ay; cbx += p[i].bx; cby += p[i].by; }
     cax /= 4; cay /= 4; cbx /= 4; cby /= 4;
@@ -507,7 +508,7 @@ __device__ double ordered_sum(int nm, double* buf /*kFinishChunk shared*/, F ter
 // Least-squares refit over the points with keep[i] != 0: the centroid,
 // scale and normal-matrix sums each run in index order as in the reference;
 // the 72 matrix entries are accumulated by 72 threads side by side.
-__device__ bool block_fit(const PairIO& j, int nm, const std::uint8_t* keep, double* out,
+__device__ inline bool block_fit(const PairIO& j, int nm, const std::uint8_t* keep, double* out,
                           Pt* cpts /*kFinishChunk shared*/, std::uint8_t* ckeep) {
     __shared__ double sums[6];
     __shared__ int kept;
@@ -754,6 +755,7 @@ __global__ __launch_bounds__(kFinishThreads) void finish_kernel(const __grid_con
     if (t == 0) {
         s->evaluated = j.c.hypotheses;
         s->result = res;
+        if (j.result_out) *j.result_out = res;
     }
 }
 

@@ -190,6 +190,60 @@ int stitch_s5_estimate(const stitch_keypoints* a, const stitch_keypoints* b, con
                        const stitch_s5_config* config, uint8_t* inlier_mask, stitch_homography_result* output,
                        void* workspace, size_t workspace_bytes, void* stream);
 
+/* --------------------------------------------------------- batched form */
+
+/* One pair of the batched form. It bundles the per-pair arguments the
+ * reference harness passes to s2_detect (x2), s3_describe (x2), s4_match and
+ * estimate (harness/pipeline_runner.cu:366-413); every pair carries its own
+ * knobs and image sizes. scale_a/scale_b map original to working
+ * coordinates as in src/common/geometry.hpp:119-131; orig_w == 0 means the
+ * identity at the image's size. s5.previous_hypotheses must be 0. */
+typedef struct stitch_pair_desc {
+    stitch_image_view image_a, image_b; /* device GRAY8 */
+    stitch_scale_info scale_a, scale_b;
+    stitch_s2_config s2;
+    stitch_s4_config s4;
+    stitch_s5_config s5;
+} stitch_pair_desc;
+
+/* Opaque plan of a batch (host object; owns a pinned staging buffer for the
+ * device job tables and, after stitch_batch_capture, a CUDA graph). */
+typedef struct stitch_batch stitch_batch;
+
+/* No reference counterpart (batched form). Validates every pair with the
+ * stage rules and lays out one device workspace holding all intermediates
+ * and outputs. On INVALID_ARGUMENT, *bad_pair (if non-NULL) is the first
+ * offending pair. */
+int stitch_batch_create(int n_pairs, const stitch_pair_desc* pairs, stitch_batch** plan,
+                        size_t* workspace_bytes, int* bad_pair);
+/* No reference counterpart (batched form). Enqueues the whole chain for all
+ * pairs on `stream`: results are identical, bit for bit, to calling the
+ * stages pair by pair. results_pinned (n entries, may be NULL) receives the
+ * homography results once the stream completes. */
+int stitch_batch_enqueue(stitch_batch* plan, void* workspace, size_t workspace_bytes,
+                         stitch_homography_result* results_pinned, void* stream);
+/* No reference counterpart (batched form). Captures stitch_batch_enqueue with
+ * these arguments into a CUDA graph held by the plan (the stream must not be
+ * capturing already); stitch_batch_launch replays it. */
+int stitch_batch_capture(stitch_batch* plan, void* workspace, size_t workspace_bytes,
+                         stitch_homography_result* results_pinned, void* stream);
+int stitch_batch_launch(stitch_batch* plan, void* stream);
+/* No reference counterpart (batched form). Device views of pair `pair`'s
+ * outputs inside `workspace` (any pointer argument may be NULL). */
+int stitch_batch_pair_outputs(const stitch_batch* plan, void* workspace, int pair, stitch_keypoints* kp_a,
+                              stitch_keypoints* kp_b, stitch_descriptors* desc_a, stitch_descriptors* desc_b,
+                              stitch_matches* matches, uint8_t** inlier_mask, stitch_homography_result** result);
+void stitch_batch_destroy(stitch_batch* plan);
+/* Per-kernel timing hook of the batched form (like the reference's S2/S3
+ * event marks, src/s2_s3/s2_s3_marks.hpp:16-34): `events` holds
+ * STITCH_BATCH_MARKS cudaEvent_t recorded, in order, after the table upload,
+ * fast_nms, select+scatter, harris, sort, blur, describe, knn_popc,
+ * knn_merge, accept, prepare, search and finish kernels (a skipped kernel
+ * still records its mark). Applies to later enqueues and captures; NULL
+ * turns the marks off. */
+#define STITCH_BATCH_MARKS 13
+int stitch_batch_set_marks(stitch_batch* plan, void* const* events, int count);
+
 #ifdef __cplusplus
 }
 #endif
