@@ -346,12 +346,16 @@ Status Plan::enqueue(void* ws, std::size_t bytes, stitch_homography_result* host
     int launches = 0;
     int next_mark = 0;
     bool marks_ok = true;
+    cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+    if (marked && cudaStreamIsCapturing(s, &capturing) != cudaSuccess) return Status::CUDA_ERROR;
     auto go = [&](int blocks) { launches += blocks > 0; return blocks > 0; };
     auto mark = [&] {
-        // External: under stream capture this becomes an event-record node,
-        // so replays of the graph record the mark too.
+        // Under stream capture the record must be external to become an
+        // event-record node, so that replays of the graph record the mark.
         if (marked && marks[next_mark])
-            marks_ok &= cudaEventRecordWithFlags(marks[next_mark], s, cudaEventRecordExternal) == cudaSuccess;
+            marks_ok &= (capturing == cudaStreamCaptureStatusActive
+                             ? cudaEventRecordWithFlags(marks[next_mark], s, cudaEventRecordExternal)
+                             : cudaEventRecord(marks[next_mark], s)) == cudaSuccess;
         ++next_mark;
     };
     mark();  // tables uploaded, counts cleared
