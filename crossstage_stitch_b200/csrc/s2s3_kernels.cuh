@@ -139,6 +139,24 @@ __device__ __forceinline__ int fast_score(const std::uint8_t* p, int stride, int
     d[13] = v - p[1 * stride - 3];
     d[14] = v - p[2 * stride - 2];
     d[15] = v - p[3 * stride - 1];
+    // Exact corner test: the score exceeds the threshold iff some 9-pixel arc
+    // is entirely darker (d > thr) or entirely brighter (-d > thr). Find a
+    // circular run of 9 set bits in either 16-bit mask.
+    unsigned dark_bits = 0, bright_bits = 0;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+        dark_bits |= static_cast<unsigned>(d[k] > thr) << k;
+        bright_bits |= static_cast<unsigned>(d[k] < -thr) << k;
+    }
+    auto run9 = [](unsigned m) {
+        const unsigned w = m | (m << 16);
+        unsigned r = w & (w >> 1);
+        r &= r >> 2;
+        r &= r >> 4;
+        r &= w >> 8;
+        return (r & 0xffffu) != 0u;
+    };
+    if (!run9(dark_bits) && !run9(bright_bits)) return 0;
     // Offset to unsigned so both arc kinds are minima of non-negative values:
     // dark arc = min over the arc of (d + 256) - 256, bright arc = min over
     // the arc of (256 - d) - 256. (CUDA 12.9 ptxas at -O1 and above
@@ -567,7 +585,9 @@ __global__ __launch_bounds__(256) void blur_kernel(const __grid_constant__ Src s
 
 // ---------------------------------------------------------- S3 describe
 
-__constant__ int kOrbPattern[1024] = {
+// Global (not __constant__): each thread reads a different pair, which the
+// constant cache would serialise.
+__device__ const int4 kOrbPattern[256] = {
 #include "orb_pattern_31.inc"
 };
 
@@ -616,19 +636,21 @@ __global__ __launch_bounds__(kDescWarps * 32) void describe_kernel(const __grid_
     DescribeJob j;
     int local;
     if (!src.find(blockIdx.x, kDescKind, &j, &local)) return;
+    // The grid covers the capacity; blocks past the keypoint count leave now.
+    const int count = min(*j.count, j.capacity);
+    if (local * kDescWarps >= count) return;
     {
         const int p = threadIdx.x;  // 256 threads, one pattern pair each
-        const int l = p >> 3, jj = p & 7;
-        const int* q = &kOrbPattern[4 * p];
-        pat[jj][l] = (static_cast<std::uint32_t>(q[0] & 0xff)) |
-                     (static_cast<std::uint32_t>(q[1] & 0xff) << 8) |
-                     (static_cast<std::uint32_t>(q[2] & 0xff) << 16) |
-                     (static_cast<std::uint32_t>(q[3] & 0xff) << 24);
+        const int4 q = kOrbPattern[p];
+        pat[p & 7][p >> 3] = (static_cast<std::uint32_t>(q.x & 0xff)) |
+                             (static_cast<std::uint32_t>(q.y & 0xff) << 8) |
+                             (static_cast<std::uint32_t>(q.z & 0xff) << 16) |
+                             (static_cast<std::uint32_t>(q.w & 0xff) << 24);
     }
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const int index = local * kDescWarps + (threadIdx.x >> 5);
-    if (index >= j.capacity || index >= *j.count) return;
+    if (index >= count) return;
     std::uint8_t* row = j.out + static_cast<std::size_t>(index) * j.row_stride;
     const int x = __float2int_rn(j.x[index]);
     const int y = __float2int_rn(j.y[index]);

@@ -17,10 +17,11 @@
 //                             src/s5/s5.cu:139-212
 //
 // Layout of the work: a warp owns HPW consecutive hypotheses; lanes
-// 0..HPW-1 each build one model, then the whole warp scores the models one by
-// one. Lane l of the warp plays the reference's virtual lanes l, l+32, l+64
-// and l+96, so both the per-lane sums and the reduction tree are the
-// reference's, operation for operation.
+// 0..HPW-1 each draw one sample and test it for degeneracy, then the whole
+// warp fits each usable sample (the 8x9 system in shared memory, entries split
+// over the lanes) and scores it. Lane l of the warp plays the reference's
+// virtual lanes l, l+32, l+64 and l+96, so both the per-lane sums and the
+// reduction tree are the reference's, operation for operation.
 #pragma once
 
 #include <cfloat>
@@ -187,9 +188,12 @@ __device__ __forceinline__ double coord(const Pt& p, int image, int axis) {
 
 // No three of the four points (in either image) nearly collinear.
 __device__ __forceinline__ bool nondegenerate(const Pt* p) {
+#pragma unroll
     for (int image = 0; image < 2; ++image) {
         double scale = 0.0;
+#pragma unroll
         for (int i = 0; i < 4; ++i)
+#pragma unroll
             for (int j = 0; j < i; ++j) {
                 const double dx = coord(p[i], image, 0) - coord(p[j], image, 0);
                 const double dy = coord(p[i], image, 1) - coord(p[j], image, 1);
@@ -197,8 +201,11 @@ __device__ __forceinline__ bool nondegenerate(const Pt* p) {
                 if (d > scale) scale = d;
             }
         if (!(scale > 0.0) || !fin(scale)) return false;
+#pragma unroll
         for (int i = 0; i < 4; ++i)
+#pragma unroll
             for (int j = i + 1; j < 4; ++j)
+#pragma unroll
                 for (int k = j + 1; k < 4; ++k) {
                     const double x1 = coord(p[j], image, 0) - coord(p[i], image, 0);
                     const double y1 = coord(p[j], image, 1) - coord(p[i], image, 1);
@@ -252,6 +259,191 @@ __device__ __forceinline__ bool solve_normalised(double (*m)[9], double cax, dou
         }
     }
     double h[9];
+    for (int i = 0; i < 8; ++i) h[i] = m[i][8];
+    h[8] = 1.0;
+    const double den_a[9] = {1.0 / sa, 0, cax, 0, 1.0 / sa, cay, 0, 0, 1};
+    const double nrm_b[9] = {sb, 0, -sb * cbx, 0, sb, -sb * cby, 0, 0, 1};
+    double tmp[9];
+    mat3_mul(den_a, h, tmp);
+    mat3_mul(tmp, nrm_b, out);
+    return h_normalize(out);
+}
+
+// Gauss-Jordan of solve_normalised, run by all 32 lanes of a warp on M in
+// shared memory (warp-private). Every entry goes through the serial
+// solver's exact sequence of operations, so the model is bit-identical;
+// lanes only split the independent per-entry work. Returns the same
+// validity on every lane, and every lane holds the model in out.
+__device__ inline bool warp_solve(double (*M)[9], double cax, double cay, double cbx, double cby, double sa,
+                                  double sb, double* out) {
+    const int lane = threadIdx.x & 31;
+    __syncwarp();
+    double max_entry = 0.0;
+    for (int i = 0; i < 8; ++i)
+        if (fabs(M[i][i]) > max_entry) max_entry = fabs(M[i][i]);
+    for (int c = 0; c < 8; ++c) {
+        int piv = c;
+        for (int r = c + 1; r < 8; ++r)
+            if (fabs(M[r][c]) > fabs(M[piv][c])) piv = r;
+        const double pv = M[piv][c];
+        if (!fin(pv) || fabs(pv) <= 1e-12 * max_entry) return false;
+        __syncwarp();
+        if (lane >= c && lane < 9) {
+            const double t = M[c][lane];
+            M[c][lane] = M[piv][lane];
+            M[piv][lane] = t;
+        }
+        __syncwarp();
+        const double div = M[c][c];
+        __syncwarp();
+        if (lane >= c && lane < 9) M[c][lane] /= div;
+        __syncwarp();
+        // entries (r, jx), r != c, jx >= c: M[r][jx] -= f_r * M[c][jx] with
+        // f_r = M[r][c] read before any entry of row r changes
+        double f[3], pr[3];
+        int rr[3], jj[3];
+        bool own[3];
+#pragma unroll
+        for (int s = 0; s < 3; ++s) {
+            const int e = lane + 32 * s;
+            rr[s] = e / 9;
+            jj[s] = e % 9;
+            own[s] = e < 72 && rr[s] != c && jj[s] >= c;
+            f[s] = own[s] ? M[rr[s]][c] : 0.0;
+            pr[s] = own[s] ? M[c][jj[s]] : 0.0;
+        }
+        __syncwarp();
+#pragma unroll
+        for (int s = 0; s < 3; ++s)
+            if (own[s]) M[rr[s]][jj[s]] -= f[s] * pr[s];
+        __syncwarp();
+    }
+    double h[9];
+    for (int i = 0; i < 8; ++i) h[i] = M[i][8];
+    h[8] = 1.0;
+    __syncwarp();
+    const double den_a[9] = {1.0 / sa, 0, cax, 0, 1.0 / sa, cay, 0, 0, 1};
+    const double nrm_b[9] = {sb, 0, -sb * cbx, 0, sb, -sb * cby, 0, 0, 1};
+    double tmp[9];
+    mat3_mul(den_a, h, tmp);
+    mat3_mul(tmp, nrm_b, out);
+    return h_normalize(out);
+}
+
+// Minimal 4-point model computed by a whole warp (all lanes pass the same
+// points): normalisation on every lane, the 72 normal-matrix entries split
+// over the lanes (each summed over the 4 points in order), then
+// warp_solve. Bit-identical to fit4.
+__device__ inline bool warp_fit4(const Pt* p, double (*M)[9], double* out) {
+    const int lane = threadIdx.x & 31;
+    double cax = 0, cay = 0, cbx = 0, cby = 0;
+    for (int i = 0; i < 4; ++i) { cax += p[i].ax; cay += p[i].ay; cbx += p[i].bx; cby += p[i].by; }
+    cax /= 4; cay /= 4; cbx /= 4; cby /= 4;
+    double va = 0.0, vb = 0.0;
+    for (int i = 0; i < 4; ++i) {
+        va += (p[i].ax - cax) * (p[i].ax - cax) + (p[i].ay - cay) * (p[i].ay - cay);
+        vb += (p[i].bx - cbx) * (p[i].bx - cbx) + (p[i].by - cby) * (p[i].by - cby);
+    }
+    if (!(va > 0.0) || !(vb > 0.0) || !fin(va) || !fin(vb)) return false;
+    const double sa = sqrt(2.0 * 4 / va);
+    const double sb = sqrt(2.0 * 4 / vb);
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+        const int e = lane + 32 * s;
+        if (e >= 72) continue;
+        const int r = e / 9, c = e % 9;
+        double acc = 0.0;
+        for (int i = 0; i < 4; ++i) {
+            const double x = (p[i].bx - cbx) * sb, y = (p[i].by - cby) * sb;
+            const double u = (p[i].ax - cax) * sa, v = (p[i].ay - cay) * sa;
+            acc += design(0, r, x, y, u, v) * design(0, c, x, y, u, v) +
+                   design(1, r, x, y, u, v) * design(1, c, x, y, u, v);
+        }
+        M[r][c] = acc;
+    }
+    return warp_solve(M, cax, cay, cbx, cby, sa, sb, out);
+}
+
+// Minimal 4-point model on one thread with the 8x9 system in registers:
+// every loop is unrolled and the pivot row swap is a predicated select per
+// entry, so no entry is indexed at run time. Same operations, in the same
+// order per entry, as fit4; bit-identical results.
+__device__ __forceinline__ bool fit4_regs(const Pt* p, double* out) {
+    double cax = 0, cay = 0, cbx = 0, cby = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) { cax += p[i].ax; cay += p[i].ay; cbx += p[i].bx; cby += p[i].by; }
+    cax /= 4; cay /= 4; cbx /= 4; cby /= 4;
+    double va = 0.0, vb = 0.0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        va += (p[i].ax - cax) * (p[i].ax - cax) + (p[i].ay - cay) * (p[i].ay - cay);
+        vb += (p[i].bx - cbx) * (p[i].bx - cbx) + (p[i].by - cby) * (p[i].by - cby);
+    }
+    if (!(va > 0.0) || !(vb > 0.0) || !fin(va) || !fin(vb)) return false;
+    const double sa = sqrt(2.0 * 4 / va);
+    const double sb = sqrt(2.0 * 4 / vb);
+    double m[8][9];
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+#pragma unroll
+        for (int c = 0; c < 9; ++c) m[r][c] = 0.0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const double x = (p[i].bx - cbx) * sb, y = (p[i].by - cby) * sb;
+        const double u = (p[i].ax - cax) * sa, v = (p[i].ay - cay) * sa;
+        const double r0[9] = {x, y, 1, 0, 0, 0, -u * x, -u * y, u};
+        const double r1[9] = {0, 0, 0, x, y, 1, -v * x, -v * y, v};
+#pragma unroll
+        for (int r = 0; r < 8; ++r)
+#pragma unroll
+            for (int c = 0; c < 9; ++c) m[r][c] += r0[r] * r0[c] + r1[r] * r1[c];
+    }
+    double max_entry = 0.0;
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+        if (fabs(m[i][i]) > max_entry) max_entry = fabs(m[i][i]);
+    // A failed pivot makes the model invalid; the loop still runs to the
+    // end (an early exit would stop full unrolling) and the values computed
+    // after a failure are discarded.
+    bool solvable = true;
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        int piv = c;
+        double best = fabs(m[c][c]);
+        double pv = m[c][c];
+#pragma unroll
+        for (int r = c + 1; r < 8; ++r)
+            if (fabs(m[r][c]) > best) { best = fabs(m[r][c]); piv = r; pv = m[r][c]; }
+        solvable = solvable && fin(pv) && !(fabs(pv) <= 1e-12 * max_entry);
+        // (loops run over all columns with a compile-time skip of jx < c, a
+        // form that keeps every entry in a register after unrolling)
+#pragma unroll
+        for (int r = c + 1; r < 8; ++r) {
+            const bool sw = r == piv;
+#pragma unroll
+            for (int jx = 0; jx < 9; ++jx) {
+                if (jx < c) continue;
+                const double a = m[c][jx], b = m[r][jx];
+                m[c][jx] = sw ? b : a;
+                m[r][jx] = sw ? a : b;
+            }
+        }
+        const double div = m[c][c];
+#pragma unroll
+        for (int jx = 0; jx < 9; ++jx)
+            if (jx >= c) m[c][jx] /= div;
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            if (r == c) continue;
+            const double f = m[r][c];
+#pragma unroll
+            for (int jx = 0; jx < 9; ++jx)
+                if (jx >= c) m[r][jx] -= f * m[c][jx];
+        }
+    }
+    if (!solvable) return false;
+    double h[9];
+#pragma unroll
     for (int i = 0; i < 8; ++i) h[i] = m[i][8];
     h[8] = 1.0;
     const double den_a[9] = {1.0 / sa, 0, cax, 0, 1.0 / sa, cay, 0, 0, 1};
@@ -385,7 +577,7 @@ struct SearchJob {
 // round is HPW consecutive hypotheses. The block's best model goes to
 // block_best[b].
 template <class Src>
-__global__ __launch_bounds__(kSearchThreads, 2) void search_kernel(const __grid_constant__ Src src) {
+__global__ __launch_bounds__(kSearchThreads, 1) void search_kernel(const __grid_constant__ Src src) {
     extern __shared__ float4 pts[];
     __shared__ Model warp_best[kSearchWarps];
     SearchJob sj;
@@ -414,13 +606,14 @@ __global__ __launch_bounds__(kSearchThreads, 2) void search_kernel(const __grid_
         for (int round = block * kSearchWarps + warp; round < rounds; round += stride) {
             const int h0 = sj.first + round * hpw;
             const int hend = min(sj.first + sj.count, h0 + hpw);
-            // lanes 0..hpw-1 build one model each
+            // lanes 0..hpw-1 build one model each (system in registers)
             double hm[9];
             int valid = 0;
             if (lane < hend - h0) {
                 int idx[4] = {0, 0, 0, 0};
                 sample_four(nm, seed, h0 + lane, idx);
                 Pt f[4];
+#pragma unroll
                 for (int k = 0; k < 4; ++k) {
                     if (idx[k] < kStagePoints) {
                         const float4 q = pts[idx[k]];
@@ -429,8 +622,9 @@ __global__ __launch_bounds__(kSearchThreads, 2) void search_kernel(const __grid_
                         f[k] = gather(j, idx[k]);
                     }
                 }
-                valid = nondegenerate(f) && fit4(f, hm) && valid_domain(hm, bw, bh);
+                valid = nondegenerate(f) && fit4_regs(f, hm) && valid_domain(hm, bw, bh);
             }
+            // then the whole warp scores the valid models one by one
             for (int k = 0; k < hend - h0; ++k) {
                 if (!__shfl_sync(0xffffffffu, valid, k)) continue;
                 double h[9];
@@ -583,7 +777,10 @@ __device__ inline bool block_fit(const PairIO& j, int nm, const std::uint8_t* ke
         }
     }
     __syncthreads();
-    if (t == 0) ok = solve_normalised(m, cax, cay, cbx, cby, sa, sb, out);
+    if (t < 32) {
+        const bool solved = warp_solve(m, cax, cay, cbx, cby, sa, sb, out);
+        if (t == 0) ok = solved;
+    }
     __syncthreads();
     return ok;
 }
