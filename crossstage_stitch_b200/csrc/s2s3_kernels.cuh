@@ -660,18 +660,21 @@ __global__ __launch_bounds__(kDescWarps * 32) void describe_kernel(const __grid_
     }
     const int pitch = j.pitch;
     const std::uint8_t* centre = j.image + static_cast<std::size_t>(y) * pitch + x;
+    // Moments as exact integer sums over the disc: lane l owns column
+    // u = l - 15 and walks the 31 rows, one coalesced row segment per step.
     int m10 = 0, m01 = 0;
-    if (lane == 0) {
-        for (int u = -15; u <= 15; ++u) m10 += u * centre[u];
-    } else if (lane <= 15) {
-        const int d = disc_half_width(lane);
-        int vsum = 0;
-        for (int u = -d; u <= d; ++u) {
-            const int up = centre[u + lane * pitch], down = centre[u - lane * pitch];
-            vsum += up - down;
-            m10 += u * (up + down);
+    {
+        const int u = lane - 15;
+        const int au = u < 0 ? -u : u;
+#pragma unroll
+        for (int v = -15; v <= 15; ++v) {
+            const int av = v < 0 ? -v : v;
+            if (lane < 31 && au <= disc_half_width(av)) {
+                const int val = centre[v * pitch + u];
+                m10 += u * val;
+                m01 += v * val;
+            }
         }
-        m01 = lane * vsum;
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {

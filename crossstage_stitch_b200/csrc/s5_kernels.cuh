@@ -69,7 +69,7 @@ constexpr int kSearchWarps = kSearchThreads / 32;
 constexpr int kMaxSearchBlocks = 2 * kSmCount;
 constexpr int kStagePoints = 4096;  // matched points staged in shared memory per search block
 constexpr int kFinishThreads = 256;
-constexpr int kFinishChunk = 512;
+constexpr int kFinishChunk = 256;
 
 // Inputs of one pair, as the caller passed them.
 struct PairIO {
@@ -702,7 +702,7 @@ __device__ double ordered_sum(int nm, double* buf /*kFinishChunk shared*/, F ter
 // Least-squares refit over the points with keep[i] != 0: the centroid,
 // scale and normal-matrix sums each run in index order as in the reference;
 // the 72 matrix entries are accumulated by 72 threads side by side.
-__device__ inline bool block_fit(const PairIO& j, int nm, const std::uint8_t* keep, double* out,
+__device__ inline bool block_fit(const PairIO& j, int nm, const std::uint8_t* keep, double* out, double (*dv)[10],
                           Pt* cpts /*kFinishChunk shared*/, std::uint8_t* ckeep) {
     __shared__ double sums[6];
     __shared__ int kept;
@@ -756,22 +756,35 @@ __device__ inline bool block_fit(const PairIO& j, int nm, const std::uint8_t* ke
     if (!(va > 0.0) || !(vb > 0.0) || !fin(va) || !fin(vb)) return false;
     const double sa = sqrt(2.0 * count / va);
     const double sb = sqrt(2.0 * count / vb);
-    // pass 3: normal matrix, entry (r, c) on thread 9r + c
+    // pass 3: normal matrix, entry (r, c) on thread 9r + c. Each point's ten
+    // design values are computed once (by the point's thread) into dv; a
+    // matrix thread reads its four factors by index:
+    // dv = {x, y, 1, 0, u, v, -u x, -u y, -v x, -v y},
+    // row 0 = dv[{0,1,2,3,3,3,6,7,4}], row 1 = dv[{3,3,3,0,1,2,8,9,5}].
+    constexpr unsigned char kRow0[9] = {0, 1, 2, 3, 3, 3, 6, 7, 4};
+    constexpr unsigned char kRow1[9] = {3, 3, 3, 0, 1, 2, 8, 9, 5};
     const int r = t / 9, c = t % 9;
+    const int i0r = t < 72 ? kRow0[r] : 0, i0c = t < 72 ? kRow0[c] : 0;
+    const int i1r = t < 72 ? kRow1[r] : 0, i1c = t < 72 ? kRow1[c] : 0;
     for (int base = 0; base < nm; base += kFinishChunk) {
         const int n = min(kFinishChunk, nm - base);
         __syncthreads();
-        for (int i = t; i < n; i += blockDim.x) { cpts[i] = gather(j, base + i); ckeep[i] = keep[base + i]; }
+        for (int i = t; i < n; i += blockDim.x) {
+            const Pt p = gather(j, base + i);
+            ckeep[i] = keep[base + i];
+            const double x = (p.bx - cbx) * sb, y = (p.by - cby) * sb;
+            const double u = (p.ax - cax) * sa, v = (p.ay - cay) * sa;
+            double* d = dv[i];
+            d[0] = x; d[1] = y; d[2] = 1.0; d[3] = 0.0; d[4] = u; d[5] = v;
+            d[6] = -u * x; d[7] = -u * y; d[8] = -v * x; d[9] = -v * y;
+        }
         __syncthreads();
         if (t < 72) {
             double acc = m[r][c];
             for (int i = 0; i < n; ++i) {
                 if (!ckeep[i]) continue;
-                const Pt p = cpts[i];
-                const double x = (p.bx - cbx) * sb, y = (p.by - cby) * sb;
-                const double u = (p.ax - cax) * sa, v = (p.ay - cay) * sa;
-                acc += design(0, r, x, y, u, v) * design(0, c, x, y, u, v) +
-                       design(1, r, x, y, u, v) * design(1, c, x, y, u, v);
+                const double* d = dv[i];
+                acc += d[i0r] * d[i0c] + d[i1r] * d[i1c];
             }
             m[r][c] = acc;
         }
@@ -788,11 +801,12 @@ __device__ inline bool block_fit(const PairIO& j, int nm, const std::uint8_t* ke
 // One block per pair: fold the search blocks' winners into the saved raw
 // winner, refine, and build the mask and the result.
 template <class Src>
-__global__ __launch_bounds__(kFinishThreads) void finish_kernel(const __grid_constant__ Src src) {
+__global__ __launch_bounds__(kFinishThreads, 1) void finish_kernel(const __grid_constant__ Src src) {
     __shared__ int red_src[kFinishThreads];
     __shared__ double buf[kFinishChunk];
     __shared__ Pt cpts[kFinishChunk];
     __shared__ std::uint8_t ckeep[kFinishChunk];
+    __shared__ double dv[kFinishChunk][10];
     __shared__ Model model, cand;
     __shared__ HomographyResult res;
     __shared__ int cand_ok, inl;
@@ -853,7 +867,7 @@ __global__ __launch_bounds__(kFinishThreads) void finish_kernel(const __grid_con
             for (int i = t; i < nm; i += kFinishThreads) j.mask[i] = residual2(h, gather(j, i)) <= thr2;
             __syncthreads();
             double ch[9];
-            const bool fitted = block_fit(j, nm, j.mask, ch, cpts, ckeep);
+            const bool fitted = block_fit(j, nm, j.mask, ch, dv, cpts, ckeep);
             if (t == 0) {
                 cand_ok = fitted && valid_domain(ch, bw, bh);
                 for (int e = 0; e < 9; ++e) cand.h[e] = ch[e];
