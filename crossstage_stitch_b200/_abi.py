@@ -85,10 +85,15 @@ class S5Config(C.Structure):
                 ("generation", C.c_uint64)]
 
 
+class PyramidConfig(C.Structure):
+    """stitch_pyramid_config: levels 1 (or 0) is the single-level path."""
+    _fields_ = [("levels", C.c_int), ("scale_factor", C.c_float)]
+
+
 class PairDesc(C.Structure):
     """stitch_pair_desc: one pair of the batched form."""
     _fields_ = [("image_a", ImageView), ("image_b", ImageView), ("scale_a", ScaleInfo), ("scale_b", ScaleInfo),
-                ("s2", S2Config), ("s4", S4Config), ("s5", S5Config)]
+                ("s2", S2Config), ("s4", S4Config), ("s5", S5Config), ("pyramid", PyramidConfig)]
 
 
 P = C.POINTER
@@ -110,6 +115,9 @@ PROTOTYPES: dict[str, tuple] = {
                                      C.c_void_p]),
     "stitch_s3_describe_marked": (C.c_int, [P(ImageView), P(Keypoints), P(Descriptors), C.c_void_p,
                                             C.c_size_t, C.c_void_p, C.c_void_p]),
+    "stitch_pyramid_workspace_bytes": (C.c_int, [C.c_int, C.c_int, P(S2Config), P(PyramidConfig), _size_p]),
+    "stitch_pyramid_detect_describe": (C.c_int, [P(ImageView), P(S2Config), P(PyramidConfig), P(Keypoints),
+                                                 P(Descriptors), C.c_void_p, C.c_size_t, C.c_void_p]),
     "stitch_s4_workspace_bytes": (C.c_int, [C.c_int, C.c_int, P(S4Config), _size_p]),
     "stitch_s4_knn_top2": (C.c_int, [P(Keypoints), P(Descriptors), P(Keypoints), P(Descriptors), C.c_void_p,
                                      C.c_void_p]),
@@ -133,7 +141,7 @@ PROTOTYPES: dict[str, tuple] = {
     "stitch_batch_set_marks": (C.c_int, [C.c_void_p, P(C.c_void_p), C.c_int]),
 }
 
-BATCH_MARKS = ("tables", "fast_nms", "select_scatter", "harris", "sort_topk", "blur", "describe", "knn_popc",
+BATCH_MARKS = ("tables", "pyramid", "fast_nms", "select_scatter", "harris", "sort_topk", "blur", "describe", "knn_popc",
                "knn_merge", "accept", "prepare", "search", "finish")
 
 _LIB: C.CDLL | None = None

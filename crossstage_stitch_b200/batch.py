@@ -21,6 +21,7 @@ def pair_desc(img_a: torch.Tensor, img_b: torch.Tensor, knobs: Knobs, size_a=Non
     d.image_a = ImageView(img_a.data_ptr(), wa, ha, img_a.stride(0), 1)
     d.image_b = ImageView(img_b.data_ptr(), wb, hb, img_b.stride(0), 1)
     d.s2, d.s4, d.s5 = knobs.s2(), knobs.s4(), knobs.s5()
+    d.pyramid = knobs.pyramid()
     return d
 
 

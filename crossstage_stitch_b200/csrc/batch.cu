@@ -3,14 +3,19 @@
 // device job table and a block-prefix array. The per-pair stage semantics
 // are unchanged, so results equal the per-pair calls bit for bit.
 //
+// With a scale pyramid (levels > 1) an image contributes one detect and one
+// describe job per layer and one resize job per layer above the first; the
+// resize chain runs first, one launch per layer depth over all images.
+//
 // Workspace layout (one caller allocation, 256-byte aligned regions):
-//   counts   int[3n]      keypoint counts (2 per pair) and match counts,
-//                         zeroed at the start of every run
-//   hists    u32[2n][256] FAST histograms, zeroed at the start of every run
+//   counts   int[3n + L]  keypoint counts (2 per pair), match counts and the
+//                         L pyramid layer counts, zeroed every run
+//   hists    u32[J][256]  FAST histograms of the J detect jobs, zeroed every run
 //   results  HomographyResult[n]
 //   tables   job tables + prefixes, copied from pinned host staging
 //   per pair: keypoints x/y/response, descriptors, S2 and S3 workspaces per
-//             image, matches, inlier mask, S4 and S5 workspaces
+//             image (or its pyramid workspace), matches, inlier mask, S4 and
+//             S5 workspaces
 #include <algorithm>
 #include <cstring>
 #include <mutex>
@@ -23,6 +28,7 @@ namespace {
 
 using s2s3::DescribeJob;
 using s2s3::DetectJob;
+using s2s3::ResizeJob;
 using s4k::AcceptJob;
 using s4k::KnnJob;
 using s5k::PairIO;
@@ -37,12 +43,13 @@ bool small_image(const stitch_image_view& v) { return v.width <= 2 * s2::kEdge |
 // Device job tables, in this order inside the table block.
 enum Table {
     kDetJobs, kDetPrefix, kDesJobs, kDesPrefix, kKnnJobs, kKnnPrefix, kMergePrefix, kAccJobs, kAccPrefix,
-    kPairJobs, kPairPrefix, kSearchJobs, kSearchPrefix, kTables
+    kPairJobs, kPairPrefix, kSearchJobs, kSearchPrefix, kRsJobs, kRsPrefix, kTables
 };
 
 void set_attributes_once() {
     static std::once_flag flag;
     std::call_once(flag, [] {
+        static_assert(kTables <= 16, "table offsets");
         cudaFuncSetAttribute(s2s3::sort_topk_kernel<s2s3::JobTable<DetectJob>>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                              s2s3::kSortCap * static_cast<int>(sizeof(std::uint64_t)));
@@ -69,9 +76,11 @@ Status Plan::build(int n_pairs, const stitch_pair_desc* p, int* bad_pair) {
         const auto& c2 = *reinterpret_cast<const s2::Config*>(&q.s2);
         const auto& c4 = *reinterpret_cast<const s4::Config*>(&q.s4);
         const auto& c5 = *reinterpret_cast<const s5::Config*>(&q.s5);
+        if (q.pyramid.levels == 0) q.pyramid.levels = 1;
         bool ok = s2s3::valid_gray(view(q.image_a)) && s2s3::valid_gray(view(q.image_b)) &&
                   s2s3::valid_detect_config(c2) && std::isfinite(c4.ratio_threshold) && c4.ratio_threshold > 0 &&
-                  c4.ratio_threshold < 1 && s5k::valid_config(c5) && c5.previous_hypotheses == 0;
+                  c4.ratio_threshold < 1 && s5k::valid_config(c5) && c5.previous_hypotheses == 0 &&
+                  s2s3::valid_pyramid(q.pyramid.levels, q.pyramid.scale_factor);
         for (int s = 0; s < 2 && ok; ++s) {
             stitch_scale_info& si = s ? q.scale_b : q.scale_a;
             const stitch_image_view& im = s ? q.image_b : q.image_a;
@@ -84,13 +93,39 @@ Status Plan::build(int n_pairs, const stitch_pair_desc* p, int* bad_pair) {
             return Status::INVALID_ARGUMENT;
         }
     }
-    // 2. layout
+    // 2. jobs per image: one single-level job, or one per pyramid layer
+    n_det = n_layers = n_resize = 0;
+    max_levels = 1;
+    for (int i = 0; i < n; ++i) {
+        auto& o = off[i];
+        const auto& q = pairs[i];
+        for (int s = 0; s < 2; ++s) {
+            const stitch_image_view& im = s ? q.image_b : q.image_a;
+            o.pyramid[s] = q.pyramid.levels > 1;
+            o.job0[s] = n_det;
+            o.layer0[s] = n_layers;
+            if (!o.pyramid[s]) {
+                ++n_det;
+                continue;
+            }
+            if (!s2s3::pyramid_layout(im.width, im.height, q.s2.max_keypoints, q.pyramid.levels,
+                                      q.pyramid.scale_factor, &o.pyr[s])) {
+                if (bad_pair) *bad_pair = i;
+                return Status::INVALID_ARGUMENT;
+            }
+            const int L = o.pyr[s].plan.levels;
+            n_det += L;
+            n_layers += L;
+            n_resize += L > 1 ? L - 1 : 0;
+            max_levels = std::max(max_levels, L);
+        }
+    }
+    // 3. layout
     Layout lay;
-    const std::size_t counts = lay.take(3 * static_cast<std::size_t>(n), sizeof(int));
-    const std::size_t hists = lay.take(2 * static_cast<std::size_t>(n) * 256, sizeof(std::uint32_t));
+    const std::size_t counts = lay.take(3 * static_cast<std::size_t>(n) + n_layers, sizeof(int));
+    hists = lay.take(static_cast<std::size_t>(std::max(n_det, 1)) * 256, sizeof(std::uint32_t));
+    zeroed = lay.cursor;
     results = lay.take(n, sizeof(HomographyResult));
-    (void)counts;
-    (void)hists;
     for (int i = 0; i < n; ++i) {
         auto& o = off[i];
         const auto& q = pairs[i];
@@ -103,6 +138,10 @@ Status Plan::build(int n_pairs, const stitch_pair_desc* p, int* bad_pair) {
             o.kr[s] = lay.take(kk, sizeof(float));
             o.kcount[s] = counts + (2 * static_cast<std::size_t>(i) + s) * sizeof(int);
             o.desc[s] = lay.take(kk, 32);
+            if (o.pyramid[s]) {
+                o.pyrws[s] = lay.take(o.pyr[s].total, 1);
+                continue;
+            }
             if (!s2s3::detect_layout(im.width, im.height, k, &o.det[s]) ||
                 !s2s3::describe_layout(im.width, im.height, &o.des[s])) {
                 if (bad_pair) *bad_pair = i;
@@ -120,25 +159,20 @@ Status Plan::build(int n_pairs, const stitch_pair_desc* p, int* bad_pair) {
         o.s4ws = lay.take(o.match.total, 1);
         o.s5ws = lay.take(s5k::estimate_workspace_bytes(), 1);
     }
-    // 3. launch shapes
-    std::fill(std::begin(det_blocks), std::end(det_blocks), 0);
-    std::fill(std::begin(des_blocks), std::end(des_blocks), 0);
+    // 4. launch shapes (block counts are final once stage_tables has run)
     int max_cand = 0, max_cap_m = 1;
     for (int i = 0; i < n; ++i) {
         const auto& q = pairs[i];
         for (int s = 0; s < 2; ++s) {
             const stitch_image_view& im = s ? q.image_b : q.image_a;
-            const auto& d = off[i].det[s];
-            if (q.s2.max_keypoints > 0 && !small_image(im)) {
-                det_blocks[s2s3::kFastKind] += d.tiles;
-                det_blocks[s2s3::kChunkKind] += d.chunks;
-                det_blocks[s2s3::kHarrisKind] += ceil_div(d.candidates, s2s3::kHarrisThreads);
-                det_blocks[s2s3::kSortKind] += 1;
-                max_cand = std::max(max_cand, d.candidates);
-            }
-            if (q.s2.max_keypoints > 0) {
-                des_blocks[s2s3::kBlurKind] += off[i].des[s].tiles;
-                des_blocks[s2s3::kDescKind] += ceil_div(q.s2.max_keypoints, s2s3::kDescWarps);
+            if (off[i].pyramid[s]) {
+                for (int l = 0; l < off[i].pyr[s].plan.levels; ++l) {
+                    int b[s2s3::kDetectKinds];
+                    s2s3::pyramid_detect_blocks(off[i].pyr[s], l, b);
+                    if (b[s2s3::kSortKind]) max_cand = std::max(max_cand, off[i].pyr[s].det[l].candidates);
+                }
+            } else if (q.s2.max_keypoints > 0 && !small_image(im)) {
+                max_cand = std::max(max_cand, off[i].det[s].candidates);
             }
         }
         max_cap_m = std::max(max_cap_m, q.s2.max_keypoints);
@@ -167,17 +201,18 @@ Status Plan::build(int n_pairs, const stitch_pair_desc* p, int* bad_pair) {
         if (rounds_at >= 2 * kSmCount) break;
     }
     search_blocks = static_cast<int>(rounds_at);
-    // 4. table block layout
+    // 5. table block layout
     std::size_t cur = 0;
     auto put = [&](int t, std::size_t bytes) {
         cur = (cur + 15) / 16 * 16;
         offsets[t] = cur;
         cur += bytes;
     };
-    put(kDetJobs, 2 * n * sizeof(DetectJob));
-    put(kDetPrefix, s2s3::kDetectKinds * (2 * n + 1) * sizeof(int));
-    put(kDesJobs, 2 * n * sizeof(DescribeJob));
-    put(kDesPrefix, s2s3::kDescribeKinds * (2 * n + 1) * sizeof(int));
+    const std::size_t nd = static_cast<std::size_t>(n_det), nr = static_cast<std::size_t>(n_resize);
+    put(kDetJobs, nd * sizeof(DetectJob));
+    put(kDetPrefix, s2s3::kDetectKinds * (nd + 1) * sizeof(int));
+    put(kDesJobs, nd * sizeof(DescribeJob));
+    put(kDesPrefix, s2s3::kDescribeKinds * (nd + 1) * sizeof(int));
     put(kKnnJobs, n_knn * sizeof(KnnJob));
     put(kKnnPrefix, (n_knn + 1) * sizeof(int));
     put(kMergePrefix, (n_knn + 1) * sizeof(int));
@@ -187,6 +222,8 @@ Status Plan::build(int n_pairs, const stitch_pair_desc* p, int* bad_pair) {
     put(kPairPrefix, (n + 1) * sizeof(int));
     put(kSearchJobs, n * sizeof(SearchJob));
     put(kSearchPrefix, (n + 1) * sizeof(int));
+    put(kRsJobs, nr * sizeof(ResizeJob));
+    put(kRsPrefix, static_cast<std::size_t>(resize_kinds()) * (nr + 1) * sizeof(int));
     table_bytes = cur;
     tables = lay.take(table_bytes, 1);
     if (!lay.ok) return Status::INVALID_ARGUMENT;
@@ -215,8 +252,27 @@ Status Plan::stage_tables(void* ws) {
     auto* pp = reinterpret_cast<int*>(T + offsets[kPairPrefix]);
     auto* rj = reinterpret_cast<SearchJob*>(T + offsets[kSearchJobs]);
     auto* rp = reinterpret_cast<int*>(T + offsets[kSearchPrefix]);
-    std::uint32_t* hists = at<std::uint32_t>(ws, hists_offset());
+    auto* zj = reinterpret_cast<ResizeJob*>(T + offsets[kRsJobs]);
+    auto* zp = reinterpret_cast<int*>(T + offsets[kRsPrefix]);
+    std::uint32_t* hist_base = at<std::uint32_t>(ws, hists);
+    int* layer_counts = at<int>(ws, 0) + 3 * static_cast<std::size_t>(n);
+    const int nd = n_det, nr = n_resize, rkinds = resize_kinds();
     int run_det[s2s3::kDetectKinds] = {}, run_des[s2s3::kDescribeKinds] = {};
+    int run_rs[s2s3::kMaxLevels] = {};
+    int rjob = 0;
+    auto add_job = [&](int idx, const DetectJob& d, const DescribeJob& e, const int (&db)[s2s3::kDetectKinds],
+                       const int (&sb)[s2s3::kDescribeKinds]) {
+        dj[idx] = d;
+        sj[idx] = e;
+        for (int kind = 0; kind < s2s3::kDetectKinds; ++kind) {
+            dp[kind * (nd + 1) + idx] = run_det[kind];
+            run_det[kind] += db[kind];
+        }
+        for (int kind = 0; kind < s2s3::kDescribeKinds; ++kind) {
+            sp[kind * (nd + 1) + idx] = run_des[kind];
+            run_des[kind] += sb[kind];
+        }
+    };
     int qtiles_total = 0;
     for (int i = 0; i < n; ++i) {
         const int dirs = pairs[i].s4.cross_check ? 2 : 1;
@@ -236,26 +292,39 @@ Status Plan::stage_tables(void* ws) {
             kps[s] = Keypoints{at<float>(ws, o.kx[s]), at<float>(ws, o.ky[s]), at<float>(ws, o.kr[s]), k,
                                at<int>(ws, o.kcount[s])};
             desc[s] = Descriptors{DescriptorType::BINARY_U8, 32, 32, at<std::uint8_t>(ws, o.desc[s])};
-            const int idx = 2 * i + s;
-            DetectJob d = s2s3::make_detect_job(view(im), *reinterpret_cast<const s2::Config*>(&q.s2), kps[s],
-                                                at<void>(ws, o.s2ws[s]), o.det[s]);
-            d.hist = hists + static_cast<std::size_t>(idx) * 256;
-            dj[idx] = d;
+            const auto& c2 = *reinterpret_cast<const s2::Config*>(&q.s2);
+            const int idx = o.job0[s];
+            if (o.pyramid[s]) {
+                const auto& pl = o.pyr[s];
+                s2s3::PyramidJobs pjobs;
+                s2s3::make_pyramid_jobs(view(im), c2, kps[s], desc[s], at<void>(ws, o.pyrws[s]), pl,
+                                        layer_counts + o.layer0[s], hist_base + static_cast<std::size_t>(idx) * 256,
+                                        &pjobs);
+                for (int l = 0; l < pl.plan.levels; ++l) {
+                    int db[s2s3::kDetectKinds], sb[s2s3::kDescribeKinds];
+                    s2s3::pyramid_detect_blocks(pl, l, db);
+                    s2s3::pyramid_describe_blocks(pl, l, sb);
+                    add_job(idx + l, pjobs.detect[l], pjobs.describe[l], db, sb);
+                }
+                for (int l = 1; l < pl.plan.levels; ++l, ++rjob) {
+                    zj[rjob] = pjobs.resize[l];
+                    for (int kind = 0; kind < rkinds; ++kind) {
+                        zp[kind * (nr + 1) + rjob] = run_rs[kind];
+                        run_rs[kind] += kind == l - 1 ? pl.resize_tiles[l] : 0;
+                    }
+                }
+                continue;
+            }
+            DetectJob d = s2s3::make_detect_job(view(im), c2, kps[s], at<void>(ws, o.s2ws[s]), o.det[s]);
+            d.hist = hist_base + static_cast<std::size_t>(idx) * 256;
             const bool active = k > 0 && !small_image(im);
-            const int blocks[s2s3::kDetectKinds] = {
+            const int db[s2s3::kDetectKinds] = {
                 active ? o.det[s].tiles : 0, active ? o.det[s].chunks : 0,
                 active ? ceil_div(o.det[s].candidates, s2s3::kHarrisThreads) : 0, active ? 1 : 0};
-            for (int kind = 0; kind < s2s3::kDetectKinds; ++kind) {
-                dp[kind * (2 * n + 1) + idx] = run_det[kind];
-                run_det[kind] += blocks[kind];
-            }
-            sj[idx] = s2s3::make_describe_job(view(im), kps[s], desc[s], at<void>(ws, o.s3ws[s]), o.des[s]);
-            const int dblocks[s2s3::kDescribeKinds] = {k > 0 ? o.des[s].tiles : 0,
-                                                       k > 0 ? ceil_div(k, s2s3::kDescWarps) : 0};
-            for (int kind = 0; kind < s2s3::kDescribeKinds; ++kind) {
-                sp[kind * (2 * n + 1) + idx] = run_des[kind];
-                run_des[kind] += dblocks[kind];
-            }
+            const int sb[s2s3::kDescribeKinds] = {k > 0 ? o.des[s].tiles : 0,
+                                                  k > 0 ? ceil_div(k, s2s3::kDescWarps) : 0};
+            add_job(idx, d, s2s3::make_describe_job(view(im), kps[s], desc[s], at<void>(ws, o.s3ws[s]), o.des[s]),
+                    db, sb);
         }
         // S4 (forward, then reverse when the mutual check is on)
         auto* fwd = at<s4k::Top2>(ws, o.s4ws + o.match.forward);
@@ -309,8 +378,10 @@ Status Plan::stage_tables(void* ws) {
         rp[i] = run_search;
         run_search += io.search_blocks;
     }
-    for (int kind = 0; kind < s2s3::kDetectKinds; ++kind) dp[kind * (2 * n + 1) + 2 * n] = run_det[kind];
-    for (int kind = 0; kind < s2s3::kDescribeKinds; ++kind) sp[kind * (2 * n + 1) + 2 * n] = run_des[kind];
+    for (int kind = 0; kind < s2s3::kDetectKinds; ++kind) dp[kind * (nd + 1) + nd] = run_det[kind];
+    for (int kind = 0; kind < s2s3::kDescribeKinds; ++kind) sp[kind * (nd + 1) + nd] = run_des[kind];
+    for (int kind = 0; kind < rkinds; ++kind) zp[kind * (nr + 1) + nr] = run_rs[kind];
+    for (int kind = 0; kind < s2s3::kMaxLevels; ++kind) rs_blocks[kind] = kind < rkinds ? run_rs[kind] : 0;
     kp[n_knn] = run_knn;
     mp[n_knn] = run_merge;
     ap[n] = n;
@@ -334,15 +405,17 @@ Status Plan::enqueue(void* ws, std::size_t bytes, stitch_homography_result* host
     unsigned char* T = at<unsigned char>(ws, tables);
     if (cudaMemcpyAsync(T, staging, table_bytes, cudaMemcpyHostToDevice, s) != cudaSuccess) return Status::CUDA_ERROR;
     // counts and histograms: contiguous at the start, zeroed together
-    const std::size_t hist_end = hists_offset() + 2 * static_cast<std::size_t>(n) * 256 * sizeof(std::uint32_t);
-    if (cudaMemsetAsync(ws, 0, hist_end, s) != cudaSuccess) return Status::CUDA_ERROR;
+    if (cudaMemsetAsync(ws, 0, zeroed, s) != cudaSuccess) return Status::CUDA_ERROR;
 
     using DetSrc = s2s3::JobTable<DetectJob>;
     using DesSrc = s2s3::JobTable<DescribeJob>;
+    using RsSrc = s2s3::JobTable<ResizeJob>;
     const DetSrc det{reinterpret_cast<const DetectJob*>(T + offsets[kDetJobs]),
-                     reinterpret_cast<const int*>(T + offsets[kDetPrefix]), 2 * n};
+                     reinterpret_cast<const int*>(T + offsets[kDetPrefix]), n_det};
     const DesSrc des{reinterpret_cast<const DescribeJob*>(T + offsets[kDesJobs]),
-                     reinterpret_cast<const int*>(T + offsets[kDesPrefix]), 2 * n};
+                     reinterpret_cast<const int*>(T + offsets[kDesPrefix]), n_det};
+    const RsSrc rs{reinterpret_cast<const ResizeJob*>(T + offsets[kRsJobs]),
+                   reinterpret_cast<const int*>(T + offsets[kRsPrefix]), n_resize};
     int launches = 0;
     int next_mark = 0;
     bool marks_ok = true;
@@ -359,6 +432,9 @@ Status Plan::enqueue(void* ws, std::size_t bytes, stitch_homography_result* host
         ++next_mark;
     };
     mark();  // tables uploaded, counts cleared
+    for (int kind = 0; kind + 1 < max_levels; ++kind)  // layer kind + 1 of every pyramid image
+        if (go(rs_blocks[kind])) s2s3::resize_kernel<RsSrc><<<rs_blocks[kind], 256, 0, s>>>(rs, kind);
+    mark();
     if (go(det_blocks[s2s3::kFastKind])) s2s3::fast_nms_kernel<DetSrc><<<det_blocks[s2s3::kFastKind], 256, 0, s>>>(det);
     mark();
     if (go(det_blocks[s2s3::kChunkKind])) {

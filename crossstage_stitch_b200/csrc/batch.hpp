@@ -19,6 +19,12 @@ struct PairOffsets {
     s2s3::DetectLayout det[2];
     s2s3::DescribeLayout des[2];
     s4k::MatchLayout match;
+    // scale pyramid (levels > 1): layer workspace, first layer count and
+    // first detect job of each image
+    bool pyramid[2];
+    s2s3::PyramidLayout pyr[2];
+    std::size_t pyrws[2];
+    int layer0[2], job0[2];
 };
 
 class Plan {
@@ -31,8 +37,14 @@ public:
     std::size_t table_bytes = 0;
     std::size_t total = 0;
     // launch shapes
+    int n_det = 0;     // detect/describe jobs: one per image, one per layer of a pyramid image
+    int n_layers = 0;  // layer counts kept after the 3n image and match counts
+    int n_resize = 0;  // resize jobs (layers 1.. of every pyramid image)
+    int max_levels = 1;
+    std::size_t hists = 0, zeroed = 0;  // FAST histograms u32[n_det][256]; bytes zeroed per run
     int det_blocks[s2s3::kDetectKinds] = {};
     int des_blocks[s2s3::kDescribeKinds] = {};
+    int rs_blocks[s2s3::kMaxLevels] = {};  // resize launch of layer kind + 1
     int knn_blocks = 0, merge_blocks = 0, n_knn = 0;
     int search_blocks = 0;
     int sort_smem = 0, search_smem = 0;
@@ -49,12 +61,7 @@ public:
     bool marked = false;
 
     ~Plan();
-    // Histograms follow the counts region (int[3n]) at the workspace start.
-    std::size_t hists_offset() const {
-        Layout lay;
-        lay.take(3 * static_cast<std::size_t>(n), sizeof(int));
-        return lay.take(2 * static_cast<std::size_t>(n) * 256, sizeof(std::uint32_t));
-    }
+    int resize_kinds() const { return max_levels > 1 ? max_levels - 1 : 1; }
     Status build(int n_pairs, const stitch_pair_desc* p, int* bad_pair);
     Status stage_tables(void* ws);
     Status enqueue(void* ws, std::size_t bytes, stitch_homography_result* host_results, cudaStream_t s);

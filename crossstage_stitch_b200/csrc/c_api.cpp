@@ -41,13 +41,20 @@ cudaStream_t stream_of(void* s) { return static_cast<cudaStream_t>(s); }
 }  // namespace
 
 namespace stitch::b200 {
+namespace s2s3 {  // pyramid.cu
+Status pyramid_workspace_bytes(int w, int h, const s2::Config& c, int levels, float scale_factor,
+                               std::size_t* bytes);
+Status pyramid_detect_describe(const ImageView& image, const s2::Config& c, int levels, float scale_factor,
+                               const Keypoints& out, const Descriptors& desc, void* ws, std::size_t ws_bytes,
+                               cudaStream_t stream);
+}  // namespace s2s3
 static std::atomic<long long> g_launches{0};
 void note_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 }  // namespace stitch::b200
 
 extern "C" {
 
-int stitch_abi_version(void) { return 1; }
+int stitch_abi_version(void) { return 2; }
 
 long long stitch_launch_count(void) { return stitch::b200::g_launches.load(std::memory_order_relaxed); }
 
@@ -136,6 +143,22 @@ int stitch_s3_describe_marked(const stitch_image_view* im, const stitch_keypoint
     const s2_s3::detail::S3Marks marks{static_cast<cudaEvent_t>(e_blur)};
     return code(s2_s3::detail::s3_describe_marked(as<ImageView>(im), as<Keypoints>(kp), as<Descriptors>(out), ws,
                                                   ws_bytes, stream_of(stream), marks));
+}
+
+int stitch_pyramid_workspace_bytes(int w, int h, const stitch_s2_config* c, const stitch_pyramid_config* p,
+                                   size_t* bytes) {
+    if (!c || !p) return kInvalid;
+    return code(b200::s2s3::pyramid_workspace_bytes(w, h, as<s2::Config>(c), p->levels ? p->levels : 1,
+                                                    p->scale_factor, bytes));
+}
+
+int stitch_pyramid_detect_describe(const stitch_image_view* im, const stitch_s2_config* c,
+                                   const stitch_pyramid_config* p, const stitch_keypoints* kp,
+                                   const stitch_descriptors* desc, void* ws, size_t ws_bytes, void* stream) {
+    if (!im || !c || !p || !kp || !desc) return kInvalid;
+    return code(b200::s2s3::pyramid_detect_describe(as<ImageView>(im), as<s2::Config>(c), p->levels ? p->levels : 1,
+                                                    p->scale_factor, as<Keypoints>(kp), as<Descriptors>(desc), ws,
+                                                    ws_bytes, stream_of(stream)));
 }
 
 int stitch_s4_workspace_bytes(int ca, int cb, const stitch_s4_config* c, size_t* bytes) {

@@ -28,4 +28,59 @@ DescribeJob make_describe_job(const ImageView& im, const Keypoints& kp, const De
 // Dynamic shared memory of sort_topk_kernel for `candidates` keys.
 int sort_smem_bytes(int candidates);
 
+// ------------------------------------------------------- scale pyramid
+
+// Layers of one image (OpenCV ORB level semantics): layer l has scale
+// s_l = float(double(sf)^l) and size cvRound(W * (1.f / s_l)) x
+// cvRound(H * (1.f / s_l)); layer l >= 1 is resized from layer l - 1. Only
+// layers whose sides both exceed 2 * kEdge are built (smaller ones hold no
+// keypoint). Budgets split K geometrically (cv::ORB's nfeaturesPerLevel),
+// each share clamped so that the total is exactly K.
+struct LevelPlan {
+    int levels = 0;  // layers built
+    int width[kMaxLevels] = {}, height[kMaxLevels] = {}, budget[kMaxLevels] = {};
+    float scale[kMaxLevels] = {};
+};
+
+bool valid_pyramid(int levels, float scale_factor);
+LevelPlan level_plan(int w, int h, int k, int levels, float scale_factor);
+
+// Workspace of one image's pyramid. `zeroed` (layer counts int[levels],
+// then FAST histograms u32[levels][256]) must be zero before each run.
+struct PyramidLayout {
+    LevelPlan plan;
+    std::size_t counts, hists, zeroed_bytes;
+    std::size_t image[kMaxLevels];  // dense layer images, l >= 1
+    std::size_t kx[kMaxLevels], ky[kMaxLevels], kr[kMaxLevels];  // layer keypoints
+    std::size_t detect[kMaxLevels], describe[kMaxLevels];
+    DetectLayout det[kMaxLevels];
+    DescribeLayout des[kMaxLevels];
+    int resize_tiles[kMaxLevels];
+    std::size_t total;
+};
+
+bool pyramid_layout(int w, int h, int k, int levels, float scale_factor, PyramidLayout* out);
+
+struct PyramidJobs {
+    ResizeJob resize[kMaxLevels];  // entries 1 .. levels-1
+    DetectJob detect[kMaxLevels];
+    DescribeJob describe[kMaxLevels];
+};
+
+// Jobs of every layer over the workspace `ws` laid out by `l`; the layer
+// counts and histograms are `counts` and `hists` (the layout's own unless
+// the caller keeps them elsewhere).
+void make_pyramid_jobs(const ImageView& im, const s2::Config& c, const Keypoints& out, const Descriptors& desc,
+                       void* ws, const PyramidLayout& l, int* counts, std::uint32_t* hists, PyramidJobs* jobs);
+
+// Block count of each detect/describe kind for layer i (0 when inactive).
+void pyramid_detect_blocks(const PyramidLayout& l, int layer, int (&blocks)[kDetectKinds]);
+void pyramid_describe_blocks(const PyramidLayout& l, int layer, int (&blocks)[kDescribeKinds]);
+
+Status pyramid_workspace_bytes(int w, int h, const s2::Config& c, int levels, float scale_factor,
+                               std::size_t* bytes);
+Status pyramid_detect_describe(const ImageView& image, const s2::Config& c, int levels, float scale_factor,
+                               const Keypoints& out, const Descriptors& desc, void* ws, std::size_t ws_bytes,
+                               cudaStream_t stream);
+
 }  // namespace stitch::b200::s2s3

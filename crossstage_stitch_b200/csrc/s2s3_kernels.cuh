@@ -61,6 +61,29 @@ struct DescribeJob {
     std::uint8_t* out;  // rows of row_stride bytes
     int row_stride;
     int tiles_x, tiles;  // blur tiles
+    // Pyramid layer (level_counts != null): the layer's keypoints are in
+    // layer coordinates in x/y/response; the describe kernel writes them,
+    // multiplied by `scale`, and their descriptors to the image's
+    // concatenated outputs after the keypoints of lower layers
+    // (level_counts[0..level-1]) and adds the layer's count to *out_count.
+    const float* response;
+    float* out_x;
+    float* out_y;
+    float* out_response;  // may be null
+    int* out_count;
+    const int* level_counts;
+    int level;
+    float scale;
+};
+
+// One pyramid layer: `dst` (dense) resized from `src` by fixed-point
+// bilinear interpolation (cv::resize INTER_LINEAR_EXACT on 8-bit images).
+struct ResizeJob {
+    const std::uint8_t* src;
+    int src_width, src_height, src_pitch;
+    std::uint8_t* dst;
+    int width, height;
+    int tiles_x, tiles;
 };
 
 // Per-image job passed by value.
@@ -93,6 +116,22 @@ template <class Job> struct JobTable {
     }
 };
 
+// A few jobs passed by value (the layers of one image's pyramid):
+// first[kind][i] is the first block of job i; linear search.
+template <class Job, int kJobs, int kKinds> struct InlineTable {
+    Job jobs[kJobs];
+    int first[kKinds][kJobs + 1];
+    int n;
+    __device__ bool find(int block, int kind, Job* j, int* local) const {
+        if (block >= first[kind][n]) return false;
+        int i = 0;
+        while (i + 1 < n && first[kind][i + 1] <= block) ++i;
+        *j = jobs[i];
+        *local = block - first[kind][i];
+        return true;
+    }
+};
+
 enum DetectKind { kFastKind = 0, kChunkKind = 1, kHarrisKind = 2, kSortKind = 3, kDetectKinds = 4 };
 enum DescribeKind { kBlurKind = 0, kDescKind = 1, kDescribeKinds = 2 };
 
@@ -106,6 +145,8 @@ constexpr int kSortThreads = 1024;
 constexpr int kBlurTileW = 64, kBlurTileH = 32;
 constexpr int kDescWarps = 8;
 constexpr int kEdge = 31;
+constexpr int kResizeTileW = 64, kResizeTileH = 16;
+constexpr int kMaxLevels = 16;
 
 // ------------------------------------------------------------- FAST + NMS
 
@@ -520,6 +561,62 @@ __global__ __launch_bounds__(kHarrisThreads) void rank_topk_kernel(const __grid_
     if (slot < n && rank < j.max_keypoints) write_keypoint(j, rank, key);
 }
 
+// ------------------------------------------------------ pyramid layers
+
+// Source index and 8-bit weight of the right neighbour for destination
+// index v of a src -> dst linear resize: f = (v + 0.5) * (1 / (dst / src)) -
+// 0.5 in double, weight rint((f - floor f) * 256). Indices left of the
+// source (every index when src == 1) read pixel 0 with weight 0, indices past
+// the last interval read pixel src - 1 with weight 0.
+__device__ __forceinline__ int2 linear_exact_tap(int v, int src, int dst) {
+    const double scale = 1.0 / (static_cast<double>(dst) / static_cast<double>(src));
+    const double f = scale * (static_cast<double>(v) + 0.5) - 0.5;
+    const double fl = floor(f);
+    if (src == 1 || fl < 0.0) return make_int2(0, 0);
+    if (fl >= static_cast<double>(src - 1)) return make_int2(src - 1, 0);
+    return make_int2(static_cast<int>(fl), static_cast<int>(rint((f - fl) * 256.0)));
+}
+
+// One block = one 64x16 tile of the layer: per-column and per-row taps once
+// in shared memory, then each output is
+//   (h(r0) * (256 - wy) + h(r1) * wy + 2^15) >> 16,
+//   h(r) = src[r][c0] * (256 - wx) + src[r][c1] * wx,
+// the integer form of the 8-bit fixed-point horizontal pass followed by the
+// vertical pass with one final rounding.
+template <class Src>
+__global__ __launch_bounds__(256) void resize_kernel(const __grid_constant__ Src src, int kind) {
+    __shared__ int2 xtap[kResizeTileW];
+    __shared__ int2 ytap[kResizeTileH];
+    ResizeJob j;
+    int local;
+    if (!src.find(blockIdx.x, kind, &j, &local)) return;
+    const int y0 = (local / j.tiles_x) * kResizeTileH;
+    const int x0 = (local % j.tiles_x) * kResizeTileW;
+    const int t = threadIdx.x;
+    if (t < kResizeTileW) xtap[t] = linear_exact_tap(min(x0 + t, j.width - 1), j.src_width, j.width);
+    else if (t < kResizeTileW + kResizeTileH)
+        ytap[t - kResizeTileW] = linear_exact_tap(min(y0 + t - kResizeTileW, j.height - 1), j.src_height, j.height);
+    __syncthreads();
+    const int c = t & (kResizeTileW - 1);
+    const int x = x0 + c;
+    if (x >= j.width) return;
+    const int2 tx = xtap[c];
+    const int xa = tx.x, xb = min(tx.x + 1, j.src_width - 1);
+    const int wx1 = tx.y, wx0 = 256 - tx.y;
+#pragma unroll
+    for (int r = t / kResizeTileW; r < kResizeTileH; r += 256 / kResizeTileW) {
+        const int y = y0 + r;
+        if (y >= j.height) break;
+        const int2 ty = ytap[r];
+        const std::uint8_t* ra = j.src + static_cast<std::size_t>(ty.x) * j.src_pitch;
+        const std::uint8_t* rb = j.src + static_cast<std::size_t>(min(ty.x + 1, j.src_height - 1)) * j.src_pitch;
+        const int ha = ra[xa] * wx0 + ra[xb] * wx1;
+        const int hb = rb[xa] * wx0 + rb[xb] * wx1;
+        const int v = ha * (256 - ty.y) + hb * ty.y;
+        j.dst[static_cast<std::size_t>(y) * j.width + x] = static_cast<std::uint8_t>((v + (1 << 15)) >> 16);
+    }
+}
+
 // ------------------------------------------------------------- S3 blur
 
 // float32 taps of a 7-tap, sigma-2 Gaussian (exp in float64, normalised,
@@ -638,6 +735,11 @@ __global__ __launch_bounds__(kDescWarps * 32) void describe_kernel(const __grid_
     if (!src.find(blockIdx.x, kDescKind, &j, &local)) return;
     // The grid covers the capacity; blocks past the keypoint count leave now.
     const int count = min(*j.count, j.capacity);
+    int base = 0;  // first output row of this layer
+    if (j.level_counts) {
+        if (local == 0 && threadIdx.x == 0) atomicAdd(j.out_count, count);
+        for (int m = 0; m < j.level; ++m) base += j.level_counts[m];
+    }
     if (local * kDescWarps >= count) return;
     {
         const int p = threadIdx.x;  // 256 threads, one pattern pair each
@@ -651,9 +753,14 @@ __global__ __launch_bounds__(kDescWarps * 32) void describe_kernel(const __grid_
     const int lane = threadIdx.x & 31;
     const int index = local * kDescWarps + (threadIdx.x >> 5);
     if (index >= count) return;
-    std::uint8_t* row = j.out + static_cast<std::size_t>(index) * j.row_stride;
+    std::uint8_t* row = j.out + static_cast<std::size_t>(base + index) * j.row_stride;
     const int x = __float2int_rn(j.x[index]);
     const int y = __float2int_rn(j.y[index]);
+    if (j.level_counts && lane == 0) {
+        j.out_x[base + index] = __fmul_rn(j.x[index], j.scale);
+        j.out_y[base + index] = __fmul_rn(j.y[index], j.scale);
+        if (j.out_response) j.out_response[base + index] = j.response[index];
+    }
     if (x < kEdge || x >= j.width - kEdge || y < kEdge || y >= j.height - kEdge) {
         row[lane] = 0;
         return;

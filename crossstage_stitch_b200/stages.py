@@ -7,7 +7,8 @@ src/s5/s5.hpp:23-39); every call goes through the C ABI of libstitch_b200.so
 and returns the Status code. PairRunner reproduces the reference harness's
 fixed-config pair run (harness/pipeline_runner.cu:335-416): buffers are
 allocated once for the largest image and K, then each pair runs
-S2(A), S2(B), S3(A), S3(B), S4, S5 on one stream and synchronises once.
+S2(A), S2(B), S3(A), S3(B), S4, S5 on one stream and synchronises once
+(with pyramid levels > 1, S2+S3 of each image is one pyramid call).
 """
 from __future__ import annotations
 
@@ -19,7 +20,7 @@ import torch
 
 from . import _abi
 from ._abi import (BINARY_U8, GRAY8, Descriptors, HomographyResult, ImageView, Keypoints, Matches,
-                   S2Config, S4Config, S5Config, ScaleInfo, StageError, Status, Top2)
+                   PyramidConfig, S2Config, S4Config, S5Config, ScaleInfo, StageError, Status, Top2)
 
 ref = C.byref
 
@@ -63,7 +64,8 @@ def check(where: str, status: int) -> None:
 class Knobs:
     """Per-pair knobs: the reference's stage Config values
     (src/s2_s3/s2.hpp:19-23, src/s4/s4.hpp:8-11, src/s5/s5.hpp:11-19) with
-    the harness defaults (harness/harness_types.hpp:23-29)."""
+    the harness defaults (harness/harness_types.hpp:23-29), plus the pyramid
+    levels knob (levels 1 is the reference's single-level S2/S3)."""
     fast_threshold: int = 20
     max_keypoints: int = 1000
     harris_k: float = 0.04
@@ -75,6 +77,8 @@ class Knobs:
     threshold: float = 3.0
     seed: int = 0
     generation: int = 1
+    levels: int = 1
+    scale_factor: float = 1.2
 
     def s2(self) -> S2Config:
         return S2Config(self.fast_threshold, self.max_keypoints, self.harris_k)
@@ -88,6 +92,9 @@ class Knobs:
     def s5(self, previous: int = 0) -> S5Config:
         return S5Config(self.hypotheses, previous, self.batch_size, self.refinement_steps, self.threshold,
                         self.seed, self.generation)
+
+    def pyramid(self) -> PyramidConfig:
+        return PyramidConfig(self.levels, self.scale_factor)
 
 
 def result_dict(r: HomographyResult) -> dict:
@@ -164,6 +171,18 @@ class PairRunner:
         self.ws5 = workspace(self.s5_bytes, self.device)
         self.pinned = torch.zeros(C.sizeof(HomographyResult), dtype=torch.uint8, pin_memory=True)
         self.result = HomographyResult.from_address(self.pinned.data_ptr())
+        self.wsp: dict[tuple[int, float], tuple[torch.Tensor, int]] = {}
+
+    def pyramid_workspace(self, knobs: Knobs) -> tuple[torch.Tensor, int]:
+        """Workspace of the pyramid S2/S3 call for the largest image and K at
+        these levels (allocated on first use)."""
+        key = (knobs.levels, float(np.float32(knobs.scale_factor)))
+        if key not in self.wsp:
+            b = C.c_size_t()
+            check("pyramid_workspace_bytes", lib().stitch_pyramid_workspace_bytes(
+                self.max_w, self.max_h, ref(S2Config(20, self.max_k, 0.04)), ref(knobs.pyramid()), ref(b)))
+            self.wsp[key] = (workspace(b.value, self.device), b.value)
+        return self.wsp[key]
 
     def matches_view(self, capacity: int) -> Matches:
         return Matches(self.idx_a.data_ptr(), self.idx_b.data_ptr(), self.dist.data_ptr(), capacity,
@@ -180,15 +199,23 @@ class PairRunner:
         dims = ((wa, ha), (wb, hb))
         imgs = self.img if images is None else images
         c2 = knobs.s2()
-        for i in range(2):
-            iv = image_view(imgs[i], *dims[i])
-            check("s2_detect", L.stitch_s2_detect(ref(iv), ref(c2), ref(self.feat[i].keypoints(k)),
-                                                  ptr(self.ws2[i]), self.s2_bytes, s))
-        for i in range(2):
-            iv = image_view(imgs[i], *dims[i])
-            check("s3_describe", L.stitch_s3_describe(ref(iv), ref(self.feat[i].keypoints(k)),
-                                                      ref(self.feat[i].descriptors()), ptr(self.ws3),
-                                                      self.s3_bytes, s))
+        if knobs.levels > 1:
+            wsp, nbytes = self.pyramid_workspace(knobs)
+            for i in range(2):
+                iv = image_view(imgs[i], *dims[i])
+                check("pyramid_detect_describe", L.stitch_pyramid_detect_describe(
+                    ref(iv), ref(c2), ref(knobs.pyramid()), ref(self.feat[i].keypoints(k)),
+                    ref(self.feat[i].descriptors()), ptr(wsp), nbytes, s))
+        else:
+            for i in range(2):
+                iv = image_view(imgs[i], *dims[i])
+                check("s2_detect", L.stitch_s2_detect(ref(iv), ref(c2), ref(self.feat[i].keypoints(k)),
+                                                      ptr(self.ws2[i]), self.s2_bytes, s))
+            for i in range(2):
+                iv = image_view(imgs[i], *dims[i])
+                check("s3_describe", L.stitch_s3_describe(ref(iv), ref(self.feat[i].keypoints(k)),
+                                                          ref(self.feat[i].descriptors()), ptr(self.ws3),
+                                                          self.s3_bytes, s))
         ka, kb = self.feat[0].keypoints(k), self.feat[1].keypoints(k)
         da, db = self.feat[0].descriptors(), self.feat[1].descriptors()
         m = self.matches_view(k)

@@ -150,6 +150,34 @@ int stitch_s3_describe_marked(const stitch_image_view* image, const stitch_keypo
                               const stitch_descriptors* output, void* workspace, size_t workspace_bytes,
                               void* stream, void* after_blur);
 
+/* -------------------------------------------------------- scale pyramid */
+
+/* The pyramid-levels knob. No reference counterpart: the reference's S2/S3
+ * are single-level (docs/decisions/s2-s3-orb.md:84). levels 1 (or 0) is the
+ * reference's single-level path; levels 2..16 follow cv::ORB's layers with
+ * scale_factor in (1, 16] taken as a float like cv::ORB::create's. */
+typedef struct stitch_pyramid_config {
+    int levels;
+    float scale_factor;
+} stitch_pyramid_config;
+
+/* No reference counterpart. Workspace of stitch_pyramid_detect_describe. */
+int stitch_pyramid_workspace_bytes(int width, int height, const stitch_s2_config* config,
+                                   const stitch_pyramid_config* pyramid, size_t* bytes);
+/* No reference counterpart. S2 + S3 over the scale pyramid of one image:
+ * layer l (scale s_l = float(sf^l), size cvRound(W / s_l) x cvRound(H / s_l),
+ * built from layer l-1 by INTER_LINEAR_EXACT resizing) gets its share of the
+ * K keypoints (cv::ORB's geometric split, the total exactly K) and runs the
+ * single-level S2 and S3 (src/s2_s3/s2.cu, src/s2_s3/s3.cu); keypoints come
+ * out level by level in level-0 coordinates (x, y multiplied by s_l in
+ * float), with their descriptors in the same rows. Layers with a side of at
+ * most 62 pixels hold no keypoints. With levels 1 the results equal
+ * stitch_s2_detect followed by stitch_s3_describe. */
+int stitch_pyramid_detect_describe(const stitch_image_view* image, const stitch_s2_config* config,
+                                   const stitch_pyramid_config* pyramid, const stitch_keypoints* keypoints,
+                                   const stitch_descriptors* descriptors, void* workspace,
+                                   size_t workspace_bytes, void* stream);
+
 /* ------------------------------------------------------------------- S4 */
 
 /* src/s4/s4.hpp:25-26 (stitch::s4::s4_workspace_bytes). */
@@ -197,13 +225,16 @@ int stitch_s5_estimate(const stitch_keypoints* a, const stitch_keypoints* b, con
  * estimate (harness/pipeline_runner.cu:366-413); every pair carries its own
  * knobs and image sizes. scale_a/scale_b map original to working
  * coordinates as in src/common/geometry.hpp:119-131; orig_w == 0 means the
- * identity at the image's size. s5.previous_hypotheses must be 0. */
+ * identity at the image's size. s5.previous_hypotheses must be 0.
+ * pyramid.levels 0 or 1 is the single-level path; more levels run S2/S3 as
+ * stitch_pyramid_detect_describe does. */
 typedef struct stitch_pair_desc {
     stitch_image_view image_a, image_b; /* device GRAY8 */
     stitch_scale_info scale_a, scale_b;
     stitch_s2_config s2;
     stitch_s4_config s4;
     stitch_s5_config s5;
+    stitch_pyramid_config pyramid;
 } stitch_pair_desc;
 
 /* Opaque plan of a batch (host object; owns a pinned staging buffer for the
@@ -237,11 +268,11 @@ void stitch_batch_destroy(stitch_batch* plan);
 /* Per-kernel timing hook of the batched form (like the reference's S2/S3
  * event marks, src/s2_s3/s2_s3_marks.hpp:16-34): `events` holds
  * STITCH_BATCH_MARKS cudaEvent_t recorded, in order, after the table upload,
- * fast_nms, select+scatter, harris, sort, blur, describe, knn_popc,
- * knn_merge, accept, prepare, search and finish kernels (a skipped kernel
- * still records its mark). Applies to later enqueues and captures; NULL
- * turns the marks off. */
-#define STITCH_BATCH_MARKS 13
+ * the pyramid resize chain, fast_nms, select+scatter, harris, sort, blur,
+ * describe, knn_popc, knn_merge, accept, prepare, search and finish kernels
+ * (a skipped kernel still records its mark). Applies to later enqueues and
+ * captures; NULL turns the marks off. */
+#define STITCH_BATCH_MARKS 14
 int stitch_batch_set_marks(stitch_batch* plan, void* const* events, int count);
 
 #ifdef __cplusplus

@@ -1,10 +1,11 @@
-"""The whole per-pair chain on the CPU: S2/S3 (s2s3.py), S4 and S5
-(liboracle.so). Test infrastructure only."""
+"""The whole per-pair chain on the CPU: S2/S3 (s2s3.py, or pyramid.py when
+the knobs ask for more than one level), S4 and S5 (liboracle.so). Test
+infrastructure only."""
 from __future__ import annotations
 
 import numpy as np
 
-from . import c_oracle, s2s3
+from . import c_oracle, pyramid
 
 
 def match(desc_a: np.ndarray, desc_b: np.ndarray, ratio: float, cross_check: bool):
@@ -16,8 +17,9 @@ def match(desc_a: np.ndarray, desc_b: np.ndarray, ratio: float, cross_check: boo
 def run_pair(gray_a: np.ndarray, gray_b: np.ndarray, knobs, scale=1.0) -> dict:
     """knobs: any object with the fields of stages.Knobs."""
     k = knobs.max_keypoints
-    ka, da = s2s3.detect_and_describe(gray_a, knobs.fast_threshold, k, knobs.harris_k)
-    kb, db = s2s3.detect_and_describe(gray_b, knobs.fast_threshold, k, knobs.harris_k)
+    levels, factor = getattr(knobs, "levels", 1), getattr(knobs, "scale_factor", 1.2)
+    ka, da = pyramid.detect_and_describe(gray_a, knobs.fast_threshold, k, levels, factor, knobs.harris_k)
+    kb, db = pyramid.detect_and_describe(gray_b, knobs.fast_threshold, k, levels, factor, knobs.harris_k)
     ia, ib, dist = match(da, db, knobs.ratio, knobs.cross_check)
     nm = ia.shape[0]
     pts = np.stack([ka[ia, 0], ka[ia, 1], kb[ib, 0], kb[ib, 1]], 1).astype(np.float64) if nm else \

@@ -112,3 +112,28 @@ def test_host_validation_needs_no_device():
     kp = _abi.Keypoints(0, 0, 0, 10, 0)
     assert L.stitch_s2_detect(C.byref(iv), C.byref(S2Config(20, 10, 0.04)), C.byref(kp), None, 0, None) \
         == Status.INVALID_ARGUMENT
+
+
+def test_pyramid_workspace_and_validation():
+    """The pyramid knob's checks and workspace query are host-only."""
+    L = _abi.load()
+    b = C.c_size_t()
+    cfg = S2Config(20, 1000, 0.04)
+    for levels, factor in ((17, 1.2), (8, 1.0), (8, float("nan")), (8, 16.5), (-1, 1.2)):
+        assert L.stitch_pyramid_workspace_bytes(512, 512, C.byref(cfg), C.byref(_abi.PyramidConfig(levels, factor)),
+                                                C.byref(b)) == Status.INVALID_ARGUMENT, (levels, factor)
+    sizes = []
+    for levels in (1, 2, 8):
+        assert L.stitch_pyramid_workspace_bytes(512, 512, C.byref(cfg), C.byref(_abi.PyramidConfig(levels, 1.2)),
+                                                C.byref(b)) == 0
+        sizes.append(b.value)
+    assert sizes[0] < sizes[1] < sizes[2]
+    # levels 0 means one level; a factor is not needed then
+    assert L.stitch_pyramid_workspace_bytes(512, 512, C.byref(cfg), C.byref(_abi.PyramidConfig(0, 0.0)),
+                                            C.byref(b)) == 0 and b.value == sizes[0]
+    iv = _abi.ImageView(0, 64, 64, 64, 1)
+    kp = _abi.Keypoints(0, 0, 0, 10, 0)
+    ds = _abi.Descriptors(0, 32, 32, 0)
+    assert L.stitch_pyramid_detect_describe(C.byref(iv), C.byref(S2Config(20, 10, 0.04)),
+                                            C.byref(_abi.PyramidConfig(8, 1.2)), C.byref(kp), C.byref(ds), None, 0,
+                                            None) == Status.INVALID_ARGUMENT
