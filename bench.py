@@ -6,9 +6,10 @@ form vs the plain per-pair form, on one B200 per rank.
 Workload: 64 synthetic 512x512 pairs, the batched-registration
 configuration. Each pair is built from blobs, rectangles and band-limited
 noise, then warped by a random homography. Knobs: K = 2000 keypoints per
-image, FAST 20, ratio 0.8, R = 2000, tau = 3 px, 1 refinement, single-level
-ORB. One step registers all 64 pairs. The inputs fit in L2, so a 512 MB
-buffer is written between timed steps to flush it (outside the timed span).
+image, FAST 20, ratio 0.8, R = 2000, tau = 3 px, 1 refinement, ORB on an
+8-level pyramid at scale 1.2. One step registers all 64 pairs. The inputs
+fit in L2, so a 512 MB buffer is written between timed steps to flush it
+(outside the timed span).
 
 - value: the batched form. One captured CUDA graph runs every stage for
   all 64 pairs, with the images resident in HBM. It is device-timed with
@@ -46,13 +47,31 @@ N_PAIRS = 64
 SIZE = 512
 K = 2000
 R = 2000
-WORKLOAD = "batched registration, 64 pairs 512x512 u8, K=2000, FAST 20, ratio 0.8, R=2000, tau 3 px, 1 level"
+LEVELS = 8
+SCALE = 1.2
+WORKLOAD = ("batched registration, 64 pairs 512x512 u8, K=2000, FAST 20, 8-level pyramid at 1.2, ratio 0.8, "
+            "R=2000, tau 3 px")
 PEAKS = ROOT / "MEASURED_PEAKS.json"
 
 
 def knobs_for(i):
     from crossstage_stitch_b200 import stages, synth
-    return stages.Knobs(max_keypoints=K, hypotheses=R, seed=synth.BASE_SEED + i, threshold=3.0)
+    return stages.Knobs(max_keypoints=K, hypotheses=R, seed=synth.BASE_SEED + i, threshold=3.0, levels=LEVELS,
+                        scale_factor=SCALE)
+
+
+def layer_pixels(w, h):
+    """Pixels of each pyramid layer (sizes cvRound(W / s_l) in float32)."""
+    import numpy as np
+    sf = float(np.float32(SCALE))
+    out = []
+    for l in range(LEVELS):
+        inv = np.float32(1.0) / np.float32(sf ** l)
+        lw, lh = int(np.rint(np.float32(w) * inv)), int(np.rint(np.float32(h) * inv))
+        if lw <= 62 or lh <= 62:
+            break
+        out.append(lw * lh)
+    return out
 
 
 class Clocks:
@@ -131,10 +150,13 @@ def algorithmic_work(batch, n_pairs, counts):
     """Per-kernel algorithmic work of one step (bytes for pixel kernels,
     ops for matching and estimation), from the actual keypoint and match
     counts (counts: list of (n_a, n_b, n_matches))."""
-    px = 2 * n_pairs * SIZE * SIZE
+    layers = layer_pixels(SIZE, SIZE)
+    px = 2 * n_pairs * sum(layers)                      # every layer of both images
+    resized = 2 * n_pairs * sum(layers[l - 1] + layers[l] for l in range(1, len(layers)))
     knn_pairs = sum(a * b for a, b, _ in counts)
     resid = sum(R * m for _, _, m in counts)
     return {
+        "pyramid": ("hbm", 1.0 * resized, "GB/s"),       # previous layer read + layer write
         "fast_nms": ("hbm", 2.0 * px, "GB/s"),           # image read + maxima write
         "select_scatter": ("hbm", 2.0 * px, "GB/s"),     # maxima read twice
         "blur": ("hbm", 2.0 * px, "GB/s"),               # image read + blurred write
@@ -280,7 +302,7 @@ def main():
                 "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/i32/f64",
                 "data": "synthetic",
                 "config": {"workload": WORKLOAD, "form": "batched (CUDA graph, 1 launch per stage kernel)",
-                           "pairs_per_step": N_PAIRS, "pyramid_levels": 1,
+                           "pairs_per_step": N_PAIRS, "pyramid_levels": LEVELS, "scale_factor": SCALE,
                            "l2": "512 MB flush between steps (inputs 33.5 MB < L2)",
                            "parallelism": f"replicas x{world}"},
                 "p50_pair_ms": t_batch / args.steps, "p99_pair_ms": t_batch / args.steps,
