@@ -321,10 +321,12 @@ Status Plan::stage_tables(void* ws) {
             const int db[s2s3::kDetectKinds] = {
                 active ? o.det[s].tiles : 0, active ? o.det[s].chunks : 0,
                 active ? ceil_div(o.det[s].candidates, s2s3::kHarrisThreads) : 0, active ? 1 : 0};
-            const int sb[s2s3::kDescribeKinds] = {k > 0 ? o.des[s].tiles : 0,
-                                                  k > 0 ? ceil_div(k, s2s3::kDescWarps) : 0};
-            add_job(idx, d, s2s3::make_describe_job(view(im), kps[s], desc[s], at<void>(ws, o.s3ws[s]), o.des[s]),
-                    db, sb);
+            // the FAST kernel writes the blur; no blur launch
+            const int sb[s2s3::kDescribeKinds] = {0, k > 0 ? ceil_div(k, s2s3::kDescWarps) : 0};
+            const DescribeJob e =
+                s2s3::make_describe_job(view(im), kps[s], desc[s], at<void>(ws, o.s3ws[s]), o.des[s]);
+            d.blurred = e.blurred;
+            add_job(idx, d, e, db, sb);
         }
         // S4 (forward, then reverse when the mutual check is on)
         auto* fwd = at<s4k::Top2>(ws, o.s4ws + o.match.forward);

@@ -1,8 +1,8 @@
 // Scale-pyramid S2/S3 of one image: layers 1..L-1 resized in a chain, then
 // S2 and S3 of every layer in the same launches (the layers' jobs travel as
-// kernel parameters), each layer's keypoints and descriptors written by the
-// describe kernel straight into the image's concatenated outputs in level-0
-// coordinates.
+// kernel parameters; the FAST kernel also writes each layer's blur), each
+// layer's keypoints and descriptors written by the describe kernel straight
+// into the image's concatenated outputs in level-0 coordinates.
 //
 // The reference has no pyramid (docs/decisions/s2-s3-orb.md:84): its S2/S3
 // are single-level (src/s2_s3/s2.cu, src/s2_s3/s3.cu). The layer semantics
@@ -123,6 +123,7 @@ void make_pyramid_jobs(const ImageView& im, const s2::Config& c, const Keypoints
         s.level = i;
         s.scale = p.scale[i];
         jobs->describe[i] = s;
+        jobs->detect[i].blurred = s.blurred;  // the FAST kernel writes the layer's blur
     }
 }
 
@@ -137,7 +138,7 @@ void pyramid_detect_blocks(const PyramidLayout& l, int i, int (&blocks)[kDetectK
 
 void pyramid_describe_blocks(const PyramidLayout& l, int i, int (&blocks)[kDescribeKinds]) {
     const bool active = i < l.plan.levels && l.plan.budget[i] > 0;
-    blocks[kBlurKind] = active ? l.des[i].tiles : 0;
+    blocks[kBlurKind] = 0;  // fused into the FAST kernel
     blocks[kDescKind] = active ? ceil_div(l.plan.budget[i], kDescWarps) : 0;
 }
 
@@ -225,10 +226,9 @@ Status pyramid_detect_describe(const ImageView& image, const s2::Config& c, int 
             ++launches;
         }
     }
-    if (des.first[kBlurKind][n]) {
-        blur_kernel<DesSrc><<<des.first[kBlurKind][n], 256, 0, stream>>>(des);
+    if (des.first[kDescKind][n]) {
         describe_kernel<DesSrc><<<des.first[kDescKind][n], kDescWarps * 32, 0, stream>>>(des);
-        launches += 2;
+        ++launches;
     }
     note_launches(launches);
     return launch_status();

@@ -46,6 +46,9 @@ struct DetectJob {
     float* y;
     float* response;  // may be null
     int* count;
+    // optional: the S3 blur of the image (dense, width x height), written by
+    // the FAST kernel when set
+    std::uint8_t* blurred;
     // launch bookkeeping
     int tiles_x, tiles, chunks, candidates;
 };
@@ -150,111 +153,157 @@ constexpr int kMaxLevels = 16;
 
 // ------------------------------------------------------------- FAST + NMS
 
-// FAST-9 score of the pixel at p (row stride `stride`): for each of the 16
-// circular 9-pixel arcs take the smallest centre-minus-ring difference (arc
-// darker) and the smallest ring-minus-centre difference (arc brighter); the
-// score is the largest of these minus one when it exceeds the threshold.
-// Pixels that cannot reach the threshold leave after four compass loads.
-__device__ __forceinline__ int fast_score(const std::uint8_t* p, int stride, int thr) {
+// float32 taps of a 7-tap, sigma-2 Gaussian (exp in float64, normalised,
+// rounded to float32); equal to cv::getGaussianKernel(7, 2, CV_32F).
+__device__ __forceinline__ float blur_tap(int i) {
+    switch (i) {
+        case 0: case 6: return 0x1.1f5f62p-4f;
+        case 1: case 5: return 0x1.0c70fcp-3f;
+        case 2: case 4: return 0x1.869472p-3f;
+        default: return 0x1.ba95c0p-3f;
+    }
+}
+
+// Border reflection without repeating the edge pixel (BORDER_REFLECT_101).
+__device__ __forceinline__ int reflect101(int i, int n) {
+    if (n == 1) return 0;
+    while (i < 0 || i >= n) i = i < 0 ? -i : 2 * n - 2 - i;
+    return i;
+}
+
+// Necessary condition for a FAST-9 corner: a 9-pixel arc always holds two of
+// the four compass pixels, so two of them must be beyond the threshold on
+// the same side.
+__device__ __forceinline__ bool fast_compass(const std::uint8_t* p, int stride, int thr) {
     const int v = p[0];
     const int s0 = p[3 * stride], s4 = p[3], s8 = p[-3 * stride], s12 = p[-3];
-    // A qualifying 9-arc always contains two of the four compass pixels.
     const int hi = v + thr, lo = v - thr;
     const int n_bright = (s0 > hi) + (s4 > hi) + (s8 > hi) + (s12 > hi);
     const int n_dark = (s0 < lo) + (s4 < lo) + (s8 < lo) + (s12 < lo);
-    if (n_bright < 2 && n_dark < 2) return 0;
-    int d[16];
-    d[0] = v - s0;
-    d[1] = v - p[3 * stride + 1];
-    d[2] = v - p[2 * stride + 2];
-    d[3] = v - p[1 * stride + 3];
-    d[4] = v - s4;
-    d[5] = v - p[-1 * stride + 3];
-    d[6] = v - p[-2 * stride + 2];
-    d[7] = v - p[-3 * stride + 1];
-    d[8] = v - s8;
-    d[9] = v - p[-3 * stride - 1];
-    d[10] = v - p[-2 * stride - 2];
-    d[11] = v - p[-1 * stride - 3];
-    d[12] = v - s12;
-    d[13] = v - p[1 * stride - 3];
-    d[14] = v - p[2 * stride - 2];
-    d[15] = v - p[3 * stride - 1];
-    // Exact corner test: the score exceeds the threshold iff some 9-pixel arc
-    // is entirely darker (d > thr) or entirely brighter (-d > thr). Find a
-    // circular run of 9 set bits in either 16-bit mask.
-    unsigned dark_bits = 0, bright_bits = 0;
+    return n_bright >= 2 || n_dark >= 2;
+}
+
+// FAST-9 score of the pixel at p (row stride `stride`), 0 when it is not a
+// corner. With d_k = centre - ring_k over the 16-pixel circle, a 9-pixel arc
+// scores min(d) when darker and min(-d) when brighter; the raw score is the
+// largest over the 16 arcs of both kinds, the pixel is a corner iff the raw
+// score exceeds the threshold, and it then scores raw - 1. Both kinds run
+// at once as unsigned 16-bit lanes q_k = (d_k + 256) | (256 - d_k) << 16
+// (all in [1, 511]); 9-wide arc minima come from 2-, 4- and 8-wide ones.
+// (CUDA 12.9 ptxas at -O1 and above miscompiles the signed
+// max(min(arc), -max(arc)) form of this score on sm_100; this unsigned
+// form is exact at every optimisation level.)
+__device__ __forceinline__ int fast_score(const std::uint8_t* p, int stride, int thr) {
+    const int v = p[0];
+    const int ring[16] = {p[3 * stride],      p[3 * stride + 1],  p[2 * stride + 2],  p[stride + 3],
+                          p[3],               p[-stride + 3],     p[-2 * stride + 2], p[-3 * stride + 1],
+                          p[-3 * stride],     p[-3 * stride - 1], p[-2 * stride - 2], p[-stride - 3],
+                          p[-3],              p[stride - 3],      p[2 * stride - 2],  p[3 * stride - 1]};
+    unsigned q[16], m2[16], m4[16], m8[16];
 #pragma unroll
     for (int k = 0; k < 16; ++k) {
-        dark_bits |= static_cast<unsigned>(d[k] > thr) << k;
-        bright_bits |= static_cast<unsigned>(d[k] < -thr) << k;
+        const int d = v - ring[k];
+        q[k] = static_cast<unsigned>(d + 256) | (static_cast<unsigned>(256 - d) << 16);
     }
-    auto run9 = [](unsigned m) {
-        const unsigned w = m | (m << 16);
-        unsigned r = w & (w >> 1);
-        r &= r >> 2;
-        r &= r >> 4;
-        r &= w >> 8;
-        return (r & 0xffffu) != 0u;
-    };
-    if (!run9(dark_bits) && !run9(bright_bits)) return 0;
-    // Offset to unsigned so both arc kinds are minima of non-negative values:
-    // dark arc = min over the arc of (d + 256) - 256, bright arc = min over
-    // the arc of (256 - d) - 256. (CUDA 12.9 ptxas at -O1 and above
-    // miscompiles the signed max(min(arc), -max(arc)) form of this score on
-    // sm_100; this unsigned form is exact at every optimisation level.)
-    unsigned dark[16], bright[16];
 #pragma unroll
-    for (int k = 0; k < 16; ++k) {
-        dark[k] = static_cast<unsigned>(d[k] + 256);
-        bright[k] = 512u - dark[k];
-    }
+    for (int k = 0; k < 16; ++k) m2[k] = __vminu2(q[k], q[(k + 1) & 15]);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) m4[k] = __vminu2(m2[k], m2[(k + 2) & 15]);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) m8[k] = __vminu2(m4[k], m4[(k + 4) & 15]);
     unsigned best = 0;
 #pragma unroll
-    for (int k = 0; k < 16; ++k) {
-        unsigned a = 0xffffffffu, b = 0xffffffffu;
-#pragma unroll
-        for (int t = 0; t < 9; ++t) {
-            a = min(a, dark[(k + t) & 15]);
-            b = min(b, bright[(k + t) & 15]);
-        }
-        best = max(best, max(a, b));
-    }
-    const int score = static_cast<int>(best) - 256;
+    for (int k = 0; k < 16; ++k) best = __vmaxu2(best, __vminu2(m8[k], q[(k + 8) & 15]));
+    const unsigned lo = best & 0xffffu, hi = best >> 16;
+    const int score = static_cast<int>(lo > hi ? lo : hi) - 256;
     return score > thr ? score - 1 : 0;
 }
 
-// One block = one 64x32 output tile: stage the tile with a 4-pixel halo in
-// shared memory, score the tile plus a 1-pixel ring, keep strict 3x3 maxima
-// inside the 31-pixel edge margin, write the maxima map and add the
-// survivors' scores to the image histogram.
+constexpr int kFastPos = kFastScH * kFastScW;  // positions scored per tile (tile + 1-pixel ring)
+
+// One block = one 64x32 output tile:
+//   1. stage the tile with a 4-pixel halo in shared memory, reflected at the
+//      image border (FAST never reads outside the image, the blur does);
+//   2. run the compass test on the tile plus a 1-pixel ring and list the
+//      survivors, so that full scores are computed on full warps;
+//   3. score the survivors; keep strict 3x3 maxima inside the 31-pixel edge
+//      margin, write the maxima map and add their scores to the histogram.
+// With j.blurred set the block also writes the tile of the S3 7x7 blur
+// (rows pass, then columns pass; per output the taps summed first to last
+// with each product and sum rounded on its own, then rounded half-to-even
+// and clamped), bit for bit the blur_kernel result.
 template <class Src>
 __global__ __launch_bounds__(256) void fast_nms_kernel(const __grid_constant__ Src src) {
     __shared__ std::uint8_t in[kFastInH][kFastInW];
     __shared__ std::uint8_t sc[kFastScH][kFastScW];
+    __shared__ std::uint16_t cand[kFastPos];
     __shared__ std::uint32_t hist[256];
+    __shared__ float rows[kFastTileH + 6][kFastTileW];
+    __shared__ int n_cand;
     DetectJob j;
     int local;
     if (!src.find(blockIdx.x, kFastKind, &j, &local)) return;
-    const int tid = threadIdx.x;
+    const int tid = threadIdx.x, lane = tid & 31;
     const int W = j.width, H = j.height;
     const int y0 = (local / j.tiles_x) * kFastTileH;
     const int x0 = (local % j.tiles_x) * kFastTileW;
     hist[tid] = 0;
+    if (tid == 0) n_cand = 0;
+    const bool inside = x0 >= 4 && y0 >= 4 && x0 + kFastTileW + 4 <= W && y0 + kFastTileH + 4 <= H;
     for (int i = tid; i < kFastInH * kFastInW; i += 256) {
         const int r = i / kFastInW, c = i - r * kFastInW;
-        const int gy = y0 - 4 + r, gx = x0 - 4 + c;
-        in[r][c] = (gx >= 0 && gx < W && gy >= 0 && gy < H)
-                       ? j.image[static_cast<std::size_t>(gy) * j.pitch + gx] : 0;
+        int gy = y0 - 4 + r, gx = x0 - 4 + c;
+        if (!inside) {
+            gy = reflect101(gy, H);
+            gx = reflect101(gx, W);
+        }
+        in[r][c] = j.image[static_cast<std::size_t>(gy) * j.pitch + gx];
     }
     __syncthreads();
-    for (int i = tid; i < kFastScH * kFastScW; i += 256) {
-        const int r = i / kFastScW, c = i - r * kFastScW;
-        const int gy = y0 - 1 + r, gx = x0 - 1 + c;
-        int s = 0;
-        if (gx >= 3 && gx < W - 3 && gy >= 3 && gy < H - 3)
-            s = fast_score(&in[r + 3][c + 3], kFastInW, j.threshold);
-        sc[r][c] = static_cast<std::uint8_t>(s);
+    for (int i0 = 0; i0 < kFastPos; i0 += 256) {  // same trip count on every thread
+        const int i = i0 + tid;
+        bool pass = false;
+        if (i < kFastPos) {
+            const int r = i / kFastScW, c = i - r * kFastScW;
+            const int gy = y0 - 1 + r, gx = x0 - 1 + c;
+            sc[r][c] = 0;
+            pass = gx >= 3 && gx < W - 3 && gy >= 3 && gy < H - 3 &&
+                   fast_compass(&in[r + 3][c + 3], kFastInW, j.threshold);
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, pass);
+        int base = 0;
+        if (lane == 0 && m) base = atomicAdd(&n_cand, __popc(m));
+        base = __shfl_sync(0xffffffffu, base, 0);
+        if (pass) cand[base + __popc(m & ((1u << lane) - 1u))] = static_cast<std::uint16_t>(i);
+    }
+    if (j.blurred) {  // blur rows pass: image rows y0-3 .. y0+34, columns x0 .. x0+63
+        for (int i = tid; i < (kFastTileH + 6) * kFastTileW; i += 256) {
+            const int r = i / kFastTileW, c = i - r * kFastTileW;
+            float acc = 0.0f;
+#pragma unroll
+            for (int t = 0; t < 7; ++t)
+                acc = __fadd_rn(acc, __fmul_rn(blur_tap(t), static_cast<float>(in[r + 1][c + 1 + t])));
+            rows[r][c] = acc;
+        }
+    }
+    __syncthreads();
+    const int nc = n_cand;
+    for (int i = tid; i < nc; i += 256) {
+        const int pos = cand[i];
+        const int r = pos / kFastScW, c = pos - r * kFastScW;
+        sc[r][c] = static_cast<std::uint8_t>(fast_score(&in[r + 3][c + 3], kFastInW, j.threshold));
+    }
+    if (j.blurred) {  // blur columns pass
+        for (int i = tid; i < kFastTileH * kFastTileW; i += 256) {
+            const int r = i / kFastTileW, c = i - r * kFastTileW;
+            const int gy = y0 + r, gx = x0 + c;
+            if (gx >= W || gy >= H) continue;
+            float acc = 0.0f;
+#pragma unroll
+            for (int t = 0; t < 7; ++t) acc = __fadd_rn(acc, __fmul_rn(blur_tap(t), rows[r + t][c]));
+            j.blurred[static_cast<std::size_t>(gy) * W + gx] =
+                static_cast<std::uint8_t>(__float2int_rn(fminf(fmaxf(acc, 0.0f), 255.0f)));
+        }
     }
     __syncthreads();
     for (int i = tid; i < kFastTileW * kFastTileH; i += 256) {
@@ -618,24 +667,6 @@ __global__ __launch_bounds__(256) void resize_kernel(const __grid_constant__ Src
 }
 
 // ------------------------------------------------------------- S3 blur
-
-// float32 taps of a 7-tap, sigma-2 Gaussian (exp in float64, normalised,
-// rounded to float32); equal to cv::getGaussianKernel(7, 2, CV_32F).
-__device__ __forceinline__ float blur_tap(int i) {
-    switch (i) {
-        case 0: case 6: return 0x1.1f5f62p-4f;
-        case 1: case 5: return 0x1.0c70fcp-3f;
-        case 2: case 4: return 0x1.869472p-3f;
-        default: return 0x1.ba95c0p-3f;
-    }
-}
-
-// Border reflection without repeating the edge pixel (BORDER_REFLECT_101).
-__device__ __forceinline__ int reflect101(int i, int n) {
-    if (n == 1) return 0;
-    while (i < 0 || i >= n) i = i < 0 ? -i : 2 * n - 2 - i;
-    return i;
-}
 
 // One block = one 64x32 tile: rows pass into a float tile with a 3-row halo,
 // then the columns pass; per output the taps are summed first to last with
