@@ -54,6 +54,9 @@ LevelPlan level_plan(int w, int h, int k, int levels, float sf) {
     return p;
 }
 
+// Rows of the layer images start on 16-byte boundaries.
+int layer_pitch(int width) { return (width + 15) / 16 * 16; }
+
 bool pyramid_layout(int w, int h, int k, int levels, float sf, PyramidLayout* out) {
     if (!out || !valid_image_shape(w, h) || k < 0 || k > INT_MAX / s2::kCandidateFactor ||
         !valid_pyramid(levels, sf))
@@ -68,7 +71,7 @@ bool pyramid_layout(int w, int h, int k, int levels, float sf, PyramidLayout* ou
     for (int i = 0; i < n; ++i) {
         const int lw = l.plan.width[i], lh = l.plan.height[i];
         const std::size_t kk = static_cast<std::size_t>(l.plan.budget[i] > 0 ? l.plan.budget[i] : 1);
-        l.image[i] = i ? lay.take(static_cast<std::size_t>(lw) * static_cast<std::size_t>(lh), 1) : 0;
+        l.image[i] = i ? lay.take(static_cast<std::size_t>(layer_pitch(lw)) * static_cast<std::size_t>(lh), 1) : 0;
         l.kx[i] = lay.take(kk, sizeof(float));
         l.ky[i] = lay.take(kk, sizeof(float));
         l.kr[i] = lay.take(kk, sizeof(float));
@@ -93,15 +96,16 @@ void make_pyramid_jobs(const ImageView& im, const s2::Config& c, const Keypoints
             layer.data = at_offset<std::uint8_t>(ws, l.image[i]);
             layer.width = p.width[i];
             layer.height = p.height[i];
-            layer.pitch_bytes = p.width[i];
+            layer.pitch_bytes = layer_pitch(p.width[i]);
             ResizeJob r{};
             r.src = i == 1 ? im.data : at_offset<std::uint8_t>(ws, l.image[i - 1]);
             r.src_width = p.width[i - 1];
             r.src_height = p.height[i - 1];
-            r.src_pitch = i == 1 ? im.pitch_bytes : p.width[i - 1];
+            r.src_pitch = i == 1 ? im.pitch_bytes : layer_pitch(p.width[i - 1]);
             r.dst = const_cast<std::uint8_t*>(layer.data);
             r.width = p.width[i];
             r.height = p.height[i];
+            r.pitch = layer.pitch_bytes;
             r.tiles_x = ceil_div(p.width[i], kResizeTileW);
             r.tiles = l.resize_tiles[i];
             jobs->resize[i] = r;

@@ -85,7 +85,7 @@ struct ResizeJob {
     const std::uint8_t* src;
     int src_width, src_height, src_pitch;
     std::uint8_t* dst;
-    int width, height;
+    int width, height, pitch;
     int tiles_x, tiles;
 };
 
@@ -613,12 +613,15 @@ __global__ __launch_bounds__(kHarrisThreads) void rank_topk_kernel(const __grid_
 // ------------------------------------------------------ pyramid layers
 
 // Source index and 8-bit weight of the right neighbour for destination
-// index v of a src -> dst linear resize: f = (v + 0.5) * (1 / (dst / src)) -
-// 0.5 in double, weight rint((f - floor f) * 256). Indices left of the
-// source (every index when src == 1) read pixel 0 with weight 0, indices past
-// the last interval read pixel src - 1 with weight 0.
-__device__ __forceinline__ int2 linear_exact_tap(int v, int src, int dst) {
-    const double scale = 1.0 / (static_cast<double>(dst) / static_cast<double>(src));
+// index v of a src -> dst linear resize: f = (v + 0.5) * scale - 0.5 in
+// double with scale = 1 / (dst / src), weight rint((f - floor f) * 256).
+// Indices left of the source (every index when src == 1) read pixel 0 with
+// weight 0, indices past the last interval read pixel src - 1 with weight 0.
+__device__ __forceinline__ double linear_exact_scale(int src, int dst) {
+    return 1.0 / (static_cast<double>(dst) / static_cast<double>(src));
+}
+
+__device__ __forceinline__ int2 linear_exact_tap(int v, int src, double scale) {
     const double f = scale * (static_cast<double>(v) + 0.5) - 0.5;
     const double fl = floor(f);
     if (src == 1 || fl < 0.0) return make_int2(0, 0);
@@ -636,15 +639,19 @@ template <class Src>
 __global__ __launch_bounds__(256) void resize_kernel(const __grid_constant__ Src src, int kind) {
     __shared__ int2 xtap[kResizeTileW];
     __shared__ int2 ytap[kResizeTileH];
+    __shared__ double scale[2];
     ResizeJob j;
     int local;
     if (!src.find(blockIdx.x, kind, &j, &local)) return;
     const int y0 = (local / j.tiles_x) * kResizeTileH;
     const int x0 = (local % j.tiles_x) * kResizeTileW;
     const int t = threadIdx.x;
-    if (t < kResizeTileW) xtap[t] = linear_exact_tap(min(x0 + t, j.width - 1), j.src_width, j.width);
+    if (t == 0) scale[0] = linear_exact_scale(j.src_width, j.width);
+    if (t == 32) scale[1] = linear_exact_scale(j.src_height, j.height);
+    __syncthreads();
+    if (t < kResizeTileW) xtap[t] = linear_exact_tap(min(x0 + t, j.width - 1), j.src_width, scale[0]);
     else if (t < kResizeTileW + kResizeTileH)
-        ytap[t - kResizeTileW] = linear_exact_tap(min(y0 + t - kResizeTileW, j.height - 1), j.src_height, j.height);
+        ytap[t - kResizeTileW] = linear_exact_tap(min(y0 + t - kResizeTileW, j.height - 1), j.src_height, scale[1]);
     __syncthreads();
     const int c = t & (kResizeTileW - 1);
     const int x = x0 + c;
@@ -662,7 +669,7 @@ __global__ __launch_bounds__(256) void resize_kernel(const __grid_constant__ Src
         const int ha = ra[xa] * wx0 + ra[xb] * wx1;
         const int hb = rb[xa] * wx0 + rb[xb] * wx1;
         const int v = ha * (256 - ty.y) + hb * ty.y;
-        j.dst[static_cast<std::size_t>(y) * j.width + x] = static_cast<std::uint8_t>((v + (1 << 15)) >> 16);
+        j.dst[static_cast<std::size_t>(y) * j.pitch + x] = static_cast<std::uint8_t>((v + (1 << 15)) >> 16);
     }
 }
 

@@ -576,8 +576,12 @@ struct SearchJob {
 // Block b of a pair walks warp rounds b*8 + w, b*8 + w + 8*blocks, ...; a
 // round is HPW consecutive hypotheses. The block's best model goes to
 // block_best[b].
+// Three blocks per SM: the register-resident 4-point fit then spills to
+// L1-backed local memory, but it is a small share of the work, and the
+// scoring loop gains the occupancy (1 block: 0.62 ms, 3 blocks: 0.43 ms for
+// 64 pairs x 2000 hypotheses x ~530 matches).
 template <class Src>
-__global__ __launch_bounds__(kSearchThreads, 1) void search_kernel(const __grid_constant__ Src src) {
+__global__ __launch_bounds__(kSearchThreads, 3) void search_kernel(const __grid_constant__ Src src) {
     extern __shared__ float4 pts[];
     __shared__ Model warp_best[kSearchWarps];
     SearchJob sj;
@@ -689,6 +693,7 @@ __device__ double ordered_sum(int nm, double* buf /*kFinishChunk shared*/, F ter
         __syncthreads();
         if (threadIdx.x == 0) {
             double t = total;
+#pragma unroll 8
             for (int i = 0; i < n; ++i) t += buf[i];
             total = t;
         }
@@ -703,7 +708,7 @@ __device__ double ordered_sum(int nm, double* buf /*kFinishChunk shared*/, F ter
 // scale and normal-matrix sums each run in index order as in the reference;
 // the 72 matrix entries are accumulated by 72 threads side by side.
 __device__ inline bool block_fit(const PairIO& j, int nm, const std::uint8_t* keep, double* out, double (*dv)[10],
-                          Pt* cpts /*kFinishChunk shared*/, std::uint8_t* ckeep) {
+                          std::uint8_t* ckeep /*kFinishChunk shared*/) {
     __shared__ double sums[6];
     __shared__ int kept;
     __shared__ double m[8][9];
@@ -712,23 +717,33 @@ __device__ inline bool block_fit(const PairIO& j, int nm, const std::uint8_t* ke
     if (t < 6) sums[t] = 0.0;
     if (t == 6) kept = 0;
     if (t < 72) m[t / 9][t % 9] = 0.0;
+    // Each sum below starts at +0.0 and runs in index order on one thread
+    // over terms the block computed beforehand; a dropped point contributes
+    // +0.0, which leaves such a sum bit-identical to skipping the point
+    // (round-to-nearest never turns a sum that starts at +0.0 into -0.0).
     // pass 1: centroids
+    int mine = 0;
     for (int base = 0; base < nm; base += kFinishChunk) {
         const int n = min(kFinishChunk, nm - base);
         __syncthreads();
-        for (int i = t; i < n; i += blockDim.x) { cpts[i] = gather(j, base + i); ckeep[i] = keep[base + i]; }
+        for (int i = t; i < n; i += blockDim.x) {
+            const Pt p = gather(j, base + i);
+            const bool k = keep[base + i] != 0;
+            mine += k ? 1 : 0;
+            dv[i][0] = k ? p.ax : 0.0;
+            dv[i][1] = k ? p.ay : 0.0;
+            dv[i][2] = k ? p.bx : 0.0;
+            dv[i][3] = k ? p.by : 0.0;
+        }
         __syncthreads();
         if (t < 4) {
             double a = sums[t];
-            for (int i = 0; i < n; ++i)
-                if (ckeep[i]) a += t == 0 ? cpts[i].ax : t == 1 ? cpts[i].ay : t == 2 ? cpts[i].bx : cpts[i].by;
+#pragma unroll 8
+            for (int i = 0; i < n; ++i) a += dv[i][t];
             sums[t] = a;
-        } else if (t == 4) {
-            int c = kept;
-            for (int i = 0; i < n; ++i) c += ckeep[i] ? 1 : 0;
-            kept = c;
         }
     }
+    if (mine) atomicAdd(&kept, mine);
     __syncthreads();
     const int count = kept;
     if (count < 4) return false;
@@ -737,18 +752,19 @@ __device__ inline bool block_fit(const PairIO& j, int nm, const std::uint8_t* ke
     for (int base = 0; base < nm; base += kFinishChunk) {
         const int n = min(kFinishChunk, nm - base);
         __syncthreads();
-        for (int i = t; i < n; i += blockDim.x) { cpts[i] = gather(j, base + i); ckeep[i] = keep[base + i]; }
+        for (int i = t; i < n; i += blockDim.x) {
+            const Pt p = gather(j, base + i);
+            const bool k = keep[base + i] != 0;
+            dv[i][0] = k ? (p.ax - cax) * (p.ax - cax) + (p.ay - cay) * (p.ay - cay) : 0.0;
+            dv[i][1] = k ? (p.bx - cbx) * (p.bx - cbx) + (p.by - cby) * (p.by - cby) : 0.0;
+        }
         __syncthreads();
-        if (t == 0) {
-            double va = sums[4];
-            for (int i = 0; i < n; ++i)
-                if (ckeep[i]) va += (cpts[i].ax - cax) * (cpts[i].ax - cax) + (cpts[i].ay - cay) * (cpts[i].ay - cay);
-            sums[4] = va;
-        } else if (t == 32) {
-            double vb = sums[5];
-            for (int i = 0; i < n; ++i)
-                if (ckeep[i]) vb += (cpts[i].bx - cbx) * (cpts[i].bx - cbx) + (cpts[i].by - cby) * (cpts[i].by - cby);
-            sums[5] = vb;
+        if (t == 0 || t == 32) {
+            const int col = t ? 1 : 0;
+            double a = sums[4 + col];
+#pragma unroll 8
+            for (int i = 0; i < n; ++i) a += dv[i][col];
+            sums[4 + col] = a;
         }
     }
     __syncthreads();
@@ -781,10 +797,11 @@ __device__ inline bool block_fit(const PairIO& j, int nm, const std::uint8_t* ke
         __syncthreads();
         if (t < 72) {
             double acc = m[r][c];
+#pragma unroll 4
             for (int i = 0; i < n; ++i) {
-                if (!ckeep[i]) continue;
                 const double* d = dv[i];
-                acc += d[i0r] * d[i0c] + d[i1r] * d[i1c];
+                const double term = d[i0r] * d[i0c] + d[i1r] * d[i1c];
+                acc += ckeep[i] ? term : 0.0;
             }
             m[r][c] = acc;
         }
@@ -804,7 +821,6 @@ template <class Src>
 __global__ __launch_bounds__(kFinishThreads, 1) void finish_kernel(const __grid_constant__ Src src) {
     __shared__ int red_src[kFinishThreads];
     __shared__ double buf[kFinishChunk];
-    __shared__ Pt cpts[kFinishChunk];
     __shared__ std::uint8_t ckeep[kFinishChunk];
     __shared__ double dv[kFinishChunk][10];
     __shared__ Model model, cand;
@@ -867,7 +883,7 @@ __global__ __launch_bounds__(kFinishThreads, 1) void finish_kernel(const __grid_
             for (int i = t; i < nm; i += kFinishThreads) j.mask[i] = residual2(h, gather(j, i)) <= thr2;
             __syncthreads();
             double ch[9];
-            const bool fitted = block_fit(j, nm, j.mask, ch, dv, cpts, ckeep);
+            const bool fitted = block_fit(j, nm, j.mask, ch, dv, ckeep);
             if (t == 0) {
                 cand_ok = fitted && valid_domain(ch, bw, bh);
                 for (int e = 0; e < 9; ++e) cand.h[e] = ch[e];
