@@ -146,6 +146,162 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+N_MIXED = 256
+SERVED_RATES = (500, 1000, 2000)
+SERVED_SECONDS = 3.0
+SERVED_POOL = 48
+
+
+def mixed_pair_job(i):
+    """One pair of the mixed-resolution workload (runs in a spawned worker)."""
+    sys.path.insert(0, str(ROOT))
+    from crossstage_stitch_b200 import synth
+    p, kn = synth.mixed_pair(i)
+    return p.gray_a, p.gray_b, kn
+
+
+def make_mixed(n: int, workers: int):
+    import multiprocessing as mp
+    with mp.get_context("spawn").Pool(workers) as pool:
+        return pool.map(mixed_pair_job, range(n), chunksize=1)
+
+
+def mixed_knobs(kn, seed):
+    from crossstage_stitch_b200 import stages
+    return stages.Knobs(max_keypoints=kn["max_keypoints"], fast_threshold=kn["fast_threshold"],
+                        hypotheses=kn["hypotheses"], seed=seed, levels=LEVELS, scale_factor=SCALE)
+
+
+def run_mixed(mixed, steps, warmup, dev, flush):
+    """Mixed-resolution workload: the batched graph over all pairs vs the plain
+    per-pair stages, same pairs and knobs, images resident on the device."""
+    import torch
+    from crossstage_stitch_b200 import batch, stages, synth
+    knobs = [mixed_knobs(kn, synth.BASE_SEED + 100000 + i) for i, (_, _, kn) in enumerate(mixed)]
+    imgs = [(torch.from_numpy(a).to(dev), torch.from_numpy(b).to(dev)) for a, b, _ in mixed]
+    b = batch.Batch([batch.pair_desc(ia, ib, k) for (ia, ib), k in zip(imgs, knobs)], device=dev)
+    b.capture()
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    times = []
+    for it in range(warmup + steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        e0.record(stream)
+        b.launch(stream)
+        e1.record(stream)
+        e1.synchronize()
+        if it >= warmup:
+            times.append(e0.elapsed_time(e1))
+    t_batch = sum(times) / len(times)
+    W = max(max(a.shape[1], bb.shape[1]) for a, bb, _ in mixed)
+    H = max(max(a.shape[0], bb.shape[0]) for a, bb, _ in mixed)
+    runner = stages.PairRunner(W, H, max(k.max_keypoints for k in knobs), max_r=max(k.hypotheses for k in knobs),
+                               device=dev)
+    lat = []
+
+    def plain(record):
+        for (ia, ib), k in zip(imgs, knobs):
+            f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            f0.record(stream)
+            runner.enqueue(ia.shape[1], ia.shape[0], ib.shape[1], ib.shape[0], k, stream, images=(ia, ib))
+            f1.record(stream)
+            stream.synchronize()
+            if record:
+                lat.append(f0.elapsed_time(f1))
+
+    plain(False)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    plain(True)
+    e1.record(stream)
+    e1.synchronize()
+    t_plain = e0.elapsed_time(e1)
+    lat.sort()
+    n = len(mixed)
+    mpx = sum(a.size + bb.size for a, bb, _ in mixed) / n / 1e6
+    del b
+    return {"workload": f"{n} mixed pairs from {{640x480, 1280x720, 1920x1080, 3840x2160}}, K in {{500, 2000, 8000}}, "
+                        f"FAST in {{10, 20, 40}}, R in {{500, 2000, 8000}}, 8 levels at 1.2, repeated-texture outliers",
+            "pairs": n, "mean_mpx_per_pair": round(mpx, 3),
+            "batched": {"value": n / (t_batch / 1e3), "unit": "pairs/s", "ms_per_step": t_batch},
+            "plain_per_pair": {"value": n / (t_plain / 1e3), "unit": "pairs/s", "p50_ms": lat[len(lat) // 2],
+                               "p99_ms": lat[int(0.99 * (len(lat) - 1))]},
+            "batched_over_plain": (n / (t_batch / 1e3)) / (n / (t_plain / 1e3))}
+
+
+def percentile(v, q):
+    v = sorted(v)
+    return v[min(len(v) - 1, int(q * (len(v) - 1) + 0.5))] if v else None
+
+
+def run_served(mixed, dev):
+    """Open-loop Poisson arrivals of the mixed pairs (per-request seeds) at each
+    rate for SERVED_SECONDS: the served form (8 GB arena) against the plain
+    per-pair stages serving the same trace one request at a time. Latency runs
+    from submit (before the host-to-device copies) to the result on the host."""
+    import numpy as np
+    import torch
+    from crossstage_stitch_b200 import stages, synth
+    from crossstage_stitch_b200.server import Server, pinned_image
+    pool = [(pinned_image(a), pinned_image(b), kn) for a, b, kn in mixed[:SERVED_POOL]]
+    W = max(max(a.shape[1], b.shape[1]) for a, b, _ in pool)
+    H = max(max(a.shape[0], b.shape[0]) for a, b, _ in pool)
+    runner = stages.PairRunner(W, H, 8000, max_r=8000, device=dev)
+    dev_a = torch.empty((H, W), dtype=torch.uint8, device=dev)
+    dev_b = torch.empty((H, W), dtype=torch.uint8, device=dev)
+    out = []
+    for rate in SERVED_RATES:
+        rng = np.random.default_rng(synth.BASE_SEED + rate)
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, int(rate * SERVED_SECONDS * 1.2)))
+        arrivals = arrivals[arrivals < SERVED_SECONDS]
+        picks = rng.integers(0, len(pool), len(arrivals))
+        # served form
+        srv = Server(arena_bytes=8 << 30, max_batch=64, streams=2, device=dev.index)
+        for i in range(min(8, len(pool))):          # warm-up requests, not timed
+            srv.submit(pool[i][0], pool[i][1], mixed_knobs(pool[i][2], 1), tag=1 << 40 | i)
+        srv.drain()
+        res, t0 = [], time.perf_counter()
+        for n, (t, p) in enumerate(zip(arrivals, picks)):
+            while True:
+                rem = t - (time.perf_counter() - t0)
+                if rem <= 0:
+                    break
+                res += srv.poll()
+                if rem > 5e-4:
+                    time.sleep(2e-4)
+            a, b, kn = pool[p]
+            assert srv.submit(a, b, mixed_knobs(kn, synth.BASE_SEED + 500000 + n), tag=n) == 0
+        res += srv.drain()
+        span = max(r["done_ms"] for r in res) - min(r["submit_ms"] for r in res)
+        srv.close()
+        lat = [r["latency_ms"] for r in res]
+        # plain per-pair on the same trace, first come first served, within the same window + 2 s
+        plat, t0 = [], time.perf_counter()
+        for n, (t, p) in enumerate(zip(arrivals, picks)):
+            while time.perf_counter() - t0 < t:
+                pass
+            if time.perf_counter() - t0 > SERVED_SECONDS + 2.0:
+                break
+            a, b, kn = pool[p]
+            h, w = a.shape
+            hb, wb = b.shape
+            dev_a[:h, :w].copy_(a, non_blocking=True)
+            dev_b[:hb, :wb].copy_(b, non_blocking=True)
+            runner.enqueue(w, h, wb, hb, mixed_knobs(kn, synth.BASE_SEED + 500000 + n), images=(dev_a, dev_b))
+            torch.cuda.current_stream().synchronize()
+            plat.append(1e3 * (time.perf_counter() - t0 - t))
+        out.append({"offered_pairs_s": rate, "requests": len(arrivals),
+                    "throughput_pairs_s": len(res) / (span / 1e3), "p50_ms": percentile(lat, 0.5),
+                    "p99_ms": percentile(lat, 0.99), "drop_rate": 0.0,
+                    "mean_batch_pairs": sum(r["batch_pairs"] for r in res) / len(res),
+                    "plain_per_pair": {"p50_ms": percentile(plat, 0.5), "p99_ms": percentile(plat, 0.99),
+                                       "completed": len(plat),
+                                       "drop_rate": 1.0 - len(plat) / len(arrivals)}})
+    return {"arrivals": "open-loop Poisson", "seconds_per_rate": SERVED_SECONDS, "hbm_budget_bytes": 8 << 30,
+            "request_pool": f"{len(pool)} mixed-resolution pairs, per-request S5 seeds", "rates": out}
+
+
 def algorithmic_work(batch, n_pairs, counts):
     """Per-kernel algorithmic work of one step (bytes for pixel kernels,
     ops for matching and estimation), from the actual keypoint and match
@@ -172,6 +328,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-resolution and served sections")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -184,6 +341,9 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(32, min(os.cpu_count() or 1, 32))   # spawned pool, before any CUDA work
+    mixed = None
+    if rank == 0 and world == 1 and not args.no_mixed:
+        mixed = make_mixed(N_MIXED, min(os.cpu_count() or 1, 32))   # spawned pool, before any CUDA work
 
     import torch
     import torch.distributed as dist
@@ -267,6 +427,11 @@ def main():
     t_plain = start.elapsed_time(stop)
     lat.sort()
 
+    mixed_res = served_res = None
+    if mixed is not None:
+        mixed_res = run_mixed(mixed, max(3, args.steps // 2), args.warmup, dev, flush)
+        served_res = run_served(mixed, dev)
+
     counts = []
     for i in range(N_PAIRS):
         o = b.outputs(i)
@@ -315,7 +480,8 @@ def main():
                 "kernel_ms": {k: round(v, 5) for k, v in kern.items()}, "kernel_ms_sum": ksum,
                 "keypoints_mean": statistics.mean(a + b_ for a, b_, _ in counts) / 2,
                 "matches_mean": statistics.mean(m for _, _, m in counts),
-                "gpu_launches": launches, "clocks": clk, "roofline": roof, "cpu_baseline": cpu}
+                "gpu_launches": launches, "clocks": clk, "roofline": roof, "cpu_baseline": cpu,
+                "mixed": mixed_res, "served": served_res}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

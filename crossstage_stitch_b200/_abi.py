@@ -96,6 +96,28 @@ class PairDesc(C.Structure):
                 ("s2", S2Config), ("s4", S4Config), ("s5", S5Config), ("pyramid", PyramidConfig)]
 
 
+class ServerConfig(C.Structure):
+    """stitch_server_config."""
+    _fields_ = [("arena", C.c_void_p), ("arena_bytes", C.c_size_t), ("device", C.c_int), ("max_batch", C.c_int),
+                ("streams", C.c_int)]
+
+
+class Request(C.Structure):
+    """stitch_request: one pair for the served form (host images)."""
+    _fields_ = [("host_a", C.c_void_p), ("host_b", C.c_void_p),
+                ("width_a", C.c_int), ("height_a", C.c_int), ("pitch_a", C.c_int),
+                ("width_b", C.c_int), ("height_b", C.c_int), ("pitch_b", C.c_int),
+                ("scale_a", ScaleInfo), ("scale_b", ScaleInfo), ("s2", S2Config), ("s4", S4Config),
+                ("s5", S5Config), ("pyramid", PyramidConfig), ("tag", C.c_uint64)]
+
+
+class ServerResult(C.Structure):
+    """stitch_server_result."""
+    _fields_ = [("tag", C.c_uint64), ("submit_ms", C.c_double), ("launch_ms", C.c_double),
+                ("done_ms", C.c_double), ("batch_pairs", C.c_int), ("status", C.c_int),
+                ("result", HomographyResult)]
+
+
 P = C.POINTER
 _size_p = P(C.c_size_t)
 
@@ -139,6 +161,11 @@ PROTOTYPES: dict[str, tuple] = {
                                             P(C.c_void_p)]),
     "stitch_batch_destroy": (None, [C.c_void_p]),
     "stitch_batch_set_marks": (C.c_int, [C.c_void_p, P(C.c_void_p), C.c_int]),
+    "stitch_server_create": (C.c_int, [P(ServerConfig), P(C.c_void_p)]),
+    "stitch_server_submit": (C.c_int, [C.c_void_p, P(Request)]),
+    "stitch_server_poll": (C.c_int, [C.c_void_p, P(ServerResult), C.c_int, P(C.c_int)]),
+    "stitch_server_outstanding": (C.c_int, [C.c_void_p]),
+    "stitch_server_destroy": (None, [C.c_void_p]),
 }
 
 BATCH_MARKS = ("tables", "pyramid", "fast_nms", "select_scatter", "harris", "sort_topk", "blur", "describe", "knn_popc",

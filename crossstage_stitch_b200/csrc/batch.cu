@@ -62,10 +62,10 @@ void set_attributes_once() {
 Plan::~Plan() {
     if (graph_exec) cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(graph_exec));
     if (graph) cudaGraphDestroy(static_cast<cudaGraph_t>(graph));
-    if (staging) cudaFreeHost(staging);
+    if (staging && owns_staging) cudaFreeHost(staging);
 }
 
-Status Plan::build(int n_pairs, const stitch_pair_desc* p, int* bad_pair) {
+Status Plan::build(int n_pairs, const stitch_pair_desc* p, int* bad_pair, bool alloc_staging) {
     if (n_pairs <= 0 || !p) return Status::INVALID_ARGUMENT;
     n = n_pairs;
     pairs.assign(p, p + n);
@@ -228,10 +228,12 @@ Status Plan::build(int n_pairs, const stitch_pair_desc* p, int* bad_pair) {
     tables = lay.take(table_bytes, 1);
     if (!lay.ok) return Status::INVALID_ARGUMENT;
     total = lay.cursor;
+    if (!alloc_staging) return Status::OK;
     if (cudaHostAlloc(reinterpret_cast<void**>(&staging), table_bytes, cudaHostAllocDefault) != cudaSuccess) {
         staging = nullptr;
         return Status::CUDA_ERROR;
     }
+    owns_staging = true;
     // Block counts of every launch are final once stage_tables has run.
     return Status::OK;
 }

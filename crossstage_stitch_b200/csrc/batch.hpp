@@ -50,8 +50,10 @@ public:
     int sort_smem = 0, search_smem = 0;
     bool rank_fallback = false;
     int hpw = 8;
-    // host staging of the tables (pinned), filled for one workspace address
+    // host staging of the tables (pinned), filled for one workspace address;
+    // either allocated by build() or lent by the caller (use_staging)
     unsigned char* staging = nullptr;
+    bool owns_staging = false;
     const void* staged_for = nullptr;
     // captured graph
     void* graph = nullptr;       // cudaGraph_t
@@ -62,7 +64,15 @@ public:
 
     ~Plan();
     int resize_kinds() const { return max_levels > 1 ? max_levels - 1 : 1; }
-    Status build(int n_pairs, const stitch_pair_desc* p, int* bad_pair);
+    // Validates the pairs and lays out the workspace (host work only), then,
+    // with alloc_staging, allocates the pinned staging of the job tables.
+    Status build(int n_pairs, const stitch_pair_desc* p, int* bad_pair, bool alloc_staging = true);
+    // Lends a pinned buffer of at least table_bytes as the staging.
+    void use_staging(unsigned char* buf) {
+        staging = buf;
+        owns_staging = false;
+        staged_for = nullptr;
+    }
     Status stage_tables(void* ws);
     Status enqueue(void* ws, std::size_t bytes, stitch_homography_result* host_results, cudaStream_t s);
 };

@@ -1,0 +1,400 @@
+// Served form: a device-resident request loop with continuous batching.
+//
+// Requests (two host GRAY8 images and per-pair knobs) are queued by
+// stitch_server_submit. One dispatcher thread admits them in arrival order
+// into batches: a batch takes as many waiting requests as fit (in pairs and
+// in one contiguous region of the caller's device arena, whose size is the
+// HBM admission budget) and is launched on a free stream as soon as one is
+// free, so a batch formed from requests that arrived while others were on
+// the GPU overlaps them. Each batch copies its images into the arena, runs
+// the batched registration chain (batch.cu: every kernel once for all of
+// its pairs), and copies the homography results back; when its event
+// completes the region and the stream return to the pool and the results
+// are handed to stitch_server_poll. A pair's result does not depend on the
+// batch it ran in: the batched chain equals the per-pair stages bit for bit.
+//
+// No reference counterpart: the reference registers one pair at a time
+// (harness/pipeline_runner.cu:335-416).
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <thread>
+#include <vector>
+
+#include "batch.hpp"
+
+namespace stitch::b200::serve {
+
+using batch::Plan;
+
+namespace {
+
+constexpr std::size_t kAlign = 256;
+constexpr std::size_t kStagingPerPair = 16 << 10;  // pinned job-table bytes reserved per pair
+
+std::size_t round_up(std::size_t v, std::size_t a) { return (v + a - 1) / a * a; }
+int image_pitch(int w) { return (w + 15) / 16 * 16; }
+
+std::size_t image_bytes(const stitch_request& r) {
+    return round_up(static_cast<std::size_t>(image_pitch(r.width_a)) * r.height_a, kAlign) +
+           round_up(static_cast<std::size_t>(image_pitch(r.width_b)) * r.height_b, kAlign);
+}
+
+// First-fit allocator over [0, size) with coalescing frees.
+class Arena {
+public:
+    explicit Arena(std::size_t size) { free_[0] = size; }
+    bool alloc(std::size_t bytes, std::size_t* off) {
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second < bytes) continue;
+            *off = it->first;
+            const std::size_t rest = it->second - bytes;
+            const std::size_t next = it->first + bytes;
+            free_.erase(it);
+            if (rest) free_[next] = rest;
+            return true;
+        }
+        return false;
+    }
+    void release(std::size_t off, std::size_t bytes) {
+        auto it = free_.emplace(off, bytes).first;
+        auto next = std::next(it);
+        if (next != free_.end() && it->first + it->second == next->first) {
+            it->second += next->second;
+            free_.erase(next);
+        }
+        if (it != free_.begin()) {
+            auto prev = std::prev(it);
+            if (prev->first + prev->second == it->first) {
+                prev->second += it->second;
+                free_.erase(it);
+            }
+        }
+    }
+    std::size_t largest() const {
+        std::size_t m = 0;
+        for (const auto& f : free_) m = std::max(m, f.second);
+        return m;
+    }
+
+private:
+    std::map<std::size_t, std::size_t> free_;
+};
+
+struct Request {
+    stitch_request r;
+    double submit_ms = 0.0;
+    std::size_t footprint = 0;  // images + its share of a batch workspace, alone
+};
+
+struct Slot {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+    unsigned char* staging = nullptr;           // pinned job tables
+    stitch_homography_result* results = nullptr;  // pinned, max_batch entries
+    std::unique_ptr<Plan> plan;
+    std::vector<Request> reqs;
+    std::size_t offset = 0, bytes = 0;
+    double launch_ms = 0.0;
+    bool busy = false;
+};
+
+// Pair descriptor of a request whose images start at `a` and `b`.
+stitch_pair_desc pair_desc(const stitch_request& r, const unsigned char* a, const unsigned char* b) {
+    stitch_pair_desc d{};
+    d.image_a = stitch_image_view{const_cast<std::uint8_t*>(a), r.width_a, r.height_a, image_pitch(r.width_a), 1};
+    d.image_b = stitch_image_view{const_cast<std::uint8_t*>(b), r.width_b, r.height_b, image_pitch(r.width_b), 1};
+    d.scale_a = r.scale_a;
+    d.scale_b = r.scale_b;
+    d.s2 = r.s2;
+    d.s4 = r.s4;
+    d.s5 = r.s5;
+    d.pyramid = r.pyramid;
+    return d;
+}
+
+}  // namespace
+
+class Server {
+public:
+    explicit Server(const stitch_server_config& c) : cfg_(c), arena_(c.arena_bytes) {
+        t0_ = std::chrono::steady_clock::now();
+    }
+    ~Server() { shutdown(); }
+
+    Status start() {
+        if (cudaSetDevice(cfg_.device) != cudaSuccess) return Status::CUDA_ERROR;
+        slots_.resize(cfg_.streams);
+        for (auto& s : slots_) {
+            if (cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking) != cudaSuccess ||
+                cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming) != cudaSuccess ||
+                cudaHostAlloc(reinterpret_cast<void**>(&s.staging), staging_cap(), cudaHostAllocDefault) !=
+                    cudaSuccess ||
+                cudaHostAlloc(reinterpret_cast<void**>(&s.results),
+                              cfg_.max_batch * sizeof(stitch_homography_result), cudaHostAllocDefault) != cudaSuccess)
+                return Status::CUDA_ERROR;
+        }
+        worker_ = std::thread([this] { loop(); });
+        return Status::OK;
+    }
+
+    Status submit(const stitch_request& r) {
+        if (!r.host_a || !r.host_b || r.pitch_a < r.width_a || r.pitch_b < r.width_b) return Status::INVALID_ARGUMENT;
+        Request q;
+        q.r = r;
+        // footprint: the request alone in a batch (host layout only)
+        const auto* fake = reinterpret_cast<const unsigned char*>(kAlign);
+        stitch_pair_desc d = pair_desc(r, fake, fake);
+        Plan p;
+        int bad = -1;
+        const Status st = p.build(1, &d, &bad, false);
+        if (st != Status::OK) return st;
+        q.footprint = image_bytes(r) + round_up(p.total, kAlign);
+        if (q.footprint > cfg_.arena_bytes || p.table_bytes > staging_cap()) return Status::INSUFFICIENT_WORKSPACE;
+        q.submit_ms = now_ms();
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            if (stopping_) return Status::INVALID_ARGUMENT;
+            incoming_.push_back(q);
+            ++outstanding_;
+        }
+        cv_.notify_one();
+        return Status::OK;
+    }
+
+    int poll(stitch_server_result* out, int max) {
+        std::lock_guard<std::mutex> g(mu_);
+        const int n = std::min<int>(max, static_cast<int>(done_.size()));
+        for (int i = 0; i < n; ++i) out[i] = done_[i];
+        done_.erase(done_.begin(), done_.begin() + n);
+        return n;
+    }
+
+    int outstanding() {
+        std::lock_guard<std::mutex> g(mu_);
+        return outstanding_;
+    }
+
+    void shutdown() {
+        {
+            std::lock_guard<std::mutex> g(mu_);
+            if (stopping_ && !worker_.joinable()) return;
+            stopping_ = true;
+        }
+        cv_.notify_all();
+        if (worker_.joinable()) worker_.join();
+        for (auto& s : slots_) {
+            if (s.stream) cudaStreamSynchronize(s.stream);
+            s.plan.reset();
+            if (s.done) cudaEventDestroy(s.done);
+            if (s.stream) cudaStreamDestroy(s.stream);
+            if (s.staging) cudaFreeHost(s.staging);
+            if (s.results) cudaFreeHost(s.results);
+            s = Slot{};
+        }
+    }
+
+private:
+    std::size_t staging_cap() const { return kStagingPerPair * cfg_.max_batch + (64 << 10); }
+
+    double now_ms() const {
+        return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0_).count();
+    }
+
+    void finish(Slot& s, Status launch_status) {
+        const double t = now_ms();
+        std::vector<stitch_server_result> out;
+        for (std::size_t i = 0; i < s.reqs.size(); ++i) {
+            stitch_server_result r{};
+            r.tag = s.reqs[i].r.tag;
+            r.submit_ms = s.reqs[i].submit_ms;
+            r.launch_ms = s.launch_ms;
+            r.done_ms = t;
+            r.batch_pairs = static_cast<int>(s.reqs.size());
+            r.status = static_cast<int>(launch_status);
+            if (launch_status == Status::OK) r.result = s.results[i];
+            out.push_back(r);
+        }
+        if (s.bytes) arena_.release(s.offset, s.bytes);
+        s.plan.reset();
+        s.reqs.clear();
+        s.bytes = 0;
+        s.busy = false;
+        std::lock_guard<std::mutex> g(mu_);
+        done_.insert(done_.end(), out.begin(), out.end());
+        outstanding_ -= static_cast<int>(out.size());
+    }
+
+    // Forms a batch from the head of the queue and launches it on slot s.
+    bool launch(Slot& s) {
+        if (pending_.empty()) return false;
+        const std::size_t room = arena_.largest();
+        std::size_t need = 0;
+        int n = 0;
+        while (n < static_cast<int>(pending_.size()) && n < cfg_.max_batch &&
+               need + pending_[n].footprint + (64 << 10) <= room) {
+            need += pending_[n].footprint;
+            ++n;
+        }
+        if (n == 0) return false;  // the head waits for memory to free up
+        for (; n > 0; --n) {
+            // images first, then the batch workspace
+            std::vector<std::size_t> img_off(2 * n);
+            std::size_t images = 0;
+            for (int i = 0; i < n; ++i) {
+                const auto& r = pending_[i].r;
+                img_off[2 * i] = images;
+                images += round_up(static_cast<std::size_t>(image_pitch(r.width_a)) * r.height_a, kAlign);
+                img_off[2 * i + 1] = images;
+                images += round_up(static_cast<std::size_t>(image_pitch(r.width_b)) * r.height_b, kAlign);
+            }
+            // lay out with placeholder addresses to size the region
+            auto plan = std::make_unique<Plan>();
+            std::vector<stitch_pair_desc> descs(n);
+            const auto* base0 = reinterpret_cast<const unsigned char*>(kAlign);
+            for (int i = 0; i < n; ++i)
+                descs[i] = pair_desc(pending_[i].r, base0 + img_off[2 * i], base0 + img_off[2 * i + 1]);
+            int bad = -1;
+            if (plan->build(n, descs.data(), &bad, false) != Status::OK) {
+                // a request that passed submit cannot fail here; drop the head
+                s.reqs.assign(pending_.begin(), pending_.begin() + 1);
+                pending_.pop_front();
+                finish(s, Status::INVALID_ARGUMENT);
+                return true;
+            }
+            if (plan->table_bytes > staging_cap()) continue;
+            const std::size_t bytes = images + round_up(plan->total, kAlign);
+            std::size_t off = 0;
+            if (!arena_.alloc(bytes, &off)) continue;
+            auto* base = static_cast<unsigned char*>(cfg_.arena) + off;
+            for (int i = 0; i < n; ++i)
+                descs[i] = pair_desc(pending_[i].r, base + img_off[2 * i], base + img_off[2 * i + 1]);
+            plan = std::make_unique<Plan>();
+            if (plan->build(n, descs.data(), &bad, false) != Status::OK) {
+                arena_.release(off, bytes);
+                return false;
+            }
+            plan->use_staging(s.staging);
+            s.reqs.assign(pending_.begin(), pending_.begin() + n);
+            pending_.erase(pending_.begin(), pending_.begin() + n);
+            s.offset = off;
+            s.bytes = bytes;
+            s.launch_ms = now_ms();
+            s.busy = true;
+            Status st = Status::OK;
+            for (int i = 0; i < n && st == Status::OK; ++i) {
+                const auto& r = s.reqs[i].r;
+                if (cudaMemcpy2DAsync(base + img_off[2 * i], image_pitch(r.width_a), r.host_a, r.pitch_a, r.width_a,
+                                      r.height_a, cudaMemcpyHostToDevice, s.stream) != cudaSuccess ||
+                    cudaMemcpy2DAsync(base + img_off[2 * i + 1], image_pitch(r.width_b), r.host_b, r.pitch_b,
+                                      r.width_b, r.height_b, cudaMemcpyHostToDevice, s.stream) != cudaSuccess)
+                    st = Status::CUDA_ERROR;
+            }
+            if (st == Status::OK) st = plan->enqueue(base + images, bytes - images, s.results, s.stream);
+            if (st == Status::OK && cudaEventRecord(s.done, s.stream) != cudaSuccess) st = Status::CUDA_ERROR;
+            s.plan = std::move(plan);
+            if (st != Status::OK) {
+                cudaStreamSynchronize(s.stream);
+                finish(s, st);
+            }
+            return true;
+        }
+        return false;
+    }
+
+    void loop() {
+        cudaSetDevice(cfg_.device);
+        for (;;) {
+            bool busy = false;
+            {
+                std::unique_lock<std::mutex> g(mu_);
+                for (const auto& s : slots_) busy |= s.busy;
+                if (incoming_.empty() && pending_.empty() && !busy) {
+                    if (stopping_) return;
+                    cv_.wait(g, [&] { return stopping_ || !incoming_.empty(); });
+                }
+                while (!incoming_.empty()) {
+                    pending_.push_back(incoming_.front());
+                    incoming_.pop_front();
+                }
+            }
+            bool progressed = false;
+            for (auto& s : slots_) {
+                if (s.busy && cudaEventQuery(s.done) == cudaSuccess) {
+                    finish(s, Status::OK);
+                    progressed = true;
+                }
+            }
+            for (auto& s : slots_) {
+                if (!s.busy && launch(s)) progressed = true;
+            }
+            if (!progressed) std::this_thread::sleep_for(std::chrono::microseconds(20));
+        }
+    }
+
+    stitch_server_config cfg_;
+    Arena arena_;
+    std::chrono::steady_clock::time_point t0_;
+    std::vector<Slot> slots_;
+    std::deque<Request> pending_;  // dispatcher thread only
+    std::thread worker_;
+    std::mutex mu_;
+    std::condition_variable cv_;
+    std::deque<Request> incoming_;             // guarded by mu_
+    std::vector<stitch_server_result> done_;   // guarded by mu_
+    int outstanding_ = 0;                      // guarded by mu_
+    bool stopping_ = false;                    // guarded by mu_
+};
+
+}  // namespace stitch::b200::serve
+
+using stitch::Status;
+using stitch::b200::serve::Server;
+
+struct stitch_server {
+    std::unique_ptr<Server> impl;
+};
+
+extern "C" {
+
+int stitch_server_create(const stitch_server_config* config, stitch_server** out) {
+    if (!config || !out || !config->arena || config->arena_bytes == 0 ||
+        reinterpret_cast<std::uintptr_t>(config->arena) % 256 != 0 || config->max_batch < 0 || config->streams < 0)
+        return static_cast<int>(Status::INVALID_ARGUMENT);
+    *out = nullptr;
+    stitch_server_config c = *config;
+    if (c.max_batch == 0) c.max_batch = 64;
+    if (c.streams == 0) c.streams = 2;
+    auto* s = new (std::nothrow) stitch_server;
+    if (!s) return static_cast<int>(Status::CUDA_ERROR);
+    s->impl = std::make_unique<Server>(c);
+    const Status st = s->impl->start();
+    if (st != Status::OK) {
+        delete s;
+        return static_cast<int>(st);
+    }
+    *out = s;
+    return 0;
+}
+
+int stitch_server_submit(stitch_server* s, const stitch_request* r) {
+    if (!s || !r) return static_cast<int>(Status::INVALID_ARGUMENT);
+    return static_cast<int>(s->impl->submit(*r));
+}
+
+int stitch_server_poll(stitch_server* s, stitch_server_result* out, int max, int* count) {
+    if (!s || !count || max < 0 || (max > 0 && !out)) return static_cast<int>(Status::INVALID_ARGUMENT);
+    *count = s->impl->poll(out, max);
+    return 0;
+}
+
+int stitch_server_outstanding(stitch_server* s) { return s ? s->impl->outstanding() : -1; }
+
+void stitch_server_destroy(stitch_server* s) { delete s; }
+
+}  // extern "C"

@@ -1,0 +1,100 @@
+"""Served form: a native request loop (C ABI stitch_server_*) that admits
+image pairs of uneven size under an HBM budget and batches them
+continuously; see csrc/server.cu."""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+import torch
+
+from . import _abi
+from ._abi import Request, ServerConfig, ServerResult, StageError
+from .stages import Knobs, result_dict
+
+
+def pinned_image(gray) -> torch.Tensor:
+    """A pinned host uint8 (rows, cols) tensor holding `gray`."""
+    if isinstance(gray, torch.Tensor) and gray.is_pinned() and gray.dtype == torch.uint8:
+        return gray
+    t = torch.empty(tuple(gray.shape), dtype=torch.uint8, pin_memory=True)
+    t.copy_(torch.as_tensor(np.ascontiguousarray(gray)))
+    return t
+
+
+class Server:
+    """Owns the device arena (its size is the admission budget) and the
+    native server. Images passed to submit() are kept alive until their
+    result has been polled."""
+
+    def __init__(self, arena_bytes: int = 8 << 30, max_batch: int = 64, streams: int = 2, device=None):
+        self.lib = _abi.load()
+        self.device = torch.device("cuda", torch.cuda.current_device() if device is None else device)
+        self.arena = torch.empty(arena_bytes, dtype=torch.uint8, device=self.device)
+        cfg = ServerConfig(self.arena.data_ptr(), arena_bytes, self.device.index, max_batch, streams)
+        h = C.c_void_p()
+        st = self.lib.stitch_server_create(C.byref(cfg), C.byref(h))
+        if st != 0:
+            raise StageError("stitch_server_create", st)
+        self.handle = h
+        self.held: dict[int, tuple] = {}
+        self._buf = (ServerResult * 256)()
+
+    def submit(self, gray_a, gray_b, knobs: Knobs, tag: int, scale_a=None, scale_b=None) -> int:
+        """Queues one pair; returns the status code (0 = queued)."""
+        a, b = pinned_image(gray_a), pinned_image(gray_b)
+        r = Request()
+        r.host_a, r.host_b = a.data_ptr(), b.data_ptr()
+        r.width_a, r.height_a, r.pitch_a = a.shape[1], a.shape[0], a.stride(0)
+        r.width_b, r.height_b, r.pitch_b = b.shape[1], b.shape[0], b.stride(0)
+        if scale_a is not None:
+            r.scale_a = scale_a
+        if scale_b is not None:
+            r.scale_b = scale_b
+        r.s2, r.s4, r.s5, r.pyramid = knobs.s2(), knobs.s4(), knobs.s5(), knobs.pyramid()
+        r.tag = tag
+        self.held[tag] = (a, b)
+        st = self.lib.stitch_server_submit(self.handle, C.byref(r))
+        if st != 0:
+            del self.held[tag]
+        return st
+
+    def poll(self) -> list[dict]:
+        out = []
+        while True:
+            n = C.c_int()
+            st = self.lib.stitch_server_poll(self.handle, self._buf, len(self._buf), C.byref(n))
+            if st != 0:
+                raise StageError("stitch_server_poll", st)
+            for i in range(n.value):
+                r = self._buf[i]
+                d = result_dict(r.result) if r.status == 0 else {"status": r.status}
+                d.update(tag=r.tag, submit_ms=r.submit_ms, launch_ms=r.launch_ms, done_ms=r.done_ms,
+                         latency_ms=r.done_ms - r.submit_ms, batch_pairs=r.batch_pairs, run_status=r.status)
+                self.held.pop(r.tag, None)
+                out.append(d)
+            if n.value < len(self._buf):
+                return out
+
+    def outstanding(self) -> int:
+        return self.lib.stitch_server_outstanding(self.handle)
+
+    def close(self) -> None:
+        """Finishes the queued work and stops the server; results not polled
+        by then are dropped."""
+        if getattr(self, "handle", None):
+            self.lib.stitch_server_destroy(self.handle)
+            self.handle = None
+
+    def drain(self, timeout_s: float = 120.0) -> list[dict]:
+        import time
+        out, t0 = [], time.time()
+        while self.outstanding() > 0:
+            out += self.poll()
+            if time.time() - t0 > timeout_s:
+                raise TimeoutError(f"{self.outstanding()} requests still outstanding")
+            time.sleep(0.0005)
+        return out + self.poll()
+
+    def __del__(self):
+        self.close()

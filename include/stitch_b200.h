@@ -275,6 +275,65 @@ void stitch_batch_destroy(stitch_batch* plan);
 #define STITCH_BATCH_MARKS 14
 int stitch_batch_set_marks(stitch_batch* plan, void* const* events, int count);
 
+/* ---------------------------------------------------------- served form */
+
+/* No reference counterpart (served form). The server owns no device memory:
+ * `arena` (256-byte aligned, arena_bytes long, on `device`) is the caller's,
+ * and its size is the HBM admission budget. Requests are admitted in
+ * arrival order into batches of at most max_batch pairs (0: 64) that fit in
+ * the arena; up to `streams` batches (0: 2) run at once. */
+typedef struct stitch_server_config {
+    void* arena;
+    size_t arena_bytes;
+    int device;
+    int max_batch;
+    int streams;
+} stitch_server_config;
+
+/* One pair to register. The images are host GRAY8 rows (pinned memory lets
+ * the copies overlap; pageable memory works, synchronously) and must stay
+ * valid until the request's result is polled. scale_a/scale_b as in
+ * stitch_pair_desc. `tag` is returned with the result. */
+typedef struct stitch_request {
+    const uint8_t* host_a;
+    const uint8_t* host_b;
+    int width_a, height_a, pitch_a;
+    int width_b, height_b, pitch_b;
+    stitch_scale_info scale_a, scale_b;
+    stitch_s2_config s2;
+    stitch_s4_config s4;
+    stitch_s5_config s5;
+    stitch_pyramid_config pyramid;
+    uint64_t tag;
+} stitch_request;
+
+/* Completed request. Times are milliseconds on a steady clock since the
+ * server was created: submit (stitch_server_submit), launch (its batch
+ * enqueued) and done (the dispatcher saw its batch complete, results on the
+ * host). status is 0 unless the request could not run. */
+typedef struct stitch_server_result {
+    uint64_t tag;
+    double submit_ms, launch_ms, done_ms;
+    int batch_pairs;
+    int status;
+    stitch_homography_result result;
+} stitch_server_result;
+
+typedef struct stitch_server stitch_server;
+
+/* No reference counterpart (served form). Starts the dispatcher thread. */
+int stitch_server_create(const stitch_server_config* config, stitch_server** server);
+/* No reference counterpart. Queues one request (thread-safe, returns at
+ * once). INVALID_ARGUMENT for knobs or sizes the stages reject;
+ * INSUFFICIENT_WORKSPACE when the request alone needs more than the arena. */
+int stitch_server_submit(stitch_server* server, const stitch_request* request);
+/* No reference counterpart. Moves up to `max` completed results to `out`. */
+int stitch_server_poll(stitch_server* server, stitch_server_result* out, int max, int* count);
+/* No reference counterpart. Requests submitted and not yet polled-ready. */
+int stitch_server_outstanding(stitch_server* server);
+/* No reference counterpart. Finishes the queued requests, then stops. */
+void stitch_server_destroy(stitch_server* server);
+
 #ifdef __cplusplus
 }
 #endif

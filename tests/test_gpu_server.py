@@ -1,0 +1,101 @@
+"""The served form: requests of uneven size and knobs, submitted while
+others are on the GPU, are admitted under the arena budget, batched
+continuously, and each result equals the same pair registered alone by the
+plain per-pair path (bit for bit: status, match and inlier counts, H)."""
+import time
+
+import numpy as np
+import pytest
+
+from crossstage_stitch_b200 import stages, synth
+from crossstage_stitch_b200.server import Server
+
+pytestmark = pytest.mark.gpu
+
+
+def requests():
+    out = []
+    for i in range(6):
+        p = synth.config0_pair(30 + i)
+        out.append((p.gray_a, p.gray_b, stages.Knobs(max_keypoints=1000, seed=300 + i, levels=8)))
+    for i in range(4):
+        p, kn = synth.mixed_pair(i)
+        if p.gray_a.shape[0] > 1100:
+            continue
+        out.append((p.gray_a, p.gray_b, stages.Knobs(max_keypoints=kn["max_keypoints"],
+                                                      fast_threshold=kn["fast_threshold"],
+                                                      hypotheses=kn["hypotheses"], seed=400 + i, levels=8)))
+    p = synth.config0_pair(40)
+    out.append((p.gray_a, p.gray_b[:300, :420].copy(), stages.Knobs(max_keypoints=500, seed=7)))  # single level
+    rng = np.random.default_rng(4)
+    tiny = rng.integers(0, 256, (60, 200), dtype=np.uint8)
+    out.append((tiny, tiny.copy(), stages.Knobs(max_keypoints=100, hypotheses=64, seed=2, levels=8)))
+    return out
+
+
+@pytest.fixture(scope="module")
+def reqs(cuda):
+    return requests()
+
+
+@pytest.fixture(scope="module")
+def alone(reqs):
+    W = max(max(a.shape[1], b.shape[1]) for a, b, _ in reqs)
+    H = max(max(a.shape[0], b.shape[0]) for a, b, _ in reqs)
+    K = max(k.max_keypoints for _, _, k in reqs)
+    runner = stages.PairRunner(W, H, K, max_r=8000)
+    return [runner.run(a, b, k) for a, b, k in reqs]
+
+
+def same(got, want):
+    assert got["run_status"] == 0
+    assert got["status"] == want["status"]
+    assert got["num_matches"] == want["num_matches"] and got["num_inliers"] == want["num_inliers"]
+    np.testing.assert_array_equal(got["H"], want["H"])
+    np.testing.assert_array_equal(got["H_s"], want["H_s"])
+
+
+def test_results_equal_alone_in_the_mix(reqs, alone):
+    srv = Server(arena_bytes=2 << 30, max_batch=8, streams=2)
+    got = {}
+    order = list(range(len(reqs))) * 2   # every request twice, in two waves
+    for n, i in enumerate(order):
+        a, b, k = reqs[i]
+        assert srv.submit(a, b, k, tag=n) == 0
+        if n % 3 == 2:
+            time.sleep(0.002)             # let batches start while more arrive
+        for r in srv.poll():
+            got[r["tag"]] = r
+    for r in srv.drain():
+        got[r["tag"]] = r
+    srv.close()
+    assert len(got) == len(order)
+    batches = {r["batch_pairs"] for r in got.values()}
+    assert max(batches) > 1               # some requests really ran together
+    for n, i in enumerate(order):
+        same(got[n], alone[i])
+        assert got[n]["submit_ms"] <= got[n]["launch_ms"] <= got[n]["done_ms"]
+
+
+def test_admission_under_a_small_budget(reqs, alone):
+    # a 512x512 8-level pair needs about 5 MB: room for two at a time
+    srv = Server(arena_bytes=12 << 20, max_batch=64, streams=3)
+    for n in range(8):
+        a, b, k = reqs[n % 6]
+        assert srv.submit(a, b, k, tag=n) == 0
+    res = srv.drain()
+    srv.close()
+    assert len(res) == 8
+    assert max(r["batch_pairs"] for r in res) <= 2   # the budget split the work
+    for r in res:
+        same(r, alone[r["tag"] % 6])
+
+
+def test_rejections(reqs):
+    srv = Server(arena_bytes=2 << 20, max_batch=4, streams=1)
+    a, b, k = reqs[0]
+    assert srv.submit(a, b, k, tag=1) == 2                     # larger than the whole arena
+    bad = stages.Knobs(max_keypoints=100, ratio=1.5)
+    assert srv.submit(a[:100, :100].copy(), b[:100, :100].copy(), bad, tag=2) == 1
+    assert srv.outstanding() == 0
+    srv.close()
