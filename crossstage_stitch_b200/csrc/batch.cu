@@ -143,7 +143,7 @@ Status Plan::build(int n_pairs, const stitch_pair_desc* p, int* bad_pair, bool a
                 continue;
             }
             if (!s2s3::detect_layout(im.width, im.height, k, &o.det[s]) ||
-                !s2s3::describe_layout(im.width, im.height, &o.des[s])) {
+                !s2s3::describe_layout(im.width, im.height, &o.des[s], 16)) {
                 if (bad_pair) *bad_pair = i;
                 return Status::INVALID_ARGUMENT;
             }
@@ -187,7 +187,7 @@ Status Plan::build(int n_pairs, const stitch_pair_desc* p, int* bad_pair, bool a
         const int k = pairs[i].s2.max_keypoints;
         const int dirs = pairs[i].s4.cross_check ? 2 : 1;
         n_knn += dirs;
-        qtiles_total += dirs * (k > 0 ? ceil_div(k, s4k::kQueryThreads) : 0);
+        qtiles_total += dirs * (k > 0 ? ceil_div(k, s4k::kQueryTile) : 0);
     }
     const int want_splits = std::max(1, ceil_div(2 * kSmCount, std::max(qtiles_total, 1)));
     knn_blocks = merge_blocks = 0;
@@ -279,7 +279,7 @@ Status Plan::stage_tables(void* ws) {
     for (int i = 0; i < n; ++i) {
         const int dirs = pairs[i].s4.cross_check ? 2 : 1;
         const int k = pairs[i].s2.max_keypoints;
-        qtiles_total += dirs * (k > 0 ? ceil_div(k, s4k::kQueryThreads) : 0);
+        qtiles_total += dirs * (k > 0 ? ceil_div(k, s4k::kQueryTile) : 0);
     }
     const int want_splits = std::max(1, ceil_div(2 * kSmCount, std::max(qtiles_total, 1)));
     int knn = 0, run_knn = 0, run_merge = 0, run_search = 0;
@@ -328,6 +328,7 @@ Status Plan::stage_tables(void* ws) {
             const DescribeJob e =
                 s2s3::make_describe_job(view(im), kps[s], desc[s], at<void>(ws, o.s3ws[s]), o.des[s]);
             d.blurred = e.blurred;
+            d.blur_pitch = e.blur_pitch;
             add_job(idx, d, e, db, sb);
         }
         // S4 (forward, then reverse when the mutual check is on)
@@ -336,7 +337,7 @@ Status Plan::stage_tables(void* ws) {
         const int dirs = q.s4.cross_check ? 2 : 1;
         for (int dir = 0; dir < dirs; ++dir) {
             const int qs = dir ? 1 : 0, ts = dir ? 0 : 1;
-            const int qt = k > 0 ? ceil_div(k, s4k::kQueryThreads) : 0;
+            const int qt = k > 0 ? ceil_div(k, s4k::kQueryTile) : 0;
             const int stages = std::max(1, ceil_div(std::max(k, 1), s4k::kTrainStage));
             const int splits = std::min(want_splits, stages);
             const int rows = ceil_div(stages, splits) * s4k::kTrainStage;
@@ -464,7 +465,7 @@ Status Plan::enqueue(void* ws, std::size_t bytes, stitch_homography_result* host
     using KnnSrc = s4k::JobTable<KnnJob>;
     const auto* kjobs = reinterpret_cast<const KnnJob*>(T + offsets[kKnnJobs]);
     if (go(knn_blocks))
-        s4k::knn_popc_kernel<KnnSrc><<<knn_blocks, s4k::kQueryThreads, 0, s>>>(
+        s4k::knn_popc_kernel<KnnSrc, s4k::kQueriesPerThread><<<knn_blocks, s4k::kQueryThreads, 0, s>>>(
             KnnSrc{kjobs, reinterpret_cast<const int*>(T + offsets[kKnnPrefix]), n_knn});
     mark();
     if (go(merge_blocks))

@@ -75,7 +75,7 @@ bool pyramid_layout(int w, int h, int k, int levels, float sf, PyramidLayout* ou
         l.kx[i] = lay.take(kk, sizeof(float));
         l.ky[i] = lay.take(kk, sizeof(float));
         l.kr[i] = lay.take(kk, sizeof(float));
-        if (!detect_layout(lw, lh, l.plan.budget[i], &l.det[i]) || !describe_layout(lw, lh, &l.des[i]))
+        if (!detect_layout(lw, lh, l.plan.budget[i], &l.det[i]) || !describe_layout(lw, lh, &l.des[i], 16))
             return false;
         l.detect[i] = lay.take(l.det[i].total, 1);
         l.describe[i] = lay.take(l.des[i].total, 1);
@@ -128,6 +128,7 @@ void make_pyramid_jobs(const ImageView& im, const s2::Config& c, const Keypoints
         s.scale = p.scale[i];
         jobs->describe[i] = s;
         jobs->detect[i].blurred = s.blurred;  // the FAST kernel writes the layer's blur
+        jobs->detect[i].blur_pitch = s.blur_pitch;
     }
 }
 

@@ -45,11 +45,12 @@ bool detect_layout(int w, int h, int k, DetectLayout* out) {
     return true;
 }
 
-bool describe_layout(int w, int h, DescribeLayout* out) {
+bool describe_layout(int w, int h, DescribeLayout* out, int pitch_align) {
     if (!out || !valid_image_shape(w, h)) return false;
     Layout lay;
     DescribeLayout l{};
-    l.blurred = lay.take(static_cast<std::size_t>(w) * static_cast<std::size_t>(h), 1);
+    l.blur_pitch = (w + pitch_align - 1) / pitch_align * pitch_align;
+    l.blurred = lay.take(static_cast<std::size_t>(l.blur_pitch) * static_cast<std::size_t>(h), 1);
     if (!lay.ok) return false;
     l.total = lay.cursor;
     l.tiles_x = ceil_div(w, kBlurTileW);
@@ -179,6 +180,7 @@ DescribeJob make_describe_job(const ImageView& im, const Keypoints& kp, const De
     j.height = im.height;
     j.pitch = im.pitch_bytes;
     j.blurred = at_offset<std::uint8_t>(ws, l.blurred);
+    j.blur_pitch = l.blur_pitch;
     j.x = kp.x;
     j.y = kp.y;
     j.count = kp.d_count;

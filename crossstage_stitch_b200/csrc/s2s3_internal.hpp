@@ -13,6 +13,7 @@ struct DetectLayout {
 
 struct DescribeLayout {
     std::size_t blurred, total;  // blurred image first, at offset 0
+    int blur_pitch;
     int tiles_x, tiles;
 };
 
@@ -20,7 +21,9 @@ bool valid_image_shape(int w, int h);
 bool valid_gray(const ImageView& im);
 bool valid_detect_config(const s2::Config& c);
 bool detect_layout(int w, int h, int k, DetectLayout* out);
-bool describe_layout(int w, int h, DescribeLayout* out);
+// pitch_align 1: the blurred image is dense (the per-image S3 call); 16:
+// rows start on 16-byte boundaries (the fused batched and pyramid paths).
+bool describe_layout(int w, int h, DescribeLayout* out, int pitch_align = 1);
 DetectJob make_detect_job(const ImageView& im, const s2::Config& c, const Keypoints& out, void* ws,
                           const DetectLayout& l);
 DescribeJob make_describe_job(const ImageView& im, const Keypoints& kp, const Descriptors& out, void* ws,

@@ -46,9 +46,10 @@ struct DetectJob {
     float* y;
     float* response;  // may be null
     int* count;
-    // optional: the S3 blur of the image (dense, width x height), written by
-    // the FAST kernel when set
+    // optional: the S3 blur of the image (rows of blur_pitch bytes), written
+    // by the FAST kernel when set
     std::uint8_t* blurred;
+    int blur_pitch;
     // launch bookkeeping
     int tiles_x, tiles, chunks, candidates;
 };
@@ -56,7 +57,8 @@ struct DetectJob {
 struct DescribeJob {
     const std::uint8_t* image;
     int width, height, pitch;
-    std::uint8_t* blurred;  // dense width*height
+    std::uint8_t* blurred;  // rows of blur_pitch bytes
+    int blur_pitch;
     const float* x;
     const float* y;
     const int* count;
@@ -219,27 +221,50 @@ __device__ __forceinline__ int fast_score(const std::uint8_t* p, int stride, int
     return score > thr ? score - 1 : 0;
 }
 
-constexpr int kFastPos = kFastScH * kFastScW;  // positions scored per tile (tile + 1-pixel ring)
+// Shared-memory tile of the FAST kernel: rows of kInStride bytes holding
+// image columns x0-16 .. x0+79; the halo-4 column c (image x0-4+c) is at byte
+// c + kInOff. Scores: rows of kScStride bytes, position (r, c) = image
+// (y0-1+r, x0-1+c).
+constexpr int kInStride = 96, kInOff = 12;
+constexpr int kScStride = 68;
+constexpr int kScGroups = kScStride / 4;  // groups of 4 positions per score row
+
+// Byte k of w as a float (exact: 2^23 + b - 2^23).
+__device__ __forceinline__ float byte_float(std::uint32_t w, int k) {
+    return __fsub_rn(__uint_as_float(__byte_perm(w, 0x4B000000u, 0x7440u + k)), 8388608.0f);
+}
+
+// Rounds a blur sum half-to-even after clamping to [0, 255] (clamping the
+// float first gives the same byte for every finite sum).
+__device__ __forceinline__ std::uint32_t blur_byte(float acc) {
+    return static_cast<std::uint32_t>(__float2int_rn(fminf(fmaxf(acc, 0.0f), 255.0f)));
+}
 
 // One block = one 64x32 output tile:
-//   1. stage the tile with a 4-pixel halo in shared memory, reflected at the
-//      image border (FAST never reads outside the image, the blur does);
-//   2. run the compass test on the tile plus a 1-pixel ring and list the
-//      survivors, so that full scores are computed on full warps;
+//   1. stage the tile with a 4-pixel halo in shared memory: one 16-byte load
+//      per thread for interior tiles of 16-byte aligned images, byte loads
+//      reflected at the border otherwise (FAST never reads outside the
+//      image, the blur does);
+//   2. run the compass test on the tile plus a 1-pixel ring, 4 positions per
+//      thread with per-byte SIMD compares, and list the survivors so that
+//      full scores are computed on full warps;
 //   3. score the survivors; keep strict 3x3 maxima inside the 31-pixel edge
-//      margin, write the maxima map and add their scores to the histogram.
+//      margin (4 pixels per thread, per-byte compares), write the maxima map
+//      and add their scores to the histogram.
 // With j.blurred set the block also writes the tile of the S3 7x7 blur
 // (rows pass, then columns pass; per output the taps summed first to last
 // with each product and sum rounded on its own, then rounded half-to-even
 // and clamped), bit for bit the blur_kernel result.
 template <class Src>
 __global__ __launch_bounds__(256) void fast_nms_kernel(const __grid_constant__ Src src) {
-    __shared__ std::uint8_t in[kFastInH][kFastInW];
-    __shared__ std::uint8_t sc[kFastScH][kFastScW];
-    __shared__ std::uint16_t cand[kFastPos];
+    __shared__ __align__(16) std::uint8_t in[kFastInH][kInStride];
+    __shared__ __align__(16) std::uint8_t sc[kFastScH][kScStride];
+    __shared__ std::uint16_t cand[kFastScH * kScGroups];
     __shared__ std::uint32_t hist[256];
-    __shared__ float rows[kFastTileH + 6][kFastTileW];
+    __shared__ __align__(16) float rows[kFastTileH + 6][kFastTileW];
     __shared__ int n_cand;
+    __shared__ std::size_t row_at[kFastInH];  // reflected row offsets (border tiles)
+    __shared__ int col_at[kInStride];          // reflected image columns (border tiles)
     DetectJob j;
     int local;
     if (!src.find(blockIdx.x, kFastKind, &j, &local)) return;
@@ -249,76 +274,177 @@ __global__ __launch_bounds__(256) void fast_nms_kernel(const __grid_constant__ S
     const int x0 = (local % j.tiles_x) * kFastTileW;
     hist[tid] = 0;
     if (tid == 0) n_cand = 0;
-    const bool inside = x0 >= 4 && y0 >= 4 && x0 + kFastTileW + 4 <= W && y0 + kFastTileH + 4 <= H;
-    for (int i = tid; i < kFastInH * kFastInW; i += 256) {
-        const int r = i / kFastInW, c = i - r * kFastInW;
-        int gy = y0 - 4 + r, gx = x0 - 4 + c;
-        if (!inside) {
-            gy = reflect101(gy, H);
-            gx = reflect101(gx, W);
+    // 1. stage
+    const bool vec = ((reinterpret_cast<std::uintptr_t>(j.image) | static_cast<std::uintptr_t>(j.pitch)) & 15) == 0 &&
+                     x0 >= 16 && x0 + 80 <= W && y0 >= 4 && y0 + kFastTileH + 4 <= H;
+    if (vec) {
+        if (tid < kFastInH * (kInStride / 16)) {
+            const int r = tid / (kInStride / 16), q = tid - r * (kInStride / 16);
+            *reinterpret_cast<uint4*>(&in[r][16 * q]) = *reinterpret_cast<const uint4*>(
+                j.image + static_cast<std::size_t>(y0 - 4 + r) * j.pitch + (x0 - 16 + 16 * q));
         }
-        in[r][c] = j.image[static_cast<std::size_t>(gy) * j.pitch + gx];
+    } else {
+        if (tid < kFastInH) row_at[tid] = static_cast<std::size_t>(reflect101(y0 - 4 + tid, H)) * j.pitch;
+        else if (tid < kFastInH + kInStride) col_at[tid - kFastInH] = reflect101(x0 - 16 + (tid - kFastInH), W);
+        __syncthreads();
+        for (int i = tid; i < kFastInH * (kInStride / 4); i += 256) {
+            const int r = i / (kInStride / 4), b = 4 * (i - r * (kInStride / 4));
+            const std::uint8_t* row = j.image + row_at[r];
+            *reinterpret_cast<std::uint32_t*>(&in[r][b]) =
+                static_cast<std::uint32_t>(row[col_at[b]]) | (static_cast<std::uint32_t>(row[col_at[b + 1]]) << 8) |
+                (static_cast<std::uint32_t>(row[col_at[b + 2]]) << 16) |
+                (static_cast<std::uint32_t>(row[col_at[b + 3]]) << 24);
+        }
     }
     __syncthreads();
-    for (int i0 = 0; i0 < kFastPos; i0 += 256) {  // same trip count on every thread
-        const int i = i0 + tid;
-        bool pass = false;
-        if (i < kFastPos) {
-            const int r = i / kFastScW, c = i - r * kFastScW;
-            const int gy = y0 - 1 + r, gx = x0 - 1 + c;
-            sc[r][c] = 0;
-            pass = gx >= 3 && gx < W - 3 && gy >= 3 && gy < H - 3 &&
-                   fast_compass(&in[r + 3][c + 3], kFastInW, j.threshold);
-        }
-        const unsigned m = __ballot_sync(0xffffffffu, pass);
-        int base = 0;
-        if (lane == 0 && m) base = atomicAdd(&n_cand, __popc(m));
-        base = __shfl_sync(0xffffffffu, base, 0);
-        if (pass) cand[base + __popc(m & ((1u << lane) - 1u))] = static_cast<std::uint16_t>(i);
-    }
-    if (j.blurred) {  // blur rows pass: image rows y0-3 .. y0+34, columns x0 .. x0+63
-        for (int i = tid; i < (kFastTileH + 6) * kFastTileW; i += 256) {
-            const int r = i / kFastTileW, c = i - r * kFastTileW;
-            float acc = 0.0f;
+    // 2. compass test: thread (q, rb) takes positions 4q .. 4q+3 of rows rb,
+    // rb + 15, rb + 30; groups with a survivor are listed as
+    // (group << 4 | survivor bits)
+    const std::uint32_t thr4 = static_cast<std::uint32_t>(j.threshold) * 0x01010101u;
+    constexpr std::uint32_t kOnes = 0x01010101u, kTwos = 0x02020202u;
+    {
+        constexpr int kRowSets = 256 / kScGroups;  // 15
+        const int q = tid % kScGroups, rb = tid / kScGroups, c = 4 * q;
+        unsigned colmask = 0;
 #pragma unroll
-            for (int t = 0; t < 7; ++t)
-                acc = __fadd_rn(acc, __fmul_rn(blur_tap(t), static_cast<float>(in[r + 1][c + 1 + t])));
-            rows[r][c] = acc;
+        for (int k = 0; k < 4; ++k) {
+            const int gx = x0 - 1 + c + k;
+            if (c + k < kFastScW && gx >= 3 && gx < W - 3) colmask |= 1u << k;
+        }
+        for (int it = 0; it < (kFastScH + kRowSets - 1) / kRowSets; ++it) {  // same trip count everywhere
+            const int r = rb + it * kRowSets;
+            unsigned bits = 0;
+            if (rb < kRowSets && r < kFastScH) {
+                *reinterpret_cast<std::uint32_t*>(&sc[r][c]) = 0u;
+                const int gy = y0 - 1 + r;
+                if (colmask && gy >= 3 && gy < H - 3) {
+                    const int w = q + 3;  // word holding halo columns c .. c+3 (bytes c+12 .. c+15)
+                    const auto* mid = reinterpret_cast<const std::uint32_t*>(&in[r + 3][0]);
+                    const auto* bot = reinterpret_cast<const std::uint32_t*>(&in[r + 6][0]);
+                    const auto* top = reinterpret_cast<const std::uint32_t*>(&in[r][0]);
+                    const std::uint32_t a0 = mid[w], a1 = mid[w + 1], a2 = mid[w + 2];
+                    const std::uint32_t v = __funnelshift_r(a0, a1, 24);   // centres, halo columns c+3 .. c+6
+                    const std::uint32_t s12 = a0;                          // 3 left
+                    const std::uint32_t s4 = __funnelshift_r(a1, a2, 16);  // 3 right
+                    const std::uint32_t s0 = __funnelshift_r(bot[w], bot[w + 1], 24);  // 3 down
+                    const std::uint32_t s8 = __funnelshift_r(top[w], top[w + 1], 24);  // 3 up
+                    const std::uint32_t hi = __vaddus4(v, thr4), lo = __vsubus4(v, thr4);
+                    const std::uint32_t nb = (__vcmpgtu4(s0, hi) & kOnes) + (__vcmpgtu4(s4, hi) & kOnes) +
+                                             (__vcmpgtu4(s8, hi) & kOnes) + (__vcmpgtu4(s12, hi) & kOnes);
+                    const std::uint32_t nd = (__vcmpltu4(s0, lo) & kOnes) + (__vcmpltu4(s4, lo) & kOnes) +
+                                             (__vcmpltu4(s8, lo) & kOnes) + (__vcmpltu4(s12, lo) & kOnes);
+                    const std::uint32_t pass = (__vcmpgeu4(nb, kTwos) | __vcmpgeu4(nd, kTwos)) & kOnes;
+                    bits = (pass | (pass >> 7) | (pass >> 14) | (pass >> 21)) & colmask;
+                }
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, bits != 0);
+            int base = 0;
+            if (lane == 0 && m) base = atomicAdd(&n_cand, __popc(m));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            if (bits)
+                cand[base + __popc(m & ((1u << lane) - 1u))] =
+                    static_cast<std::uint16_t>(((r * kScGroups + q) << 4) | bits);
+        }
+    }
+    if (j.blurred) {  // blur rows pass: 4 outputs per thread, image rows y0-3 .. y0+34
+        for (int g = tid; g < (kFastTileH + 6) * (kFastTileW / 4); g += 256) {
+            const int rr = g / (kFastTileW / 4), q = g - rr * (kFastTileW / 4);
+            const auto* rw = reinterpret_cast<const std::uint32_t*>(&in[rr + 1][0]);
+            const std::uint32_t b0 = rw[q + 3], b1 = rw[q + 4], b2 = rw[q + 5];  // bytes 4q+12 .. 4q+23
+            // output 4q+k reads halo columns 4q+k+1 .. 4q+k+7, i.e. x[1+k .. 7+k]
+            float x[11];
+            x[1] = byte_float(b0, 1); x[2] = byte_float(b0, 2); x[3] = byte_float(b0, 3);
+            x[4] = byte_float(b1, 0); x[5] = byte_float(b1, 1); x[6] = byte_float(b1, 2); x[7] = byte_float(b1, 3);
+            x[8] = byte_float(b2, 0); x[9] = byte_float(b2, 1); x[10] = byte_float(b2, 2);
+            float out[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                float acc = __fmul_rn(blur_tap(0), x[1 + k]);  // 0 + a nonnegative product is the product
+#pragma unroll
+                for (int t = 1; t < 7; ++t) acc = __fadd_rn(acc, __fmul_rn(blur_tap(t), x[1 + k + t]));
+                out[k] = acc;
+            }
+            *reinterpret_cast<float4*>(&rows[rr][4 * q]) = make_float4(out[0], out[1], out[2], out[3]);
         }
     }
     __syncthreads();
     const int nc = n_cand;
     for (int i = tid; i < nc; i += 256) {
-        const int pos = cand[i];
-        const int r = pos / kFastScW, c = pos - r * kFastScW;
-        sc[r][c] = static_cast<std::uint8_t>(fast_score(&in[r + 3][c + 3], kFastInW, j.threshold));
+        const int e = cand[i];
+        const int grp = e >> 4, r = grp / kScGroups, c0 = 4 * (grp - r * kScGroups);
+        for (unsigned bits = e & 0xfu; bits; bits &= bits - 1) {
+            const int c = c0 + __ffs(bits) - 1;
+            sc[r][c] = static_cast<std::uint8_t>(fast_score(&in[r + 3][c + 3 + kInOff], kInStride, j.threshold));
+        }
     }
-    if (j.blurred) {  // blur columns pass
-        for (int i = tid; i < kFastTileH * kFastTileW; i += 256) {
-            const int r = i / kFastTileW, c = i - r * kFastTileW;
-            const int gy = y0 + r, gx = x0 + c;
-            if (gx >= W || gy >= H) continue;
-            float acc = 0.0f;
+    if (j.blurred) {  // blur columns pass: rows 2p, 2p+1 and columns 4q .. 4q+3 per thread
+        const int p = tid / (kFastTileW / 4), q = tid - p * (kFastTileW / 4);
+        float4 v[8];
 #pragma unroll
-            for (int t = 0; t < 7; ++t) acc = __fadd_rn(acc, __fmul_rn(blur_tap(t), rows[r + t][c]));
-            j.blurred[static_cast<std::size_t>(gy) * W + gx] =
-                static_cast<std::uint8_t>(__float2int_rn(fminf(fmaxf(acc, 0.0f), 255.0f)));
+        for (int t = 0; t < 8; ++t) v[t] = *reinterpret_cast<const float4*>(&rows[2 * p + t][4 * q]);
+#pragma unroll
+        for (int o = 0; o < 2; ++o) {
+            const int gy = y0 + 2 * p + o, gx = x0 + 4 * q;
+            float4 acc = make_float4(__fmul_rn(blur_tap(0), v[o].x), __fmul_rn(blur_tap(0), v[o].y),
+                                     __fmul_rn(blur_tap(0), v[o].z), __fmul_rn(blur_tap(0), v[o].w));
+#pragma unroll
+            for (int t = 1; t < 7; ++t) {
+                const float tap = blur_tap(t);
+                acc.x = __fadd_rn(acc.x, __fmul_rn(tap, v[o + t].x));
+                acc.y = __fadd_rn(acc.y, __fmul_rn(tap, v[o + t].y));
+                acc.z = __fadd_rn(acc.z, __fmul_rn(tap, v[o + t].z));
+                acc.w = __fadd_rn(acc.w, __fmul_rn(tap, v[o + t].w));
+            }
+            if (gy >= H || gx >= W) continue;
+            const std::uint32_t packed =
+                blur_byte(acc.x) | (blur_byte(acc.y) << 8) | (blur_byte(acc.z) << 16) | (blur_byte(acc.w) << 24);
+            std::uint8_t* dst = j.blurred + static_cast<std::size_t>(gy) * j.blur_pitch + gx;
+            if (gx + 3 < W && (reinterpret_cast<std::uintptr_t>(dst) & 3) == 0) {
+                *reinterpret_cast<std::uint32_t*>(dst) = packed;
+            } else {
+#pragma unroll
+                for (int k = 0; k < 4; ++k)
+                    if (gx + k < W) dst[k] = static_cast<std::uint8_t>(packed >> (8 * k));
+            }
         }
     }
     __syncthreads();
-    for (int i = tid; i < kFastTileW * kFastTileH; i += 256) {
-        const int r = i / kFastTileW, c = i - r * kFastTileW;
-        const int gy = y0 + r, gx = x0 + c;
-        if (gx >= W || gy >= H) continue;
-        const int s = sc[r + 1][c + 1];
-        bool keep = s > 0 && gx >= kEdge && gx < W - kEdge && gy >= kEdge && gy < H - kEdge;
-        if (keep) {
-            keep = s > sc[r][c] && s > sc[r][c + 1] && s > sc[r][c + 2] && s > sc[r + 1][c] &&
-                   s > sc[r + 1][c + 2] && s > sc[r + 2][c] && s > sc[r + 2][c + 1] &&
-                   s > sc[r + 2][c + 2];
+    // 3. strict 3x3 maxima, 4 pixels (r, 4q .. 4q+3) per thread
+    for (int g = tid; g < kFastTileH * (kFastTileW / 4); g += 256) {
+        const int r = g / (kFastTileW / 4), q = g - r * (kFastTileW / 4);
+        const int gy = y0 + r, gx = x0 + 4 * q;
+        if (gy >= H || gx >= W) continue;
+        const auto* up = reinterpret_cast<const std::uint32_t*>(&sc[r][0]);
+        const auto* md = reinterpret_cast<const std::uint32_t*>(&sc[r + 1][0]);
+        const auto* dn = reinterpret_cast<const std::uint32_t*>(&sc[r + 2][0]);
+        const std::uint32_t u0 = up[q], u1 = up[q + 1], m0 = md[q], m1 = md[q + 1], d0 = dn[q], d1 = dn[q + 1];
+        const std::uint32_t sv = __funnelshift_r(m0, m1, 8);
+        std::uint32_t keep = __vcmpgtu4(sv, 0u);
+        keep &= __vcmpgtu4(sv, u0) & __vcmpgtu4(sv, __funnelshift_r(u0, u1, 8)) &
+                __vcmpgtu4(sv, __funnelshift_r(u0, u1, 16));
+        keep &= __vcmpgtu4(sv, m0) & __vcmpgtu4(sv, __funnelshift_r(m0, m1, 16));
+        keep &= __vcmpgtu4(sv, d0) & __vcmpgtu4(sv, __funnelshift_r(d0, d1, 8)) &
+                __vcmpgtu4(sv, __funnelshift_r(d0, d1, 16));
+        if (gy < kEdge || gy >= H - kEdge) keep = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (gx + k < kEdge || gx + k >= W - kEdge) keep &= ~(0xffu << (8 * k));
+        const std::uint32_t out = sv & keep;
+        std::uint8_t* dst = j.maxima + static_cast<std::size_t>(gy) * W + gx;
+        if (gx + 3 < W && (reinterpret_cast<std::uintptr_t>(dst) & 3) == 0) {
+            *reinterpret_cast<std::uint32_t*>(dst) = out;
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (gx + k < W) dst[k] = static_cast<std::uint8_t>(out >> (8 * k));
         }
-        j.maxima[static_cast<std::size_t>(gy) * W + gx] = keep ? static_cast<std::uint8_t>(s) : 0;
-        if (keep) atomicAdd(&hist[s], 1u);
+        if (out) {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const std::uint32_t b = (out >> (8 * k)) & 0xffu;
+                if (b) atomicAdd(&hist[b], 1u);
+            }
+        }
     }
     __syncthreads();
     if (hist[tid]) atomicAdd(&j.hist[tid], hist[tid]);
@@ -630,7 +756,8 @@ __device__ __forceinline__ int2 linear_exact_tap(int v, int src, double scale) {
 }
 
 // One block = one 64x16 tile of the layer: per-column and per-row taps once
-// in shared memory, then each output is
+// in shared memory, then 4 horizontally adjacent outputs per thread (one
+// 32-bit store), each
 //   (h(r0) * (256 - wy) + h(r1) * wy + 2^15) >> 16,
 //   h(r) = src[r][c0] * (256 - wx) + src[r][c1] * wx,
 // the integer form of the 8-bit fixed-point horizontal pass followed by the
@@ -653,23 +780,30 @@ __global__ __launch_bounds__(256) void resize_kernel(const __grid_constant__ Src
     else if (t < kResizeTileW + kResizeTileH)
         ytap[t - kResizeTileW] = linear_exact_tap(min(y0 + t - kResizeTileW, j.height - 1), j.src_height, scale[1]);
     __syncthreads();
-    const int c = t & (kResizeTileW - 1);
-    const int x = x0 + c;
-    if (x >= j.width) return;
-    const int2 tx = xtap[c];
-    const int xa = tx.x, xb = min(tx.x + 1, j.src_width - 1);
-    const int wx1 = tx.y, wx0 = 256 - tx.y;
+    const int r = t >> 4, c = 4 * (t & 15);
+    const int y = y0 + r, x = x0 + c;
+    if (y >= j.height || x >= j.width) return;
+    const int2 ty = ytap[r];
+    const std::uint8_t* pa = j.src + static_cast<std::size_t>(ty.x) * j.src_pitch;
+    const std::uint8_t* pb = j.src + static_cast<std::size_t>(min(ty.x + 1, j.src_height - 1)) * j.src_pitch;
+    std::uint32_t packed = 0;
 #pragma unroll
-    for (int r = t / kResizeTileW; r < kResizeTileH; r += 256 / kResizeTileW) {
-        const int y = y0 + r;
-        if (y >= j.height) break;
-        const int2 ty = ytap[r];
-        const std::uint8_t* ra = j.src + static_cast<std::size_t>(ty.x) * j.src_pitch;
-        const std::uint8_t* rb = j.src + static_cast<std::size_t>(min(ty.x + 1, j.src_height - 1)) * j.src_pitch;
-        const int ha = ra[xa] * wx0 + ra[xb] * wx1;
-        const int hb = rb[xa] * wx0 + rb[xb] * wx1;
+    for (int k = 0; k < 4; ++k) {
+        const int2 tx = xtap[c + k];  // columns past the layer edge repeat the last tap
+        const int xa = tx.x, xb = min(tx.x + 1, j.src_width - 1);
+        const int wx1 = tx.y, wx0 = 256 - tx.y;
+        const int ha = __ldg(pa + xa) * wx0 + __ldg(pa + xb) * wx1;
+        const int hb = __ldg(pb + xa) * wx0 + __ldg(pb + xb) * wx1;
         const int v = ha * (256 - ty.y) + hb * ty.y;
-        j.dst[static_cast<std::size_t>(y) * j.pitch + x] = static_cast<std::uint8_t>((v + (1 << 15)) >> 16);
+        packed |= static_cast<std::uint32_t>((v + (1 << 15)) >> 16) << (8 * k);
+    }
+    std::uint8_t* dst = j.dst + static_cast<std::size_t>(y) * j.pitch + x;
+    if (x + 3 < j.width && (reinterpret_cast<std::uintptr_t>(dst) & 3) == 0) {
+        *reinterpret_cast<std::uint32_t*>(dst) = packed;
+    } else {
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+            if (x + k < j.width) dst[k] = static_cast<std::uint8_t>(packed >> (8 * k));
     }
 }
 
@@ -713,7 +847,7 @@ __global__ __launch_bounds__(256) void blur_kernel(const __grid_constant__ Src s
         // Clamping the float to [0, 255] before rounding half-to-even gives
         // the same byte as rounding then clamping the integer, for every
         // finite acc, and keeps signed integer min/max out of this kernel.
-        j.blurred[static_cast<std::size_t>(gy) * W + gx] =
+        j.blurred[static_cast<std::size_t>(gy) * j.blur_pitch + gx] =
             static_cast<std::uint8_t>(__float2int_rn(fminf(fmaxf(acc, 0.0f), 255.0f)));
     }
 }
@@ -835,7 +969,7 @@ __global__ __launch_bounds__(kDescWarps * 32) void describe_kernel(const __grid_
     }
     a = __shfl_sync(0xffffffffu, a, 0);
     b = __shfl_sync(0xffffffffu, b, 0);
-    const std::uint8_t* smooth = j.blurred + static_cast<std::size_t>(y) * j.width + x;
+    const std::uint8_t* smooth = j.blurred + static_cast<std::size_t>(y) * j.blur_pitch + x;
     int value = 0;
 #pragma unroll
     for (int jj = 0; jj < 8; ++jj) {
@@ -844,8 +978,8 @@ __global__ __launch_bounds__(kDescWarps * 32) void describe_kernel(const __grid_
         const int y0 = static_cast<int>(static_cast<std::int8_t>((pk >> 8) & 0xff));
         const int x1 = static_cast<int>(static_cast<std::int8_t>((pk >> 16) & 0xff));
         const int y1 = static_cast<int>(static_cast<std::int8_t>((pk >> 24) & 0xff));
-        const int t0 = rotated_sample(smooth, j.width, x0, y0, a, b);
-        const int t1 = rotated_sample(smooth, j.width, x1, y1, a, b);
+        const int t0 = rotated_sample(smooth, j.blur_pitch, x0, y0, a, b);
+        const int t1 = rotated_sample(smooth, j.blur_pitch, x1, y1, a, b);
         value |= (t0 < t1) << jj;
     }
     row[lane] = static_cast<std::uint8_t>(value);

@@ -104,7 +104,7 @@ Status launch_direction(const Keypoints& qk, const Descriptors& qd, const Keypoi
     if (popc_eligible(qd, td, tk.capacity)) {
         using Src = OneJob<KnnJob>;
         const Src src{make_knn_job(qk, qd, tk, td, q_tiles, splits, rows, partial, out)};
-        knn_popc_kernel<Src><<<q_tiles * splits, kQueryThreads, 0, stream>>>(src);
+        knn_popc_kernel<Src, 1><<<q_tiles * splits, kQueryThreads, 0, stream>>>(src);
         if (splits > 1) knn_merge_kernel<Src><<<ceil_div(qk.capacity, 256), 256, 0, stream>>>(src);
         note_launches(splits > 1 ? 2 : 1);
     } else {

@@ -29,6 +29,10 @@ namespace stitch::b200::s4k {
 using Top2 = ::stitch::s4::Top2;
 
 constexpr int kQueryThreads = 128;
+// Queries held per thread by the batched chain (1 measured fastest: 4 per
+// thread cost more in occupancy than it saved in shared-memory reads).
+constexpr int kQueriesPerThread = 1;
+constexpr int kQueryTile = kQueryThreads * kQueriesPerThread;  // queries per batched popc block
 constexpr int kTrainStage = 256;   // train rows per shared-memory stage
 constexpr int kIndexBits = 23;     // train index bits of a key
 constexpr std::uint32_t kEmptyKey = 0xffffffffu;
@@ -43,7 +47,7 @@ struct Side {
 
 struct KnnJob {
     Side query, train;
-    int q_tiles;         // ceil(query.capacity / kQueryThreads)
+    int q_tiles;         // ceil(query.capacity / (kQueryThreads * queries per thread))
     int splits;          // train partitions
     int rows_per_split;  // multiple of kTrainStage
     uint2* partial;      // [splits][query.capacity] (k1, k2); unused when splits == 1
@@ -97,27 +101,33 @@ __device__ __forceinline__ void keep2(std::uint32_t& k1, std::uint32_t& k2, std:
     k1 = min(k1, k);
 }
 
-// Block = kQueryThreads queries x one train partition.
-template <class Src>
+// Block = kQ * 128 queries x one train partition. Thread t holds queries
+// t, t + 128, ... of the tile in registers, so each staged train row read
+// from shared memory serves kQ queries.
+template <class Src, int kQ>
 __global__ __launch_bounds__(kQueryThreads) void knn_popc_kernel(const __grid_constant__ Src src) {
     __shared__ uint4 stage[kTrainStage * 2];
     KnnJob j;
     int local;
     if (!src.find(blockIdx.x, &j, &local)) return;
     const int qt = local % j.q_tiles, split = local / j.q_tiles;
-    const int q = qt * kQueryThreads + threadIdx.x;
     int nq, nt;
     const bool ok = counts_valid(j, &nq, &nt);
     const int t0 = split * j.rows_per_split;
     const int t1 = ok ? min(nt, t0 + j.rows_per_split) : t0;
-    uint4 qa = make_uint4(0, 0, 0, 0), qb = qa;
-    const bool active = ok && q < nq;
-    if (active) {
-        const uint4* row = reinterpret_cast<const uint4*>(j.query.rows + static_cast<std::size_t>(q) * j.query.stride);
-        qa = row[0];
-        qb = row[1];
+    uint4 qa[kQ], qb[kQ];
+    std::uint32_t k1[kQ], k2[kQ];
+#pragma unroll
+    for (int u = 0; u < kQ; ++u) {
+        const int q = (qt * kQ + u) * kQueryThreads + threadIdx.x;
+        qa[u] = qb[u] = make_uint4(0, 0, 0, 0);
+        if (ok && q < nq) {
+            const uint4* row = reinterpret_cast<const uint4*>(j.query.rows + static_cast<std::size_t>(q) * j.query.stride);
+            qa[u] = row[0];
+            qb[u] = row[1];
+        }
+        k1[u] = k2[u] = kEmptyKey;
     }
-    std::uint32_t k1 = kEmptyKey, k2 = kEmptyKey;
     for (int base = t0; base < t1; base += kTrainStage) {
         const int rows = min(kTrainStage, t1 - base);
         for (int i = threadIdx.x; i < rows * 2; i += kQueryThreads) {
@@ -126,21 +136,31 @@ __global__ __launch_bounds__(kQueryThreads) void knn_popc_kernel(const __grid_co
             stage[i] = row[i & 1];
         }
         __syncthreads();
-#pragma unroll 4
+#pragma unroll 2
         for (int r = 0; r < rows; ++r) {
             const uint4 a = stage[2 * r], b = stage[2 * r + 1];
-            const int d = __popc(qa.x ^ a.x) + __popc(qa.y ^ a.y) + __popc(qa.z ^ a.z) + __popc(qa.w ^ a.w) +
-                          __popc(qb.x ^ b.x) + __popc(qb.y ^ b.y) + __popc(qb.z ^ b.z) + __popc(qb.w ^ b.w);
-            keep2(k1, k2, (static_cast<std::uint32_t>(d) << kIndexBits) | static_cast<std::uint32_t>(base + r));
+            const std::uint32_t idx = static_cast<std::uint32_t>(base + r);
+#pragma unroll
+            for (int u = 0; u < kQ; ++u) {
+                const int d = __popc(qa[u].x ^ a.x) + __popc(qa[u].y ^ a.y) + __popc(qa[u].z ^ a.z) +
+                              __popc(qa[u].w ^ a.w) + __popc(qb[u].x ^ b.x) + __popc(qb[u].y ^ b.y) +
+                              __popc(qb[u].z ^ b.z) + __popc(qb[u].w ^ b.w);
+                keep2(k1[u], k2[u], (static_cast<std::uint32_t>(d) << kIndexBits) | idx);
+            }
         }
         __syncthreads();
     }
-    if (q >= j.query.capacity) return;
-    if (!active) k1 = k2 = kEmptyKey;
-    if (j.splits == 1) {
-        j.top2[q] = top2_from_keys(k1, k2);
-    } else {
-        j.partial[static_cast<std::size_t>(split) * j.query.capacity + q] = make_uint2(k1, k2);
+#pragma unroll
+    for (int u = 0; u < kQ; ++u) {
+        const int q = (qt * kQ + u) * kQueryThreads + threadIdx.x;
+        if (q >= j.query.capacity) continue;
+        const bool active = ok && q < nq;
+        const std::uint32_t a1 = active ? k1[u] : kEmptyKey, a2 = active ? k2[u] : kEmptyKey;
+        if (j.splits == 1) {
+            j.top2[q] = top2_from_keys(a1, a2);
+        } else {
+            j.partial[static_cast<std::size_t>(split) * j.query.capacity + q] = make_uint2(a1, a2);
+        }
     }
 }
 
