@@ -128,6 +128,11 @@ PROTOTYPES: dict[str, tuple] = {
     "stitch_launch_count": (C.c_longlong, []),
     "stitch_make_scale_info": (C.c_int, [C.c_int, C.c_int, C.c_double, P(ScaleInfo)]),
     "stitch_to_original": (C.c_int, [P(C.c_double)] * 4),
+    "stitch_s1_preprocess": (C.c_int, [P(ImageView), P(ImageView), C.c_double, P(ImageView), P(ImageView),
+                                       P(ScaleInfo), P(ScaleInfo), C.c_void_p]),
+    "stitch_s1_preprocess_single": (C.c_int, [P(ImageView), C.c_double, P(ImageView), P(ScaleInfo), C.c_void_p]),
+    "stitch_s1_compute_gradient": (C.c_int, [P(ImageView), P(ImageView), C.c_void_p, P(C.c_double),
+                                             P(C.c_double), C.c_void_p]),
     "stitch_s2_workspace_bytes": (C.c_int, [C.c_int, C.c_int, P(S2Config), _size_p]),
     "stitch_s2_detect": (C.c_int, [P(ImageView), P(S2Config), P(Keypoints), C.c_void_p, C.c_size_t, C.c_void_p]),
     "stitch_s2_detect_marked": (C.c_int, [P(ImageView), P(S2Config), P(Keypoints), C.c_void_p, C.c_size_t,

@@ -93,6 +93,30 @@ struct HomographyResult {
     Status status;
 };
 
+namespace s1 {
+// src/s1/s1.hpp:14-20 and :40-46: S1 needs no device workspace; the gradient
+// probe needs 32 bytes.
+inline Status s1_workspace_bytes(int orig_w, int orig_h, double scale, std::size_t* bytes) {
+    if (bytes == nullptr || orig_w <= 0 || orig_h <= 0 || !(scale > 0.0) || scale > 1.0)
+        return Status::INVALID_ARGUMENT;
+    *bytes = 0;
+    return Status::OK;
+}
+inline Status s1_gradient_workspace_bytes(std::size_t* bytes) {
+    if (bytes == nullptr) return Status::INVALID_ARGUMENT;
+    *bytes = 32;
+    return Status::OK;
+}
+Status s1_preprocess_single(const ImageView& in, double scale, ImageView* out, ScaleInfo* scale_info,
+                            cudaStream_t stream);
+Status s1_preprocess(const ImageView& img_a, const ImageView& img_b, double scale, ImageView* out_a,
+                     ImageView* out_b, ScaleInfo* scale_a, ScaleInfo* scale_b, cudaStream_t stream);
+Status s1_compute_gradient(const ImageView& gray_a, const ImageView& gray_b, void* d_workspace,
+                           double* pinned_gradient_a, double* pinned_gradient_b, cudaStream_t stream);
+Status s1_compute_gradient_single(const ImageView& gray, void* d_workspace, double* pinned_gradient,
+                                  cudaStream_t stream);
+}  // namespace s1
+
 namespace s2 {
 constexpr int kEdge = 31;
 constexpr int kCandidateFactor = 2;

@@ -121,6 +121,24 @@ int stitch_make_scale_info(int width, int height, double scale, stitch_scale_inf
 /* src/common/geometry.hpp:157-163 (to_original): H = D_A^-1 H_s D_B. */
 int stitch_to_original(const double* h_s, const double* d_a, const double* d_b, double* h_out);
 
+/* ------------------------------------------------------------------- S1 */
+
+/* src/s1/s1.hpp:33-38 (stitch::s1::s1_preprocess): RGB8 images A and B to
+ * GRAY8 at scale S in (0, 1] (15-bit integer gray, area resize), one launch.
+ * Writes scale_a/scale_b (make_scale_info); out_a/out_b must already have
+ * the working sizes. No device workspace (src/s1/s1.hpp:14-20). */
+int stitch_s1_preprocess(const stitch_image_view* img_a, const stitch_image_view* img_b, double scale,
+                         stitch_image_view* out_a, stitch_image_view* out_b, stitch_scale_info* scale_a,
+                         stitch_scale_info* scale_b, void* stream);
+/* src/s1/s1.hpp:25-27 (stitch::s1::s1_preprocess_single). */
+int stitch_s1_preprocess_single(const stitch_image_view* img, double scale, stitch_image_view* out,
+                                stitch_scale_info* scale_info, void* stream);
+/* src/s1/s1.hpp:53-56 (stitch::s1::s1_compute_gradient): mean absolute
+ * gradient of two GRAY8 images into pinned host doubles; workspace 32 device
+ * bytes (src/s1/s1.hpp:40-46). */
+int stitch_s1_compute_gradient(const stitch_image_view* gray_a, const stitch_image_view* gray_b, void* workspace,
+                               double* pinned_gradient_a, double* pinned_gradient_b, void* stream);
+
 /* ------------------------------------------------------------------- S2 */
 
 /* src/s2_s3/s2.hpp:26-27 (stitch::s2::s2_workspace_bytes). */

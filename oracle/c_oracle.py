@@ -46,6 +46,9 @@ def lib() -> C.CDLL:
         L.oracle_s4_accept.restype = ip
         L.oracle_residual2.argtypes = [vp, C.c_double, C.c_double, C.c_double, C.c_double]
         L.oracle_residual2.restype = C.c_double
+        L.oracle_s1.argtypes = [vp, ip, ip, ip, ip, ip, vp]
+        L.oracle_s1_gradient.argtypes = [vp, ip, ip, ip]
+        L.oracle_s1_gradient.restype = C.c_double
         L.oracle_splitmix64.argtypes = [C.c_uint64]
         L.oracle_splitmix64.restype = C.c_uint64
         L.oracle_sample_four.argtypes = [ip, C.c_uint64, ip, vp]
@@ -134,3 +137,18 @@ def s5(points: np.ndarray, mask_capacity: int, hypotheses: int, threshold: float
            "inlier_coverage": res.inlier_coverage, "reproj_residual": res.reproj_residual,
            "status": res.status}
     return out, mask[:mask_capacity], best
+
+
+def s1(rgb: np.ndarray, work_w: int, work_h: int) -> np.ndarray:
+    """S1 of an (h, w, 3) uint8 RGB image to (work_h, work_w) GRAY8."""
+    rgb = np.ascontiguousarray(rgb, dtype=np.uint8)
+    h, w, _ = rgb.shape
+    out = np.zeros((work_h, work_w), np.uint8)
+    lib().oracle_s1(rgb.ctypes.data, w, h, 3 * w, work_w, work_h, out.ctypes.data)
+    return out
+
+
+def s1_gradient(gray: np.ndarray) -> float:
+    gray = np.ascontiguousarray(gray, dtype=np.uint8)
+    h, w = gray.shape
+    return lib().oracle_s1_gradient(gray.ctypes.data, w, h, w)

@@ -1,8 +1,9 @@
 // Test infrastructure only. extern "C" entry points over the reference's own
-// S2..S5 stage functions, linked with the reference sources built for sm_100a
+// S1..S5 stage functions, linked with the reference sources built for sm_100a
 // by `make -C oracle ref`. Arguments use the same plain-data layouts as
 // include/stitch_b200.h, so tests pass identical structs to both libraries.
 #include "common/types.hpp"
+#include "s1/s1.hpp"
 #include "s2_s3/s2.hpp"
 #include "s2_s3/s3.hpp"
 #include "s4/s4.hpp"
@@ -16,6 +17,13 @@ cudaStream_t st(void* s) { return static_cast<cudaStream_t>(s); }
 }  // namespace
 
 extern "C" {
+int ref_s1_preprocess(const ImageView* a, const ImageView* b, double scale, ImageView* oa, ImageView* ob,
+                      ScaleInfo* sa, ScaleInfo* sb, void* s) {
+    return code(s1::s1_preprocess(*a, *b, scale, oa, ob, sa, sb, st(s)));
+}
+int ref_s1_compute_gradient(const ImageView* a, const ImageView* b, void* ws, double* ga, double* gb, void* s) {
+    return code(s1::s1_compute_gradient(*a, *b, ws, ga, gb, st(s)));
+}
 int ref_s2_workspace_bytes(int w, int h, const s2::Config* c, std::size_t* b) {
     return code(s2::s2_workspace_bytes(w, h, *c, b));
 }

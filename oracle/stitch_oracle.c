@@ -482,3 +482,68 @@ int oracle_make_scale_info(int w, int h, double s, int* work_wh, double* sxy, do
     memcpy(d, dd, sizeof(dd));
     return O_OK;
 }
+
+/* ---------------------------------------------------------------- S1
+ * src/s1/s1.cu:33-107, :116-141: 15-bit integer gray; S = 1 direct; exact
+ * 2x2 ((sum + 2) >> 2) and 4x4 (float sum * 0.0625, round half to even)
+ * averages; otherwise a float box filter whose weighted sum the reference's
+ * nvcc build accumulates with a fused multiply-add (total += g * (wx * wy)),
+ * restated with C99 fmaf. */
+static int s1_gray(const uint8_t* p) { return (9798 * p[0] + 19235 * p[1] + 3735 * p[2] + 16384) >> 15; }
+
+void oracle_s1(const uint8_t* rgb, int w, int h, int pitch, int work_w, int work_h, uint8_t* out) {
+    const float inv_sx = (float)w / (float)work_w, inv_sy = (float)h / (float)work_h;
+    const float scale_area = 1.0f / (inv_sx * inv_sy);
+    const int mode = (w == work_w && h == work_h) ? 0
+                     : (w == 2 * work_w && h == 2 * work_h) ? 1
+                     : (w == 4 * work_w && h == 4 * work_h) ? 2 : 3;
+    for (int yd = 0; yd < work_h; ++yd) {
+        for (int xd = 0; xd < work_w; ++xd) {
+            int v;
+            if (mode == 0) {
+                v = s1_gray(rgb + (size_t)yd * pitch + 3 * xd);
+            } else if (mode == 1) {
+                const uint8_t* r0 = rgb + (size_t)(2 * yd) * pitch + 6 * xd;
+                const uint8_t* r1 = r0 + pitch;
+                v = (s1_gray(r0) + s1_gray(r0 + 3) + s1_gray(r1) + s1_gray(r1 + 3) + 2) >> 2;
+            } else if (mode == 2) {
+                int sum = 0;
+                for (int dy = 0; dy < 4; ++dy)
+                    for (int dx = 0; dx < 4; ++dx) sum += s1_gray(rgb + (size_t)(4 * yd + dy) * pitch + 12 * xd + 3 * dx);
+                v = (int)nearbyintf((float)sum * 0.0625f);
+            } else {
+                const float fsy1 = (float)yd * inv_sy, fsy2 = (float)(yd + 1) * inv_sy;
+                const float fsx1 = (float)xd * inv_sx, fsx2 = (float)(xd + 1) * inv_sx;
+                const int y0 = (int)floorf(fsy1), y1 = (int)ceilf(fsy2);
+                const int x0 = (int)floorf(fsx1), x1 = (int)ceilf(fsx2);
+                float total = 0.0f;
+                for (int ys = y0; ys < y1 && ys < h; ++ys) {
+                    const float wy = fmaxf(0.0f, fminf((float)(ys + 1), fsy2) - fmaxf((float)ys, fsy1));
+                    if (wy <= 0.0f) continue;
+                    for (int xs = x0; xs < x1 && xs < w; ++xs) {
+                        const float wx = fmaxf(0.0f, fminf((float)(xs + 1), fsx2) - fmaxf((float)xs, fsx1));
+                        if (wx <= 0.0f) continue;
+                        const float ww = wx * wy;
+                        total = fmaf((float)s1_gray(rgb + (size_t)ys * pitch + 3 * xs), ww, total);
+                    }
+                }
+                v = (int)nearbyintf(total * scale_area);
+            }
+            out[(size_t)yd * work_w + xd] = (uint8_t)v;
+        }
+    }
+}
+
+/* src/s1/s1.cu:147-205: (sum |I(x+1,y) - I(x,y)| + sum |I(x,y+1) - I(x,y)|)
+ * / (255 (h (w-1) + w (h-1))). */
+double oracle_s1_gradient(const uint8_t* g, int w, int h, int pitch) {
+    unsigned long long sum = 0;
+    for (int y = 0; y < h; ++y)
+        for (int x = 0; x < w; ++x) {
+            const int c = g[(size_t)y * pitch + x];
+            if (x + 1 < w) sum += (unsigned long long)abs(g[(size_t)y * pitch + x + 1] - c);
+            if (y + 1 < h) sum += (unsigned long long)abs(g[(size_t)(y + 1) * pitch + x] - c);
+        }
+    const unsigned long long edges = (unsigned long long)h * (w - 1) + (unsigned long long)w * (h - 1);
+    return edges ? (double)sum / (255.0 * (double)edges) : 0.0;
+}
