@@ -108,7 +108,8 @@ class Request(C.Structure):
                 ("width_a", C.c_int), ("height_a", C.c_int), ("pitch_a", C.c_int),
                 ("width_b", C.c_int), ("height_b", C.c_int), ("pitch_b", C.c_int),
                 ("scale_a", ScaleInfo), ("scale_b", ScaleInfo), ("s2", S2Config), ("s4", S4Config),
-                ("s5", S5Config), ("pyramid", PyramidConfig), ("tag", C.c_uint64)]
+                ("s5", S5Config), ("pyramid", PyramidConfig), ("rgb", C.c_int), ("scale", C.c_double),
+                ("tag", C.c_uint64)]
 
 
 class ServerResult(C.Structure):

@@ -16,19 +16,10 @@
 // each thread produces 4 horizontally adjacent outputs.
 #include <cmath>
 
-#include "common.cuh"
-#include "stitch_b200.h"
+#include "s1_internal.hpp"
+#include "s2s3_kernels.cuh"
 
 namespace stitch::b200::s1k {
-
-struct Params {
-    const std::uint8_t* src;
-    int src_pitch, orig_w, orig_h;
-    std::uint8_t* dst;
-    int dst_pitch, work_w, work_h;
-    float inv_sx, inv_sy, scale_area;
-    int mode;  // 0 direct, 1 2x2 average, 2 4x4 average, 3 float box filter
-};
 
 struct Pair {
     Params img[2];
@@ -88,6 +79,33 @@ __global__ __launch_bounds__(kS1BlockX * kS1BlockY) void s1_kernel(const __grid_
 #pragma unroll
     for (int k = 0; k < 4; ++k)
         if (x + k < p.work_w) dst[k] = static_cast<std::uint8_t>(s1_pixel(p, x + k, y));
+}
+
+// Batched form: one launch over the images of many requests; each block
+// finds its (image, 64x16 output tile) through a device job table.
+template <class Src>
+__global__ __launch_bounds__(256) void s1_batch_kernel(const __grid_constant__ Src src) {
+    BatchJob j;
+    int local;
+    if (!src.find(blockIdx.x, 0, &j, &local)) return;
+    const Params& p = j.p;
+    const int x = (local % j.tiles_x) * kBatchTileW + 4 * (threadIdx.x & 15);
+    const int y = (local / j.tiles_x) * kBatchTileH + (threadIdx.x >> 4);
+    if (y >= p.work_h || x >= p.work_w) return;
+    std::uint8_t* dst = p.dst + static_cast<std::size_t>(y) * p.dst_pitch + x;
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+        if (x + k < p.work_w) dst[k] = static_cast<std::uint8_t>(s1_pixel(p, x + k, y));
+}
+
+Status batch_job(const ImageView& in, const ImageView& out, const ScaleInfo& si, BatchJob* j);
+
+Status batch_enqueue(const BatchJob* device_jobs, const int* device_prefix, int n, int blocks, cudaStream_t stream) {
+    if (blocks <= 0) return Status::OK;
+    using Src = s2s3::JobTable<BatchJob>;
+    s1_batch_kernel<Src><<<blocks, 256, 0, stream>>>(Src{device_jobs, device_prefix, n});
+    note_launches(1);
+    return launch_status();
 }
 
 // Sum of |I(x+1, y) - I(x, y)| and |I(x, y+1) - I(x, y)| per image into
@@ -202,6 +220,15 @@ Status gradient(const ImageView* imgs, int n, void* ws, double* const* pinned, c
 }
 
 }  // namespace
+
+Status batch_job(const ImageView& in, const ImageView& out, const ScaleInfo& si, BatchJob* j) {
+    const Status s = fill(in, out, si, &j->p);
+    if (s != Status::OK) return s;
+    j->tiles_x = ceil_div(out.width, kBatchTileW);
+    j->tiles = j->tiles_x * ceil_div(out.height, kBatchTileH);
+    return Status::OK;
+}
+
 }  // namespace stitch::b200::s1k
 
 namespace stitch::s1 {

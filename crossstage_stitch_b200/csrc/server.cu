@@ -27,6 +27,7 @@
 #include <vector>
 
 #include "batch.hpp"
+#include "s1_internal.hpp"
 
 namespace stitch::b200::serve {
 
@@ -40,9 +41,43 @@ constexpr std::size_t kStagingPerPair = 16 << 10;  // pinned job-table bytes res
 std::size_t round_up(std::size_t v, std::size_t a) { return (v + a - 1) / a * a; }
 int image_pitch(int w) { return (w + 15) / 16 * 16; }
 
-std::size_t image_bytes(const stitch_request& r) {
-    return round_up(static_cast<std::size_t>(image_pitch(r.width_a)) * r.height_a, kAlign) +
-           round_up(static_cast<std::size_t>(image_pitch(r.width_b)) * r.height_b, kAlign);
+// Device images of one request: the host copies (GRAY8, or RGB8 rows of 3w
+// bytes) and, for RGB8, the working-size GRAY8 images S1 writes.
+struct Geometry {
+    bool rgb = false;
+    int wa = 0, ha = 0, wb = 0, hb = 0;  // working (registered) sizes
+    stitch_scale_info sa{}, sb{};
+    std::size_t bytes() const { return host_a + host_b + (rgb ? work_a + work_b : 0); }
+    std::size_t host_a = 0, host_b = 0, work_a = 0, work_b = 0;
+};
+
+std::size_t plane(int row_bytes, int rows) {
+    return round_up(static_cast<std::size_t>(image_pitch(row_bytes)) * static_cast<std::size_t>(rows), kAlign);
+}
+
+Status geometry(const stitch_request& r, Geometry* g) {
+    g->rgb = r.rgb != 0;
+    if (!g->rgb) {
+        if (r.pitch_a < r.width_a || r.pitch_b < r.width_b || (r.scale != 0.0 && r.scale != 1.0))
+            return Status::INVALID_ARGUMENT;
+        g->wa = r.width_a, g->ha = r.height_a, g->wb = r.width_b, g->hb = r.height_b;
+        g->sa = r.scale_a;
+        g->sb = r.scale_b;
+        g->host_a = plane(r.width_a, r.height_a);
+        g->host_b = plane(r.width_b, r.height_b);
+        return Status::OK;
+    }
+    const double s = r.scale == 0.0 ? 1.0 : r.scale;
+    if (r.width_a <= 0 || r.width_b <= 0 || r.pitch_a < 3 * r.width_a || r.pitch_b < 3 * r.width_b ||
+        stitch_make_scale_info(r.width_a, r.height_a, s, &g->sa) != 0 ||
+        stitch_make_scale_info(r.width_b, r.height_b, s, &g->sb) != 0)
+        return Status::INVALID_ARGUMENT;
+    g->wa = g->sa.work_w, g->ha = g->sa.work_h, g->wb = g->sb.work_w, g->hb = g->sb.work_h;
+    g->host_a = plane(3 * r.width_a, r.height_a);
+    g->host_b = plane(3 * r.width_b, r.height_b);
+    g->work_a = plane(g->wa, g->ha);
+    g->work_b = plane(g->wb, g->hb);
+    return Status::OK;
 }
 
 // First-fit allocator over [0, size) with coalescing frees.
@@ -88,6 +123,7 @@ private:
 
 struct Request {
     stitch_request r;
+    Geometry g;
     double submit_ms = 0.0;
     std::size_t footprint = 0;  // images + its share of a batch workspace, alone
 };
@@ -96,6 +132,7 @@ struct Slot {
     cudaStream_t stream = nullptr;
     cudaEvent_t done = nullptr;
     unsigned char* staging = nullptr;           // pinned job tables
+    unsigned char* s1_staging = nullptr;        // pinned S1 job table (2 jobs per pair) + prefix
     stitch_homography_result* results = nullptr;  // pinned, max_batch entries
     std::unique_ptr<Plan> plan;
     std::vector<Request> reqs;
@@ -104,13 +141,16 @@ struct Slot {
     bool busy = false;
 };
 
-// Pair descriptor of a request whose images start at `a` and `b`.
-stitch_pair_desc pair_desc(const stitch_request& r, const unsigned char* a, const unsigned char* b) {
+// Pair descriptor of a request whose registered (GRAY8) images start at
+// `a` and `b`.
+stitch_pair_desc pair_desc(const Request& q, const unsigned char* a, const unsigned char* b) {
+    const stitch_request& r = q.r;
+    const Geometry& g = q.g;
     stitch_pair_desc d{};
-    d.image_a = stitch_image_view{const_cast<std::uint8_t*>(a), r.width_a, r.height_a, image_pitch(r.width_a), 1};
-    d.image_b = stitch_image_view{const_cast<std::uint8_t*>(b), r.width_b, r.height_b, image_pitch(r.width_b), 1};
-    d.scale_a = r.scale_a;
-    d.scale_b = r.scale_b;
+    d.image_a = stitch_image_view{const_cast<std::uint8_t*>(a), g.wa, g.ha, image_pitch(g.wa), 1};
+    d.image_b = stitch_image_view{const_cast<std::uint8_t*>(b), g.wb, g.hb, image_pitch(g.wb), 1};
+    d.scale_a = g.sa;
+    d.scale_b = g.sb;
     d.s2 = r.s2;
     d.s4 = r.s4;
     d.s5 = r.s5;
@@ -135,6 +175,8 @@ public:
                 cudaEventCreateWithFlags(&s.done, cudaEventDisableTiming) != cudaSuccess ||
                 cudaHostAlloc(reinterpret_cast<void**>(&s.staging), staging_cap(), cudaHostAllocDefault) !=
                     cudaSuccess ||
+                cudaHostAlloc(reinterpret_cast<void**>(&s.s1_staging), s1_staging_bytes(), cudaHostAllocDefault) !=
+                    cudaSuccess ||
                 cudaHostAlloc(reinterpret_cast<void**>(&s.results),
                               cfg_.max_batch * sizeof(stitch_homography_result), cudaHostAllocDefault) != cudaSuccess)
                 return Status::CUDA_ERROR;
@@ -144,17 +186,19 @@ public:
     }
 
     Status submit(const stitch_request& r) {
-        if (!r.host_a || !r.host_b || r.pitch_a < r.width_a || r.pitch_b < r.width_b) return Status::INVALID_ARGUMENT;
+        if (!r.host_a || !r.host_b) return Status::INVALID_ARGUMENT;
         Request q;
         q.r = r;
+        Status st = geometry(r, &q.g);
+        if (st != Status::OK) return st;
         // footprint: the request alone in a batch (host layout only)
         const auto* fake = reinterpret_cast<const unsigned char*>(kAlign);
-        stitch_pair_desc d = pair_desc(r, fake, fake);
+        stitch_pair_desc d = pair_desc(q, fake, fake);
         Plan p;
         int bad = -1;
-        const Status st = p.build(1, &d, &bad, false);
+        st = p.build(1, &d, &bad, false);
         if (st != Status::OK) return st;
-        q.footprint = image_bytes(r) + round_up(p.total, kAlign);
+        q.footprint = q.g.bytes() + round_up(p.total, kAlign) + (q.g.rgb ? kAlign : 0);
         if (q.footprint > cfg_.arena_bytes || p.table_bytes > staging_cap()) return Status::INSUFFICIENT_WORKSPACE;
         q.submit_ms = now_ms();
         {
@@ -194,6 +238,7 @@ public:
             if (s.done) cudaEventDestroy(s.done);
             if (s.stream) cudaStreamDestroy(s.stream);
             if (s.staging) cudaFreeHost(s.staging);
+            if (s.s1_staging) cudaFreeHost(s.s1_staging);
             if (s.results) cudaFreeHost(s.results);
             s = Slot{};
         }
@@ -201,6 +246,8 @@ public:
 
 private:
     std::size_t staging_cap() const { return kStagingPerPair * cfg_.max_batch + (64 << 10); }
+    std::size_t s1_jobs_bytes() const { return round_up(2 * cfg_.max_batch * sizeof(b200::s1k::BatchJob), kAlign); }
+    std::size_t s1_staging_bytes() const { return s1_jobs_bytes() + (2 * cfg_.max_batch + 1) * sizeof(int); }
 
     double now_ms() const {
         return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0_).count();
@@ -243,22 +290,38 @@ private:
         }
         if (n == 0) return false;  // the head waits for memory to free up
         for (; n > 0; --n) {
-            // images first, then the batch workspace
-            std::vector<std::size_t> img_off(2 * n);
+            // host-copied images, S1 outputs, the S1 job table, then the batch workspace
+            std::vector<std::size_t> host_off(2 * n), reg_off(2 * n);
             std::size_t images = 0;
+            int rgb_images = 0;
             for (int i = 0; i < n; ++i) {
-                const auto& r = pending_[i].r;
-                img_off[2 * i] = images;
-                images += round_up(static_cast<std::size_t>(image_pitch(r.width_a)) * r.height_a, kAlign);
-                img_off[2 * i + 1] = images;
-                images += round_up(static_cast<std::size_t>(image_pitch(r.width_b)) * r.height_b, kAlign);
+                const Geometry& g = pending_[i].g;
+                host_off[2 * i] = images;
+                images += g.host_a;
+                host_off[2 * i + 1] = images;
+                images += g.host_b;
             }
+            for (int i = 0; i < n; ++i) {
+                const Geometry& g = pending_[i].g;
+                if (!g.rgb) {
+                    reg_off[2 * i] = host_off[2 * i];
+                    reg_off[2 * i + 1] = host_off[2 * i + 1];
+                    continue;
+                }
+                reg_off[2 * i] = images;
+                images += g.work_a;
+                reg_off[2 * i + 1] = images;
+                images += g.work_b;
+                rgb_images += 2;
+            }
+            const std::size_t s1_tables = images;
+            if (rgb_images) images += round_up(s1_staging_bytes(), kAlign);
             // lay out with placeholder addresses to size the region
             auto plan = std::make_unique<Plan>();
             std::vector<stitch_pair_desc> descs(n);
             const auto* base0 = reinterpret_cast<const unsigned char*>(kAlign);
             for (int i = 0; i < n; ++i)
-                descs[i] = pair_desc(pending_[i].r, base0 + img_off[2 * i], base0 + img_off[2 * i + 1]);
+                descs[i] = pair_desc(pending_[i], base0 + reg_off[2 * i], base0 + reg_off[2 * i + 1]);
             int bad = -1;
             if (plan->build(n, descs.data(), &bad, false) != Status::OK) {
                 // a request that passed submit cannot fail here; drop the head
@@ -273,7 +336,7 @@ private:
             if (!arena_.alloc(bytes, &off)) continue;
             auto* base = static_cast<unsigned char*>(cfg_.arena) + off;
             for (int i = 0; i < n; ++i)
-                descs[i] = pair_desc(pending_[i].r, base + img_off[2 * i], base + img_off[2 * i + 1]);
+                descs[i] = pair_desc(pending_[i], base + reg_off[2 * i], base + reg_off[2 * i + 1]);
             plan = std::make_unique<Plan>();
             if (plan->build(n, descs.data(), &bad, false) != Status::OK) {
                 arena_.release(off, bytes);
@@ -287,13 +350,46 @@ private:
             s.launch_ms = now_ms();
             s.busy = true;
             Status st = Status::OK;
+            // host -> device copies (RGB8 rows are 3 * width bytes)
             for (int i = 0; i < n && st == Status::OK; ++i) {
                 const auto& r = s.reqs[i].r;
-                if (cudaMemcpy2DAsync(base + img_off[2 * i], image_pitch(r.width_a), r.host_a, r.pitch_a, r.width_a,
-                                      r.height_a, cudaMemcpyHostToDevice, s.stream) != cudaSuccess ||
-                    cudaMemcpy2DAsync(base + img_off[2 * i + 1], image_pitch(r.width_b), r.host_b, r.pitch_b,
-                                      r.width_b, r.height_b, cudaMemcpyHostToDevice, s.stream) != cudaSuccess)
+                const int ca = (s.reqs[i].g.rgb ? 3 : 1) * r.width_a, cb = (s.reqs[i].g.rgb ? 3 : 1) * r.width_b;
+                if (cudaMemcpy2DAsync(base + host_off[2 * i], image_pitch(ca), r.host_a, r.pitch_a, ca, r.height_a,
+                                      cudaMemcpyHostToDevice, s.stream) != cudaSuccess ||
+                    cudaMemcpy2DAsync(base + host_off[2 * i + 1], image_pitch(cb), r.host_b, r.pitch_b, cb,
+                                      r.height_b, cudaMemcpyHostToDevice, s.stream) != cudaSuccess)
                     st = Status::CUDA_ERROR;
+            }
+            // S1 for the RGB8 requests: one launch over all their images
+            if (st == Status::OK && rgb_images) {
+                auto* jobs = reinterpret_cast<b200::s1k::BatchJob*>(s.s1_staging);
+                auto* prefix = reinterpret_cast<int*>(s.s1_staging + s1_jobs_bytes());
+                int k = 0, blocks = 0;
+                for (int i = 0; i < n && st == Status::OK; ++i) {
+                    const Request& q = s.reqs[i];
+                    if (!q.g.rgb) continue;
+                    for (int side = 0; side < 2 && st == Status::OK; ++side) {
+                        const int w = side ? q.r.width_b : q.r.width_a, h = side ? q.r.height_b : q.r.height_a;
+                        const ImageView in{base + host_off[2 * i + side], w, h, image_pitch(3 * w), PixelFormat::RGB8};
+                        const stitch_scale_info& si = side ? q.g.sb : q.g.sa;
+                        const ImageView out{base + reg_off[2 * i + side], si.work_w, si.work_h, image_pitch(si.work_w),
+                                            PixelFormat::GRAY8};
+                        st = b200::s1k::batch_job(in, out, *reinterpret_cast<const ScaleInfo*>(&si), &jobs[k]);
+                        prefix[k] = blocks;
+                        blocks += jobs[k].tiles;
+                        ++k;
+                    }
+                }
+                prefix[k] = blocks;
+                auto* djobs = base + s1_tables;
+                if (st == Status::OK &&
+                    cudaMemcpyAsync(djobs, s.s1_staging, s1_staging_bytes(), cudaMemcpyHostToDevice, s.stream) !=
+                        cudaSuccess)
+                    st = Status::CUDA_ERROR;
+                if (st == Status::OK)
+                    st = b200::s1k::batch_enqueue(reinterpret_cast<const b200::s1k::BatchJob*>(djobs),
+                                                  reinterpret_cast<const int*>(djobs + s1_jobs_bytes()), k, blocks,
+                                                  s.stream);
             }
             if (st == Status::OK) st = plan->enqueue(base + images, bytes - images, s.results, s.stream);
             if (st == Status::OK && cudaEventRecord(s.done, s.stream) != cudaSuccess) st = Status::CUDA_ERROR;

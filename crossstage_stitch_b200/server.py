@@ -14,7 +14,8 @@ from .stages import Knobs, result_dict
 
 
 def pinned_image(gray) -> torch.Tensor:
-    """A pinned host uint8 (rows, cols) tensor holding `gray`."""
+    """A pinned host uint8 tensor, (rows, cols) GRAY8 or (rows, cols, 3) RGB8,
+    holding `gray`."""
     if isinstance(gray, torch.Tensor) and gray.is_pinned() and gray.dtype == torch.uint8:
         return gray
     t = torch.empty(tuple(gray.shape), dtype=torch.uint8, pin_memory=True)
@@ -40,13 +41,17 @@ class Server:
         self.held: dict[int, tuple] = {}
         self._buf = (ServerResult * 256)()
 
-    def submit(self, gray_a, gray_b, knobs: Knobs, tag: int, scale_a=None, scale_b=None) -> int:
-        """Queues one pair; returns the status code (0 = queued)."""
+    def submit(self, gray_a, gray_b, knobs: Knobs, tag: int, scale_a=None, scale_b=None, s1_scale: float = 1.0) -> int:
+        """Queues one pair; returns the status code (0 = queued). (rows, cols, 3)
+        images are RGB8: the server converts and resizes them with S1 at
+        s1_scale on the device and returns H in their original coordinates."""
         a, b = pinned_image(gray_a), pinned_image(gray_b)
         r = Request()
         r.host_a, r.host_b = a.data_ptr(), b.data_ptr()
         r.width_a, r.height_a, r.pitch_a = a.shape[1], a.shape[0], a.stride(0)
         r.width_b, r.height_b, r.pitch_b = b.shape[1], b.shape[0], b.stride(0)
+        r.rgb = 1 if a.dim() == 3 else 0
+        r.scale = s1_scale if r.rgb else 0.0
         if scale_a is not None:
             r.scale_a = scale_a
         if scale_b is not None:

@@ -308,10 +308,14 @@ typedef struct stitch_server_config {
     int streams;
 } stitch_server_config;
 
-/* One pair to register. The images are host GRAY8 rows (pinned memory lets
- * the copies overlap; pageable memory works, synchronously) and must stay
- * valid until the request's result is polled. scale_a/scale_b as in
- * stitch_pair_desc. `tag` is returned with the result. */
+/* One pair to register. The images are host rows (pinned memory lets the
+ * copies overlap; pageable memory works, synchronously) and must stay valid
+ * until the request's result is polled. With rgb = 0 they are GRAY8 and
+ * scale_a/scale_b are as in stitch_pair_desc. With rgb = 1 they are RGB8:
+ * the server runs S1 (src/s1/s1.hpp:33-38) at `scale` (0 means 1) on the
+ * device first, registers the working-size GRAY8 images, and returns H in
+ * the original coordinates (scale_a/scale_b are then ignored). `tag` is
+ * returned with the result. */
 typedef struct stitch_request {
     const uint8_t* host_a;
     const uint8_t* host_b;
@@ -322,6 +326,8 @@ typedef struct stitch_request {
     stitch_s4_config s4;
     stitch_s5_config s5;
     stitch_pyramid_config pyramid;
+    int rgb;
+    double scale;
     uint64_t tag;
 } stitch_request;
 

@@ -99,3 +99,53 @@ def test_rejections(reqs):
     assert srv.submit(a[:100, :100].copy(), b[:100, :100].copy(), bad, tag=2) == 1
     assert srv.outstanding() == 0
     srv.close()
+
+
+def test_rgb_requests_run_s1_on_the_device(cuda):
+    """RGB8 requests: the server's S1 + registration equals S1 through the
+    stage call followed by the plain per-pair chain with the same ScaleInfo
+    (H in original coordinates)."""
+    import ctypes as C
+
+    import torch
+
+    from crossstage_stitch_b200 import _abi
+    from crossstage_stitch_b200._abi import ImageView, ScaleInfo
+
+    L = _abi.load()
+    rng = np.random.default_rng(11)
+    cases = []
+    for i, scale in enumerate((1.0, 0.5, 0.75)):
+        p = synth.config0_pair(50 + i)
+        # RGB views whose S1 gray is close to the synthetic gray scene
+        noise = rng.integers(-3, 4, p.gray_a.shape + (3,))
+        a = np.clip(p.gray_a[..., None].astype(int) + noise, 0, 255).astype(np.uint8)
+        b = np.clip(p.gray_b[..., None].astype(int) + noise[::-1], 0, 255).astype(np.uint8)
+        cases.append((a, b, scale, stages.Knobs(max_keypoints=800, seed=500 + i, levels=8)))
+    srv = Server(arena_bytes=1 << 30, max_batch=8, streams=2)
+    for n, (a, b, scale, k) in enumerate(cases):
+        assert srv.submit(a, b, k, tag=n, s1_scale=scale) == 0
+    got = {r["tag"]: r for r in srv.drain()}
+    srv.close()
+    runner = stages.PairRunner(512, 512, 800)
+    for n, (a, b, scale, k) in enumerate(cases):
+        h, w, _ = a.shape
+        ta = torch.from_numpy(a.reshape(h, 3 * w)).cuda()
+        tb = torch.from_numpy(b.reshape(h, 3 * w)).cuda()
+        si_a, si_b = ScaleInfo(), ScaleInfo()
+        assert L.stitch_make_scale_info(w, h, scale, C.byref(si_a)) == 0
+        assert L.stitch_make_scale_info(w, h, scale, C.byref(si_b)) == 0
+        ga = torch.zeros((si_a.work_h, si_a.work_w), dtype=torch.uint8, device="cuda")
+        gb = torch.zeros((si_b.work_h, si_b.work_w), dtype=torch.uint8, device="cuda")
+        va, vb = ImageView(ta.data_ptr(), w, h, ta.stride(0), 0), ImageView(tb.data_ptr(), w, h, tb.stride(0), 0)
+        oa = ImageView(ga.data_ptr(), si_a.work_w, si_a.work_h, ga.stride(0), 1)
+        ob = ImageView(gb.data_ptr(), si_b.work_w, si_b.work_h, gb.stride(0), 1)
+        s2a, s2b = ScaleInfo(), ScaleInfo()
+        assert L.stitch_s1_preprocess(C.byref(va), C.byref(vb), scale, C.byref(oa), C.byref(ob), C.byref(s2a),
+                                      C.byref(s2b), None) == 0
+        torch.cuda.synchronize()
+        runner.enqueue(si_a.work_w, si_a.work_h, si_b.work_w, si_b.work_h, k, scale_a=si_a, scale_b=si_b,
+                       images=(ga, gb))
+        torch.cuda.synchronize()
+        want = stages.result_dict(runner.result)
+        same(got[n], want)
