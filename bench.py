@@ -329,6 +329,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-resolution and served sections")
+    ap.add_argument("--runs-csv", default=None,
+                    help="write the timed plain per-pair runs as rows of the reference harness's runs.csv")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -405,7 +407,7 @@ def main():
 
     # ---- plain per-pair form (drop-in stages, one pair at a time)
     runner = stages.PairRunner(SIZE, SIZE, K, max_r=R, device=dev)
-    lat = []
+    lat, plain_results = [], []
 
     def plain_step(record):
         for i in range(N_PAIRS):
@@ -417,6 +419,7 @@ def main():
             stream.synchronize()
             if record:
                 lat.append(e0.elapsed_time(e1))
+                plain_results.append(stages.result_dict(runner.result))
 
     plain_step(False)
     torch.cuda.synchronize()
@@ -425,6 +428,14 @@ def main():
     stop.record(stream)
     stop.synchronize()
     t_plain = start.elapsed_time(stop)
+    if args.runs_csv and rank == 0:
+        from crossstage_stitch_b200 import runs
+        with open(args.runs_csv, "w") as f:
+            f.write(runs.header())
+            for i, (res, ms) in enumerate(zip(plain_results, lat)):
+                f.write(runs.row(runs.record_from_result(res, f"synthetic_{rank * N_PAIRS + i}", knobs[i], S=1.0,
+                                                         run_id="bench", dataset="synthetic", t_e2e=ms,
+                                                         num_levels=LEVELS)))
     lat.sort()
 
     mixed_res = served_res = None
