@@ -434,8 +434,7 @@ def main():
             f.write(runs.header())
             for i, (res, ms) in enumerate(zip(plain_results, lat)):
                 f.write(runs.row(runs.record_from_result(res, f"synthetic_{rank * N_PAIRS + i}", knobs[i], S=1.0,
-                                                         run_id="bench", dataset="synthetic", t_e2e=ms,
-                                                         num_levels=LEVELS)))
+                                                         run_id="bench", dataset="synthetic", t_e2e=ms)))
     lat.sort()
 
     mixed_res = served_res = None
