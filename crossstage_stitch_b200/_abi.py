@@ -146,6 +146,9 @@ PROTOTYPES: dict[str, tuple] = {
     "stitch_pyramid_workspace_bytes": (C.c_int, [C.c_int, C.c_int, P(S2Config), P(PyramidConfig), _size_p]),
     "stitch_pyramid_detect_describe": (C.c_int, [P(ImageView), P(S2Config), P(PyramidConfig), P(Keypoints),
                                                  P(Descriptors), C.c_void_p, C.c_size_t, C.c_void_p]),
+    "stitch_s4_set_matcher": (C.c_int, [C.c_int]),
+    "stitch_s4_matcher": (C.c_int, []),
+    "stitch_s4_tc_errors": (C.c_int, []),
     "stitch_s4_workspace_bytes": (C.c_int, [C.c_int, C.c_int, P(S4Config), _size_p]),
     "stitch_s4_knn_top2": (C.c_int, [P(Keypoints), P(Descriptors), P(Keypoints), P(Descriptors), C.c_void_p,
                                      C.c_void_p]),

@@ -464,9 +464,15 @@ Status Plan::enqueue(void* ws, std::size_t bytes, stitch_homography_result* host
 
     using KnnSrc = s4k::JobTable<KnnJob>;
     const auto* kjobs = reinterpret_cast<const KnnJob*>(T + offsets[kKnnJobs]);
-    if (go(knn_blocks))
-        s4k::knn_popc_kernel<KnnSrc, s4k::kQueriesPerThread><<<knn_blocks, s4k::kQueryThreads, 0, s>>>(
-            KnnSrc{kjobs, reinterpret_cast<const int*>(T + offsets[kKnnPrefix]), n_knn});
+    if (go(knn_blocks)) {
+        const KnnSrc ks{kjobs, reinterpret_cast<const int*>(T + offsets[kKnnPrefix]), n_knn};
+        if (s4k::matcher() == s4k::kMatcherTensor) {
+            if (!s4k::enable_tc_smem<KnnSrc>()) return Status::CUDA_ERROR;
+            s4k::knn_tc_kernel<KnnSrc><<<knn_blocks, s4k::kQueryThreads, s4k::kTcSmem, s>>>(ks);
+        } else {
+            s4k::knn_popc_kernel<KnnSrc, s4k::kQueriesPerThread><<<knn_blocks, s4k::kQueryThreads, 0, s>>>(ks);
+        }
+    }
     mark();
     if (go(merge_blocks))
         s4k::knn_merge_kernel<KnnSrc><<<merge_blocks, 256, 0, s>>>(
@@ -502,6 +508,16 @@ Status Plan::enqueue(void* ws, std::size_t bytes, stitch_homography_result* host
 }
 
 }  // namespace stitch::b200::batch
+
+namespace stitch::b200::s4k {
+int take_batch_tc_error() {
+    int v = 0;
+    if (cudaMemcpyFromSymbol(&v, g_tc_error, sizeof(int)) != cudaSuccess) return -1;
+    const int zero = 0;
+    if (v && cudaMemcpyToSymbol(g_tc_error, &zero, sizeof(int)) != cudaSuccess) return -1;
+    return v;
+}
+}  // namespace stitch::b200::s4k
 
 using stitch::Status;
 using stitch::b200::batch::Plan;

@@ -6,6 +6,7 @@
 // Top2 array sits at offset 0 of the workspace, where s4_forward_neighbors
 // exposes it to later consumers.
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <limits>
 
@@ -94,6 +95,12 @@ KnnJob make_knn_job(const Keypoints& qk, const Descriptors& qd, const Keypoints&
 }
 
 namespace {
+std::atomic<int> g_matcher{kMatcherPopc};
+}  // namespace
+
+int matcher() { return g_matcher.load(std::memory_order_relaxed); }
+
+namespace {
 
 // One direction of the exact top-2 search into `out` (capacity of the query
 // side entries); partial may be null only when the plan has one split.
@@ -104,7 +111,12 @@ Status launch_direction(const Keypoints& qk, const Descriptors& qd, const Keypoi
     if (popc_eligible(qd, td, tk.capacity)) {
         using Src = OneJob<KnnJob>;
         const Src src{make_knn_job(qk, qd, tk, td, q_tiles, splits, rows, partial, out)};
-        knn_popc_kernel<Src, 1><<<q_tiles * splits, kQueryThreads, 0, stream>>>(src);
+        if (matcher() == kMatcherTensor) {
+            if (!enable_tc_smem<Src>()) return Status::CUDA_ERROR;
+            knn_tc_kernel<Src><<<q_tiles * splits, kQueryThreads, kTcSmem, stream>>>(src);
+        } else {
+            knn_popc_kernel<Src, 1><<<q_tiles * splits, kQueryThreads, 0, stream>>>(src);
+        }
         if (splits > 1) knn_merge_kernel<Src><<<ceil_div(qk.capacity, 256), 256, 0, stream>>>(src);
         note_launches(splits > 1 ? 2 : 1);
     } else {
@@ -207,3 +219,26 @@ Status s4_forward_neighbors(int capacity_a, int capacity_b, const Config& config
 }
 
 }  // namespace stitch::s4
+
+extern "C" {
+
+int stitch_s4_set_matcher(int kind) {
+    using namespace stitch::b200::s4k;
+    if (kind != kMatcherPopc && kind != kMatcherTensor) return static_cast<int>(stitch::Status::INVALID_ARGUMENT);
+    g_matcher.store(kind, std::memory_order_relaxed);
+    return 0;
+}
+
+int stitch_s4_matcher(void) { return stitch::b200::s4k::matcher(); }
+
+int stitch_s4_tc_errors(void) {
+    using namespace stitch::b200::s4k;
+    int mine = 0;
+    if (cudaMemcpyFromSymbol(&mine, g_tc_error, sizeof(int)) != cudaSuccess) return -1;
+    const int zero = 0;
+    if (mine && cudaMemcpyToSymbol(g_tc_error, &zero, sizeof(int)) != cudaSuccess) return -1;
+    const int batch = take_batch_tc_error();
+    return batch < 0 ? -1 : (mine | batch);
+}
+
+}  // extern "C"

@@ -1,6 +1,8 @@
 // S4 layout and job builders shared by the per-pair call and the batched chain.
 #pragma once
 
+#include <mutex>
+
 #include "s4_kernels.cuh"
 
 namespace stitch::b200::s4k {
@@ -14,6 +16,28 @@ struct MatchLayout {
 bool valid_side(const Keypoints& k, const Descriptors& d);
 bool valid_pair(const Keypoints& a, const Descriptors& da, const Keypoints& b, const Descriptors& db);
 bool popc_eligible(const Descriptors& q, const Descriptors& t, int capacity_train);
+
+// Binary matcher used by every S4 launch of this process: kMatcherPopc (the
+// __popc tile kernel) or kMatcherTensor (tcgen05 kind::i8). Results are
+// identical; the choice only changes speed.
+constexpr int kMatcherPopc = 0, kMatcherTensor = 1;
+int matcher();
+// Opts the tensor-core kernel for a job source in to its shared memory
+// (once per device); false if the device refuses.
+template <class Src> bool enable_tc_smem() {
+    static std::once_flag flags[64];
+    static bool ok[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return false;
+    std::call_once(flags[dev], [&] {
+        ok[dev] = cudaFuncSetAttribute(knn_tc_kernel<Src>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem) ==
+                  cudaSuccess;
+    });
+    return ok[dev];
+}
+// Reads and clears the tensor-core error word of the batched chain's
+// translation unit (batch.cu).
+int take_batch_tc_error();
 void plan_split(int capacity_q, int capacity_t, int* q_tiles, int* splits, int* rows_per_split);
 bool match_layout(int capacity_a, int capacity_b, bool cross, MatchLayout* out);
 KnnJob make_knn_job(const Keypoints& qk, const Descriptors& qd, const Keypoints& tk, const Descriptors& td,

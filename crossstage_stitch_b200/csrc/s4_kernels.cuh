@@ -164,6 +164,191 @@ __global__ __launch_bounds__(kQueryThreads) void knn_popc_kernel(const __grid_co
     }
 }
 
+// ------------------------------------------------- tensor-core matcher
+//
+// Exact Hamming distance on the 5th-generation tensor cores: every
+// descriptor bit b becomes the int8 value +1 (b = 1) or -1 (b = 0), so for
+// two 256-bit descriptors dot = 256 - 2 * Hamming, and tcgen05.mma
+// kind::i8 (int32 accumulation, exact) gives dot for a 128-query x
+// 256-train tile in TMEM. The block walks the same train partition as the
+// popc kernel; each query's thread reads its row of dot products back with
+// tcgen05.ld and keeps the two smallest (distance << 23 | train index)
+// keys, so results equal knn_popc_kernel's bit for bit.
+//
+// Shared memory holds the expanded queries (128 rows x 256 bytes) and one
+// train stage (256 rows x 256 bytes) in the K-major 128-byte-swizzle layout
+// tcgen05 reads: per 128-byte K block, 8-row groups of 1024 bytes, 16-byte
+// chunk c of row r stored at chunk c ^ (r % 8).
+constexpr int kTcRowsA = kQueryThreads;       // 128 queries (MMA M)
+constexpr int kTcRowsB = kTrainStage;         // 256 train rows (MMA N)
+constexpr int kTcBytesA = kTcRowsA * 256, kTcBytesB = kTcRowsB * 256;
+constexpr int kTcSmem = kTcBytesA + kTcBytesB + 1024 + 64;  // + alignment slack + barrier/slot
+constexpr long long kTcWaitLimit = 1ll << 26;  // mbarrier polls before giving up
+
+// Error word of the tensor-core matcher (one per translation unit): set when
+// an MMA completion wait runs out (the block then stops, frees its TMEM and
+// leaves its outputs unwritten).
+static __device__ int g_tc_error;
+
+__device__ __forceinline__ std::uint32_t smem_u32(const void* p) {
+    return static_cast<std::uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Bits 0..3 of n as the int8 values +1 / -1 in bytes 0..3.
+__device__ __forceinline__ std::uint32_t pm_one4(std::uint32_t n) {
+    const std::uint32_t spread = (n * 0x00204081u) & 0x01010101u;
+    return 0x01010101u | ((spread ^ 0x01010101u) * 0xFEu);
+}
+
+// Writes descriptor row `row` (32 bytes at src; zeros when src is null) of
+// a tile of `rows` rows into the swizzled layout at `tile`.
+__device__ __forceinline__ void stage_pm_row(std::uint8_t* tile, int rows, int row, const std::uint8_t* src) {
+    uint4 w[2] = {make_uint4(0, 0, 0, 0), make_uint4(0, 0, 0, 0)};
+    if (src) {
+        w[0] = reinterpret_cast<const uint4*>(src)[0];
+        w[1] = reinterpret_cast<const uint4*>(src)[1];
+    }
+    const std::uint32_t words[8] = {w[0].x, w[0].y, w[0].z, w[0].w, w[1].x, w[1].y, w[1].z, w[1].w};
+    std::uint8_t* base = tile + (row >> 3) * 1024 + (row & 7) * 128;
+#pragma unroll
+    for (int h = 0; h < 16; ++h) {  // 16 descriptor bits -> one 16-byte chunk
+        const std::uint32_t bits = (words[h >> 1] >> (16 * (h & 1))) & 0xffffu;
+        const int kb = h >> 3, c = h & 7;
+        uint4 v;
+        v.x = src ? pm_one4(bits & 0xf) : 0u;
+        v.y = src ? pm_one4((bits >> 4) & 0xf) : 0u;
+        v.z = src ? pm_one4((bits >> 8) & 0xf) : 0u;
+        v.w = src ? pm_one4((bits >> 12) & 0xf) : 0u;
+        *reinterpret_cast<uint4*>(base + kb * rows * 128 + ((c ^ (row & 7)) << 4)) = v;
+    }
+}
+
+// Shared-memory matrix descriptor: K-major, 128-byte swizzle, 8-row groups
+// 1024 bytes apart (SBO), version 1.
+__device__ __forceinline__ std::uint64_t sw128_desc(std::uint32_t addr) {
+    return static_cast<std::uint64_t>((addr >> 4) & 0x3fffu) | (1ull << 16) | (64ull << 32) | (1ull << 46) |
+           (2ull << 61);
+}
+
+// kind::i8 instruction descriptor: s32 accumulator, signed A and B, both
+// K-major, N = 256, M = 128.
+constexpr std::uint32_t kTcIdesc = (2u << 4) | (1u << 7) | (1u << 10) | ((kTcRowsB >> 3) << 17) | ((kTcRowsA >> 4) << 24);
+
+template <class Src>
+__global__ __launch_bounds__(kQueryThreads, 1) void knn_tc_kernel(const __grid_constant__ Src src) {
+    extern __shared__ std::uint8_t dyn[];
+    KnnJob j;
+    int local;
+    if (!src.find(blockIdx.x, &j, &local)) return;
+    std::uint8_t* tileA = reinterpret_cast<std::uint8_t*>((reinterpret_cast<std::uintptr_t>(dyn) + 1023) & ~std::uintptr_t(1023));
+    std::uint8_t* tileB = tileA + kTcBytesA;
+    auto* bar = reinterpret_cast<std::uint64_t*>(tileB + kTcBytesB);
+    auto* tmem_slot = reinterpret_cast<std::uint32_t*>(bar + 1);
+    auto* stop = reinterpret_cast<int*>(tmem_slot + 1);
+    const int tid = threadIdx.x, warp = tid >> 5;
+    const int qt = local % j.q_tiles, split = local / j.q_tiles;
+    int nq, nt;
+    const bool ok = counts_valid(j, &nq, &nt);
+    const int t0 = split * j.rows_per_split;
+    const int t1 = ok ? min(nt, t0 + j.rows_per_split) : t0;
+    const int q = qt * kTcRowsA + tid;
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(kTcRowsB));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        *stop = 0;
+    }
+    stage_pm_row(tileA, kTcRowsA, tid,
+                 ok && q < nq ? j.query.rows + static_cast<std::size_t>(q) * j.query.stride : nullptr);
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const std::uint32_t tmem = *tmem_slot;
+    std::uint32_t k1 = kEmptyKey, k2 = kEmptyKey;
+    std::uint32_t phase = 0;
+    for (int base = t0; base < t1; base += kTcRowsB) {
+        for (int r = tid; r < kTcRowsB; r += kQueryThreads)
+            stage_pm_row(tileB, kTcRowsB, r,
+                         base + r < t1 ? j.train.rows + static_cast<std::size_t>(base + r) * j.train.stride : nullptr);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            const std::uint32_t a0 = smem_u32(tileA), b0 = smem_u32(tileB);
+#pragma unroll
+            for (int s = 0; s < 8; ++s) {  // K = 256 in slices of 32 bytes
+                const std::uint32_t koff = (s & 3) * 32;  // within the 128-byte swizzle atom
+                const std::uint64_t da = sw128_desc(a0 + (s >> 2) * kTcRowsA * 128 + koff);
+                const std::uint64_t db = sw128_desc(b0 + (s >> 2) * kTcRowsB * 128 + koff);
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
+                    "l"(da), "l"(db), "r"(kTcIdesc), "r"(s));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_u32(bar))
+                         : "memory");
+        }
+        // bounded wait for the MMA chain of this stage
+        std::uint32_t done = 0;
+        for (long long it = 0; it < kTcWaitLimit && !done; ++it) {
+            asm volatile(
+                "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                "selp.u32 %0, 1, 0, p;\n\t}\n"
+                : "=r"(done)
+                : "r"(smem_u32(bar)), "r"(phase)
+                : "memory");
+        }
+        if (!done) *stop = 1;
+        __syncthreads();
+        if (*stop) break;
+        phase ^= 1u;
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        // this thread's query row: 256 dot products in 8 loads of 32 columns
+#pragma unroll 1
+        for (int c = 0; c < kTcRowsB; c += 32) {
+            std::uint32_t v[32];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
+                "[%32];"
+                : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                  "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                  "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+                  "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+                  "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                : "r"(tmem + (static_cast<std::uint32_t>(warp * 32) << 16) + static_cast<std::uint32_t>(c)));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int i = 0; i < 32; ++i) {
+                const int t = base + c + i;
+                // (256 - dot) = 2 * Hamming, so its << 22 is the distance << 23
+                const std::uint32_t key = ((256u - v[i]) << 22) | static_cast<std::uint32_t>(t);
+                if (t < t1) keep2(k1, k2, key);
+            }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;");
+        __syncthreads();  // TMEM and the train stage are free for the next stage
+    }
+    const bool failed = *stop != 0;
+    if (failed && tid == 0) atomicExch(&g_tc_error, 1);
+    if (!failed && q < j.query.capacity) {
+        const bool active = ok && q < nq;
+        const std::uint32_t a1 = active ? k1 : kEmptyKey, a2 = active ? k2 : kEmptyKey;
+        if (j.splits == 1) {
+            j.top2[q] = top2_from_keys(a1, a2);
+        } else {
+            j.partial[static_cast<std::size_t>(split) * j.query.capacity + q] = make_uint2(a1, a2);
+        }
+    }
+    __syncthreads();
+    if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcRowsB));
+}
+
 // Thread per query: the two smallest keys over all train partitions.
 template <class Src>
 __global__ __launch_bounds__(256) void knn_merge_kernel(const __grid_constant__ Src src) {

@@ -198,6 +198,16 @@ int stitch_pyramid_detect_describe(const stitch_image_view* image, const stitch_
 
 /* ------------------------------------------------------------------- S4 */
 
+/* No reference counterpart. Chooses the exact binary matcher every later S4
+ * launch of this process uses (stitch_s4_* calls and the batched and served
+ * forms): 0 the __popc tile kernel, 1 the tcgen05 kind::i8 tensor-core
+ * kernel (descriptor bits as +-1 int8, Hamming = (256 - dot) / 2). Results
+ * are identical. stitch_s4_tc_errors reads and clears the tensor-core
+ * kernel's error word (1: an MMA completion wait ran out; -1: read failed). */
+int stitch_s4_set_matcher(int kind);
+int stitch_s4_matcher(void);
+int stitch_s4_tc_errors(void);
+
 /* src/s4/s4.hpp:25-26 (stitch::s4::s4_workspace_bytes). */
 int stitch_s4_workspace_bytes(int capacity_a, int capacity_b, const stitch_s4_config* config,
                               size_t* bytes);
