@@ -302,6 +302,75 @@ def run_served(mixed, dev):
             "request_pool": f"{len(pool)} mixed-resolution pairs, per-request S5 seeds", "rates": out}
 
 
+def planted_descriptors(nq, nt, seed):
+    """Uniform 256-bit rows; 30 % of queries get a planted partner at
+    Binomial(256, 0.05) distance, 5 % a second one at the same distance."""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    q = rng.integers(0, 256, (nq, 32), dtype=np.uint8)
+    t = rng.integers(0, 256, (nt, 32), dtype=np.uint8)
+    for qi in rng.choice(nq, size=int(0.3 * nq), replace=False):
+        d = rng.binomial(256, 0.05)
+        for _ in range(2 if rng.random() < 0.05 / 0.3 else 1):
+            row = np.unpackbits(q[qi]).copy()
+            row[rng.choice(256, size=d, replace=False)] ^= 1
+            t[rng.integers(0, nt)] = np.packbits(row)
+    return q, t
+
+
+def run_matching(dev, reps=20):
+    """Matching microbenchmark: 8192 x 8192 planted 256-bit descriptors, the
+    exact top-2 (s4_knn_top2) with the __popc kernel and with the tcgen05
+    kind::i8 kernel; both must agree bit for bit."""
+    import ctypes as C
+    import torch
+    from crossstage_stitch_b200 import _abi, synth
+    from crossstage_stitch_b200._abi import Descriptors, Keypoints
+    L = _abi.load()
+    n = 8192
+    q, t = planted_descriptors(n, n, synth.BASE_SEED)
+    dq, dt = torch.from_numpy(q).to(dev), torch.from_numpy(t).to(dev)
+    cnt = torch.tensor([n], dtype=torch.int32, device=dev)
+    kq = Keypoints(0, 0, 0, n, cnt.data_ptr())
+    kt = Keypoints(0, 0, 0, n, cnt.data_ptr())
+    Dq, Dt = Descriptors(0, 32, 32, dq.data_ptr()), Descriptors(0, 32, 32, dt.data_ptr())
+    out = {}
+    tops = {}
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    before = L.stitch_s4_matcher()
+    for name, kind in (("popc", 0), ("tensor", 1)):
+        assert L.stitch_s4_set_matcher(kind) == 0
+        top = torch.zeros((n, 24), dtype=torch.uint8, device=dev)
+        call = lambda: L.stitch_s4_knn_top2(C.byref(kq), C.byref(Dq), C.byref(kt), C.byref(Dt),
+                                            C.c_void_p(top.data_ptr()), C.c_void_p(stream.cuda_stream))
+        for _ in range(3):
+            assert call() == 0
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(reps):
+            call()
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / reps
+        tops[name] = top.cpu()
+        out[name] = {"ms": ms, "pairs_per_s": n * n / (ms / 1e3)}
+    L.stitch_s4_set_matcher(before)
+    errors = L.stitch_s4_tc_errors()
+    peaks = json.loads(PEAKS.read_text()) if PEAKS.exists() else {}
+    int_peak = 148 * 64 * 1.965e9 * 3 / 1e12
+    out["popc"].update(achieved=24.0 * n * n / (out["popc"]["ms"] / 1e3) / 1e12, unit="Tops/s", peak=int_peak,
+                       peak_source="nominal INT32 issue rate (64 lanes x 3 ops/clk/SM)")
+    t_peak = 2 * peaks.get("bf16_tflops", 1590.0)
+    out["tensor"].update(achieved=512.0 * n * n / (out["tensor"]["ms"] / 1e3) / 1e12, unit="Tops/s", peak=t_peak,
+                         peak_source="dense int8 = 2 x measured bf16 burst")
+    for v in out.values():
+        v["frac"] = v["achieved"] / v["peak"]
+    return {"workload": "8192 x 8192 planted 256-bit descriptors, exact kNN-2 (one direction)",
+            "bit_exact": bool(torch.equal(tops["popc"], tops["tensor"])), "tc_errors": errors,
+            "chosen": "tensor" if out["tensor"]["ms"] < out["popc"]["ms"] else "popc", **out}
+
+
 def algorithmic_work(batch, n_pairs, counts):
     """Per-kernel algorithmic work of one step (bytes for pixel kernels,
     ops for matching and estimation), from the actual keypoint and match
@@ -316,7 +385,8 @@ def algorithmic_work(batch, n_pairs, counts):
         "fast_nms": ("hbm", 2.0 * px, "GB/s"),           # image read + maxima write
         "select_scatter": ("hbm", 2.0 * px, "GB/s"),     # maxima read twice
         "blur": ("hbm", 2.0 * px, "GB/s"),               # image read + blurred write
-        "knn_popc": ("int", 24.0 * knn_pairs, "Tops/s"),  # 8 XOR + 8 POPC + 8 ADD per row pair
+        # descriptor pairs x 256 int8 MACs (2 ops each) on the tensor cores
+        "knn": ("tensor", 512.0 * knn_pairs, "Tops/s"),
         "search": ("fp64", 25.0 * resid + 2000.0 * R * n_pairs, "TFLOP/s"),
     }
 
@@ -437,6 +507,7 @@ def main():
                                                          run_id="bench", dataset="synthetic", t_e2e=ms)))
     lat.sort()
 
+    matching = run_matching(dev) if rank == 0 else None
     mixed_res = served_res = None
     if mixed is not None:
         mixed_res = run_mixed(mixed, max(3, args.steps // 2), args.warmup, dev, flush)
@@ -465,6 +536,8 @@ def main():
             achieved = amount / (kern[dominant] / 1e3) / (1e9 if unit == "GB/s" else 1e12)
             if bound == "hbm":
                 peak, src = peaks.get("hbm_gbs", 6650.0), ("measured" if "hbm_gbs" in peaks else "fallback")
+            elif bound == "tensor":
+                peak, src = 2 * peaks.get("bf16_tflops", 1590.0), "dense int8 = 2 x measured bf16 burst"
             elif bound == "fp64":
                 peak, src = 37.0, "nominal B200 FP64 (no measured FP64 peak on this pool)"
             else:
@@ -491,7 +564,7 @@ def main():
                 "keypoints_mean": statistics.mean(a + b_ for a, b_, _ in counts) / 2,
                 "matches_mean": statistics.mean(m for _, _, m in counts),
                 "gpu_launches": launches, "clocks": clk, "roofline": roof, "cpu_baseline": cpu,
-                "mixed": mixed_res, "served": served_res}
+                "matching": matching, "mixed": mixed_res, "served": served_res}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

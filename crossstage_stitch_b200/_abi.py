@@ -177,7 +177,7 @@ PROTOTYPES: dict[str, tuple] = {
     "stitch_server_destroy": (None, [C.c_void_p]),
 }
 
-BATCH_MARKS = ("tables", "pyramid", "fast_nms", "select_scatter", "harris", "sort_topk", "blur", "describe", "knn_popc",
+BATCH_MARKS = ("tables", "pyramid", "fast_nms", "select_scatter", "harris", "sort_topk", "blur", "describe", "knn",
                "knn_merge", "accept", "prepare", "search", "finish")
 
 _LIB: C.CDLL | None = None

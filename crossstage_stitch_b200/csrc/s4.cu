@@ -95,7 +95,9 @@ KnnJob make_knn_job(const Keypoints& qk, const Descriptors& qd, const Keypoints&
 }
 
 namespace {
-std::atomic<int> g_matcher{kMatcherPopc};
+// The tensor-core matcher measured 2.7x faster than __popc on the batched
+// 64-pair workload (0.139 vs 0.375 ms per step), so it is the default.
+std::atomic<int> g_matcher{kMatcherTensor};
 }  // namespace
 
 int matcher() { return g_matcher.load(std::memory_order_relaxed); }

@@ -200,9 +200,9 @@ int stitch_pyramid_detect_describe(const stitch_image_view* image, const stitch_
 
 /* No reference counterpart. Chooses the exact binary matcher every later S4
  * launch of this process uses (stitch_s4_* calls and the batched and served
- * forms): 0 the __popc tile kernel, 1 the tcgen05 kind::i8 tensor-core
- * kernel (descriptor bits as +-1 int8, Hamming = (256 - dot) / 2). Results
- * are identical. stitch_s4_tc_errors reads and clears the tensor-core
+ * forms): 0 the __popc tile kernel, 1 (the default) the tcgen05 kind::i8
+ * tensor-core kernel (descriptor bits as +-1 int8, Hamming = (256 - dot) /
+ * 2). Results are identical. stitch_s4_tc_errors reads and clears the tensor-core
  * kernel's error word (1: an MMA completion wait ran out; -1: read failed). */
 int stitch_s4_set_matcher(int kind);
 int stitch_s4_matcher(void);
@@ -297,7 +297,8 @@ void stitch_batch_destroy(stitch_batch* plan);
  * event marks, src/s2_s3/s2_s3_marks.hpp:16-34): `events` holds
  * STITCH_BATCH_MARKS cudaEvent_t recorded, in order, after the table upload,
  * the pyramid resize chain, fast_nms, select+scatter, harris, sort, blur,
- * describe, knn_popc, knn_merge, accept, prepare, search and finish kernels
+ * describe, knn (tensor-core or popc matcher), knn_merge, accept, prepare,
+ * search and finish kernels
  * (a skipped kernel still records its mark). Applies to later enqueues and
  * captures; NULL turns the marks off. */
 #define STITCH_BATCH_MARKS 14

@@ -16,7 +16,13 @@ pytestmark = pytest.mark.gpu
 
 @pytest.fixture(scope="module")
 def ours(cuda):
-    return G.Lib("ours")
+    """The __popc matcher (the tensor-core one has its own module)."""
+    from crossstage_stitch_b200 import _abi
+    L = _abi.load()
+    before = L.stitch_s4_matcher()
+    assert L.stitch_s4_set_matcher(0) == 0
+    yield G.Lib("ours")
+    L.stitch_s4_set_matcher(before)
 
 
 def check(lib, a, b, ratio=0.8, cross=False, ca=None, cb=None, l2=False, pad_a=3, pad_b=7):
