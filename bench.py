@@ -399,6 +399,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-resolution and served sections")
+    ap.add_argument("--only", choices=["matching"], default=None,
+                    help="run only the matching microbenchmark (popc vs tensor cores) and print its JSON")
     ap.add_argument("--runs-csv", default=None,
                     help="write the timed plain per-pair runs as rows of the reference harness's runs.csv")
     args = ap.parse_args()
@@ -408,6 +410,12 @@ def main():
     if args.impl == "reference":
         if rank == 0:
             run_reference(args)
+        return
+
+    if args.only == "matching":
+        import torch
+        torch.cuda.set_device(local)
+        print(json.dumps(run_matching(torch.device("cuda", local), reps=args.steps)), flush=True)
         return
 
     cpu = None
