@@ -268,7 +268,10 @@ __global__ __launch_bounds__(kQueryThreads, 1) void knn_tc_kernel(const __grid_c
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     const std::uint32_t tmem = *tmem_slot;
-    std::uint32_t k1 = kEmptyKey, k2 = kEmptyKey;
+    // four independent (smallest, second) key pairs, merged at the end: keys
+    // are distinct (they carry the train index), so the merge is exact
+    std::uint32_t k1[4] = {kEmptyKey, kEmptyKey, kEmptyKey, kEmptyKey};
+    std::uint32_t k2[4] = {kEmptyKey, kEmptyKey, kEmptyKey, kEmptyKey};
     std::uint32_t phase = 0;
     for (int base = t0; base < t1; base += kTcRowsB) {
         for (int r = tid; r < kTcRowsB; r += kQueryThreads)
@@ -323,12 +326,15 @@ __global__ __launch_bounds__(kQueryThreads, 1) void knn_tc_kernel(const __grid_c
                   "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
                 : "r"(tmem + (static_cast<std::uint32_t>(warp * 32) << 16) + static_cast<std::uint32_t>(c)));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            // (256 - dot) = 2 * Hamming, so (256 - dot) << 22 is the distance << 23
+            const std::uint32_t t = static_cast<std::uint32_t>(base + c);
+            if (base + c + 32 <= t1) {
 #pragma unroll
-            for (int i = 0; i < 32; ++i) {
-                const int t = base + c + i;
-                // (256 - dot) = 2 * Hamming, so its << 22 is the distance << 23
-                const std::uint32_t key = ((256u - v[i]) << 22) | static_cast<std::uint32_t>(t);
-                if (t < t1) keep2(k1, k2, key);
+                for (int i = 0; i < 32; ++i) keep2(k1[i & 3], k2[i & 3], ((256u - v[i]) << 22) + (t + i));
+            } else {
+#pragma unroll
+                for (int i = 0; i < 32; ++i)
+                    if (base + c + i < t1) keep2(k1[i & 3], k2[i & 3], ((256u - v[i]) << 22) + (t + i));
             }
         }
         asm volatile("tcgen05.fence::before_thread_sync;");
@@ -336,9 +342,14 @@ __global__ __launch_bounds__(kQueryThreads, 1) void knn_tc_kernel(const __grid_c
     }
     const bool failed = *stop != 0;
     if (failed && tid == 0) atomicExch(&g_tc_error, 1);
+#pragma unroll
+    for (int u = 1; u < 4; ++u) {
+        keep2(k1[0], k2[0], k1[u]);
+        keep2(k1[0], k2[0], k2[u]);
+    }
     if (!failed && q < j.query.capacity) {
         const bool active = ok && q < nq;
-        const std::uint32_t a1 = active ? k1 : kEmptyKey, a2 = active ? k2 : kEmptyKey;
+        const std::uint32_t a1 = active ? k1[0] : kEmptyKey, a2 = active ? k2[0] : kEmptyKey;
         if (j.splits == 1) {
             j.top2[q] = top2_from_keys(a1, a2);
         } else {
