@@ -109,13 +109,13 @@ class Request(C.Structure):
                 ("width_b", C.c_int), ("height_b", C.c_int), ("pitch_b", C.c_int),
                 ("scale_a", ScaleInfo), ("scale_b", ScaleInfo), ("s2", S2Config), ("s4", S4Config),
                 ("s5", S5Config), ("pyramid", PyramidConfig), ("rgb", C.c_int), ("scale", C.c_double),
-                ("tag", C.c_uint64)]
+                ("retry_hypotheses", C.c_int), ("retry_min_inliers", C.c_int), ("tag", C.c_uint64)]
 
 
 class ServerResult(C.Structure):
     """stitch_server_result."""
     _fields_ = [("tag", C.c_uint64), ("submit_ms", C.c_double), ("launch_ms", C.c_double),
-                ("done_ms", C.c_double), ("batch_pairs", C.c_int), ("status", C.c_int),
+                ("done_ms", C.c_double), ("batch_pairs", C.c_int), ("status", C.c_int), ("attempts", C.c_int),
                 ("result", HomographyResult)]
 
 

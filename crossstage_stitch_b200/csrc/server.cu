@@ -137,8 +137,11 @@ struct Slot {
     std::unique_ptr<Plan> plan;
     std::vector<Request> reqs;
     std::size_t offset = 0, bytes = 0;
+    std::size_t ws_offset = 0;   // batch workspace inside the region
     double launch_ms = 0.0;
     bool busy = false;
+    bool retrying = false;       // the S5 extension retries are on the stream
+    std::vector<int> attempts;   // per request
 };
 
 // Pair descriptor of a request whose registered (GRAY8) images start at
@@ -264,17 +267,63 @@ private:
             r.done_ms = t;
             r.batch_pairs = static_cast<int>(s.reqs.size());
             r.status = static_cast<int>(launch_status);
+            r.attempts = i < s.attempts.size() ? s.attempts[i] : 1;
             if (launch_status == Status::OK) r.result = s.results[i];
             out.push_back(r);
         }
         if (s.bytes) arena_.release(s.offset, s.bytes);
         s.plan.reset();
         s.reqs.clear();
+        s.attempts.clear();
         s.bytes = 0;
         s.busy = false;
+        s.retrying = false;
         std::lock_guard<std::mutex> g(mu_);
         done_.insert(done_.end(), out.begin(), out.end());
         outstanding_ -= static_cast<int>(out.size());
+    }
+
+    // After a batch completes: requests whose result falls short of their
+    // retry bar get their saved S5 search extended to retry_hypotheses on the
+    // batch's resident buffers (src/controller/reuse.cpp:5-22). Returns true
+    // when work was enqueued (the slot stays busy until it completes).
+    bool retry(Slot& s) {
+        bool any = false;
+        auto* ws = static_cast<unsigned char*>(cfg_.arena) + s.offset + s.ws_offset;
+        for (std::size_t i = 0; i < s.reqs.size(); ++i) {
+            const stitch_request& r = s.reqs[i].r;
+            const stitch_homography_result& res = s.results[i];
+            if (r.retry_hypotheses <= r.s5.hypotheses) continue;
+            if (res.status == static_cast<int>(Status::OK) && res.num_inliers >= r.retry_min_inliers) continue;
+            if (res.status == static_cast<int>(Status::INVALID_ARGUMENT) ||
+                res.status == static_cast<int>(Status::NOT_ENOUGH_POINTS))
+                continue;  // no saved search to extend
+            const auto& o = s.plan->off[i];
+            const auto& q = s.plan->pairs[i];
+            const int k = q.s2.max_keypoints;
+            auto at = [&](std::size_t off) { return ws + off; };
+            const Keypoints ka{reinterpret_cast<float*>(at(o.kx[0])), reinterpret_cast<float*>(at(o.ky[0])),
+                               reinterpret_cast<float*>(at(o.kr[0])), k, reinterpret_cast<int*>(at(o.kcount[0]))};
+            const Keypoints kb{reinterpret_cast<float*>(at(o.kx[1])), reinterpret_cast<float*>(at(o.ky[1])),
+                               reinterpret_cast<float*>(at(o.kr[1])), k, reinterpret_cast<int*>(at(o.kcount[1]))};
+            const Matches m{reinterpret_cast<std::int32_t*>(at(o.ia)), reinterpret_cast<std::int32_t*>(at(o.ib)),
+                            reinterpret_cast<float*>(at(o.dist)), k, reinterpret_cast<int*>(at(o.mcount))};
+            s5::Config c = *reinterpret_cast<const s5::Config*>(&q.s5);
+            c.previous_hypotheses = c.hypotheses;
+            c.hypotheses = r.retry_hypotheses;
+            const Status st = s5::estimate(ka, kb, m, *reinterpret_cast<const ScaleInfo*>(&q.scale_a),
+                                           *reinterpret_cast<const ScaleInfo*>(&q.scale_b), c, at(o.mask),
+                                           reinterpret_cast<HomographyResult*>(&s.results[i]), at(o.s5ws),
+                                           b200::s5k::estimate_workspace_bytes(), s.stream);
+            if (st != Status::OK) continue;  // keep the first result
+            s.attempts[i] = 2;
+            any = true;
+        }
+        if (any && cudaEventRecord(s.done, s.stream) != cudaSuccess) {
+            cudaStreamSynchronize(s.stream);
+            return false;
+        }
+        return any;
     }
 
     // Forms a batch from the head of the queue and launches it on slot s.
@@ -347,6 +396,8 @@ private:
             pending_.erase(pending_.begin(), pending_.begin() + n);
             s.offset = off;
             s.bytes = bytes;
+            s.ws_offset = images;
+            s.attempts.assign(n, 1);
             s.launch_ms = now_ms();
             s.busy = true;
             Status st = Status::OK;
@@ -422,6 +473,13 @@ private:
             bool progressed = false;
             for (auto& s : slots_) {
                 if (s.busy && cudaEventQuery(s.done) == cudaSuccess) {
+                    if (!s.retrying) {
+                        s.retrying = true;
+                        if (retry(s)) {
+                            progressed = true;
+                            continue;
+                        }
+                    }
                     finish(s, Status::OK);
                     progressed = true;
                 }

@@ -41,10 +41,14 @@ class Server:
         self.held: dict[int, tuple] = {}
         self._buf = (ServerResult * 256)()
 
-    def submit(self, gray_a, gray_b, knobs: Knobs, tag: int, scale_a=None, scale_b=None, s1_scale: float = 1.0) -> int:
+    def submit(self, gray_a, gray_b, knobs: Knobs, tag: int, scale_a=None, scale_b=None, s1_scale: float = 1.0,
+               retry_hypotheses: int = 0, retry_min_inliers: int = 0) -> int:
         """Queues one pair; returns the status code (0 = queued). (rows, cols, 3)
         images are RGB8: the server converts and resizes them with S1 at
-        s1_scale on the device and returns H in their original coordinates."""
+        s1_scale on the device and returns H in their original coordinates.
+        retry_hypotheses > knobs.hypotheses: a result that is not OK or has
+        fewer than retry_min_inliers inliers is retried once by extending the
+        saved S5 search to retry_hypotheses."""
         a, b = pinned_image(gray_a), pinned_image(gray_b)
         r = Request()
         r.host_a, r.host_b = a.data_ptr(), b.data_ptr()
@@ -52,6 +56,7 @@ class Server:
         r.width_b, r.height_b, r.pitch_b = b.shape[1], b.shape[0], b.stride(0)
         r.rgb = 1 if a.dim() == 3 else 0
         r.scale = s1_scale if r.rgb else 0.0
+        r.retry_hypotheses, r.retry_min_inliers = retry_hypotheses, retry_min_inliers
         if scale_a is not None:
             r.scale_a = scale_a
         if scale_b is not None:
@@ -75,7 +80,8 @@ class Server:
                 r = self._buf[i]
                 d = result_dict(r.result) if r.status == 0 else {"status": r.status}
                 d.update(tag=r.tag, submit_ms=r.submit_ms, launch_ms=r.launch_ms, done_ms=r.done_ms,
-                         latency_ms=r.done_ms - r.submit_ms, batch_pairs=r.batch_pairs, run_status=r.status)
+                         latency_ms=r.done_ms - r.submit_ms, batch_pairs=r.batch_pairs, run_status=r.status,
+                         attempts=r.attempts)
                 self.held.pop(r.tag, None)
                 out.append(d)
             if n.value < len(self._buf):

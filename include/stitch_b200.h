@@ -325,8 +325,13 @@ typedef struct stitch_server_config {
  * scale_a/scale_b are as in stitch_pair_desc. With rgb = 1 they are RGB8:
  * the server runs S1 (src/s1/s1.hpp:33-38) at `scale` (0 means 1) on the
  * device first, registers the working-size GRAY8 images, and returns H in
- * the original coordinates (scale_a/scale_b are then ignored). `tag` is
- * returned with the result. */
+ * the original coordinates (scale_a/scale_b are then ignored). With
+ * retry_hypotheses > s5.hypotheses, a result whose status is not OK or
+ * whose inlier count is below retry_min_inliers is retried once by
+ * extending the saved S5 search to retry_hypotheses on the resident
+ * keypoints and matches (the controller's R escalation,
+ * src/controller/reuse.cpp:5-22: no resampling, same result as a fresh run
+ * with retry_hypotheses). `tag` is returned with the result. */
 typedef struct stitch_request {
     const uint8_t* host_a;
     const uint8_t* host_b;
@@ -339,18 +344,22 @@ typedef struct stitch_request {
     stitch_pyramid_config pyramid;
     int rgb;
     double scale;
+    int retry_hypotheses;
+    int retry_min_inliers;
     uint64_t tag;
 } stitch_request;
 
 /* Completed request. Times are milliseconds on a steady clock since the
  * server was created: submit (stitch_server_submit), launch (its batch
  * enqueued) and done (the dispatcher saw its batch complete, results on the
- * host). status is 0 unless the request could not run. */
+ * host). status is 0 unless the request could not run; attempts is 2 when
+ * the S5 extension retry ran. */
 typedef struct stitch_server_result {
     uint64_t tag;
     double submit_ms, launch_ms, done_ms;
     int batch_pairs;
     int status;
+    int attempts;
     stitch_homography_result result;
 } stitch_server_result;
 

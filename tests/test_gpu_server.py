@@ -149,3 +149,26 @@ def test_rgb_requests_run_s1_on_the_device(cuda):
         torch.cuda.synchronize()
         want = stages.result_dict(runner.result)
         same(got[n], want)
+
+
+def test_retry_extends_the_saved_search(cuda):
+    """R escalation without resampling: a request retried from R = 24 to
+    R = 2000 on its resident state gives the result of a fresh R = 2000 run;
+    a request that passes its bar keeps its first result."""
+    from dataclasses import replace
+    p = synth.config0_pair(70)
+    base = stages.Knobs(max_keypoints=1000, hypotheses=24, seed=77, levels=8)
+    srv = Server(arena_bytes=1 << 30, max_batch=8, streams=2)
+    assert srv.submit(p.gray_a, p.gray_b, base, tag=0, retry_hypotheses=2000, retry_min_inliers=10 ** 9) == 0
+    assert srv.submit(p.gray_a, p.gray_b, base, tag=1, retry_hypotheses=2000, retry_min_inliers=0) == 0
+    assert srv.submit(p.gray_a, p.gray_b, replace(base, seed=78), tag=2) == 0
+    got = {r["tag"]: r for r in srv.drain()}
+    srv.close()
+    runner = stages.PairRunner(512, 512, 1000, max_r=2000)
+    full = runner.run(p.gray_a, p.gray_b, replace(base, hypotheses=2000))
+    short = runner.run(p.gray_a, p.gray_b, base)
+    other = runner.run(p.gray_a, p.gray_b, replace(base, seed=78))
+    assert got[0]["attempts"] == 2 and got[1]["attempts"] == 1 and got[2]["attempts"] == 1
+    same(got[0], full)
+    same(got[1], short)
+    same(got[2], other)
