@@ -119,6 +119,22 @@ class ServerResult(C.Structure):
                 ("result", HomographyResult)]
 
 
+class S6Policy(C.Structure):
+    """stitch_s6_policy (src/s6/geometry.hpp:10-16)."""
+    _fields_ = [("denominator_tolerance", C.c_double), ("inverse_tolerance", C.c_double),
+                ("snap_tolerance", C.c_double), ("max_canvas_pixels", C.c_size_t)]
+
+
+class S6Geometry(C.Structure):
+    """stitch_s6_geometry (src/s6/geometry.hpp:18-34)."""
+    _fields_ = [("width", C.c_int), ("height", C.c_int), ("origin_x", C.c_int), ("origin_y", C.c_int),
+                ("width_a", C.c_int), ("height_a", C.c_int), ("width_b", C.c_int), ("height_b", C.c_int),
+                ("denominator_tolerance", C.c_double), ("snap_tolerance", C.c_double),
+                ("inverse", C.c_double * 9)]
+
+
+S6_FEATHER, S6_MULTIBAND3, S6_MULTIBAND5 = 0, 1, 2
+
 P = C.POINTER
 _size_p = P(C.c_size_t)
 
@@ -161,6 +177,12 @@ PROTOTYPES: dict[str, tuple] = {
     "stitch_s5_workspace_bytes": (C.c_int, [P(S5Config), _size_p]),
     "stitch_s5_estimate": (C.c_int, [P(Keypoints), P(Keypoints), P(Matches), P(ScaleInfo), P(ScaleInfo),
                                      P(S5Config), C.c_void_p, C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p]),
+    "stitch_s6_default_policy": (None, [P(S6Policy)]),
+    "stitch_s6_prepare_geometry": (C.c_int, [C.c_int, C.c_int, C.c_int, C.c_int, P(C.c_double), P(S6Policy),
+                                             P(S6Geometry)]),
+    "stitch_s6_workspace_bytes": (C.c_int, [P(S6Geometry), C.c_int, _size_p]),
+    "stitch_s6_render": (C.c_int, [P(ImageView), P(ImageView), P(S6Geometry), C.c_int, P(ImageView), P(ImageView),
+                                   C.c_void_p, C.c_size_t, C.c_void_p, P(C.c_uint64)]),
     "stitch_batch_create": (C.c_int, [C.c_int, P(PairDesc), P(C.c_void_p), _size_p, P(C.c_int)]),
     "stitch_batch_enqueue": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p]),
     "stitch_batch_capture": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p]),

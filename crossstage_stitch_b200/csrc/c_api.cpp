@@ -54,7 +54,7 @@ void note_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); 
 
 extern "C" {
 
-int stitch_abi_version(void) { return 2; }
+int stitch_abi_version(void) { return 3; }
 
 long long stitch_launch_count(void) { return stitch::b200::g_launches.load(std::memory_order_relaxed); }
 

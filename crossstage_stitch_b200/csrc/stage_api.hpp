@@ -194,4 +194,39 @@ Status estimate(const Keypoints& a, const Keypoints& b, const Matches& matches,
                 std::size_t workspace_bytes, cudaStream_t stream);
 }  // namespace s5
 
+namespace s6 {
+// src/s6/s6.hpp:13-19 and src/s6/geometry.hpp:9-33.
+enum class BlendMode : int { Feather = 0, Multiband3 = 1, Multiband5 = 2 };
+struct alignas(8) RenderStatistics {
+    std::uint64_t union_pixels;
+    std::uint64_t overlap_pixels;
+};
+struct GeometryPolicy {
+    double denominator_tolerance = 1e-12;
+    double inverse_tolerance = 1e-12;
+    double snap_tolerance = 1e-10;
+    std::size_t max_canvas_pixels = 16777216;
+};
+struct Geometry {
+    int width = 0;
+    int height = 0;
+    int origin_x = 0;  // original A coordinates of canvas pixel (0, 0)
+    int origin_y = 0;
+    int width_a = 0;
+    int height_a = 0;
+    int width_b = 0;
+    int height_b = 0;
+    double denominator_tolerance = 1e-12;
+    double snap_tolerance = 1e-10;
+    double inverse[9] = {};  // A-original -> B-original, normalised by its largest entry
+};
+Status prepare_geometry(int width_a, int height_a, int width_b, int height_b, const double* h,
+                        const GeometryPolicy& policy, Geometry* out);
+int effective_reductions(const Geometry& geometry, BlendMode mode);
+Status s6_workspace_bytes(const Geometry& geometry, BlendMode mode, std::size_t* bytes);
+Status render(const ImageView& a, const ImageView& b, const Geometry& geometry, BlendMode mode,
+              const ImageView& output, const ImageView& mask, void* workspace, std::size_t workspace_bytes,
+              cudaStream_t stream, RenderStatistics* statistics = nullptr);
+}  // namespace s6
+
 }  // namespace stitch

@@ -246,6 +246,44 @@ int stitch_s5_estimate(const stitch_keypoints* a, const stitch_keypoints* b, con
                        const stitch_s5_config* config, uint8_t* inlier_mask, stitch_homography_result* output,
                        void* workspace, size_t workspace_bytes, void* stream);
 
+/* ------------------------------------------------------------------- S6 */
+
+/* src/s6/geometry.hpp:10-16 (stitch::s6::GeometryPolicy). */
+typedef struct stitch_s6_policy {
+    double denominator_tolerance, inverse_tolerance, snap_tolerance;
+    size_t max_canvas_pixels;
+} stitch_s6_policy;
+/* src/s6/geometry.hpp:18-34 (stitch::s6::Geometry): the canvas (A's pixel
+ * grid from origin) and the A -> B inverse, largest entry magnitude 1. */
+typedef struct stitch_s6_geometry {
+    int width, height, origin_x, origin_y;
+    int width_a, height_a, width_b, height_b;
+    double denominator_tolerance, snap_tolerance;
+    double inverse[9];
+} stitch_s6_geometry;
+/* Blend modes of src/s6/s6.hpp:13: 0 feather, 1 multiband3, 2 multiband5.
+ * Only the feather blend renders; the multiband modes return
+ * INVALID_ARGUMENT from stitch_s6_workspace_bytes and stitch_s6_render. */
+#define STITCH_S6_FEATHER 0
+
+/* The reference's default GeometryPolicy (1e-12, 1e-12, 1e-10, 16777216). */
+void stitch_s6_default_policy(stitch_s6_policy* policy);
+/* src/s6/geometry.hpp:43-44 (stitch::s6::prepare_geometry): H maps B to A
+ * (row-major doubles); policy NULL = the default. OK, INVALID_ARGUMENT,
+ * DEGENERATE (horizon, singular, ill-conditioned) or INSUFFICIENT_WORKSPACE
+ * (canvas over the policy's pixel budget); *out is zeroed on failure. */
+int stitch_s6_prepare_geometry(int width_a, int height_a, int width_b, int height_b, const double* h,
+                               const stitch_s6_policy* policy, stitch_s6_geometry* out);
+/* src/s6/s6.hpp:26-27 (stitch::s6::s6_workspace_bytes): 0 for feather. */
+int stitch_s6_workspace_bytes(const stitch_s6_geometry* geometry, int mode, size_t* bytes);
+/* src/s6/s6.hpp:44-47 (stitch::s6::render): one launch; output RGB8 and
+ * mask GRAY8 (0/1) of the canvas size, device memory; statistics NULL or
+ * two device uint64 {union_pixels, overlap_pixels}, 8-byte aligned, reset
+ * and filled by the call. */
+int stitch_s6_render(const stitch_image_view* a, const stitch_image_view* b, const stitch_s6_geometry* geometry,
+                     int mode, const stitch_image_view* output, const stitch_image_view* mask, void* workspace,
+                     size_t workspace_bytes, void* stream, uint64_t* statistics);
+
 /* --------------------------------------------------------- batched form */
 
 /* One pair of the batched form. It bundles the per-pair arguments the

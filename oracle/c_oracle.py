@@ -28,6 +28,17 @@ class OResult(C.Structure):
                 ("reproj_residual", C.c_double), ("status", C.c_int)]
 
 
+class OS6Policy(C.Structure):
+    _fields_ = [("den_tol", C.c_double), ("inv_tol", C.c_double), ("snap_tol", C.c_double),
+                ("max_pixels", C.c_size_t)]
+
+
+class OS6Geom(C.Structure):
+    _fields_ = [("w", C.c_int), ("h", C.c_int), ("ox", C.c_int), ("oy", C.c_int), ("wa", C.c_int),
+                ("ha", C.c_int), ("wb", C.c_int), ("hb", C.c_int), ("den_tol", C.c_double),
+                ("snap_tol", C.c_double), ("inv", C.c_double * 9)]
+
+
 TOP2_DTYPE = np.dtype([("first_distance", "<f8"), ("second_distance", "<f8"),
                        ("first_index", "<i4"), ("second_index", "<i4")])
 
@@ -60,6 +71,8 @@ def lib() -> C.CDLL:
         L.oracle_s5_finish.argtypes = [ip, vp, ip, C.POINTER(OModel), ip, ip, C.c_double, ip, ip, ip, ip,
                                        ip, ip, vp, vp, vp, C.POINTER(OResult)]
         L.oracle_make_scale_info.argtypes = [ip, ip, C.c_double, vp, vp, vp]
+        L.oracle_s6_geometry.argtypes = [ip, ip, ip, ip, vp, C.POINTER(OS6Policy), C.POINTER(OS6Geom)]
+        L.oracle_s6_feather.argtypes = [vp, ip, vp, ip, C.POINTER(OS6Geom), vp, ip, vp, ip, vp]
         _lib = L
     return _lib
 
@@ -152,3 +165,30 @@ def s1_gradient(gray: np.ndarray) -> float:
     gray = np.ascontiguousarray(gray, dtype=np.uint8)
     h, w = gray.shape
     return lib().oracle_s1_gradient(gray.ctypes.data, w, h, w)
+
+
+def s6_policy(den_tol: float = 1e-12, inv_tol: float = 1e-12, snap_tol: float = 1e-10,
+              max_pixels: int = 16777216) -> OS6Policy:
+    return OS6Policy(den_tol, inv_tol, snap_tol, max_pixels)
+
+
+def s6_geometry(wa: int, ha: int, wb: int, hb: int, h, policy: OS6Policy | None = None):
+    """(status, OS6Geom) of the B -> A canvas geometry; h None passes NULL."""
+    g = OS6Geom()
+    hp = None if h is None else np.ascontiguousarray(h, np.float64).reshape(9)
+    st = lib().oracle_s6_geometry(wa, ha, wb, hb, _p(hp), C.byref(policy or s6_policy()), C.byref(g))
+    return st, g
+
+
+def s6_feather(a: np.ndarray, b: np.ndarray, g: OS6Geom):
+    """Feather render of RGB8 (h, w, 3) images a, b on geometry g:
+    (panorama (g.h, g.w, 3) uint8, mask (g.h, g.w) uint8 0/1, (union, overlap))."""
+    a = np.ascontiguousarray(a, np.uint8)
+    b = np.ascontiguousarray(b, np.uint8)
+    assert a.shape == (g.ha, g.wa, 3) and b.shape == (g.hb, g.wb, 3)
+    out = np.zeros((g.h, g.w, 3), np.uint8)
+    mask = np.zeros((g.h, g.w), np.uint8)
+    stats = np.zeros(2, np.uint64)
+    lib().oracle_s6_feather(_p(a), a.strides[0], _p(b), b.strides[0], C.byref(g), _p(out), out.strides[0],
+                            _p(mask), mask.strides[0], _p(stats))
+    return out, mask, (int(stats[0]), int(stats[1]))

@@ -1,5 +1,5 @@
 // Test infrastructure only. extern "C" entry points over the reference's own
-// S1..S5 stage functions, linked with the reference sources built for sm_100a
+// S1..S6 stage functions, linked with the reference sources built for sm_100a
 // by `make -C oracle ref`. Arguments use the same plain-data layouts as
 // include/stitch_b200.h, so tests pass identical structs to both libraries.
 #include "common/types.hpp"
@@ -8,6 +8,7 @@
 #include "s2_s3/s3.hpp"
 #include "s4/s4.hpp"
 #include "s5/s5.hpp"
+#include "s6/s6.hpp"
 
 using namespace stitch;
 
@@ -52,5 +53,14 @@ int ref_s5_estimate(const Keypoints* a, const Keypoints* b, const Matches* m, co
                     const ScaleInfo* sb, const s5::Config* c, std::uint8_t* mask, HomographyResult* out, void* ws,
                     std::size_t n, void* s) {
     return code(s5::estimate(*a, *b, *m, *sa, *sb, *c, mask, out, ws, n, st(s)));
+}
+int ref_s6_prepare_geometry(int wa, int ha, int wb, int hb, const double* h, const s6::GeometryPolicy* p,
+                            s6::Geometry* out) {
+    return code(s6::prepare_geometry(wa, ha, wb, hb, h, *p, out));
+}
+int ref_s6_render(const ImageView* a, const ImageView* b, const s6::Geometry* g, int mode, const ImageView* out,
+                  const ImageView* mask, void* ws, std::size_t n, void* s, std::uint64_t* statistics) {
+    return code(s6::render(*a, *b, *g, static_cast<s6::BlendMode>(mode), *out, *mask, ws, n, st(s),
+                           reinterpret_cast<s6::RenderStatistics*>(statistics)));
 }
 }

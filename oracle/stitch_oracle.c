@@ -1,5 +1,6 @@
-/* CPU oracle for S4 (exact Hamming / L2 top-2, ratio test, compaction) and
- * S5 (MSAC homography with counter-based sampling and refinement).
+/* CPU oracle for S4 (exact Hamming / L2 top-2, ratio test, compaction),
+ * S5 (MSAC homography with counter-based sampling and refinement), S1
+ * (integer gray and area resize) and S6 (canvas geometry, feather render).
  *
  * TEST INFRASTRUCTURE ONLY: the checker the CUDA stages are compared against.
  * The product library never links this file.
@@ -26,8 +27,11 @@
  *                      accepted only on a strictly lower loss, inlier mask
  *                      r^2 <= tau^2, telemetry, H = D_A^-1 H_s D_B)
  *   geometry ......... src/common/geometry.hpp:119-163
+ *   S1 ............... src/s1/s1.cu:33-205
+ *   S6 ............... src/s6/geometry.cpp:10-198, src/s6/s6.cu:147-215
  */
 #include <float.h>
+#include <limits.h>
 #include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
@@ -546,4 +550,272 @@ double oracle_s1_gradient(const uint8_t* g, int w, int h, int pitch) {
         }
     const unsigned long long edges = (unsigned long long)h * (w - 1) + (unsigned long long)w * (h - 1);
     return edges ? (double)sum / (255.0 * (double)edges) : 0.0;
+}
+
+/* ---------------------------------------------------------------- S6
+ * Geometry (src/s6/geometry.cpp:10-198) in x87 80-bit long double, the type
+ * the reference's host build computes in: H scaled by its largest entry; the
+ * four B corners on one side of the horizon with |w| above
+ * denominator_tolerance * (|h6| (wb-1) + |h7| (hb-1) + |h8|); the inclusive
+ * canvas floor(min) .. ceil(max) over A's pixel centres and B's projected
+ * corners, each end snapped to an integer within
+ * max(snap_tolerance, 16 eps max(1, |x|)); the pixel budget; the inverse
+ * through size-normalised coordinates (A and B centred and divided by
+ * max(1, w-1, h-1)), Gauss-Jordan with scaled partial pivoting, pivot score
+ * and ||M||inf ||M^-1||inf checked against inverse_tolerance; the A -> B
+ * inverse scaled by its largest entry.
+ * Feather (src/s6/s6.cu:147-215), per canvas pixel, double arithmetic with
+ * every product and sum rounded on its own: A sampled at the pixel, B through
+ * the inverse when |den| > denominator_tolerance * den_scale; bilinear
+ * interpolation of the pixel-centre grid (coordinates snapped as above),
+ * converted to float after / 255; distance-to-edge scores; the score-weighted
+ * mean where both cover the pixel; floor(clamp(255 c, 0, 255) + 0.5). */
+typedef struct {
+    double den_tol, inv_tol, snap_tol;
+    size_t max_pixels;
+} o_s6_policy;
+typedef struct {
+    int w, h, ox, oy, wa, ha, wb, hb;
+    double den_tol, snap_tol;
+    double inv[9];
+} o_s6_geom;
+
+typedef long double o_real;
+
+static int lfin(o_real x) { return isfinite(x); }
+static o_real lmaxr(o_real a, o_real b) { return a > b ? a : b; }
+
+static void lmul3(const o_real* a, const o_real* b, o_real* out) {
+    o_real t[9];
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) {
+            o_real s = 0;
+            for (int k = 0; k < 3; ++k) s += a[3 * r + k] * b[3 * k + c];
+            t[3 * r + c] = s;
+        }
+    memcpy(out, t, sizeof(t));
+}
+
+static int lscale(o_real* m) {
+    o_real big = 0;
+    for (int i = 0; i < 9; ++i) {
+        if (!lfin(m[i])) return 0;
+        big = lmaxr(big, fabsl(m[i]));
+    }
+    if (big == 0) return 0;
+    for (int i = 0; i < 9; ++i) m[i] /= big;
+    return 1;
+}
+
+static o_real linf(const o_real* m) {
+    o_real n = 0;
+    for (int r = 0; r < 3; ++r) {
+        o_real s = 0;
+        for (int c = 0; c < 3; ++c) s += fabsl(m[3 * r + c]);
+        n = lmaxr(n, s);
+    }
+    return n;
+}
+
+static int linvert(const o_real* m, o_real tol, o_real* inv) {
+    o_real a[3][6], rs[3];
+    memset(a, 0, sizeof(a));
+    for (int r = 0; r < 3; ++r) {
+        rs[r] = 0;
+        for (int c = 0; c < 3; ++c) {
+            a[r][c] = m[3 * r + c];
+            rs[r] = lmaxr(rs[r], fabsl(a[r][c]));
+        }
+        if (rs[r] == 0) return 0;
+        a[r][3 + r] = 1;
+    }
+    for (int col = 0; col < 3; ++col) {
+        int piv = col;
+        o_real best = 0;
+        for (int r = col; r < 3; ++r) {
+            const o_real sc = fabsl(a[r][col]) / rs[r];
+            if (sc > best) {
+                best = sc;
+                piv = r;
+            }
+        }
+        if (!lfin(best) || best <= tol) return 0;
+        if (piv != col) {
+            for (int c = 0; c < 6; ++c) {
+                const o_real t = a[piv][c];
+                a[piv][c] = a[col][c];
+                a[col][c] = t;
+            }
+            const o_real t = rs[piv];
+            rs[piv] = rs[col];
+            rs[col] = t;
+        }
+        const o_real d = a[col][col];
+        for (int c = 0; c < 6; ++c) a[col][c] /= d;
+        for (int r = 0; r < 3; ++r) {
+            if (r == col) continue;
+            const o_real f = a[r][col];
+            for (int c = 0; c < 6; ++c) a[r][c] -= f * a[col][c];
+        }
+    }
+    for (int r = 0; r < 3; ++r)
+        for (int c = 0; c < 3; ++c) {
+            if (!lfin(a[r][3 + c])) return 0;
+            inv[3 * r + c] = a[r][3 + c];
+        }
+    const o_real cond = linf(m) * linf(inv);
+    return lfin(cond) && cond * tol < 1;
+}
+
+static o_real lsnap(o_real x, double snap_tol) {
+    const o_real near = roundl(x);
+    const o_real floor_tol = 16 * (o_real)DBL_EPSILON * lmaxr(1, fabsl(x));
+    return fabsl(x - near) <= lmaxr((o_real)snap_tol, floor_tol) ? near : x;
+}
+
+#define O_INSUFFICIENT_WORKSPACE 2
+
+int oracle_s6_geometry(int wa, int ha, int wb, int hb, const double* h, const o_s6_policy* p, o_s6_geom* out) {
+    o_real m[9];
+    for (int i = 0; i < 9; ++i) m[i] = h ? h[i] : 0;
+    memset(out, 0, sizeof(*out));
+    out->den_tol = 1e-12;
+    out->snap_tol = 1e-10;
+    const int policy_ok = isfinite(p->den_tol) && p->den_tol > 0 && p->den_tol < 1 && isfinite(p->inv_tol) &&
+                          p->inv_tol > 0 && p->inv_tol < 1 && isfinite(p->snap_tol) && p->snap_tol >= 0 &&
+                          p->snap_tol < 0.5 && p->max_pixels > 0;
+    if (!h || wa <= 0 || ha <= 0 || wb <= 0 || hb <= 0 || !policy_ok) return O_INVALID_ARGUMENT;
+    if (!lscale(m)) return O_DEGENERATE;
+    const o_real bx = (o_real)wb - 1, by = (o_real)hb - 1;
+    const o_real dscale = fabsl(m[6]) * bx + fabsl(m[7]) * by + fabsl(m[8]);
+    if (!(dscale > 0) || !lfin(dscale)) return O_DEGENERATE;
+    const o_real dfloor = p->den_tol * dscale;
+    o_real lo_x = 0, lo_y = 0, hi_x = (o_real)wa - 1, hi_y = (o_real)ha - 1;
+    int side = 0;
+    for (int k = 0; k < 4; ++k) {
+        const o_real x = (k & 1) ? bx : 0, y = (k & 2) ? by : 0;
+        const o_real w = m[6] * x + m[7] * y + m[8];
+        if (!lfin(w) || fabsl(w) <= dfloor) return O_DEGENERATE;
+        const int s = w > 0 ? 1 : -1;
+        if (side != 0 && s != side) return O_DEGENERATE;
+        side = s;
+        const o_real px = (m[0] * x + m[1] * y + m[2]) / w;
+        const o_real py = (m[3] * x + m[4] * y + m[5]) / w;
+        if (!lfin(px) || !lfin(py)) return O_DEGENERATE;
+        if (px < lo_x) lo_x = px;
+        if (py < lo_y) lo_y = py;
+        if (px > hi_x) hi_x = px;
+        if (py > hi_y) hi_y = py;
+    }
+    lo_x = floorl(lsnap(lo_x, p->snap_tol));
+    lo_y = floorl(lsnap(lo_y, p->snap_tol));
+    hi_x = ceill(lsnap(hi_x, p->snap_tol));
+    hi_y = ceill(lsnap(hi_y, p->snap_tol));
+    const o_real cw = hi_x - lo_x + 1, ch = hi_y - lo_y + 1;
+    if (lo_x < INT_MIN || lo_y < INT_MIN || lo_x > INT_MAX || lo_y > INT_MAX || !lfin(cw) || !lfin(ch) || cw < 1 ||
+        ch < 1 || cw > INT_MAX || ch > INT_MAX)
+        return O_INSUFFICIENT_WORKSPACE;
+    const size_t uw = (size_t)cw, uh = (size_t)ch;
+    if (uw > SIZE_MAX / uh || uw > p->max_pixels / uh) return O_INSUFFICIENT_WORKSPACE;
+    const o_real sa = lmaxr(lmaxr(1, (o_real)wa - 1), (o_real)ha - 1);
+    const o_real sb = lmaxr(lmaxr(1, bx), by);
+    const o_real cax = ((o_real)wa - 1) / 2, cay = ((o_real)ha - 1) / 2;
+    const o_real na[9] = {1 / sa, 0, -cax / sa, 0, 1 / sa, -cay / sa, 0, 0, 1};
+    const o_real nb_inv[9] = {sb, 0, bx / 2, 0, sb, by / 2, 0, 0, 1};
+    o_real t[9], hn[9], hn_inv[9], inv[9];
+    lmul3(na, m, t);
+    lmul3(t, nb_inv, hn);
+    if (!lscale(hn) || !linvert(hn, p->inv_tol, hn_inv)) return O_DEGENERATE;
+    lmul3(nb_inv, hn_inv, t);
+    lmul3(t, na, inv);
+    if (!lscale(inv)) return O_DEGENERATE;
+    o_s6_geom g;
+    memset(&g, 0, sizeof(g));
+    g.w = (int)cw;
+    g.h = (int)ch;
+    g.ox = (int)lo_x;
+    g.oy = (int)lo_y;
+    g.wa = wa;
+    g.ha = ha;
+    g.wb = wb;
+    g.hb = hb;
+    g.den_tol = p->den_tol;
+    g.snap_tol = p->snap_tol;
+    for (int i = 0; i < 9; ++i) {
+        g.inv[i] = (double)inv[i];
+        if (!isfinite(g.inv[i])) return O_DEGENERATE;
+    }
+    *out = g;
+    return O_OK;
+}
+
+static int s6_centre(double* x, int n, double tol) {
+    if (!isfinite(*x)) return 0;
+    const double near = nearbyint(*x);
+    const double roundoff = 16 * DBL_EPSILON * fmax(1.0, fabs(*x));
+    if (fabs(*x - near) <= fmax(tol, roundoff)) *x = near;
+    return *x >= 0 && *x <= n - 1.0;
+}
+
+static int s6_sample(const uint8_t* im, int w, int h, int pitch, double x, double y, double tol, float* rgb,
+                     double* score) {
+    if (!s6_centre(&x, w, tol) || !s6_centre(&y, h, tol)) return 0;
+    const int x0 = (int)floor(x), y0 = (int)floor(y);
+    const int x1 = x0 < w - 1 ? x0 + 1 : x0, y1 = y0 < h - 1 ? y0 + 1 : y0;
+    const double ax = x - x0, ay = y - y0;
+    const uint8_t* r0 = im + (size_t)y0 * pitch;
+    const uint8_t* r1 = im + (size_t)y1 * pitch;
+    for (int c = 0; c < 3; ++c) {
+        const double top = (1 - ax) * r0[3 * x0 + c] + ax * r0[3 * x1 + c];
+        const double bottom = (1 - ax) * r1[3 * x0 + c] + ax * r1[3 * x1 + c];
+        rgb[c] = (float)(((1 - ay) * top + ay * bottom) / 255.0);
+    }
+    const double left = (x + 0.5) / w, right = (w - 0.5 - x) / w;
+    const double upper = (y + 0.5) / h, lower = (h - 0.5 - y) / h;
+    *score = fmin(fmin(left, right), fmin(upper, lower));
+    return 1;
+}
+
+static uint8_t s6_quantize(float c) {
+    float v = 255.0f * c;
+    v = fminf(255.0f, fmaxf(0.0f, v));
+    return (uint8_t)floorf(v + 0.5f);
+}
+
+/* out: RGB8 canvas (pitch out_pitch), mask 0/1 (pitch mask_pitch);
+ * stats (optional): {union, overlap}. */
+void oracle_s6_feather(const uint8_t* a, int pitch_a, const uint8_t* b, int pitch_b, const o_s6_geom* g,
+                       uint8_t* out, int out_pitch, uint8_t* mask, int mask_pitch, uint64_t* stats) {
+    uint64_t n_union = 0, n_overlap = 0;
+    const double* m = g->inv;
+    for (int y = 0; y < g->h; ++y)
+        for (int x = 0; x < g->w; ++x) {
+            const double xa = (double)x + g->ox, ya = (double)y + g->oy;
+            float ra[3] = {0, 0, 0}, rb[3] = {0, 0, 0};
+            double sa = 0, sb = 0;
+            const int ma = s6_sample(a, g->wa, g->ha, pitch_a, xa, ya, g->snap_tol, ra, &sa);
+            int mb = 0;
+            const double den = m[6] * xa + m[7] * ya + m[8];
+            const double den_scale = fabs(m[6] * xa) + fabs(m[7] * ya) + fabs(m[8]);
+            if (isfinite(den) && den_scale > 0 && fabs(den) > g->den_tol * den_scale) {
+                const double xb = (m[0] * xa + m[1] * ya + m[2]) / den;
+                const double yb = (m[3] * xa + m[4] * ya + m[5]) / den;
+                mb = s6_sample(b, g->wb, g->hb, pitch_b, xb, yb, g->snap_tol, rb, &sb);
+            }
+            mask[(size_t)y * mask_pitch + x] = (uint8_t)(ma || mb);
+            n_union += (uint64_t)(ma || mb);
+            n_overlap += (uint64_t)(ma && mb);
+            for (int c = 0; c < 3; ++c) {
+                float col;
+                if (ma && mb)
+                    col = (float)((sa * ra[c] + sb * rb[c]) / (sa + sb));
+                else
+                    col = ma ? ra[c] : rb[c];
+                out[(size_t)y * out_pitch + 3 * x + c] = s6_quantize(col);
+            }
+        }
+    if (stats) {
+        stats[0] = n_union;
+        stats[1] = n_overlap;
+    }
 }
