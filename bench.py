@@ -383,6 +383,50 @@ def run_matching(dev, reps=20):
             "chosen": "tensor" if out["tensor"]["ms"] < out["popc"]["ms"] else "popc", **out}
 
 
+def run_render(dev, flush, reps=20):
+    """S6 feather render microbenchmark: a 1920x1080 RGB pair (uniform noise)
+    under a near-identity homography with a 310 px shift and mild
+    perspective, onto its 2220x1145 canvas. L2 is flushed before every
+    launch; each launch is timed alone with CUDA events on its stream.
+    Algorithmic bytes per render: both RGB images read once (3 B/px) and the
+    canvas written once (3 B RGB + 1 B mask per pixel)."""
+    import numpy as np
+    import torch
+    from crossstage_stitch_b200 import render
+    rng = np.random.default_rng(6)
+    a = torch.from_numpy(rng.integers(0, 256, (1080, 1920, 3), dtype=np.uint8)).to(dev)
+    b = torch.from_numpy(rng.integers(0, 256, (1080, 1920, 3), dtype=np.uint8)).to(dev)
+    H = [[0.98, 0.02, 310.5], [-0.015, 1.01, 22.25], [1e-5, -2e-5, 1.0]]
+    g = render.prepare_geometry(1920, 1080, 1920, 1080, H)
+    out = torch.empty((g.height, g.width, 3), dtype=torch.uint8, device=dev)
+    mask = torch.empty((g.height, g.width), dtype=torch.uint8, device=dev)
+    stats = torch.zeros(2, dtype=torch.int64, device=dev)
+    for _ in range(3):
+        render.render(a, b, g, out, mask, stats)
+    torch.cuda.synchronize()
+    stream = torch.cuda.current_stream()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(reps)]
+    for e0, e1 in ev:
+        flush.zero_()
+        e0.record(stream)
+        render.render(a, b, g, out, mask, stats)
+        e1.record(stream)
+    torch.cuda.synchronize()
+    ms = statistics.mean(e0.elapsed_time(e1) for e0, e1 in ev)
+    px = g.width * g.height
+    nbytes = 2 * 3 * 1920 * 1080 + 4 * px
+    peaks = json.loads(PEAKS.read_text()) if PEAKS.exists() else {}
+    peak = peaks.get("hbm_gbs", 6650.0)
+    achieved = nbytes / (ms / 1e3) / 1e9
+    union, overlap = (int(v) for v in stats.cpu())
+    return {"workload": "feather render, 1920x1080 RGB pair onto a 2220x1145 canvas (L2 flushed per launch)",
+            "canvas": [g.width, g.height], "union_pixels": union, "overlap_pixels": overlap,
+            "ms_per_render": ms, "canvas_mpix_per_s": px / (ms / 1e3) / 1e6, "panoramas_per_s": 1e3 / ms,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "bytes_per_render": nbytes,
+                         "peak_source": "measured hbm_gbs" if "hbm_gbs" in peaks else "fallback"}}
+
+
 def algorithmic_work(batch, n_pairs, counts):
     """Per-kernel algorithmic work of one step (bytes for pixel kernels,
     ops for matching and estimation), from the actual keypoint and match
@@ -411,8 +455,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-resolution and served sections")
-    ap.add_argument("--only", choices=["matching"], default=None,
-                    help="run only the matching microbenchmark (popc vs tensor cores) and print its JSON")
+    ap.add_argument("--only", choices=["matching", "render"], default=None,
+                    help="run only the matching microbenchmark (popc vs tensor cores) or the S6 feather "
+                         "render microbenchmark and print its JSON")
     ap.add_argument("--runs-csv", default=None,
                     help="write the timed plain per-pair runs as rows of the reference harness's runs.csv")
     args = ap.parse_args()
@@ -428,6 +473,13 @@ def main():
         import torch
         torch.cuda.set_device(local)
         print(json.dumps(run_matching(torch.device("cuda", local), reps=args.steps)), flush=True)
+        return
+    if args.only == "render":
+        import torch
+        torch.cuda.set_device(local)
+        dev = torch.device("cuda", local)
+        print(json.dumps(run_render(dev, torch.empty(512 << 20, dtype=torch.uint8, device=dev),
+                                    reps=args.steps)), flush=True)
         return
 
     cpu = None
@@ -528,6 +580,7 @@ def main():
     lat.sort()
 
     matching = run_matching(dev) if rank == 0 else None
+    render_res = run_render(dev, flush) if rank == 0 else None
     mixed_res = served_res = None
     if mixed is not None:
         mixed_res = run_mixed(mixed, max(3, args.steps // 2), args.warmup, dev, flush)
@@ -584,7 +637,7 @@ def main():
                 "keypoints_mean": statistics.mean(a + b_ for a, b_, _ in counts) / 2,
                 "matches_mean": statistics.mean(m for _, _, m in counts),
                 "gpu_launches": launches, "clocks": clk, "roofline": roof, "cpu_baseline": cpu,
-                "matching": matching, "mixed": mixed_res, "served": served_res}
+                "matching": matching, "render": render_res, "mixed": mixed_res, "served": served_res}
         print(json.dumps(line), flush=True)
     if world > 1:
         dist.barrier()

@@ -109,14 +109,17 @@ class Request(C.Structure):
                 ("width_b", C.c_int), ("height_b", C.c_int), ("pitch_b", C.c_int),
                 ("scale_a", ScaleInfo), ("scale_b", ScaleInfo), ("s2", S2Config), ("s4", S4Config),
                 ("s5", S5Config), ("pyramid", PyramidConfig), ("rgb", C.c_int), ("scale", C.c_double),
-                ("retry_hypotheses", C.c_int), ("retry_min_inliers", C.c_int), ("tag", C.c_uint64)]
+                ("retry_hypotheses", C.c_int), ("retry_min_inliers", C.c_int), ("tag", C.c_uint64),
+                ("host_panorama", C.c_void_p), ("host_mask", C.c_void_p), ("panorama_capacity", C.c_size_t)]
 
 
 class ServerResult(C.Structure):
     """stitch_server_result."""
     _fields_ = [("tag", C.c_uint64), ("submit_ms", C.c_double), ("launch_ms", C.c_double),
                 ("done_ms", C.c_double), ("batch_pairs", C.c_int), ("status", C.c_int), ("attempts", C.c_int),
-                ("result", HomographyResult)]
+                ("result", HomographyResult), ("render_status", C.c_int), ("canvas_width", C.c_int),
+                ("canvas_height", C.c_int), ("origin_x", C.c_int), ("origin_y", C.c_int),
+                ("union_pixels", C.c_uint64), ("overlap_pixels", C.c_uint64)]
 
 
 class S6Policy(C.Structure):

@@ -30,6 +30,12 @@ static_assert(offsetof(stitch_homography_result, status) == offsetof(HomographyR
 static_assert(offsetof(stitch_s5_config, seed) == offsetof(s5::Config, seed), "s5 config");
 static_assert(offsetof(stitch_scale_info, D) == offsetof(ScaleInfo, D), "scale info");
 static_assert(offsetof(stitch_s4_config, cross_check) == offsetof(s4::Config, cross_check), "s4 config");
+SAME_LAYOUT(stitch_s6_policy, s6::GeometryPolicy);
+SAME_LAYOUT(stitch_s6_geometry, s6::Geometry);
+static_assert(offsetof(stitch_s6_policy, max_canvas_pixels) == offsetof(s6::GeometryPolicy, max_canvas_pixels),
+              "s6 policy");
+static_assert(offsetof(stitch_s6_geometry, inverse) == offsetof(s6::Geometry, inverse), "s6 geometry");
+static_assert(offsetof(stitch_s6_geometry, snap_tolerance) == offsetof(s6::Geometry, snap_tolerance), "s6 geometry");
 
 template <class T, class C> const T& as(const C* p) { return *reinterpret_cast<const T*>(p); }
 

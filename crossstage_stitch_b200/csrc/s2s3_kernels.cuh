@@ -229,10 +229,18 @@ constexpr int kInStride = 96, kInOff = 12;
 constexpr int kScStride = 68;
 constexpr int kScGroups = kScStride / 4;  // groups of 4 positions per score row
 
-// Byte k of w as a float (exact: 2^23 + b - 2^23).
-__device__ __forceinline__ float byte_float(std::uint32_t w, int k) {
-    return __fsub_rn(__uint_as_float(__byte_perm(w, 0x4B000000u, 0x7440u + k)), 8388608.0f);
+// Bytes k of wa and wb as a float pair (rows r, r + 1 of one column), each
+// exact: the float 2^23 + b (byte b placed in the low mantissa) minus 2^23.
+__device__ __forceinline__ float2 byte_pair(std::uint32_t wa, std::uint32_t wb, int k) {
+    const float2 biased = make_float2(__uint_as_float(__byte_perm(wa, 0x4B000000u, 0x7440u + k)),
+                                      __uint_as_float(__byte_perm(wb, 0x4B000000u, 0x7440u + k)));
+    return __fadd2_rn(biased, make_float2(-8388608.0f, -8388608.0f));
 }
+
+// A blur tap in both lanes of a packed pair. The sm_100 packed FP32 add and
+// multiply round each lane exactly as __fadd_rn / __fmul_rn do, so two rows
+// (or two columns) of the blur run in one instruction stream.
+__device__ __forceinline__ float2 tap_pair(int t) { return make_float2(blur_tap(t), blur_tap(t)); }
 
 // Rounds a blur sum half-to-even after clamping to [0, 255] (clamping the
 // float first gives the same byte for every finite sum).
@@ -346,25 +354,31 @@ __global__ __launch_bounds__(256) void fast_nms_kernel(const __grid_constant__ S
                     static_cast<std::uint16_t>(((r * kScGroups + q) << 4) | bits);
         }
     }
-    if (j.blurred) {  // blur rows pass: 4 outputs per thread, image rows y0-3 .. y0+34
-        for (int g = tid; g < (kFastTileH + 6) * (kFastTileW / 4); g += 256) {
-            const int rr = g / (kFastTileW / 4), q = g - rr * (kFastTileW / 4);
-            const auto* rw = reinterpret_cast<const std::uint32_t*>(&in[rr + 1][0]);
-            const std::uint32_t b0 = rw[q + 3], b1 = rw[q + 4], b2 = rw[q + 5];  // bytes 4q+12 .. 4q+23
-            // output 4q+k reads halo columns 4q+k+1 .. 4q+k+7, i.e. x[1+k .. 7+k]
-            float x[11];
-            x[1] = byte_float(b0, 1); x[2] = byte_float(b0, 2); x[3] = byte_float(b0, 3);
-            x[4] = byte_float(b1, 0); x[5] = byte_float(b1, 1); x[6] = byte_float(b1, 2); x[7] = byte_float(b1, 3);
-            x[8] = byte_float(b2, 0); x[9] = byte_float(b2, 1); x[10] = byte_float(b2, 2);
-            float out[4];
+    if (j.blurred) {  // blur rows pass: image rows y0-3 .. y0+34, two rows x 4 outputs per item
+        static_assert((kFastTileH + 6) % 2 == 0, "rows pass takes row pairs");
+        for (int g = tid; g < (kFastTileH + 6) / 2 * (kFastTileW / 4); g += 256) {
+            const int rp = g / (kFastTileW / 4), q = g - rp * (kFastTileW / 4), rr = 2 * rp;
+            const auto* ra = reinterpret_cast<const std::uint32_t*>(&in[rr + 1][0]);
+            const auto* rb = reinterpret_cast<const std::uint32_t*>(&in[rr + 2][0]);
+            const std::uint32_t a0 = ra[q + 3], a1 = ra[q + 4], a2 = ra[q + 5];  // bytes 4q+12 .. 4q+23
+            const std::uint32_t b0 = rb[q + 3], b1 = rb[q + 4], b2 = rb[q + 5];
+            // output 4q+k reads halo columns 4q+k+1 .. 4q+k+7, i.e. x[1+k .. 7+k];
+            // lane x holds row rr, lane y row rr + 1
+            float2 x[11];
+            x[1] = byte_pair(a0, b0, 1); x[2] = byte_pair(a0, b0, 2); x[3] = byte_pair(a0, b0, 3);
+            x[4] = byte_pair(a1, b1, 0); x[5] = byte_pair(a1, b1, 1); x[6] = byte_pair(a1, b1, 2);
+            x[7] = byte_pair(a1, b1, 3); x[8] = byte_pair(a2, b2, 0); x[9] = byte_pair(a2, b2, 1);
+            x[10] = byte_pair(a2, b2, 2);
+            float2 out[4];
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
-                float acc = __fmul_rn(blur_tap(0), x[1 + k]);  // 0 + a nonnegative product is the product
+                float2 acc = __fmul2_rn(tap_pair(0), x[1 + k]);  // 0 + a nonnegative product is the product
 #pragma unroll
-                for (int t = 1; t < 7; ++t) acc = __fadd_rn(acc, __fmul_rn(blur_tap(t), x[1 + k + t]));
+                for (int t = 1; t < 7; ++t) acc = __fadd2_rn(acc, __fmul2_rn(tap_pair(t), x[1 + k + t]));
                 out[k] = acc;
             }
-            *reinterpret_cast<float4*>(&rows[rr][4 * q]) = make_float4(out[0], out[1], out[2], out[3]);
+            *reinterpret_cast<float4*>(&rows[rr][4 * q]) = make_float4(out[0].x, out[1].x, out[2].x, out[3].x);
+            *reinterpret_cast<float4*>(&rows[rr + 1][4 * q]) = make_float4(out[0].y, out[1].y, out[2].y, out[3].y);
         }
     }
     __syncthreads();
@@ -385,16 +399,14 @@ __global__ __launch_bounds__(256) void fast_nms_kernel(const __grid_constant__ S
 #pragma unroll
         for (int o = 0; o < 2; ++o) {
             const int gy = y0 + 2 * p + o, gx = x0 + 4 * q;
-            float4 acc = make_float4(__fmul_rn(blur_tap(0), v[o].x), __fmul_rn(blur_tap(0), v[o].y),
-                                     __fmul_rn(blur_tap(0), v[o].z), __fmul_rn(blur_tap(0), v[o].w));
+            float2 lo = __fmul2_rn(tap_pair(0), make_float2(v[o].x, v[o].y));
+            float2 hi = __fmul2_rn(tap_pair(0), make_float2(v[o].z, v[o].w));
 #pragma unroll
             for (int t = 1; t < 7; ++t) {
-                const float tap = blur_tap(t);
-                acc.x = __fadd_rn(acc.x, __fmul_rn(tap, v[o + t].x));
-                acc.y = __fadd_rn(acc.y, __fmul_rn(tap, v[o + t].y));
-                acc.z = __fadd_rn(acc.z, __fmul_rn(tap, v[o + t].z));
-                acc.w = __fadd_rn(acc.w, __fmul_rn(tap, v[o + t].w));
+                lo = __fadd2_rn(lo, __fmul2_rn(tap_pair(t), make_float2(v[o + t].x, v[o + t].y)));
+                hi = __fadd2_rn(hi, __fmul2_rn(tap_pair(t), make_float2(v[o + t].z, v[o + t].w)));
             }
+            const float4 acc = make_float4(lo.x, lo.y, hi.x, hi.y);
             if (gy >= H || gx >= W) continue;
             const std::uint32_t packed =
                 blur_byte(acc.x) | (blur_byte(acc.y) << 8) | (blur_byte(acc.z) << 16) | (blur_byte(acc.w) << 24);

@@ -114,13 +114,24 @@ Status launch_direction(const Keypoints& qk, const Descriptors& qd, const Keypoi
         using Src = OneJob<KnnJob>;
         const Src src{make_knn_job(qk, qd, tk, td, q_tiles, splits, rows, partial, out)};
         if (matcher() == kMatcherTensor) {
+            // Two tensor-core blocks fit on an SM (shared memory), so a grid
+            // above 2 x 148 blocks leaves a second, mostly idle wave: use the
+            // largest train partition count whose grid fits one wave (never
+            // more partitions than the workspace plan holds).
+            const int stages = ceil_div(std::max(tk.capacity, 1), kTrainStage);
+            const int want = std::min(splits, std::max(1, kTcBlocksPerSm * kSmCount / std::max(q_tiles, 1)));
+            const int tc_rows = ceil_div(stages, want) * kTrainStage;
+            const int tc_splits = ceil_div(std::max(tk.capacity, 1), tc_rows);
+            const Src tc{make_knn_job(qk, qd, tk, td, q_tiles, tc_splits, tc_rows, partial, out)};
             if (!enable_tc_smem<Src>()) return Status::CUDA_ERROR;
-            knn_tc_kernel<Src><<<q_tiles * splits, kQueryThreads, kTcSmem, stream>>>(src);
+            knn_tc_kernel<Src><<<q_tiles * tc_splits, kQueryThreads, kTcSmem, stream>>>(tc);
+            if (tc_splits > 1) knn_merge_kernel<Src><<<ceil_div(qk.capacity, 256), 256, 0, stream>>>(tc);
+            note_launches(tc_splits > 1 ? 2 : 1);
         } else {
             knn_popc_kernel<Src, 1><<<q_tiles * splits, kQueryThreads, 0, stream>>>(src);
+            if (splits > 1) knn_merge_kernel<Src><<<ceil_div(qk.capacity, 256), 256, 0, stream>>>(src);
+            note_launches(splits > 1 ? 2 : 1);
         }
-        if (splits > 1) knn_merge_kernel<Src><<<ceil_div(qk.capacity, 256), 256, 0, stream>>>(src);
-        note_launches(splits > 1 ? 2 : 1);
     } else {
         const Side q{static_cast<const std::uint8_t*>(qd.data), qd.row_stride_bytes, qk.capacity, qk.d_count};
         const Side t{static_cast<const std::uint8_t*>(td.data), td.row_stride_bytes, tk.capacity, tk.d_count};

@@ -182,7 +182,9 @@ __global__ __launch_bounds__(kQueryThreads) void knn_popc_kernel(const __grid_co
 constexpr int kTcRowsA = kQueryThreads;       // 128 queries (MMA M)
 constexpr int kTcRowsB = kTrainStage;         // 256 train rows (MMA N)
 constexpr int kTcBytesA = kTcRowsA * 256, kTcBytesB = kTcRowsB * 256;
+constexpr int kTcBlocksPerSm = 2;  // resident tensor-core blocks per SM (shared memory bound)
 constexpr int kTcSmem = kTcBytesA + kTcBytesB + 1024 + 64;  // + alignment slack + barrier/slot
+static_assert(kTcBlocksPerSm * (kTcSmem + 1024) <= 228 * 1024, "tensor-core blocks per SM");
 constexpr long long kTcWaitLimit = 1ll << 26;  // mbarrier polls before giving up
 
 // Error word of the tensor-core matcher (one per translation unit): set when

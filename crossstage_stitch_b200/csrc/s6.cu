@@ -172,6 +172,16 @@ __device__ __forceinline__ bool centre_coord(double& x, int n, double tol) {
     return x >= 0 && x <= n - 1.0;
 }
 
+// Distance-to-edge score min((x + .5) / w, (w - .5 - x) / w, (y + .5) / h,
+// (h - .5 - y) / h) with two divisions: correctly rounded division by a
+// positive number preserves order, so the smaller of two quotients over the
+// same w is the quotient of the smaller numerator (both numerators >= 0.5).
+__device__ __forceinline__ double edge_score(double x, double y, double w, double h) {
+    return fmin(__ddiv_rn(fmin(__dadd_rn(x, 0.5), __dsub_rn(__dsub_rn(w, 0.5), x)), w),
+                __ddiv_rn(fmin(__dadd_rn(y, 0.5), __dsub_rn(__dsub_rn(h, 0.5), y)), h));
+}
+
+// General bilinear sample of the pixel-centre grid at (x, y).
 __device__ __forceinline__ bool sample(const ImageView& im, double x, double y, float* rgb, double& score,
                                        double tol) {
     if (!centre_coord(x, im.width, tol) || !centre_coord(y, im.height, tol)) return false;
@@ -188,9 +198,20 @@ __device__ __forceinline__ bool sample(const ImageView& im, double x, double y, 
         const double v1 = __dadd_rn(__dmul_rn(bx, r1[3 * x0 + c]), __dmul_rn(ax, r1[3 * x1 + c]));
         rgb[c] = static_cast<float>(__ddiv_rn(__dadd_rn(__dmul_rn(by, v0), __dmul_rn(ay, v1)), 255.0));
     }
-    const double w = im.width, h = im.height;
-    score = fmin(fmin(__ddiv_rn(__dadd_rn(x, 0.5), w), __ddiv_rn(__dsub_rn(__dsub_rn(w, 0.5), x), w)),
-                 fmin(__ddiv_rn(__dadd_rn(y, 0.5), h), __ddiv_rn(__dsub_rn(__dsub_rn(h, 0.5), y), h)));
+    score = edge_score(x, y, im.width, im.height);
+    return true;
+}
+
+// The same sample at integer (x, y), which is where A is sampled: no snap
+// moves it, both bilinear weights are exactly 0, so each channel is the byte
+// p itself and the colour is (float)(p / 255.0), read from `unit`.
+__device__ __forceinline__ bool sample_at_pixel(const ImageView& im, int x, int y, const float* unit, float* rgb,
+                                                double& score) {
+    if (x < 0 || x >= im.width || y < 0 || y >= im.height) return false;
+    const std::uint8_t* px = im.data + static_cast<std::size_t>(y) * im.pitch_bytes + 3 * x;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) rgb[c] = unit[px[c]];
+    score = edge_score(x, y, im.width, im.height);
     return true;
 }
 
@@ -208,17 +229,21 @@ constexpr int kS6BlockX = 32, kS6BlockY = 8;
 
 __global__ __launch_bounds__(kS6BlockX * kS6BlockY) void feather_kernel(const __grid_constant__ FeatherArgs p) {
     __shared__ unsigned long long sums[2];
+    __shared__ float unit[256];
+    static_assert(kS6BlockX * kS6BlockY == 256, "one byte value per thread");
     const s6::Geometry& g = p.g;
     const int x = blockIdx.x * kS6BlockX + threadIdx.x, y = blockIdx.y * kS6BlockY + threadIdx.y;
     const int t = threadIdx.y * kS6BlockX + threadIdx.x;
-    if (p.stats && t < 2) sums[t] = 0;
-    if (p.stats) __syncthreads();
+    unit[t] = static_cast<float>(__ddiv_rn(static_cast<double>(t), 255.0));
+    if (t < 2) sums[t] = 0;
+    __syncthreads();
     bool ma = false, mb = false;
     if (x < g.width && y < g.height) {
-        const double xa = static_cast<double>(x) + g.origin_x, ya = static_cast<double>(y) + g.origin_y;
+        const int ia = x + g.origin_x, ja = y + g.origin_y;  // no overflow: origin <= 0 < x
+        const double xa = ia, ya = ja;
         float ra[3] = {}, rb[3] = {};
         double sa = 0, sb = 0;
-        ma = sample(p.a, xa, ya, ra, sa, g.snap_tolerance);
+        ma = sample_at_pixel(p.a, ia, ja, unit, ra, sa);
         const double* m = g.inverse;
         const double den = __dadd_rn(__dadd_rn(__dmul_rn(m[6], xa), __dmul_rn(m[7], ya)), m[8]);
         const double den_scale = __dadd_rn(__dadd_rn(fabs(__dmul_rn(m[6], xa)), fabs(__dmul_rn(m[7], ya))), fabs(m[8]));

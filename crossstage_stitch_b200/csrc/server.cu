@@ -10,7 +10,9 @@
 // the batched registration chain (batch.cu: every kernel once for all of
 // its pairs), and copies the homography results back; when its event
 // completes the region and the stream return to the pool and the results
-// are handed to stitch_server_poll. A pair's result does not depend on the
+// are handed to stitch_server_poll. Two optional phases run on the same
+// stream and region before that: the S5 extension retry of requests below
+// their bar, then the S6 feather panorama of RGB requests that asked for one. A pair's result does not depend on the
 // batch it ran in: the batched chain equals the per-pair stages bit for bit.
 //
 // No reference counterpart: the reference registers one pair at a time
@@ -20,6 +22,7 @@
 #include <chrono>
 #include <condition_variable>
 #include <deque>
+#include <limits>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -125,7 +128,20 @@ struct Request {
     stitch_request r;
     Geometry g;
     double submit_ms = 0.0;
-    std::size_t footprint = 0;  // images + its share of a batch workspace, alone
+    std::size_t footprint = 0;     // images + its share of a batch workspace, alone
+    std::size_t render_bytes = 0;  // S6 canvas planes + counters (0: no panorama)
+};
+
+// S6 canvas planes of one request inside its batch region: packed RGB rows,
+// packed mask rows, then the two uint64 counters.
+std::size_t render_bytes(std::size_t capacity) {
+    return round_up(3 * capacity, kAlign) + round_up(capacity, kAlign) + kAlign;
+}
+
+// Outcome of one request's panorama, reported in its result.
+struct Panorama {
+    int status = -1;  // not asked for
+    int width = 0, height = 0, origin_x = 0, origin_y = 0;
 };
 
 struct Slot {
@@ -140,8 +156,12 @@ struct Slot {
     std::size_t ws_offset = 0;   // batch workspace inside the region
     double launch_ms = 0.0;
     bool busy = false;
-    bool retrying = false;       // the S5 extension retries are on the stream
+    int phase = 0;               // 0 registering, 1 retries enqueued, 2 panoramas enqueued
     std::vector<int> attempts;   // per request
+    std::vector<std::size_t> host_off;    // 2 per request: the copied images
+    std::vector<std::size_t> render_off;  // per request: its S6 planes (panorama requests)
+    std::vector<Panorama> panoramas;      // per request
+    std::uint64_t* render_counts = nullptr;  // pinned, 2 per request slot
 };
 
 // Pair descriptor of a request whose registered (GRAY8) images start at
@@ -181,7 +201,9 @@ public:
                 cudaHostAlloc(reinterpret_cast<void**>(&s.s1_staging), s1_staging_bytes(), cudaHostAllocDefault) !=
                     cudaSuccess ||
                 cudaHostAlloc(reinterpret_cast<void**>(&s.results),
-                              cfg_.max_batch * sizeof(stitch_homography_result), cudaHostAllocDefault) != cudaSuccess)
+                              cfg_.max_batch * sizeof(stitch_homography_result), cudaHostAllocDefault) != cudaSuccess ||
+                cudaHostAlloc(reinterpret_cast<void**>(&s.render_counts), 2 * cfg_.max_batch * sizeof(std::uint64_t),
+                              cudaHostAllocDefault) != cudaSuccess)
                 return Status::CUDA_ERROR;
         }
         worker_ = std::thread([this] { loop(); });
@@ -190,10 +212,15 @@ public:
 
     Status submit(const stitch_request& r) {
         if (!r.host_a || !r.host_b) return Status::INVALID_ARGUMENT;
+        if ((r.host_mask && !r.host_panorama) ||
+            (r.host_panorama && (!r.rgb || r.panorama_capacity == 0 ||
+                                 r.panorama_capacity > std::numeric_limits<std::size_t>::max() / 8)))
+            return Status::INVALID_ARGUMENT;
         Request q;
         q.r = r;
         Status st = geometry(r, &q.g);
         if (st != Status::OK) return st;
+        if (r.host_panorama) q.render_bytes = render_bytes(r.panorama_capacity);
         // footprint: the request alone in a batch (host layout only)
         const auto* fake = reinterpret_cast<const unsigned char*>(kAlign);
         stitch_pair_desc d = pair_desc(q, fake, fake);
@@ -201,7 +228,7 @@ public:
         int bad = -1;
         st = p.build(1, &d, &bad, false);
         if (st != Status::OK) return st;
-        q.footprint = q.g.bytes() + round_up(p.total, kAlign) + (q.g.rgb ? kAlign : 0);
+        q.footprint = q.g.bytes() + round_up(p.total, kAlign) + (q.g.rgb ? kAlign : 0) + q.render_bytes;
         if (q.footprint > cfg_.arena_bytes || p.table_bytes > staging_cap()) return Status::INSUFFICIENT_WORKSPACE;
         q.submit_ms = now_ms();
         {
@@ -243,6 +270,7 @@ public:
             if (s.staging) cudaFreeHost(s.staging);
             if (s.s1_staging) cudaFreeHost(s.s1_staging);
             if (s.results) cudaFreeHost(s.results);
+            if (s.render_counts) cudaFreeHost(s.render_counts);
             s = Slot{};
         }
     }
@@ -269,15 +297,29 @@ private:
             r.status = static_cast<int>(launch_status);
             r.attempts = i < s.attempts.size() ? s.attempts[i] : 1;
             if (launch_status == Status::OK) r.result = s.results[i];
+            r.render_status = -1;
+            if (s.reqs[i].render_bytes) {
+                const Panorama pano = i < s.panoramas.size() ? s.panoramas[i] : Panorama{};
+                r.render_status = launch_status != Status::OK ? static_cast<int>(launch_status) : pano.status;
+                if (r.render_status == static_cast<int>(Status::OK)) {
+                    r.canvas_width = pano.width;
+                    r.canvas_height = pano.height;
+                    r.origin_x = pano.origin_x;
+                    r.origin_y = pano.origin_y;
+                    r.union_pixels = s.render_counts[2 * i];
+                    r.overlap_pixels = s.render_counts[2 * i + 1];
+                }
+            }
             out.push_back(r);
         }
         if (s.bytes) arena_.release(s.offset, s.bytes);
         s.plan.reset();
         s.reqs.clear();
         s.attempts.clear();
+        s.panoramas.clear();
         s.bytes = 0;
         s.busy = false;
-        s.retrying = false;
+        s.phase = 0;
         std::lock_guard<std::mutex> g(mu_);
         done_.insert(done_.end(), out.begin(), out.end());
         outstanding_ -= static_cast<int>(out.size());
@@ -326,6 +368,63 @@ private:
         return any;
     }
 
+    // After registration (and retries): the S6 feather panorama of every
+    // request that asked for one, from its registered H in original
+    // coordinates (src/s6/geometry.cpp:106-200, src/s6/s6.cu:328-380), on the
+    // batch's resident RGB images, then copied to the caller's host buffers.
+    // Returns true when work was enqueued.
+    bool render(Slot& s) {
+        bool any = false;
+        auto* base = static_cast<unsigned char*>(cfg_.arena) + s.offset;
+        s.panoramas.assign(s.reqs.size(), Panorama{});
+        for (std::size_t i = 0; i < s.reqs.size(); ++i) {
+            const Request& q = s.reqs[i];
+            if (!q.render_bytes) continue;
+            Panorama& pano = s.panoramas[i];
+            const stitch_homography_result& res = s.results[i];
+            if (res.status != static_cast<int>(Status::OK)) {
+                pano.status = res.status;
+                continue;
+            }
+            s6::GeometryPolicy policy;
+            policy.max_canvas_pixels = std::min(policy.max_canvas_pixels, q.r.panorama_capacity);
+            s6::Geometry g;
+            Status st = s6::prepare_geometry(q.r.width_a, q.r.height_a, q.r.width_b, q.r.height_b, res.H, policy, &g);
+            pano.status = static_cast<int>(st);
+            if (st != Status::OK) continue;
+            const std::size_t px = static_cast<std::size_t>(g.width) * static_cast<std::size_t>(g.height);
+            unsigned char* out = base + s.render_off[i];
+            unsigned char* mask = out + round_up(3 * q.r.panorama_capacity, kAlign);
+            auto* counts = reinterpret_cast<s6::RenderStatistics*>(mask + round_up(q.r.panorama_capacity, kAlign));
+            const ImageView a{base + s.host_off[2 * i], q.r.width_a, q.r.height_a, image_pitch(3 * q.r.width_a),
+                              PixelFormat::RGB8};
+            const ImageView b{base + s.host_off[2 * i + 1], q.r.width_b, q.r.height_b, image_pitch(3 * q.r.width_b),
+                              PixelFormat::RGB8};
+            const ImageView vo{out, g.width, g.height, 3 * g.width, PixelFormat::RGB8};
+            const ImageView vm{mask, g.width, g.height, g.width, PixelFormat::GRAY8};
+            st = s6::render(a, b, g, s6::BlendMode::Feather, vo, vm, nullptr, 0, s.stream, counts);
+            if (st == Status::OK &&
+                (cudaMemcpyAsync(q.r.host_panorama, out, 3 * px, cudaMemcpyDeviceToHost, s.stream) != cudaSuccess ||
+                 (q.r.host_mask &&
+                  cudaMemcpyAsync(q.r.host_mask, mask, px, cudaMemcpyDeviceToHost, s.stream) != cudaSuccess) ||
+                 cudaMemcpyAsync(s.render_counts + 2 * i, counts, sizeof(s6::RenderStatistics),
+                                 cudaMemcpyDeviceToHost, s.stream) != cudaSuccess))
+                st = Status::CUDA_ERROR;
+            pano.status = static_cast<int>(st);
+            if (st != Status::OK) continue;
+            pano.width = g.width;
+            pano.height = g.height;
+            pano.origin_x = g.origin_x;
+            pano.origin_y = g.origin_y;
+            any = true;
+        }
+        if (any && cudaEventRecord(s.done, s.stream) != cudaSuccess) {
+            cudaStreamSynchronize(s.stream);
+            return false;
+        }
+        return any;
+    }
+
     // Forms a batch from the head of the queue and launches it on slot s.
     bool launch(Slot& s) {
         if (pending_.empty()) return false;
@@ -365,6 +464,11 @@ private:
             }
             const std::size_t s1_tables = images;
             if (rgb_images) images += round_up(s1_staging_bytes(), kAlign);
+            std::vector<std::size_t> render_off(n, 0);
+            for (int i = 0; i < n; ++i) {
+                render_off[i] = images;
+                images += pending_[i].render_bytes;
+            }
             // lay out with placeholder addresses to size the region
             auto plan = std::make_unique<Plan>();
             std::vector<stitch_pair_desc> descs(n);
@@ -398,6 +502,8 @@ private:
             s.bytes = bytes;
             s.ws_offset = images;
             s.attempts.assign(n, 1);
+            s.host_off = host_off;
+            s.render_off = render_off;
             s.launch_ms = now_ms();
             s.busy = true;
             Status st = Status::OK;
@@ -473,15 +579,16 @@ private:
             bool progressed = false;
             for (auto& s : slots_) {
                 if (s.busy && cudaEventQuery(s.done) == cudaSuccess) {
-                    if (!s.retrying) {
-                        s.retrying = true;
-                        if (retry(s)) {
-                            progressed = true;
-                            continue;
-                        }
+                    progressed = true;
+                    if (s.phase == 0) {
+                        s.phase = 1;
+                        if (retry(s)) continue;
+                    }
+                    if (s.phase == 1) {
+                        s.phase = 2;
+                        if (render(s)) continue;
                     }
                     finish(s, Status::OK);
-                    progressed = true;
                 }
             }
             for (auto& s : slots_) {

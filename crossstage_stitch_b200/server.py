@@ -42,13 +42,16 @@ class Server:
         self._buf = (ServerResult * 256)()
 
     def submit(self, gray_a, gray_b, knobs: Knobs, tag: int, scale_a=None, scale_b=None, s1_scale: float = 1.0,
-               retry_hypotheses: int = 0, retry_min_inliers: int = 0) -> int:
+               retry_hypotheses: int = 0, retry_min_inliers: int = 0, panorama_capacity: int = 0) -> int:
         """Queues one pair; returns the status code (0 = queued). (rows, cols, 3)
         images are RGB8: the server converts and resizes them with S1 at
         s1_scale on the device and returns H in their original coordinates.
         retry_hypotheses > knobs.hypotheses: a result that is not OK or has
         fewer than retry_min_inliers inliers is retried once by extending the
-        saved S5 search to retry_hypotheses."""
+        saved S5 search to retry_hypotheses. panorama_capacity > 0 (RGB8
+        requests): the server also renders the S6 feather panorama of the
+        original images from the returned H, for canvases of up to that many
+        pixels; poll() then returns it as "panorama" (h, w, 3) and "mask"."""
         a, b = pinned_image(gray_a), pinned_image(gray_b)
         r = Request()
         r.host_a, r.host_b = a.data_ptr(), b.data_ptr()
@@ -63,7 +66,12 @@ class Server:
             r.scale_b = scale_b
         r.s2, r.s4, r.s5, r.pyramid = knobs.s2(), knobs.s4(), knobs.s5(), knobs.pyramid()
         r.tag = tag
-        self.held[tag] = (a, b)
+        pano = mask = None
+        if panorama_capacity > 0:
+            pano = torch.empty(3 * panorama_capacity, dtype=torch.uint8, pin_memory=True)
+            mask = torch.empty(panorama_capacity, dtype=torch.uint8, pin_memory=True)
+            r.host_panorama, r.host_mask, r.panorama_capacity = pano.data_ptr(), mask.data_ptr(), panorama_capacity
+        self.held[tag] = (a, b, pano, mask)
         st = self.lib.stitch_server_submit(self.handle, C.byref(r))
         if st != 0:
             del self.held[tag]
@@ -81,8 +89,14 @@ class Server:
                 d = result_dict(r.result) if r.status == 0 else {"status": r.status}
                 d.update(tag=r.tag, submit_ms=r.submit_ms, launch_ms=r.launch_ms, done_ms=r.done_ms,
                          latency_ms=r.done_ms - r.submit_ms, batch_pairs=r.batch_pairs, run_status=r.status,
-                         attempts=r.attempts)
-                self.held.pop(r.tag, None)
+                         attempts=r.attempts, render_status=r.render_status)
+                held = self.held.pop(r.tag, None)
+                if r.render_status == 0 and held is not None:
+                    w, h = r.canvas_width, r.canvas_height
+                    d.update(panorama=held[2][:3 * w * h].numpy().reshape(h, w, 3).copy(),
+                             mask=held[3][:w * h].numpy().reshape(h, w).copy(), canvas=(w, h),
+                             origin=(r.origin_x, r.origin_y), union_pixels=r.union_pixels,
+                             overlap_pixels=r.overlap_pixels)
                 out.append(d)
             if n.value < len(self._buf):
                 return out

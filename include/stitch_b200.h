@@ -369,7 +369,16 @@ typedef struct stitch_server_config {
  * extending the saved S5 search to retry_hypotheses on the resident
  * keypoints and matches (the controller's R escalation,
  * src/controller/reuse.cpp:5-22: no resampling, same result as a fresh run
- * with retry_hypotheses). `tag` is returned with the result. */
+ * with retry_hypotheses). `tag` is returned with the result.
+ * S6 (rgb = 1 only): with host_panorama not NULL, after registration (and
+ * any retry) the server renders the feather panorama of the two original
+ * RGB images from the returned H (stitch_s6_prepare_geometry with the
+ * default policy, then stitch_s6_render) into host_panorama as packed rows
+ * of 3 * canvas width bytes and, when host_mask is not NULL, the 0/1 union
+ * mask into host_mask (packed rows of canvas width bytes).
+ * panorama_capacity is the largest canvas, in pixels, the buffers hold;
+ * that much device memory is part of the request's arena footprint. Pinned
+ * buffers keep the dispatcher from blocking on the copies. */
 typedef struct stitch_request {
     const uint8_t* host_a;
     const uint8_t* host_b;
@@ -385,13 +394,21 @@ typedef struct stitch_request {
     int retry_hypotheses;
     int retry_min_inliers;
     uint64_t tag;
+    uint8_t* host_panorama;
+    uint8_t* host_mask;
+    size_t panorama_capacity;
 } stitch_request;
 
 /* Completed request. Times are milliseconds on a steady clock since the
  * server was created: submit (stitch_server_submit), launch (its batch
  * enqueued) and done (the dispatcher saw its batch complete, results on the
  * host). status is 0 unless the request could not run; attempts is 2 when
- * the S5 extension retry ran. */
+ * the S5 extension retry ran. render_status is -1 when no panorama was
+ * asked for; otherwise the registration's status when it was not OK, else
+ * the status of the geometry (DEGENERATE, or INSUFFICIENT_WORKSPACE for a
+ * canvas above panorama_capacity or the default 16777216-pixel budget) or
+ * of the render; with 0 the canvas size, its origin in A's pixels and the
+ * union/overlap pixel counts describe the panorama written. */
 typedef struct stitch_server_result {
     uint64_t tag;
     double submit_ms, launch_ms, done_ms;
@@ -399,6 +416,9 @@ typedef struct stitch_server_result {
     int status;
     int attempts;
     stitch_homography_result result;
+    int render_status;
+    int canvas_width, canvas_height, origin_x, origin_y;
+    uint64_t union_pixels, overlap_pixels;
 } stitch_server_result;
 
 typedef struct stitch_server stitch_server;

@@ -172,3 +172,53 @@ def test_retry_extends_the_saved_search(cuda):
     same(got[0], full)
     same(got[1], short)
     same(got[2], other)
+
+
+def test_rgb_requests_render_their_panorama(cuda):
+    """S6 in the served form: the panorama and mask of each RGB request equal
+    the feather render of its original images under the returned H (the
+    stage call on the same GPU, and the oracle bit for bit); a canvas above
+    the request's capacity reports INSUFFICIENT_WORKSPACE with the
+    registration result intact; a GRAY8 request cannot ask for one."""
+    import torch
+
+    from crossstage_stitch_b200 import render
+    from oracle import c_oracle
+
+    rng = np.random.default_rng(21)
+    cases = []
+    for i, scale in enumerate((1.0, 0.5)):
+        p = synth.config0_pair(80 + i)
+        noise = rng.integers(-3, 4, p.gray_a.shape + (3,))
+        a = np.clip(p.gray_a[..., None].astype(int) + noise, 0, 255).astype(np.uint8)
+        b = np.clip(p.gray_b[..., None].astype(int) + noise[::-1], 0, 255).astype(np.uint8)
+        cases.append((a, b, scale, stages.Knobs(max_keypoints=800, seed=800 + i, levels=8)))
+    srv = Server(arena_bytes=1 << 30, max_batch=8, streams=2)
+    for n, (a, b, scale, k) in enumerate(cases):
+        assert srv.submit(a, b, k, tag=n, s1_scale=scale, panorama_capacity=4 << 20) == 0
+    a, b, scale, k = cases[0]
+    assert srv.submit(a, b, k, tag=10, s1_scale=scale, panorama_capacity=1000) == 0  # too small a canvas
+    assert srv.submit(a, b, k, tag=11, s1_scale=scale) == 0                           # no panorama
+    gray = synth.config0_pair(80)
+    assert srv.submit(gray.gray_a, gray.gray_b, k, tag=12, panorama_capacity=1 << 20) != 0
+    got = {r["tag"]: r for r in srv.drain()}
+    srv.close()
+    for n, (a, b, scale, k) in enumerate(cases):
+        r = got[n]
+        assert r["status"] == 0 and r["render_status"] == 0
+        H = r["H"]
+        g = render.prepare_geometry(a.shape[1], a.shape[0], b.shape[1], b.shape[0], H)
+        assert r["canvas"] == (g.width, g.height) and r["origin"] == (g.origin_x, g.origin_y)
+        stats = torch.zeros(2, dtype=torch.int64, device="cuda")
+        pano, mask = render.render(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda(), g, statistics=stats)
+        torch.cuda.synchronize()
+        assert np.array_equal(r["panorama"], pano.cpu().numpy()) and np.array_equal(r["mask"], mask.cpu().numpy())
+        assert [r["union_pixels"], r["overlap_pixels"]] == stats.tolist()
+        st, og = c_oracle.s6_geometry(a.shape[1], a.shape[0], b.shape[1], b.shape[0], H)
+        opano, omask, ostats = c_oracle.s6_feather(a, b, og)
+        assert st == 0 and np.array_equal(r["panorama"], opano) and np.array_equal(r["mask"], omask)
+        assert (r["union_pixels"], r["overlap_pixels"]) == ostats
+    assert got[10]["status"] == 0 and got[10]["render_status"] == 2
+    np.testing.assert_array_equal(got[10]["H"], got[0]["H"])
+    assert got[11]["render_status"] == -1 and "panorama" not in got[11]
+    np.testing.assert_array_equal(got[11]["H"], got[0]["H"])
