@@ -84,10 +84,16 @@ class Clocks:
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                          "--format=csv,noheader,nounits", "-lms", "10"],
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except OSError:
             self.proc = None
+        # the timed region starts only once the sampler is producing rows
+        t0 = time.time()
+        while self.proc is not None and self.proc.poll() is None and time.time() - t0 < 5.0:
+            if self.path.exists() and self.path.stat().st_size > 0:
+                break
+            time.sleep(0.01)
 
     def stop(self) -> dict:
         if self.proc is None:
@@ -131,17 +137,78 @@ def cpu_baseline(sample_pairs: int, workers: int) -> dict:
             "p50_ms": 1e3 * lat[len(lat) // 2], "p99_ms": 1e3 * lat[int(0.99 * (len(lat) - 1))]}
 
 
+def opencv_pair(i):
+    """One pair through OpenCV on one thread: ORB (K features, 8 levels at
+    1.2, FAST 20, Harris score, 31 px patches), brute-force Hamming kNN-2
+    with ratio 0.8, RANSAC findHomography (3 px, 2000 iterations, confidence
+    0.995). This is the product-like CPU chain of the reference's mock stages
+    (tools/mock/stages.py:58-114) at this workload's knobs; its results are
+    not the reference's."""
+    import cv2
+    import numpy as np
+    from crossstage_stitch_b200 import synth
+    cv2.setNumThreads(1)
+    p = synth.config0_pair(i)
+    t = time.perf_counter()
+    orb = cv2.ORB_create(nfeatures=K, scaleFactor=SCALE, nlevels=LEVELS, edgeThreshold=31, fastThreshold=20,
+                         scoreType=cv2.ORB_HARRIS_SCORE, patchSize=31)
+    ka, da = orb.detectAndCompute(p.gray_a, None)
+    kb, db = orb.detectAndCompute(p.gray_b, None)
+    if da is not None and db is not None and len(ka) >= 2 and len(kb) >= 2:
+        good = [m for m in cv2.BFMatcher(cv2.NORM_HAMMING).knnMatch(da, db, k=2)
+                if len(m) == 2 and m[0].distance < 0.8 * m[1].distance]
+        if len(good) >= 4:
+            src = np.float64([kb[m[0].trainIdx].pt for m in good])
+            dst = np.float64([ka[m[0].queryIdx].pt for m in good])
+            cv2.setRNGSeed(i)
+            cv2.findHomography(src, dst, cv2.RANSAC, 3.0, maxIters=2000, confidence=0.995)
+    return time.perf_counter() - t
+
+
+def opencv_baseline(n_pairs: int, workers: int) -> dict:
+    """The OpenCV chain on 1 core and on `workers` processes (spawned pool)."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    out = {"workload": f"{n_pairs} pairs of the workload, OpenCV ORB + BFMatcher + RANSAC findHomography",
+           "unit": "pairs/s", "cores": workers}
+    for n in (1, workers):
+        with ctx.Pool(n) as pool:
+            pool.map(opencv_pair, range(n))  # imports
+            t = time.perf_counter()
+            lat = sorted(pool.map(opencv_pair, range(n_pairs)))
+            wall = time.perf_counter() - t
+        key = "one_core" if n == 1 else "all_cores"
+        out[key] = n_pairs / wall
+        out[key + "_p50_ms"] = 1e3 * lat[len(lat) // 2]
+        out[key + "_p99_ms"] = 1e3 * lat[int(0.99 * (len(lat) - 1))]
+    return out
+
+
 def run_reference(args):
+    """The reference arm: the oracle chain on every host core, one pool for
+    the whole run; a step is one pair per worker process."""
+    import multiprocessing as mp
     workers = min(os.cpu_count() or 1, 32)
-    for _ in range(args.warmup):
-        cpu_baseline(workers, workers)
-    vals = [cpu_baseline(workers, workers) for _ in range(args.steps)]
-    v = statistics.median(x["value"] for x in vals)
+    ctx = mp.get_context("spawn")
+    times, lat = [], []
+    with ctx.Pool(workers) as pool:
+        pool.map(cpu_pair, [(0, 0)] * workers)  # warm the workers (imports)
+        for _ in range(args.warmup):
+            pool.map(cpu_pair, [(i % N_PAIRS, 0) for i in range(workers)])
+        for step in range(args.steps):
+            t = time.perf_counter()
+            lat += pool.map(cpu_pair, [((step * workers + i) % N_PAIRS, 0) for i in range(workers)])
+            times.append(time.perf_counter() - t)
+    v = workers * args.steps / sum(times)
+    lat.sort()
+    sample = (f"{args.steps} steps of {workers} pairs of the workload, one per process on {workers} processes "
+              f"(NumPy S2/S3 + C S4/S5 restatement of the reference)")
     line = {"impl": "reference", "metric": "pairs/s", "value": v, "unit": "pairs/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * workers / v,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/i32/f64",
             "data": "synthetic", "config": {"workload": WORKLOAD, "pairs_per_step": workers},
-            "cpu_baseline": {**vals[-1], "value": v},
+            "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": workers, "kind": "port", "sample": sample,
+                             "p50_ms": 1e3 * lat[len(lat) // 2], "p99_ms": 1e3 * lat[int(0.99 * (len(lat) - 1))]},
             "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -450,7 +517,7 @@ def algorithmic_work(batch, n_pairs, counts):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=50)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -485,6 +552,10 @@ def main():
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(32, min(os.cpu_count() or 1, 32))   # spawned pool, before any CUDA work
+        try:
+            cpu["opencv_chain"] = opencv_baseline(N_PAIRS, min(os.cpu_count() or 1, 32))
+        except ImportError as e:  # OpenCV is not part of the product
+            cpu["opencv_chain"] = {"unavailable": str(e)}
     mixed = None
     if rank == 0 and world == 1 and not args.no_mixed:
         mixed = make_mixed(N_MIXED, min(os.cpu_count() or 1, 32))   # spawned pool, before any CUDA work

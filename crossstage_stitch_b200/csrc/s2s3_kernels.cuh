@@ -173,18 +173,6 @@ __device__ __forceinline__ int reflect101(int i, int n) {
     return i;
 }
 
-// Necessary condition for a FAST-9 corner: a 9-pixel arc always holds two of
-// the four compass pixels, so two of them must be beyond the threshold on
-// the same side.
-__device__ __forceinline__ bool fast_compass(const std::uint8_t* p, int stride, int thr) {
-    const int v = p[0];
-    const int s0 = p[3 * stride], s4 = p[3], s8 = p[-3 * stride], s12 = p[-3];
-    const int hi = v + thr, lo = v - thr;
-    const int n_bright = (s0 > hi) + (s4 > hi) + (s8 > hi) + (s12 > hi);
-    const int n_dark = (s0 < lo) + (s4 < lo) + (s8 < lo) + (s12 < lo);
-    return n_bright >= 2 || n_dark >= 2;
-}
-
 // FAST-9 score of the pixel at p (row stride `stride`), 0 when it is not a
 // corner. With d_k = centre - ring_k over the 16-pixel circle, a 9-pixel arc
 // scores min(d) when darker and min(-d) when brighter; the raw score is the
@@ -219,6 +207,27 @@ __device__ __forceinline__ int fast_score(const std::uint8_t* p, int stride, int
     const unsigned lo = best & 0xffffu, hi = best >> 16;
     const int score = static_cast<int>(lo > hi ? lo : hi) - 256;
     return score > thr ? score - 1 : 0;
+}
+
+// Compass test of two pixels in 16-bit lanes (values 0..255), a necessary
+// condition for a FAST-9 corner: a 9-pixel arc always holds two of the four
+// compass pixels, so two of them must be beyond the threshold on the same
+// side, i.e. the second largest is brighter than v + t or the second
+// smallest darker than v - t. A
+// min/max network gives both (a = max(s0, s4), b = min(s0, s4), likewise
+// c, d for s8, s12; p = min(a, c), q = max(b, d); second largest max(p, q),
+// second smallest min(p, q)); x >= y per lane is the top bit of
+// (x | 0x8000) - y, with no borrow between lanes for x, y < 0x8000.
+// thr1 = (t + 1) in both lanes. Returns 0x8000 per passing lane.
+__device__ __forceinline__ std::uint32_t compass_pass2(std::uint32_t v, std::uint32_t s0, std::uint32_t s4,
+                                                       std::uint32_t s8, std::uint32_t s12, std::uint32_t thr1) {
+    const std::uint32_t a = __vmaxu2(s0, s4), b = __vminu2(s0, s4);
+    const std::uint32_t c = __vmaxu2(s8, s12), d = __vminu2(s8, s12);
+    const std::uint32_t p = __vminu2(a, c), q = __vmaxu2(b, d);
+    constexpr std::uint32_t kTop = 0x80008000u;
+    const std::uint32_t bright = ((__vmaxu2(p, q) | kTop) - (v + thr1)) & kTop;  // 2nd largest >= v + t + 1
+    const std::uint32_t dark = ((v | kTop) - (__vminu2(p, q) + thr1)) & kTop;    // v >= 2nd smallest + t + 1
+    return bright | dark;
 }
 
 // Shared-memory tile of the FAST kernel: rows of kInStride bytes holding
@@ -264,7 +273,7 @@ __device__ __forceinline__ std::uint32_t blur_byte(float acc) {
 // with each product and sum rounded on its own, then rounded half-to-even
 // and clamped), bit for bit the blur_kernel result.
 template <class Src>
-__global__ __launch_bounds__(256) void fast_nms_kernel(const __grid_constant__ Src src) {
+__global__ __launch_bounds__(256, 5) void fast_nms_kernel(const __grid_constant__ Src src) {
     __shared__ __align__(16) std::uint8_t in[kFastInH][kInStride];
     __shared__ __align__(16) std::uint8_t sc[kFastScH][kScStride];
     __shared__ std::uint16_t cand[kFastScH * kScGroups];
@@ -308,8 +317,7 @@ __global__ __launch_bounds__(256) void fast_nms_kernel(const __grid_constant__ S
     // 2. compass test: thread (q, rb) takes positions 4q .. 4q+3 of rows rb,
     // rb + 15, rb + 30; groups with a survivor are listed as
     // (group << 4 | survivor bits)
-    const std::uint32_t thr4 = static_cast<std::uint32_t>(j.threshold) * 0x01010101u;
-    constexpr std::uint32_t kOnes = 0x01010101u, kTwos = 0x02020202u;
+    const std::uint32_t thr1 = static_cast<std::uint32_t>(j.threshold + 1) * 0x00010001u;
     {
         constexpr int kRowSets = 256 / kScGroups;  // 15
         const int q = tid % kScGroups, rb = tid / kScGroups, c = 4 * q;
@@ -336,13 +344,14 @@ __global__ __launch_bounds__(256) void fast_nms_kernel(const __grid_constant__ S
                     const std::uint32_t s4 = __funnelshift_r(a1, a2, 16);  // 3 right
                     const std::uint32_t s0 = __funnelshift_r(bot[w], bot[w + 1], 24);  // 3 down
                     const std::uint32_t s8 = __funnelshift_r(top[w], top[w + 1], 24);  // 3 up
-                    const std::uint32_t hi = __vaddus4(v, thr4), lo = __vsubus4(v, thr4);
-                    const std::uint32_t nb = (__vcmpgtu4(s0, hi) & kOnes) + (__vcmpgtu4(s4, hi) & kOnes) +
-                                             (__vcmpgtu4(s8, hi) & kOnes) + (__vcmpgtu4(s12, hi) & kOnes);
-                    const std::uint32_t nd = (__vcmpltu4(s0, lo) & kOnes) + (__vcmpltu4(s4, lo) & kOnes) +
-                                             (__vcmpltu4(s8, lo) & kOnes) + (__vcmpltu4(s12, lo) & kOnes);
-                    const std::uint32_t pass = (__vcmpgeu4(nb, kTwos) | __vcmpgeu4(nd, kTwos)) & kOnes;
-                    bits = (pass | (pass >> 7) | (pass >> 14) | (pass >> 21)) & colmask;
+                    const std::uint32_t plo = compass_pass2(__byte_perm(v, 0, 0x4140), __byte_perm(s0, 0, 0x4140),
+                                                            __byte_perm(s4, 0, 0x4140), __byte_perm(s8, 0, 0x4140),
+                                                            __byte_perm(s12, 0, 0x4140), thr1);
+                    const std::uint32_t phi = compass_pass2(__byte_perm(v, 0, 0x4342), __byte_perm(s0, 0, 0x4342),
+                                                            __byte_perm(s4, 0, 0x4342), __byte_perm(s8, 0, 0x4342),
+                                                            __byte_perm(s12, 0, 0x4342), thr1);
+                    bits = (((plo >> 15) & 1u) | ((plo >> 30) & 2u) | ((phi >> 13) & 4u) | ((phi >> 28) & 8u)) &
+                           colmask;
                 }
             }
             const unsigned m = __ballot_sync(0xffffffffu, bits != 0);

@@ -141,9 +141,11 @@ class PairRunner:
     on one stream, exactly as the reference harness calls them."""
 
     def __init__(self, max_w: int, max_h: int, max_k: int, max_r: int = 8192, device: str | int = "cuda",
-                 cross_check: bool = False):
+                 cross_check: bool = False, stage_lib=None):
+        """stage_lib: an object with the stitch_* stage entry points of
+        include/stitch_b200.h (default: this library)."""
         self.device = torch.device(device)
-        L = lib()
+        self.L = L = stage_lib if stage_lib is not None else lib()
         self.max_w, self.max_h, self.max_k = max_w, max_h, max_k
         self.img = [torch.zeros((max_h, max_w), dtype=torch.uint8, device=self.device) for _ in range(2)]
         self.feat = [ImageFeatures(max_k, self.device) for _ in range(2)]
@@ -179,7 +181,7 @@ class PairRunner:
         key = (knobs.levels, float(np.float32(knobs.scale_factor)))
         if key not in self.wsp:
             b = C.c_size_t()
-            check("pyramid_workspace_bytes", lib().stitch_pyramid_workspace_bytes(
+            check("pyramid_workspace_bytes", self.L.stitch_pyramid_workspace_bytes(
                 self.max_w, self.max_h, ref(S2Config(20, self.max_k, 0.04)), ref(knobs.pyramid()), ref(b)))
             self.wsp[key] = (workspace(b.value, self.device), b.value)
         return self.wsp[key]
@@ -193,7 +195,7 @@ class PairRunner:
                 images: tuple[torch.Tensor, torch.Tensor] | None = None) -> None:
         """Enqueues S2..S5 (no sync) for the pair in self.img[0/1], or in
         `images` (two device uint8 tensors) when given."""
-        L = lib()
+        L = self.L
         s = stream_handle(stream)
         k = knobs.max_keypoints
         dims = ((wa, ha), (wb, hb))
