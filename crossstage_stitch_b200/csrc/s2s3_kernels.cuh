@@ -150,7 +150,8 @@ constexpr int kSortThreads = 1024;
 constexpr int kBlurTileW = 64, kBlurTileH = 32;
 constexpr int kDescWarps = 8;
 constexpr int kEdge = 31;
-constexpr int kResizeTileW = 64, kResizeTileH = 16;
+constexpr int kResizeTileW = 64, kResizeTileH = 64;
+constexpr int kResizeSrcRows = 2 * kResizeTileH + 2;  // source rows a tile stages (layer ratio <= 2)
 constexpr int kMaxLevels = 16;
 
 // ------------------------------------------------------------- FAST + NMS
@@ -776,17 +777,21 @@ __device__ __forceinline__ int2 linear_exact_tap(int v, int src, double scale) {
     return make_int2(static_cast<int>(fl), static_cast<int>(rint((f - fl) * 256.0)));
 }
 
-// One block = one 64x16 tile of the layer: per-column and per-row taps once
-// in shared memory, then 4 horizontally adjacent outputs per thread (one
-// 32-bit store), each
-//   (h(r0) * (256 - wy) + h(r1) * wy + 2^15) >> 16,
-//   h(r) = src[r][c0] * (256 - wx) + src[r][c1] * wx,
+// One block = one 64x64 tile of the layer, separable: per-column and per-row
+// taps once in shared memory; then the horizontal pass once per source row
+// the tile needs,
+//   h(r, c) = src[r][c0] * (256 - wx) + src[r][c1] * wx   (< 2^16),
+// kept as uint16 in shared memory; then the vertical pass, 4 horizontally
+// adjacent outputs per thread (one 32-bit store),
+//   (h(r0, c) * (256 - wy) + h(r1, c) * wy + 2^15) >> 16,
 // the integer form of the 8-bit fixed-point horizontal pass followed by the
-// vertical pass with one final rounding.
+// vertical pass with one final rounding. Tiles whose source rows exceed the
+// shared buffer (layer ratios above 2) read the source bytes directly.
 template <class Src>
 __global__ __launch_bounds__(256) void resize_kernel(const __grid_constant__ Src src, int kind) {
     __shared__ int2 xtap[kResizeTileW];
     __shared__ int2 ytap[kResizeTileH];
+    __shared__ __align__(16) std::uint16_t hrow[kResizeSrcRows][kResizeTileW];
     __shared__ double scale[2];
     ResizeJob j;
     int local;
@@ -801,30 +806,65 @@ __global__ __launch_bounds__(256) void resize_kernel(const __grid_constant__ Src
     else if (t < kResizeTileW + kResizeTileH)
         ytap[t - kResizeTileW] = linear_exact_tap(min(y0 + t - kResizeTileW, j.height - 1), j.src_height, scale[1]);
     __syncthreads();
-    const int r = t >> 4, c = 4 * (t & 15);
-    const int y = y0 + r, x = x0 + c;
-    if (y >= j.height || x >= j.width) return;
-    const int2 ty = ytap[r];
-    const std::uint8_t* pa = j.src + static_cast<std::size_t>(ty.x) * j.src_pitch;
-    const std::uint8_t* pb = j.src + static_cast<std::size_t>(min(ty.x + 1, j.src_height - 1)) * j.src_pitch;
-    std::uint32_t packed = 0;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const int2 tx = xtap[c + k];  // columns past the layer edge repeat the last tap
-        const int xa = tx.x, xb = min(tx.x + 1, j.src_width - 1);
-        const int wx1 = tx.y, wx0 = 256 - tx.y;
-        const int ha = __ldg(pa + xa) * wx0 + __ldg(pa + xb) * wx1;
-        const int hb = __ldg(pb + xa) * wx0 + __ldg(pb + xb) * wx1;
-        const int v = ha * (256 - ty.y) + hb * ty.y;
-        packed |= static_cast<std::uint32_t>((v + (1 << 15)) >> 16) << (8 * k);
+    const int sy0 = ytap[0].x;                                              // taps are nondecreasing
+    const int sy1 = min(ytap[kResizeTileH - 1].x + 1, j.src_height - 1);
+    const int nsrc = sy1 - sy0 + 1;
+    const bool staged = nsrc <= kResizeSrcRows;                             // block-uniform
+    if (staged) {
+        // horizontal pass: thread (r, c) for source row sy0 + r, output column c
+        for (int i = t; i < nsrc * kResizeTileW; i += 256) {
+            const int r = i / kResizeTileW, c = i - r * kResizeTileW;
+            const int2 tx = xtap[c];
+            const std::uint8_t* row = j.src + static_cast<std::size_t>(sy0 + r) * j.src_pitch;
+            hrow[r][c] = static_cast<std::uint16_t>(__ldg(row + tx.x) * (256 - tx.y) +
+                                                    __ldg(row + min(tx.x + 1, j.src_width - 1)) * tx.y);
+        }
+        __syncthreads();
     }
-    std::uint8_t* dst = j.dst + static_cast<std::size_t>(y) * j.pitch + x;
-    if (x + 3 < j.width && (reinterpret_cast<std::uintptr_t>(dst) & 3) == 0) {
-        *reinterpret_cast<std::uint32_t*>(dst) = packed;
-    } else {
+    // vertical pass: rows t/16 + 16 i, columns 4 (t % 16) .. +3
+    const int c = 4 * (t & 15);
+    const int x = x0 + c;
+    if (x >= j.width) return;
+    for (int rr = t >> 4; rr < kResizeTileH; rr += 16) {
+        const int y = y0 + rr;
+        if (y >= j.height) break;
+        const int2 ty = ytap[rr];
+        const int ra = ty.x, rb = min(ty.x + 1, j.src_height - 1);
+        std::uint32_t packed = 0;
+        if (staged) {
+            const uint2 ha = *reinterpret_cast<const uint2*>(&hrow[ra - sy0][c]);
+            const uint2 hb = *reinterpret_cast<const uint2*>(&hrow[rb - sy0][c]);
+            const int hav[4] = {static_cast<int>(ha.x & 0xffffu), static_cast<int>(ha.x >> 16),
+                                static_cast<int>(ha.y & 0xffffu), static_cast<int>(ha.y >> 16)};
+            const int hbv[4] = {static_cast<int>(hb.x & 0xffffu), static_cast<int>(hb.x >> 16),
+                                static_cast<int>(hb.y & 0xffffu), static_cast<int>(hb.y >> 16)};
 #pragma unroll
-        for (int k = 0; k < 4; ++k)
-            if (x + k < j.width) dst[k] = static_cast<std::uint8_t>(packed >> (8 * k));
+            for (int k = 0; k < 4; ++k) {
+                const int v = hav[k] * (256 - ty.y) + hbv[k] * ty.y;
+                packed |= static_cast<std::uint32_t>((v + (1 << 15)) >> 16) << (8 * k);
+            }
+        } else {
+            const std::uint8_t* pa = j.src + static_cast<std::size_t>(ra) * j.src_pitch;
+            const std::uint8_t* pb = j.src + static_cast<std::size_t>(rb) * j.src_pitch;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int2 tx = xtap[c + k];  // columns past the layer edge repeat the last tap
+                const int xa = tx.x, xb = min(tx.x + 1, j.src_width - 1);
+                const int wx1 = tx.y, wx0 = 256 - tx.y;
+                const int ha = __ldg(pa + xa) * wx0 + __ldg(pa + xb) * wx1;
+                const int hb = __ldg(pb + xa) * wx0 + __ldg(pb + xb) * wx1;
+                const int v = ha * (256 - ty.y) + hb * ty.y;
+                packed |= static_cast<std::uint32_t>((v + (1 << 15)) >> 16) << (8 * k);
+            }
+        }
+        std::uint8_t* dst = j.dst + static_cast<std::size_t>(y) * j.pitch + x;
+        if (x + 3 < j.width && (reinterpret_cast<std::uintptr_t>(dst) & 3) == 0) {
+            *reinterpret_cast<std::uint32_t*>(dst) = packed;
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (x + k < j.width) dst[k] = static_cast<std::uint8_t>(packed >> (8 * k));
+        }
     }
 }
 
