@@ -143,7 +143,7 @@ enum DescribeKind { kBlurKind = 0, kDescKind = 1, kDescribeKinds = 2 };
 constexpr int kFastTileW = 64, kFastTileH = 32;
 constexpr int kFastInW = kFastTileW + 8, kFastInH = kFastTileH + 8;  // halo 4 = FAST 3 + NMS 1
 constexpr int kFastScW = kFastTileW + 2, kFastScH = kFastTileH + 2;
-constexpr int kChunkPx = 8192;     // pixels per compaction block (256 threads x 32)
+constexpr int kChunkPx = 16384;    // pixels per compaction block (256 threads x 64)
 constexpr int kHarrisThreads = 256;
 constexpr int kSortCap = 16384;    // candidates sorted in shared memory by one block
 constexpr int kSortThreads = 1024;
@@ -505,19 +505,53 @@ __device__ __forceinline__ SelectParams select_params(const std::uint32_t* hist,
     return *out;
 }
 
-// Loads 32 maxima bytes of one thread (zero past the image end).
-__device__ __forceinline__ void load32(const std::uint8_t* maxima, long long first, long long pixels,
-                                       std::uint8_t (&b)[32]) {
-    if (first + 32 <= pixels) {
-        const uint4 lo = *reinterpret_cast<const uint4*>(maxima + first);
-        const uint4 hi = *reinterpret_cast<const uint4*>(maxima + first + 16);
-        const std::uint32_t w[8] = {lo.x, lo.y, lo.z, lo.w, hi.x, hi.y, hi.z, hi.w};
+// Loads the 64 maxima bytes of one thread as 16 little-endian words (zero
+// past the image end).
+__device__ __forceinline__ void load64(const std::uint8_t* maxima, long long first, long long pixels,
+                                       std::uint32_t (&w)[16]) {
+    if (first + 64 <= pixels) {
 #pragma unroll
-        for (int i = 0; i < 32; ++i) b[i] = static_cast<std::uint8_t>(w[i >> 2] >> (8 * (i & 3)));
+        for (int q = 0; q < 4; ++q) {
+            const uint4 v = *reinterpret_cast<const uint4*>(maxima + first + 16 * q);
+            w[4 * q] = v.x;
+            w[4 * q + 1] = v.y;
+            w[4 * q + 2] = v.z;
+            w[4 * q + 3] = v.w;
+        }
     } else {
 #pragma unroll
-        for (int i = 0; i < 32; ++i) b[i] = first + i < pixels ? maxima[first + i] : 0;
+        for (int q = 0; q < 16; ++q) {
+            std::uint32_t v = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const long long i = first + 4 * q + k;
+                if (i < pixels) v |= static_cast<std::uint32_t>(maxima[i]) << (8 * k);
+            }
+            w[q] = v;
+        }
     }
+}
+
+// (above << 16) + ties among the 4 maxima bytes of w (threshold >= 1, so a
+// byte equal to it is a maximum).
+__device__ __forceinline__ std::uint32_t count_word(std::uint32_t w, std::uint32_t thr) {
+    std::uint32_t packed = 0;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const std::uint32_t b = (w >> (8 * k)) & 0xffu;
+        packed += (b > thr) ? (1u << 16) : 0u;
+        packed += (b == thr) ? 1u : 0u;
+    }
+    return packed;
+}
+
+// Counts of one thread's 64 pixels; most words of a maxima map are zero.
+__device__ __forceinline__ std::uint32_t count64(const std::uint32_t (&w)[16], std::uint32_t thr) {
+    std::uint32_t packed = 0;
+#pragma unroll
+    for (int q = 0; q < 16; ++q)
+        if (w[q]) packed += count_word(w[q], thr);
+    return packed;
 }
 
 // Block-wide exclusive scan of packed (above << 16 | tie) counts (block totals
@@ -544,7 +578,7 @@ __device__ __forceinline__ std::uint32_t block_scan_packed(std::uint32_t v, std:
     return base + inc - v;
 }
 
-// Per 8192-pixel chunk: the 2K threshold (every block derives the same
+// Per 16384-pixel chunk: the 2K threshold (every block derives the same
 // one), the chunk's (above, tie) counts; chunk 0 publishes the parameters and
 // the keypoint count min(selected, K).
 template <class Src>
@@ -560,17 +594,11 @@ __global__ __launch_bounds__(256) void select_count_kernel(const __grid_constant
         *j.count = static_cast<int>(min(p.selected, static_cast<std::uint32_t>(j.max_keypoints)));
     }
     const long long pixels = static_cast<long long>(j.width) * j.height;
-    const long long first = static_cast<long long>(chunk) * kChunkPx + threadIdx.x * 32;
-    std::uint8_t b[32];
-    load32(j.maxima, first, pixels, b);
-    std::uint32_t packed = 0;
-#pragma unroll
-    for (int i = 0; i < 32; ++i) {
-        packed += (b[i] > p.threshold) ? (1u << 16) : 0u;
-        packed += (b[i] == p.threshold) ? 1u : 0u;  // threshold >= 1, so b == thr is a maximum
-    }
+    const long long first = static_cast<long long>(chunk) * kChunkPx + threadIdx.x * 64;
+    std::uint32_t w[16];
+    load64(j.maxima, first, pixels, w);
     std::uint32_t total;
-    block_scan_packed(packed, &total);
+    block_scan_packed(count64(w, p.threshold), &total);
     if (threadIdx.x == 0) {
         j.chunk_counts[2 * chunk] = total >> 16;
         j.chunk_counts[2 * chunk + 1] = total & 0xffffu;
@@ -604,27 +632,26 @@ __global__ __launch_bounds__(256) void scatter_kernel(const __grid_constant__ Sr
 #pragma unroll
     for (int w = 0; w < 8; ++w) { off_above += red[0][w]; off_tie += red[1][w]; }
     const long long pixels = static_cast<long long>(j.width) * j.height;
-    const long long first = static_cast<long long>(chunk) * kChunkPx + threadIdx.x * 32;
-    std::uint8_t b[32];
-    load32(j.maxima, first, pixels, b);
-    std::uint32_t packed = 0;
-#pragma unroll
-    for (int i = 0; i < 32; ++i) {
-        packed += (b[i] > p.threshold) ? (1u << 16) : 0u;
-        packed += (b[i] == p.threshold) ? 1u : 0u;
-    }
+    const long long first = static_cast<long long>(chunk) * kChunkPx + threadIdx.x * 64;
+    std::uint32_t w[16];
+    load64(j.maxima, first, pixels, w);
     std::uint32_t total;
-    const std::uint32_t excl = block_scan_packed(packed, &total);
+    const std::uint32_t excl = block_scan_packed(count64(w, p.threshold), &total);
     std::uint32_t ra = off_above + (excl >> 16), rt = off_tie + (excl & 0xffffu);
 #pragma unroll
-    for (int i = 0; i < 32; ++i) {
-        const std::uint64_t px = static_cast<std::uint64_t>(first + i);
-        if (b[i] > p.threshold) {
-            if (ra < p.above) j.keys[ra] = px;  // always true when map and histogram agree
-            ++ra;
-        } else if (b[i] == p.threshold) {
-            if (rt < p.ties) j.keys[p.above + rt] = px;
-            ++rt;
+    for (int q = 0; q < 16; ++q) {
+        if (!w[q]) continue;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const std::uint32_t b = (w[q] >> (8 * k)) & 0xffu;
+            const std::uint64_t px = static_cast<std::uint64_t>(first + 4 * q + k);
+            if (b > p.threshold) {
+                if (ra < p.above) j.keys[ra] = px;  // always true when map and histogram agree
+                ++ra;
+            } else if (b == p.threshold) {
+                if (rt < p.ties) j.keys[p.above + rt] = px;
+                ++rt;
+            }
         }
     }
 }
@@ -811,13 +838,28 @@ __global__ __launch_bounds__(256) void resize_kernel(const __grid_constant__ Src
     const int nsrc = sy1 - sy0 + 1;
     const bool staged = nsrc <= kResizeSrcRows;                             // block-uniform
     if (staged) {
-        // horizontal pass: thread (r, c) for source row sy0 + r, output column c
-        for (int i = t; i < nsrc * kResizeTileW; i += 256) {
-            const int r = i / kResizeTileW, c = i - r * kResizeTileW;
-            const int2 tx = xtap[c];
-            const std::uint8_t* row = j.src + static_cast<std::size_t>(sy0 + r) * j.src_pitch;
-            hrow[r][c] = static_cast<std::uint16_t>(__ldg(row + tx.x) * (256 - tx.y) +
-                                                    __ldg(row + min(tx.x + 1, j.src_width - 1)) * tx.y);
+        // horizontal pass: item i = (source row sy0 + i / 64, output column
+        // i % 64); a thread's column is fixed (256 is a multiple of 64), and
+        // four of its rows are loaded before any is used
+        const int c = t & (kResizeTileW - 1);
+        const int2 tx = xtap[c];
+        const int xa = tx.x, xb = min(tx.x + 1, j.src_width - 1), wx = tx.y;
+        const int n = nsrc * kResizeTileW;
+        for (int i0 = t; i0 < n; i0 += 4 * 256) {
+            int pa[4], pb[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int i = i0 + 256 * k;
+                const std::uint8_t* row = j.src + static_cast<std::size_t>(sy0 + (i < n ? i / kResizeTileW : 0)) *
+                                                      j.src_pitch;
+                pa[k] = i < n ? __ldg(row + xa) : 0;
+                pb[k] = i < n ? __ldg(row + xb) : 0;
+            }
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int i = i0 + 256 * k;
+                if (i < n) hrow[i / kResizeTileW][c] = static_cast<std::uint16_t>(pa[k] * (256 - wx) + pb[k] * wx);
+            }
         }
         __syncthreads();
     }
