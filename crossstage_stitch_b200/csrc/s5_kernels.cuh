@@ -580,6 +580,8 @@ struct SearchJob {
 // L1-backed local memory, but it is a small share of the work, and the
 // scoring loop gains the occupancy (1 block: 0.62 ms, 3 blocks: 0.43 ms for
 // 64 pairs x 2000 hypotheses x ~530 matches).
+constexpr int kPruneEvery = 256;  // points between the pruning checks of a model (multiple of 32)
+
 template <class Src>
 __global__ __launch_bounds__(kSearchThreads, 3) void search_kernel(const __grid_constant__ Src src) {
     extern __shared__ float4 pts[];
@@ -634,24 +636,45 @@ __global__ __launch_bounds__(kSearchThreads, 3) void search_kernel(const __grid_
                 double h[9];
 #pragma unroll
                 for (int e = 0; e < 9; ++e) h[e] = __shfl_sync(0xffffffffu, hm[e], k);
+                // Exact pruning against this warp's best so far: every term is
+                // >= 0 and a correctly rounded sum of nonnegative values is
+                // nondecreasing in each operand, so the tree sum of the partial
+                // accumulators never exceeds the final loss. Once it is above
+                // the best loss the model cannot win (ties need equal losses).
+                const bool prune = __shfl_sync(0xffffffffu, best.valid, 0) != 0;
+                const double bound = __shfl_sync(0xffffffffu, best.loss, 0);
                 double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
                 int slot = 0;
-                for (int i = lane; i < nm; i += 32) {
-                    Pt p;
-                    if (i < kStagePoints) {
-                        const float4 q = pts[i];
-                        p = Pt{q.x, q.y, q.z, q.w};
-                    } else {
-                        p = gather(j, i);
+                bool lost = false;
+                for (int base = 0; base < nm; base += 32) {  // warp-uniform trip count
+                    const int i = base + lane;
+                    if (i < nm) {
+                        Pt p;
+                        if (i < kStagePoints) {
+                            const float4 q = pts[i];
+                            p = Pt{q.x, q.y, q.z, q.w};
+                        } else {
+                            p = gather(j, i);
+                        }
+                        const double r = residual2(h, p);
+                        const double term = r < thr2 ? r : thr2;
+                        if (slot == 0) acc0 += term;
+                        else if (slot == 1) acc1 += term;
+                        else if (slot == 2) acc2 += term;
+                        else acc3 += term;
+                        slot = (slot + 1) & 3;
                     }
-                    const double r = residual2(h, p);
-                    const double term = r < thr2 ? r : thr2;
-                    if (slot == 0) acc0 += term;
-                    else if (slot == 1) acc1 += term;
-                    else if (slot == 2) acc2 += term;
-                    else acc3 += term;
-                    slot = (slot + 1) & 3;
+                    if (prune && (base & (kPruneEvery - 1)) == kPruneEvery - 32 && base + 32 < nm) {
+                        double part = (acc0 + acc2) + (acc1 + acc3);
+#pragma unroll
+                        for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
+                        if (__shfl_sync(0xffffffffu, part > bound ? 1 : 0, 0)) {
+                            lost = true;
+                            break;
+                        }
+                    }
                 }
+                if (lost) continue;
                 // virtual lanes l, l+32, l+64, l+96: strides 64 and 32 of the tree
                 double v = (acc0 + acc2) + (acc1 + acc3);
 #pragma unroll
