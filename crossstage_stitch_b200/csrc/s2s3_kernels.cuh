@@ -274,7 +274,7 @@ __device__ __forceinline__ std::uint32_t blur_byte(float acc) {
 // with each product and sum rounded on its own, then rounded half-to-even
 // and clamped), bit for bit the blur_kernel result.
 template <class Src>
-__global__ __launch_bounds__(256, 5) void fast_nms_kernel(const __grid_constant__ Src src) {
+__global__ __launch_bounds__(256, 6) void fast_nms_kernel(const __grid_constant__ Src src) {
     __shared__ __align__(16) std::uint8_t in[kFastInH][kInStride];
     __shared__ __align__(16) std::uint8_t sc[kFastScH][kScStride];
     __shared__ std::uint16_t cand[kFastScH * kScGroups];

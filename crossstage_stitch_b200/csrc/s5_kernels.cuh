@@ -499,6 +499,15 @@ __device__ __forceinline__ Pt gather(const PairIO& j, int i) {
               static_cast<double>(j.b.y[ib])};
 }
 
+// Match i of the pair: from the staged float4 copy when it is staged.
+__device__ __forceinline__ Pt point_at(const PairIO& j, const float4* pts, int i) {
+    if (i < kStagePoints) {
+        const float4 q = pts[i];
+        return Pt{q.x, q.y, q.z, q.w};
+    }
+    return gather(j, i);
+}
+
 __device__ __forceinline__ bool same_scale(const ScaleInfo& a, const ScaleInfo& b) {
     if (a.orig_w != b.orig_w || a.orig_h != b.orig_h || a.work_w != b.work_w || a.work_h != b.work_h ||
         a.sx != b.sx || a.sy != b.sy)
@@ -580,7 +589,7 @@ struct SearchJob {
 // L1-backed local memory, but it is a small share of the work, and the
 // scoring loop gains the occupancy (1 block: 0.62 ms, 3 blocks: 0.43 ms for
 // 64 pairs x 2000 hypotheses x ~530 matches).
-constexpr int kPruneEvery = 256;  // points between the pruning checks of a model (multiple of 32)
+constexpr int kPruneEvery = 256;  // points between the pruning checks of a model (multiple of 64)
 
 template <class Src>
 __global__ __launch_bounds__(kSearchThreads, 3) void search_kernel(const __grid_constant__ Src src) {
@@ -643,28 +652,28 @@ __global__ __launch_bounds__(kSearchThreads, 3) void search_kernel(const __grid_
                 // the best loss the model cannot win (ties need equal losses).
                 const bool prune = __shfl_sync(0xffffffffu, best.valid, 0) != 0;
                 const double bound = __shfl_sync(0xffffffffu, best.loss, 0);
+                // Lane l accumulates the points l, l+32, l+64, l+96 (virtual
+                // lanes, slots 0..3) and every 128 after them in order; two
+                // points per step give two independent FP64 chains. A point
+                // past nm adds +0.0, which leaves a sum of nonnegative terms
+                // (started at +0.0) bit for bit unchanged.
                 double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
-                int slot = 0;
                 bool lost = false;
-                for (int base = 0; base < nm; base += 32) {  // warp-uniform trip count
-                    const int i = base + lane;
-                    if (i < nm) {
-                        Pt p;
-                        if (i < kStagePoints) {
-                            const float4 q = pts[i];
-                            p = Pt{q.x, q.y, q.z, q.w};
-                        } else {
-                            p = gather(j, i);
-                        }
-                        const double r = residual2(h, p);
-                        const double term = r < thr2 ? r : thr2;
-                        if (slot == 0) acc0 += term;
-                        else if (slot == 1) acc1 += term;
-                        else if (slot == 2) acc2 += term;
-                        else acc3 += term;
-                        slot = (slot + 1) & 3;
+                for (int base = 0; base < nm; base += 64) {  // warp-uniform trip count
+                    const int i0 = base + lane, i1 = base + 32 + lane;
+                    const Pt p0 = point_at(j, pts, min(i0, nm - 1));
+                    const Pt p1 = point_at(j, pts, min(i1, nm - 1));
+                    const double r0 = residual2(h, p0), r1 = residual2(h, p1);
+                    const double t0 = i0 < nm ? (r0 < thr2 ? r0 : thr2) : 0.0;
+                    const double t1 = i1 < nm ? (r1 < thr2 ? r1 : thr2) : 0.0;
+                    if ((base & 127) == 0) {
+                        acc0 += t0;
+                        acc1 += t1;
+                    } else {
+                        acc2 += t0;
+                        acc3 += t1;
                     }
-                    if (prune && (base & (kPruneEvery - 1)) == kPruneEvery - 32 && base + 32 < nm) {
+                    if (prune && (base & (kPruneEvery - 1)) == kPruneEvery - 64 && base + 64 < nm) {
                         double part = (acc0 + acc2) + (acc1 + acc3);
 #pragma unroll
                         for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
