@@ -1002,9 +1002,9 @@ __device__ __forceinline__ int rotated_sample(const std::uint8_t* centre, int st
 // of the unblurred image (lane v sums rows +-v), the angle on lane 0 (float
 // fastAtan2, cos/sin evaluated in double then rounded to float), then lane l
 // packs pattern pairs 8l..8l+7 of the blurred image into descriptor byte l.
-template <class Src>
 // 8 blocks per SM (32 registers): the kernel waits on scattered patch loads,
 // so resident warps matter more than the few registers it spills.
+template <class Src>
 __global__ __launch_bounds__(kDescWarps * 32, 8) void describe_kernel(const __grid_constant__ Src src) {
     __shared__ std::uint32_t pat[8][32];  // pat[j][l] = pair 8l + j as 4 packed int8
     DescribeJob j;
