@@ -128,3 +128,85 @@ class Batch:
         out["distance"] = view(m.distance, nm, torch.float32).cpu().numpy()
         out["mask"] = view(mask.value, nm, torch.uint8).cpu().numpy()
         return out
+
+
+class StreamingBatches:
+    """The batched form over a stream of batches of one shape.
+
+    All images of a step live in one contiguous buffer (image `side` of pair
+    p at byte layout[p][side], rows of pitch_of(width) bytes), so a step's inputs
+    move with one host-to-device copy. Two device slots, each with its own
+    captured graph, alternate: step() copies the pinned host buffer into the
+    free slot on a copy stream and launches that slot's graph on the compute
+    stream when the copy lands, so the copy of one step overlaps the
+    registration of the previous one. A slot's results stay valid until the
+    step after next is launched; wait(slot) then result(slot, i) reads them.
+    The host buffer of a step must not be refilled before that step's copy
+    has finished (use two host buffers, alternating)."""
+
+    def __init__(self, sizes: list[tuple[int, int, int, int]], knobs: list[Knobs], device=None):
+        self.device = device or torch.device("cuda", torch.cuda.current_device())
+        self.sizes = list(sizes)
+        self.layout, cursor = [], 0
+        for (wa, ha, wb, hb) in self.sizes:
+            offs = []
+            for (w, h) in ((wa, ha), (wb, hb)):
+                offs.append(cursor)
+                cursor += -(-self.pitch_of(w) * h // 256) * 256
+            self.layout.append(tuple(offs))
+        self.nbytes = max(cursor, 1)
+        self.slots = [torch.empty(self.nbytes, dtype=torch.uint8, device=self.device) for _ in range(2)]
+        self.copy_stream = torch.cuda.Stream(self.device)
+        self.compute_stream = torch.cuda.Stream(self.device)
+        self.batches = []
+        for buf in self.slots:
+            descs = []
+            for (wa, ha, wb, hb), (oa, ob), k in zip(self.sizes, self.layout, knobs):
+                d = PairDesc()
+                d.image_a = ImageView(buf.data_ptr() + oa, wa, ha, self.pitch_of(wa), 1)
+                d.image_b = ImageView(buf.data_ptr() + ob, wb, hb, self.pitch_of(wb), 1)
+                d.s2, d.s4, d.s5 = k.s2(), k.s4(), k.s5()
+                d.pyramid = k.pyramid()
+                descs.append(d)
+            b = Batch(descs, self.device)
+            b.capture(self.compute_stream)
+            self.batches.append(b)
+        self.copied = [torch.cuda.Event() for _ in range(2)]
+        self.done = [torch.cuda.Event() for _ in range(2)]
+        for e in self.done:
+            e.record(self.compute_stream)
+        self.next = 0
+
+    @staticmethod
+    def pitch_of(width: int) -> int:
+        return -(-width // 16) * 16
+
+    def host_buffer(self) -> torch.Tensor:
+        """A pinned host buffer of this layout."""
+        return torch.zeros(self.nbytes, dtype=torch.uint8, pin_memory=True)
+
+    def fill(self, host: torch.Tensor, pair: int, gray_a: np.ndarray, gray_b: np.ndarray) -> None:
+        """Writes one pair's GRAY8 images into a host buffer of this layout."""
+        for side, g in enumerate((gray_a, gray_b)):
+            h, w = g.shape
+            off, pitch = self.layout[pair][side], self.pitch_of(w)
+            host[off:off + pitch * h].view(h, pitch)[:, :w].copy_(torch.from_numpy(np.ascontiguousarray(g)))
+
+    def step(self, host: torch.Tensor) -> int:
+        """Queues one step (copy, then registration); returns its slot."""
+        s = self.next
+        self.next ^= 1
+        self.copy_stream.wait_event(self.done[s])  # the slot's previous step has finished
+        with torch.cuda.stream(self.copy_stream):
+            self.slots[s].copy_(host, non_blocking=True)
+        self.copied[s].record(self.copy_stream)
+        self.compute_stream.wait_event(self.copied[s])
+        self.batches[s].launch(self.compute_stream)
+        self.done[s].record(self.compute_stream)
+        return s
+
+    def wait(self, slot: int) -> None:
+        self.done[slot].synchronize()
+
+    def result(self, slot: int, i: int) -> dict:
+        return self.batches[slot].result(i)
