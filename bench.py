@@ -562,7 +562,7 @@ def main():
 
     import torch
     import torch.distributed as dist
-    from crossstage_stitch_b200 import _abi, batch, stages, synth
+    from crossstage_stitch_b200 import _abi, batch, replicas, stages, synth
 
     torch.cuda.set_device(local)
     if world > 1:
@@ -571,8 +571,9 @@ def main():
     dev = torch.device("cuda", local)
     stream = torch.cuda.current_stream()
     L = _abi.load()
-    pairs = [synth.config0_pair(rank * N_PAIRS + i) for i in range(N_PAIRS)]
-    knobs = [knobs_for(rank * N_PAIRS + i) for i in range(N_PAIRS)]
+    mine = replicas.pair_indices(N_PAIRS, rank)  # each rank registers its own pairs (weak scaling)
+    pairs = [synth.config0_pair(g) for g in mine]
+    knobs = [knobs_for(g) for g in mine]
     host = [(torch.from_numpy(p.gray_a).pin_memory(), torch.from_numpy(p.gray_b).pin_memory()) for p in pairs]
     imgs = [(a.to(dev), b.to(dev)) for a, b in host]
     flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
@@ -687,10 +688,7 @@ def main():
         o = b.outputs(i)
         counts.append((len(o["kp_a"]), len(o["kp_b"]), len(o["idx_a"])))
 
-    tt = torch.tensor([t_batch, t_e2e, t_plain], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-    t_batch, t_e2e, t_plain = tt.tolist()
+    t_batch, t_e2e, t_plain = replicas.max_over_ranks([t_batch, t_e2e, t_plain], device=dev)
     pairs_total = N_PAIRS * args.steps * world
     if rank == 0:
         names = _abi.BATCH_MARKS

@@ -196,6 +196,7 @@ PROTOTYPES: dict[str, tuple] = {
     "stitch_batch_destroy": (None, [C.c_void_p]),
     "stitch_batch_set_marks": (C.c_int, [C.c_void_p, P(C.c_void_p), C.c_int]),
     "stitch_server_create": (C.c_int, [P(ServerConfig), P(C.c_void_p)]),
+    "stitch_server_request_bytes": (C.c_int, [P(Request), _size_p]),
     "stitch_server_submit": (C.c_int, [C.c_void_p, P(Request)]),
     "stitch_server_poll": (C.c_int, [C.c_void_p, P(ServerResult), C.c_int, P(C.c_int)]),
     "stitch_server_outstanding": (C.c_int, [C.c_void_p]),

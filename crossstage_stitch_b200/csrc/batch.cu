@@ -438,7 +438,7 @@ Status Plan::enqueue(void* ws, std::size_t bytes, stitch_homography_result* host
     };
     mark();  // tables uploaded, counts cleared
     for (int kind = 0; kind + 1 < max_levels; ++kind)  // layer kind + 1 of every pyramid image
-        if (go(rs_blocks[kind])) s2s3::resize_kernel<RsSrc><<<rs_blocks[kind], 256, 0, s>>>(rs, kind);
+        if (go(rs_blocks[kind])) s2s3::resize_kernel<RsSrc, s2s3::kResizeTileH><<<rs_blocks[kind], 256, 0, s>>>(rs, kind);
     mark();
     if (go(det_blocks[s2s3::kFastKind])) s2s3::fast_nms_kernel<DetSrc><<<det_blocks[s2s3::kFastKind], 256, 0, s>>>(det);
     mark();

@@ -57,11 +57,13 @@ LevelPlan level_plan(int w, int h, int k, int levels, float sf) {
 // Rows of the layer images start on 16-byte boundaries.
 int layer_pitch(int width) { return (width + 15) / 16 * 16; }
 
-bool pyramid_layout(int w, int h, int k, int levels, float sf, PyramidLayout* out) {
+bool pyramid_layout(int w, int h, int k, int levels, float sf, PyramidLayout* out, int resize_tile_h) {
     if (!out || !valid_image_shape(w, h) || k < 0 || k > INT_MAX / s2::kCandidateFactor ||
         !valid_pyramid(levels, sf))
         return false;
     PyramidLayout l{};
+    if (resize_tile_h < 16 || resize_tile_h > kResizeTileH || resize_tile_h % 16) return false;
+    l.resize_tile_h = resize_tile_h;
     l.plan = level_plan(w, h, k, levels, sf);
     const int n = l.plan.levels;
     Layout lay;
@@ -79,7 +81,7 @@ bool pyramid_layout(int w, int h, int k, int levels, float sf, PyramidLayout* ou
             return false;
         l.detect[i] = lay.take(l.det[i].total, 1);
         l.describe[i] = lay.take(l.des[i].total, 1);
-        l.resize_tiles[i] = i ? ceil_div(lw, kResizeTileW) * ceil_div(lh, kResizeTileH) : 0;
+        l.resize_tiles[i] = i ? ceil_div(lw, kResizeTileW) * ceil_div(lh, resize_tile_h) : 0;
     }
     if (!lay.ok) return false;
     l.total = lay.cursor;
@@ -173,7 +175,7 @@ Status pyramid_workspace_bytes(int w, int h, const s2::Config& c, int levels, fl
     if (!valid_detect_config(c) || !valid_image_shape(w, h) || !valid_pyramid(levels, sf))
         return Status::INVALID_ARGUMENT;
     PyramidLayout l;
-    if (!pyramid_layout(w, h, c.max_keypoints, levels, sf, &l)) return Status::INVALID_ARGUMENT;
+    if (!pyramid_layout(w, h, c.max_keypoints, levels, sf, &l, kSingleResizeTileH)) return Status::INVALID_ARGUMENT;
     *bytes = l.total;
     return Status::OK;
 }
@@ -187,7 +189,8 @@ Status pyramid_detect_describe(const ImageView& image, const s2::Config& c, int 
         desc.dim != s3::kDescriptorBytes || desc.row_stride_bytes < s3::kDescriptorBytes)
         return Status::INVALID_ARGUMENT;
     PyramidLayout l;
-    if (!pyramid_layout(image.width, image.height, c.max_keypoints, levels, sf, &l)) return Status::INVALID_ARGUMENT;
+    if (!pyramid_layout(image.width, image.height, c.max_keypoints, levels, sf, &l, kSingleResizeTileH))
+        return Status::INVALID_ARGUMENT;
     if (!ws || !aligned(ws, kWorkspaceAlign)) return Status::INVALID_ARGUMENT;
     if (ws_bytes < l.total) return Status::INSUFFICIENT_WORKSPACE;
     if (cudaMemsetAsync(out.d_count, 0, sizeof(int), stream) != cudaSuccess ||
@@ -201,7 +204,8 @@ Status pyramid_detect_describe(const ImageView& image, const s2::Config& c, int 
                       at_offset<std::uint32_t>(ws, l.hists), &jobs);
     int launches = 0;
     for (int i = 1; i < n; ++i) {
-        resize_kernel<OneJob<ResizeJob>><<<l.resize_tiles[i], 256, 0, stream>>>(OneJob<ResizeJob>{jobs.resize[i]}, 0);
+        resize_kernel<OneJob<ResizeJob>, kSingleResizeTileH>
+            <<<l.resize_tiles[i], 256, 0, stream>>>(OneJob<ResizeJob>{jobs.resize[i]}, 0);
         ++launches;
     }
     DetSrc det{};

@@ -59,10 +59,15 @@ struct PyramidLayout {
     DetectLayout det[kMaxLevels];
     DescribeLayout des[kMaxLevels];
     int resize_tiles[kMaxLevels];
+    int resize_tile_h;  // output rows per resize block
     std::size_t total;
 };
 
-bool pyramid_layout(int w, int h, int k, int levels, float scale_factor, PyramidLayout* out);
+// resize_tile_h: 64 rows per resize block when many images share a launch;
+// a single image's pyramid (kSingleResizeTileH) takes 16 to fill the GPU.
+constexpr int kSingleResizeTileH = 16;
+bool pyramid_layout(int w, int h, int k, int levels, float scale_factor, PyramidLayout* out,
+                    int resize_tile_h = kResizeTileH);
 
 struct PyramidJobs {
     ResizeJob resize[kMaxLevels];  // entries 1 .. levels-1

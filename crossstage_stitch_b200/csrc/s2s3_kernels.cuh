@@ -143,14 +143,14 @@ enum DescribeKind { kBlurKind = 0, kDescKind = 1, kDescribeKinds = 2 };
 constexpr int kFastTileW = 64, kFastTileH = 32;
 constexpr int kFastInW = kFastTileW + 8, kFastInH = kFastTileH + 8;  // halo 4 = FAST 3 + NMS 1
 constexpr int kFastScW = kFastTileW + 2, kFastScH = kFastTileH + 2;
-constexpr int kChunkPx = 16384;    // pixels per compaction block (256 threads x 64)
+constexpr int kChunkPx = 8192;     // pixels per compaction block (256 threads x 32)
 constexpr int kHarrisThreads = 256;
 constexpr int kSortCap = 16384;    // candidates sorted in shared memory by one block
 constexpr int kSortThreads = 1024;
 constexpr int kBlurTileW = 64, kBlurTileH = 32;
 constexpr int kDescWarps = 8;
 constexpr int kEdge = 31;
-constexpr int kResizeTileW = 64, kResizeTileH = 64;
+constexpr int kResizeTileW = 64, kResizeTileH = 64;  // widest tile; a job's tile_h may be smaller
 constexpr int kResizeSrcRows = 2 * kResizeTileH + 2;  // source rows a tile stages (layer ratio <= 2)
 constexpr int kMaxLevels = 16;
 
@@ -505,13 +505,13 @@ __device__ __forceinline__ SelectParams select_params(const std::uint32_t* hist,
     return *out;
 }
 
-// Loads the 64 maxima bytes of one thread as 16 little-endian words (zero
+// Loads the 32 maxima bytes of one thread as 8 little-endian words (zero
 // past the image end).
-__device__ __forceinline__ void load64(const std::uint8_t* maxima, long long first, long long pixels,
-                                       std::uint32_t (&w)[16]) {
-    if (first + 64 <= pixels) {
+__device__ __forceinline__ void load32(const std::uint8_t* maxima, long long first, long long pixels,
+                                       std::uint32_t (&w)[8]) {
+    if (first + 32 <= pixels) {
 #pragma unroll
-        for (int q = 0; q < 4; ++q) {
+        for (int q = 0; q < 2; ++q) {
             const uint4 v = *reinterpret_cast<const uint4*>(maxima + first + 16 * q);
             w[4 * q] = v.x;
             w[4 * q + 1] = v.y;
@@ -520,7 +520,7 @@ __device__ __forceinline__ void load64(const std::uint8_t* maxima, long long fir
         }
     } else {
 #pragma unroll
-        for (int q = 0; q < 16; ++q) {
+        for (int q = 0; q < 8; ++q) {
             std::uint32_t v = 0;
 #pragma unroll
             for (int k = 0; k < 4; ++k) {
@@ -545,11 +545,11 @@ __device__ __forceinline__ std::uint32_t count_word(std::uint32_t w, std::uint32
     return packed;
 }
 
-// Counts of one thread's 64 pixels; most words of a maxima map are zero.
-__device__ __forceinline__ std::uint32_t count64(const std::uint32_t (&w)[16], std::uint32_t thr) {
+// Counts of one thread's 32 pixels; most words of a maxima map are zero.
+__device__ __forceinline__ std::uint32_t count32(const std::uint32_t (&w)[8], std::uint32_t thr) {
     std::uint32_t packed = 0;
 #pragma unroll
-    for (int q = 0; q < 16; ++q)
+    for (int q = 0; q < 8; ++q)
         if (w[q]) packed += count_word(w[q], thr);
     return packed;
 }
@@ -578,7 +578,7 @@ __device__ __forceinline__ std::uint32_t block_scan_packed(std::uint32_t v, std:
     return base + inc - v;
 }
 
-// Per 16384-pixel chunk: the 2K threshold (every block derives the same
+// Per 8192-pixel chunk: the 2K threshold (every block derives the same
 // one), the chunk's (above, tie) counts; chunk 0 publishes the parameters and
 // the keypoint count min(selected, K).
 template <class Src>
@@ -594,11 +594,11 @@ __global__ __launch_bounds__(256) void select_count_kernel(const __grid_constant
         *j.count = static_cast<int>(min(p.selected, static_cast<std::uint32_t>(j.max_keypoints)));
     }
     const long long pixels = static_cast<long long>(j.width) * j.height;
-    const long long first = static_cast<long long>(chunk) * kChunkPx + threadIdx.x * 64;
-    std::uint32_t w[16];
-    load64(j.maxima, first, pixels, w);
+    const long long first = static_cast<long long>(chunk) * kChunkPx + threadIdx.x * 32;
+    std::uint32_t w[8];
+    load32(j.maxima, first, pixels, w);
     std::uint32_t total;
-    block_scan_packed(count64(w, p.threshold), &total);
+    block_scan_packed(count32(w, p.threshold), &total);
     if (threadIdx.x == 0) {
         j.chunk_counts[2 * chunk] = total >> 16;
         j.chunk_counts[2 * chunk + 1] = total & 0xffffu;
@@ -632,14 +632,14 @@ __global__ __launch_bounds__(256) void scatter_kernel(const __grid_constant__ Sr
 #pragma unroll
     for (int w = 0; w < 8; ++w) { off_above += red[0][w]; off_tie += red[1][w]; }
     const long long pixels = static_cast<long long>(j.width) * j.height;
-    const long long first = static_cast<long long>(chunk) * kChunkPx + threadIdx.x * 64;
-    std::uint32_t w[16];
-    load64(j.maxima, first, pixels, w);
+    const long long first = static_cast<long long>(chunk) * kChunkPx + threadIdx.x * 32;
+    std::uint32_t w[8];
+    load32(j.maxima, first, pixels, w);
     std::uint32_t total;
-    const std::uint32_t excl = block_scan_packed(count64(w, p.threshold), &total);
+    const std::uint32_t excl = block_scan_packed(count32(w, p.threshold), &total);
     std::uint32_t ra = off_above + (excl >> 16), rt = off_tie + (excl & 0xffffu);
 #pragma unroll
-    for (int q = 0; q < 16; ++q) {
+    for (int q = 0; q < 8; ++q) {
         if (!w[q]) continue;
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
@@ -804,7 +804,7 @@ __device__ __forceinline__ int2 linear_exact_tap(int v, int src, double scale) {
     return make_int2(static_cast<int>(fl), static_cast<int>(rint((f - fl) * 256.0)));
 }
 
-// One block = one 64x64 tile of the layer, separable: per-column and per-row
+// One block = one tile of 64 x kTileH (16..64) layer pixels, separable: per-column and per-row
 // taps once in shared memory; then the horizontal pass once per source row
 // the tile needs,
 //   h(r, c) = src[r][c0] * (256 - wx) + src[r][c1] * wx   (< 2^16),
@@ -814,8 +814,9 @@ __device__ __forceinline__ int2 linear_exact_tap(int v, int src, double scale) {
 // the integer form of the 8-bit fixed-point horizontal pass followed by the
 // vertical pass with one final rounding. Tiles whose source rows exceed the
 // shared buffer (layer ratios above 2) read the source bytes directly.
-template <class Src>
+template <class Src, int kTileH>
 __global__ __launch_bounds__(256) void resize_kernel(const __grid_constant__ Src src, int kind) {
+    static_assert(kTileH >= 16 && kTileH <= kResizeTileH && kTileH % 16 == 0, "resize tile height");
     __shared__ int2 xtap[kResizeTileW];
     __shared__ int2 ytap[kResizeTileH];
     __shared__ __align__(16) std::uint16_t hrow[kResizeSrcRows][kResizeTileW];
@@ -823,18 +824,19 @@ __global__ __launch_bounds__(256) void resize_kernel(const __grid_constant__ Src
     ResizeJob j;
     int local;
     if (!src.find(blockIdx.x, kind, &j, &local)) return;
-    const int y0 = (local / j.tiles_x) * kResizeTileH;
+    constexpr int th = kTileH;
+    const int y0 = (local / j.tiles_x) * th;
     const int x0 = (local % j.tiles_x) * kResizeTileW;
     const int t = threadIdx.x;
     if (t == 0) scale[0] = linear_exact_scale(j.src_width, j.width);
     if (t == 32) scale[1] = linear_exact_scale(j.src_height, j.height);
     __syncthreads();
     if (t < kResizeTileW) xtap[t] = linear_exact_tap(min(x0 + t, j.width - 1), j.src_width, scale[0]);
-    else if (t < kResizeTileW + kResizeTileH)
+    else if (t < kResizeTileW + th)
         ytap[t - kResizeTileW] = linear_exact_tap(min(y0 + t - kResizeTileW, j.height - 1), j.src_height, scale[1]);
     __syncthreads();
     const int sy0 = ytap[0].x;                                              // taps are nondecreasing
-    const int sy1 = min(ytap[kResizeTileH - 1].x + 1, j.src_height - 1);
+    const int sy1 = min(ytap[th - 1].x + 1, j.src_height - 1);
     const int nsrc = sy1 - sy0 + 1;
     const bool staged = nsrc <= kResizeSrcRows;                             // block-uniform
     if (staged) {
@@ -867,7 +869,7 @@ __global__ __launch_bounds__(256) void resize_kernel(const __grid_constant__ Src
     const int c = 4 * (t & 15);
     const int x = x0 + c;
     if (x >= j.width) return;
-    for (int rr = t >> 4; rr < kResizeTileH; rr += 16) {
+    for (int rr = t >> 4; rr < th; rr += 16) {
         const int y = y0 + rr;
         if (y >= j.height) break;
         const int2 ty = ytap[rr];

@@ -183,6 +183,29 @@ stitch_pair_desc pair_desc(const Request& q, const unsigned char* a, const unsig
 
 }  // namespace
 
+// Checks a request and fills q (knobs, image geometry, footprint: the
+// request alone in a batch, host layout only) and the job-table bytes.
+Status prepare_request(const stitch_request& r, Request* q, std::size_t* table_bytes) {
+    if (!r.host_a || !r.host_b) return Status::INVALID_ARGUMENT;
+    if ((r.host_mask && !r.host_panorama) ||
+        (r.host_panorama && (!r.rgb || r.panorama_capacity == 0 ||
+                             r.panorama_capacity > std::numeric_limits<std::size_t>::max() / 8)))
+        return Status::INVALID_ARGUMENT;
+    q->r = r;
+    Status st = geometry(r, &q->g);
+    if (st != Status::OK) return st;
+    q->render_bytes = r.host_panorama ? render_bytes(r.panorama_capacity) : 0;
+    const auto* fake = reinterpret_cast<const unsigned char*>(kAlign);
+    stitch_pair_desc d = pair_desc(*q, fake, fake);
+    Plan p;
+    int bad = -1;
+    st = p.build(1, &d, &bad, false);
+    if (st != Status::OK) return st;
+    q->footprint = q->g.bytes() + round_up(p.total, kAlign) + (q->g.rgb ? kAlign : 0) + q->render_bytes;
+    *table_bytes = p.table_bytes;
+    return Status::OK;
+}
+
 class Server {
 public:
     explicit Server(const stitch_server_config& c) : cfg_(c), arena_(c.arena_bytes) {
@@ -211,25 +234,11 @@ public:
     }
 
     Status submit(const stitch_request& r) {
-        if (!r.host_a || !r.host_b) return Status::INVALID_ARGUMENT;
-        if ((r.host_mask && !r.host_panorama) ||
-            (r.host_panorama && (!r.rgb || r.panorama_capacity == 0 ||
-                                 r.panorama_capacity > std::numeric_limits<std::size_t>::max() / 8)))
-            return Status::INVALID_ARGUMENT;
         Request q;
-        q.r = r;
-        Status st = geometry(r, &q.g);
+        std::size_t table_bytes = 0;
+        Status st = prepare_request(r, &q, &table_bytes);
         if (st != Status::OK) return st;
-        if (r.host_panorama) q.render_bytes = render_bytes(r.panorama_capacity);
-        // footprint: the request alone in a batch (host layout only)
-        const auto* fake = reinterpret_cast<const unsigned char*>(kAlign);
-        stitch_pair_desc d = pair_desc(q, fake, fake);
-        Plan p;
-        int bad = -1;
-        st = p.build(1, &d, &bad, false);
-        if (st != Status::OK) return st;
-        q.footprint = q.g.bytes() + round_up(p.total, kAlign) + (q.g.rgb ? kAlign : 0) + q.render_bytes;
-        if (q.footprint > cfg_.arena_bytes || p.table_bytes > staging_cap()) return Status::INSUFFICIENT_WORKSPACE;
+        if (q.footprint > cfg_.arena_bytes || table_bytes > staging_cap()) return Status::INSUFFICIENT_WORKSPACE;
         q.submit_ms = now_ms();
         {
             std::lock_guard<std::mutex> g(mu_);
@@ -641,6 +650,15 @@ int stitch_server_create(const stitch_server_config* config, stitch_server** out
     }
     *out = s;
     return 0;
+}
+
+int stitch_server_request_bytes(const stitch_request* r, size_t* bytes) {
+    if (!r || !bytes) return static_cast<int>(Status::INVALID_ARGUMENT);
+    stitch::b200::serve::Request q;
+    std::size_t table_bytes = 0;
+    const Status st = stitch::b200::serve::prepare_request(*r, &q, &table_bytes);
+    *bytes = st == Status::OK ? q.footprint : 0;
+    return static_cast<int>(st);
 }
 
 int stitch_server_submit(stitch_server* s, const stitch_request* r) {

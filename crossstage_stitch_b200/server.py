@@ -8,7 +8,7 @@ import ctypes as C
 import numpy as np
 import torch
 
-from . import _abi
+from . import _abi, replicas
 from ._abi import Request, ServerConfig, ServerResult, StageError
 from .stages import Knobs, result_dict
 
@@ -43,6 +43,14 @@ class Server:
 
     def submit(self, gray_a, gray_b, knobs: Knobs, tag: int, scale_a=None, scale_b=None, s1_scale: float = 1.0,
                retry_hypotheses: int = 0, retry_min_inliers: int = 0, panorama_capacity: int = 0) -> int:
+        st, r, held = self.request(gray_a, gray_b, knobs, tag, scale_a, scale_b, s1_scale, retry_hypotheses,
+                                   retry_min_inliers, panorama_capacity)
+        return st if st != 0 else self.submit_request(r, held)
+
+    def request(self, gray_a, gray_b, knobs: Knobs, tag: int, scale_a=None, scale_b=None, s1_scale: float = 1.0,
+                retry_hypotheses: int = 0, retry_min_inliers: int = 0, panorama_capacity: int = 0):
+        """(0, request, host buffers) for submit_request(); the arguments are
+        submit()'s."""
         """Queues one pair; returns the status code (0 = queued). (rows, cols, 3)
         images are RGB8: the server converts and resizes them with S1 at
         s1_scale on the device and returns H in their original coordinates.
@@ -71,10 +79,15 @@ class Server:
             pano = torch.empty(3 * panorama_capacity, dtype=torch.uint8, pin_memory=True)
             mask = torch.empty(panorama_capacity, dtype=torch.uint8, pin_memory=True)
             r.host_panorama, r.host_mask, r.panorama_capacity = pano.data_ptr(), mask.data_ptr(), panorama_capacity
-        self.held[tag] = (a, b, pano, mask)
+        return 0, r, (a, b, pano, mask)
+
+    def submit_request(self, r: Request, held) -> int:
+        """Queues a request built by request(); `held` stays alive until its
+        result is polled."""
+        self.held[r.tag] = held
         st = self.lib.stitch_server_submit(self.handle, C.byref(r))
         if st != 0:
-            del self.held[tag]
+            del self.held[r.tag]
         return st
 
     def poll(self) -> list[dict]:
@@ -123,3 +136,61 @@ class Server:
 
     def __del__(self):
         self.close()
+
+
+class MultiServer:
+    """One Server per GPU of the node and a least-loaded dispatcher over
+    their arenas: pairs are independent, so a request goes to the GPU with
+    the most free admission budget (its footprint from
+    stitch_server_request_bytes) and no collective is involved. Results
+    carry "gpu", the index into `devices`."""
+
+    def __init__(self, devices, arena_bytes: int = 8 << 30, max_batch: int = 64, streams: int = 2):
+        self.devices = list(devices)
+        self.servers = [Server(arena_bytes, max_batch, streams, device=d) for d in self.devices]
+        self.dispatch = replicas.LeastLoadedDispatcher([arena_bytes] * len(self.devices))
+        self.lib = _abi.load()
+
+    def submit(self, gray_a, gray_b, knobs: Knobs, tag: int, **kw) -> int:
+        head = self.servers[0]
+        st, r, held = head.request(gray_a, gray_b, knobs, tag, **kw)
+        if st != 0:
+            return st
+        nbytes = C.c_size_t()
+        st = self.lib.stitch_server_request_bytes(C.byref(r), C.byref(nbytes))
+        if st != 0:
+            return st
+        try:
+            gpu = self.dispatch.place(tag, nbytes.value)
+        except ValueError:
+            return int(_abi.Status.INSUFFICIENT_WORKSPACE)
+        st = self.servers[gpu].submit_request(r, held)
+        if st != 0:
+            self.dispatch.release(tag)
+        return st
+
+    def poll(self) -> list[dict]:
+        out = []
+        for g, srv in enumerate(self.servers):
+            for res in srv.poll():
+                self.dispatch.release(res["tag"])
+                res["gpu"] = g
+                out.append(res)
+        return out
+
+    def outstanding(self) -> int:
+        return sum(s.outstanding() for s in self.servers)
+
+    def drain(self, timeout_s: float = 120.0) -> list[dict]:
+        import time
+        out, t0 = [], time.time()
+        while self.outstanding() > 0:
+            out += self.poll()
+            if time.time() - t0 > timeout_s:
+                raise TimeoutError(f"{self.outstanding()} requests still outstanding")
+            time.sleep(0.0005)
+        return out + self.poll()
+
+    def close(self) -> None:
+        for s in self.servers:
+            s.close()

@@ -425,6 +425,10 @@ typedef struct stitch_server stitch_server;
 
 /* No reference counterpart (served form). Starts the dispatcher thread. */
 int stitch_server_create(const stitch_server_config* config, stitch_server** server);
+/* No reference counterpart. The device-memory footprint a request takes in
+ * an arena (the request alone in a batch); host computation only, the same
+ * checks as stitch_server_submit. For placing requests across GPUs. */
+int stitch_server_request_bytes(const stitch_request* request, size_t* bytes);
 /* No reference counterpart. Queues one request (thread-safe, returns at
  * once). INVALID_ARGUMENT for knobs or sizes the stages reject;
  * INSUFFICIENT_WORKSPACE when the request alone needs more than the arena. */

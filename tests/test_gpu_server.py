@@ -222,3 +222,24 @@ def test_rgb_requests_render_their_panorama(cuda):
     np.testing.assert_array_equal(got[10]["H"], got[0]["H"])
     assert got[11]["render_status"] == -1 and "panorama" not in got[11]
     np.testing.assert_array_equal(got[11]["H"], got[0]["H"])
+
+
+def test_multi_server_places_and_returns(reqs, alone):
+    """The multi-GPU served form on the GPUs this host has (one here):
+    requests placed by the least-loaded dispatcher come back with their GPU
+    index and the results of the plain per-pair path."""
+    import torch
+
+    from crossstage_stitch_b200.server import MultiServer
+
+    devices = list(range(torch.cuda.device_count()))
+    ms = MultiServer(devices, arena_bytes=1 << 30, max_batch=8, streams=2)
+    for n, (a, b, k) in enumerate(reqs):
+        assert ms.submit(a, b, k, tag=n) == 0
+    got = {r["tag"]: r for r in ms.drain()}
+    ms.close()
+    assert sorted(got) == list(range(len(reqs)))
+    assert ms.dispatch.used == [0] * len(devices) and not ms.dispatch.placed
+    for n, want in enumerate(alone):
+        assert got[n]["gpu"] in range(len(devices))
+        same(got[n], want)
