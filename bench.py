@@ -545,7 +545,7 @@ def main():
         import torch
         torch.cuda.set_device(local)
         dev = torch.device("cuda", local)
-        print(json.dumps(run_render(dev, torch.empty(512 << 20, dtype=torch.uint8, device=dev),
+        print(json.dumps(run_render(dev, torch.empty(128 << 20, dtype=torch.int32, device=dev),
                                     reps=args.steps)), flush=True)
         return
 
@@ -576,7 +576,7 @@ def main():
     knobs = [knobs_for(g) for g in mine]
     host = [(torch.from_numpy(p.gray_a).pin_memory(), torch.from_numpy(p.gray_b).pin_memory()) for p in pairs]
     imgs = [(a.to(dev), b.to(dev)) for a, b in host]
-    flush = torch.empty(512 << 20, dtype=torch.uint8, device=dev)
+    flush = torch.empty(128 << 20, dtype=torch.int32, device=dev)  # 512 MB, written by a vectorised fill
 
     # ---- batched form: one graph for all pairs
     b = batch.Batch([batch.pair_desc(ia, ib, k) for (ia, ib), k in zip(imgs, knobs)], device=dev)
