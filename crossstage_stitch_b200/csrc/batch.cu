@@ -43,7 +43,7 @@ bool small_image(const stitch_image_view& v) { return v.width <= 2 * s2::kEdge |
 // Device job tables, in this order inside the table block.
 enum Table {
     kDetJobs, kDetPrefix, kDesJobs, kDesPrefix, kKnnJobs, kKnnPrefix, kMergePrefix, kAccJobs, kAccPrefix,
-    kPairJobs, kPairPrefix, kSearchJobs, kSearchPrefix, kRsJobs, kRsPrefix, kTables
+    kPairJobs, kPairPrefix, kSearchJobs, kSearchPrefix, kFitPrefix, kRsJobs, kRsPrefix, kTables
 };
 
 void set_attributes_once() {
@@ -53,7 +53,8 @@ void set_attributes_once() {
         cudaFuncSetAttribute(s2s3::sort_topk_kernel<s2s3::JobTable<DetectJob>>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                              s2s3::kSortCap * static_cast<int>(sizeof(std::uint64_t)));
-        s5k::enable_search_smem_once(reinterpret_cast<const void*>(s5k::search_kernel<s5k::JobTable<SearchJob>>));
+        s5k::enable_search_smem_once(
+            reinterpret_cast<const void*>(s5k::search_kernel<s5k::JobTable<SearchJob>, true>));
     });
 }
 
@@ -158,6 +159,7 @@ Status Plan::build(int n_pairs, const stitch_pair_desc* p, int* bad_pair, bool a
         s4k::match_layout(k, k, q.s4.cross_check != 0, &o.match);
         o.s4ws = lay.take(o.match.total, 1);
         o.s5ws = lay.take(s5k::estimate_workspace_bytes(), 1);
+        o.models = lay.take(static_cast<std::size_t>(std::max(q.s5.hypotheses, 1)), sizeof(s5k::Model));
     }
     // 4. launch shapes (block counts are final once stage_tables has run)
     int max_cand = 0, max_cap_m = 1;
@@ -222,6 +224,7 @@ Status Plan::build(int n_pairs, const stitch_pair_desc* p, int* bad_pair, bool a
     put(kPairPrefix, (n + 1) * sizeof(int));
     put(kSearchJobs, n * sizeof(SearchJob));
     put(kSearchPrefix, (n + 1) * sizeof(int));
+    put(kFitPrefix, (n + 1) * sizeof(int));
     put(kRsJobs, nr * sizeof(ResizeJob));
     put(kRsPrefix, static_cast<std::size_t>(resize_kinds()) * (nr + 1) * sizeof(int));
     table_bytes = cur;
@@ -254,6 +257,7 @@ Status Plan::stage_tables(void* ws) {
     auto* pp = reinterpret_cast<int*>(T + offsets[kPairPrefix]);
     auto* rj = reinterpret_cast<SearchJob*>(T + offsets[kSearchJobs]);
     auto* rp = reinterpret_cast<int*>(T + offsets[kSearchPrefix]);
+    auto* fp = reinterpret_cast<int*>(T + offsets[kFitPrefix]);
     auto* zj = reinterpret_cast<ResizeJob*>(T + offsets[kRsJobs]);
     auto* zp = reinterpret_cast<int*>(T + offsets[kRsPrefix]);
     std::uint32_t* hist_base = at<std::uint32_t>(ws, hists);
@@ -282,7 +286,7 @@ Status Plan::stage_tables(void* ws) {
         qtiles_total += dirs * (k > 0 ? ceil_div(k, s4k::kQueryTile) : 0);
     }
     const int want_splits = std::max(1, ceil_div(2 * kSmCount, std::max(qtiles_total, 1)));
-    int knn = 0, run_knn = 0, run_merge = 0, run_search = 0;
+    int knn = 0, run_knn = 0, run_merge = 0, run_search = 0, run_fit = 0;
     for (int i = 0; i < n; ++i) {
         const auto& q = pairs[i];
         const auto& o = off[i];
@@ -379,9 +383,11 @@ Status Plan::stage_tables(void* ws) {
         io.result_out = at<HomographyResult>(ws, results) + i;
         pj[i] = io;
         pp[i] = i;
-        rj[i] = SearchJob{io, 0, q.s5.hypotheses};
+        rj[i] = SearchJob{io, 0, q.s5.hypotheses, at<s5k::Model>(ws, o.models)};
         rp[i] = run_search;
         run_search += io.search_blocks;
+        fp[i] = run_fit;
+        run_fit += io.search_blocks > 0 ? ceil_div(q.s5.hypotheses, s5k::kFitThreads) : 0;
     }
     for (int kind = 0; kind < s2s3::kDetectKinds; ++kind) dp[kind * (nd + 1) + nd] = run_det[kind];
     for (int kind = 0; kind < s2s3::kDescribeKinds; ++kind) sp[kind * (nd + 1) + nd] = run_des[kind];
@@ -392,9 +398,11 @@ Status Plan::stage_tables(void* ws) {
     ap[n] = n;
     pp[n] = n;
     rp[n] = run_search;
+    fp[n] = run_fit;
     knn_blocks = run_knn;
     merge_blocks = run_merge;
     search_blocks = run_search;
+    fit_blocks = run_fit;
     for (int kind = 0; kind < s2s3::kDetectKinds; ++kind) det_blocks[kind] = run_det[kind];
     for (int kind = 0; kind < s2s3::kDescribeKinds; ++kind) des_blocks[kind] = run_des[kind];
     staged_for = ws;
@@ -490,8 +498,12 @@ Status Plan::enqueue(void* ws, std::size_t bytes, stitch_homography_result* host
                           reinterpret_cast<const int*>(T + offsets[kPairPrefix]), n};
     if (go(n)) s5k::prepare_kernel<PairSrc><<<n, 256, 0, s>>>(pairsrc);
     mark();
+    if (go(fit_blocks))
+        s5k::fit_kernel<SearchSrc><<<fit_blocks, s5k::kFitThreads, 0, s>>>(
+            SearchSrc{reinterpret_cast<const SearchJob*>(T + offsets[kSearchJobs]),
+                      reinterpret_cast<const int*>(T + offsets[kFitPrefix]), n});
     if (go(search_blocks))
-        s5k::search_kernel<SearchSrc><<<search_blocks, s5k::kSearchThreads, search_smem, s>>>(
+        s5k::search_kernel<SearchSrc, true><<<search_blocks, s5k::kSearchThreads, search_smem, s>>>(
             SearchSrc{reinterpret_cast<const SearchJob*>(T + offsets[kSearchJobs]),
                       reinterpret_cast<const int*>(T + offsets[kSearchPrefix]), n});
     mark();

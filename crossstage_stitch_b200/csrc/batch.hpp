@@ -16,6 +16,7 @@ struct PairOffsets {
     std::size_t kx[2], ky[2], kr[2], kcount[2], desc[2];
     std::size_t s2ws[2], s3ws[2];
     std::size_t ia, ib, dist, mcount, mask, s4ws, s5ws;
+    std::size_t models;  // S5 models of the pair's hypotheses (fit_kernel -> search_kernel)
     s2s3::DetectLayout det[2];
     s2s3::DescribeLayout des[2];
     s4k::MatchLayout match;
@@ -46,7 +47,7 @@ public:
     int des_blocks[s2s3::kDescribeKinds] = {};
     int rs_blocks[s2s3::kMaxLevels] = {};  // resize launch of layer kind + 1
     int knn_blocks = 0, merge_blocks = 0, n_knn = 0;
-    int search_blocks = 0;
+    int search_blocks = 0, fit_blocks = 0;
     int sort_smem = 0, search_smem = 0;
     bool rank_fallback = false;
     int hpw = 8;

@@ -124,10 +124,12 @@ Status estimate(const Keypoints& a, const Keypoints& b, const Matches& matches, 
     if (cudaGetLastError() != cudaSuccess) return Status::CUDA_ERROR;
     if (io.search_blocks > 0) {
         using Src = OneJob<SearchJob>;
-        static const bool smem_ok = enable_search_smem_once(reinterpret_cast<const void*>(search_kernel<Src>));
+        static const bool smem_ok =
+            enable_search_smem_once(reinterpret_cast<const void*>(search_kernel<Src, false>));
         (void)smem_ok;
-        SearchJob sj{io, config.previous_hypotheses, count};
-        search_kernel<Src><<<io.search_blocks, kSearchThreads, search_smem_bytes(matches.capacity), stream>>>(Src{sj});
+        SearchJob sj{io, config.previous_hypotheses, count, nullptr};
+        search_kernel<Src, false>
+            <<<io.search_blocks, kSearchThreads, search_smem_bytes(matches.capacity), stream>>>(Src{sj});
         note_launches(1);
         if (cudaGetLastError() != cudaSuccess) return Status::CUDA_ERROR;
     }

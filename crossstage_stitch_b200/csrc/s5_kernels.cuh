@@ -580,7 +580,39 @@ __global__ __launch_bounds__(256) void prepare_kernel(const __grid_constant__ Sr
 struct SearchJob {
     PairIO io;
     int first, count;  // hypotheses [first, first + count)
+    Model* prefit;     // models of these hypotheses from fit_kernel, or null (fit in the search)
 };
+
+constexpr int kFitThreads = 128;
+
+// One thread per hypothesis h in [first, first + count): the counter-based
+// sample, the degeneracy test, the 4-point fit and the domain test, the same
+// functions the search runs in place, into prefit[h - first] (valid = 0 for
+// a rejected sample). A thread owns the whole 8x9 system, so this kernel
+// runs with all the registers it needs, apart from the scoring.
+template <class Src>
+__global__ __launch_bounds__(kFitThreads) void fit_kernel(const __grid_constant__ Src src) {
+    SearchJob sj;
+    int block;
+    if (!src.find(blockIdx.x, &sj, &block)) return;
+    const PairIO& j = sj.io;
+    const State* s = j.state;
+    const int h = sj.first + block * kFitThreads + threadIdx.x;
+    if (h >= sj.first + sj.count) return;
+    Model m{};
+    m.hypothesis = h;
+    m.valid = 0;
+    if (s->status == static_cast<int>(Status::OK)) {
+        const int nm = s->nm;
+        int idx[4] = {0, 0, 0, 0};
+        sample_four(nm, j.c.seed, h, idx);
+        Pt f[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) f[k] = gather(j, idx[k]);
+        m.valid = nondegenerate(f) && fit4_regs(f, m.h) && valid_domain(m.h, s->scale_b.work_w, s->scale_b.work_h);
+    }
+    sj.prefit[h - sj.first] = m;
+}
 
 // Block b of a pair walks warp rounds b*8 + w, b*8 + w + 8*blocks, ...; a
 // round is HPW consecutive hypotheses. The block's best model goes to
@@ -591,7 +623,10 @@ struct SearchJob {
 // 64 pairs x 2000 hypotheses x ~530 matches).
 constexpr int kPruneEvery = 256;  // points between the pruning checks of a model (multiple of 64)
 
-template <class Src>
+// kPrefit: the models come from fit_kernel (sj.prefit) and the kernel only
+// scores (batched form: 0.387 -> 0.367 ms per step with the fit kernel
+// included; 4 and 5 blocks per SM spill in the scoring loop and are slower).
+template <class Src, bool kPrefit>
 __global__ __launch_bounds__(kSearchThreads, 3) void search_kernel(const __grid_constant__ Src src) {
     extern __shared__ float4 pts[];
     __shared__ Model warp_best[kSearchWarps];
@@ -624,7 +659,9 @@ __global__ __launch_bounds__(kSearchThreads, 3) void search_kernel(const __grid_
             // lanes 0..hpw-1 build one model each (system in registers)
             double hm[9];
             int valid = 0;
-            if (lane < hend - h0) {
+            if (kPrefit) {
+                valid = lane < hend - h0 ? sj.prefit[h0 + lane - sj.first].valid : 0;
+            } else if (lane < hend - h0) {
                 int idx[4] = {0, 0, 0, 0};
                 sample_four(nm, seed, h0 + lane, idx);
                 Pt f[4];
@@ -643,8 +680,14 @@ __global__ __launch_bounds__(kSearchThreads, 3) void search_kernel(const __grid_
             for (int k = 0; k < hend - h0; ++k) {
                 if (!__shfl_sync(0xffffffffu, valid, k)) continue;
                 double h[9];
+                if (kPrefit) {
+                    const Model& mk = sj.prefit[h0 + k - sj.first];  // the same address on every lane
 #pragma unroll
-                for (int e = 0; e < 9; ++e) h[e] = __shfl_sync(0xffffffffu, hm[e], k);
+                    for (int e = 0; e < 9; ++e) h[e] = mk.h[e];
+                } else {
+#pragma unroll
+                    for (int e = 0; e < 9; ++e) h[e] = __shfl_sync(0xffffffffu, hm[e], k);
+                }
                 // Exact pruning against this warp's best so far: every term is
                 // >= 0 and a correctly rounded sum of nonnegative values is
                 // nondecreasing in each operand, so the tree sum of the partial
