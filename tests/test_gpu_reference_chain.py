@@ -91,3 +91,57 @@ def test_reference_chain_parity_and_timing(cuda, k):
         out[name] = timed(runner, pairs, knobs)
     out["ours_over_stock"] = out["ours"]["pairs_per_s"] / out["reference_stock"]["pairs_per_s"]
     print("\nREFERENCE_CHAIN " + json.dumps(out))
+
+
+def test_reference_chain_mixed_resolution(cuda):
+    """Mixed resolution (640x480 .. 3840x2160, per-pair K, FAST and R), single
+    level: the reference's stock kernels pair by pair, this library's plain
+    per-pair form, and its batched form (one graph for all pairs) on the
+    same pairs; the checker build equals ours bit for bit on two pairs."""
+    from crossstage_stitch_b200 import batch
+
+    items = [synth.mixed_pair(i) for i in range(16)]
+    pairs = [p for p, _ in items]
+    knobs = [stages.Knobs(max_keypoints=kn["max_keypoints"], fast_threshold=kn["fast_threshold"],
+                          hypotheses=kn["hypotheses"], seed=synth.BASE_SEED + i) for i, (_, kn) in enumerate(items)]
+    W = max(max(p.gray_a.shape[1], p.gray_b.shape[1]) for p in pairs)
+    H = max(max(p.gray_a.shape[0], p.gray_b.shape[0]) for p in pairs)
+    K = max(k.max_keypoints for k in knobs)
+    R = max(k.hypotheses for k in knobs)
+    ours = stages.PairRunner(W, H, K, max_r=R)
+    checker = stages.PairRunner(W, H, K, max_r=R, stage_lib=RefStages(REF / "libref_stages.so"))
+    stock = stages.PairRunner(W, H, K, max_r=R, stage_lib=RefStages(REF / "libref_stages_stock.so"))
+    small = sorted(range(16), key=lambda i: pairs[i].gray_a.size)[:2]
+    for i in small:
+        p = pairs[i]
+        r_ours = ours.run(p.gray_a, p.gray_b, knobs[i])
+        r_ref = checker.run(p.gray_a, p.gray_b, knobs[i])
+        a, b = ours.download(), checker.download()
+        for key in ("kp_a", "kp_b", "desc_a", "desc_b", "idx_a", "idx_b", "distance", "mask"):
+            assert np.array_equal(a[key], b[key]), (i, key)
+        assert int(r_ours["status"]) == int(r_ref["status"]) and r_ours["num_inliers"] == r_ref["num_inliers"]
+    out = {"workload": "16 mixed-resolution pairs (640x480 .. 3840x2160), single level, K in {500, 2000, 8000}, "
+                       "FAST in {10, 20, 40}, R in {500, 2000, 8000}; plain forms synchronise per pair",
+           "mean_mpx_per_pair": sum(p.gray_a.size + p.gray_b.size for p in pairs) / 16 / 1e6}
+    for name, runner in (("ours_plain", ours), ("reference_stock", stock)):
+        timed(runner, pairs[:2], knobs[:2])  # warm-up
+        out[name] = timed(runner, pairs, knobs)
+    imgs = [(torch.from_numpy(p.gray_a).cuda(), torch.from_numpy(p.gray_b).cuda()) for p in pairs]
+    bt = batch.Batch([batch.pair_desc(a, b, k) for (a, b), k in zip(imgs, knobs)])
+    bt.capture()
+    stream = torch.cuda.current_stream()
+    for _ in range(3):
+        bt.launch(stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(5):
+        bt.launch(stream)
+    e1.record(stream)
+    e1.synchronize()
+    out["ours_batched"] = {"pairs_per_s": 16 * 5 / (e0.elapsed_time(e1) / 1e3)}
+    for i in small:
+        np.testing.assert_array_equal(bt.result(i)["H"], ours.run(pairs[i].gray_a, pairs[i].gray_b, knobs[i])["H"])
+    out["batched_over_reference"] = out["ours_batched"]["pairs_per_s"] / out["reference_stock"]["pairs_per_s"]
+    out["plain_over_reference"] = out["ours_plain"]["pairs_per_s"] / out["reference_stock"]["pairs_per_s"]
+    print("\nREFERENCE_MIXED " + json.dumps(out))
