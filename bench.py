@@ -213,6 +213,14 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+# DRAM bytes (read + write) per launch of a kernel of the batched step, from
+# one ncu capture of this workload (dram__bytes_read.sum + dram__bytes_write.sum).
+NCU_TRAFFIC = {
+    "fast_nms": (274.42e6, "ncu, profiles/fast_nms_batch64_512_l8_ncu.md"),
+    "describe": (170.50e6, "ncu, profiles/fast_nms_batch64_512_l8_ncu.md"),
+    "search": (13.10e6, "ncu, profiles/fast_nms_batch64_512_l8_ncu.md (scoring kernel)"),
+}
+
 N_MIXED = 256
 SERVED_RATES = (500, 1000, 2000)
 SERVED_SECONDS = 3.0
@@ -505,7 +513,7 @@ def algorithmic_work(batch, n_pairs, counts):
     resid = sum(R * m for _, _, m in counts)
     return {
         "pyramid": ("hbm", 1.0 * resized, "GB/s"),       # previous layer read + layer write
-        "fast_nms": ("hbm", 2.0 * px, "GB/s"),           # image read + maxima write
+        "fast_nms": ("hbm", 3.0 * px, "GB/s"),           # image read + maxima write + blurred write (fused)
         "select_scatter": ("hbm", 2.0 * px, "GB/s"),     # maxima read twice
         "blur": ("hbm", 2.0 * px, "GB/s"),               # image read + blurred write
         # descriptor pairs x 256 int8 MACs (2 ops each) on the tensor cores
@@ -522,9 +530,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-resolution and served sections")
-    ap.add_argument("--only", choices=["matching", "render"], default=None,
-                    help="run only the matching microbenchmark (popc vs tensor cores) or the S6 feather "
-                         "render microbenchmark and print its JSON")
+    ap.add_argument("--only", choices=["matching", "render", "batched"], default=None,
+                    help="run only the matching microbenchmark (popc vs tensor cores), the S6 feather "
+                         "render microbenchmark, or the batched step with its kernel marks, and print its JSON")
     ap.add_argument("--runs-csv", default=None,
                     help="write the timed plain per-pair runs as rows of the reference harness's runs.csv")
     args = ap.parse_args()
@@ -550,6 +558,8 @@ def main():
         return
 
     cpu = None
+    if args.only == "batched":
+        args.no_cpu_baseline = args.no_mixed = True
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(32, min(os.cpu_count() or 1, 32))   # spawned pool, before any CUDA work
         try:
@@ -601,6 +611,22 @@ def main():
             for i in range(1, len(marks)):
                 per_kernel[i] += marks[i - 1].elapsed_time(marks[i])
         return total, per_kernel
+
+    if args.only == "batched":
+        for _ in range(args.warmup):
+            timed_graph(1)
+        t_b, per_k = timed_graph(args.steps)
+        (t_b,) = replicas.max_over_ranks([t_b], device=dev)
+        names = list(_abi.BATCH_MARKS)
+        if rank == 0:
+            print(json.dumps({"workload": WORKLOAD, "pairs_per_s": N_PAIRS * args.steps * world / (t_b / 1e3),
+                              "ms_per_step": t_b / args.steps,
+                              "kernel_ms": {names[i]: per_k[i] / args.steps for i in range(1, len(names))}}),
+                  flush=True)
+        if world > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
 
     # ---- end to end through the public streaming API: every step copies its
     # 128 images from a pinned host buffer (one copy, overlapped with the
@@ -710,7 +736,9 @@ def main():
             else:
                 peak, src = 148 * 64 * 1.965e9 * 3 / 1e12, "nominal INT32 issue rate (64 lanes x 3 ops/clk/SM)"
             roof = {"kernel": dominant, "bound": bound, "achieved": achieved, "peak": peak, "unit": unit,
-                    "frac": achieved / peak, "peak_source": src, "traffic": None,
+                    "frac": achieved / peak, "peak_source": src,
+                    "traffic": NCU_TRAFFIC.get(dominant, (None, None))[0],
+                    "traffic_source": NCU_TRAFFIC.get(dominant, (None, None))[1],
                     "ms_per_launch": kern[dominant]}
         line = {"metric": "pairs/s", "value": pairs_total / (t_batch / 1e3), "unit": "pairs/s", "n_gpus": world,
                 "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_batch / args.steps,
