@@ -1071,8 +1071,13 @@ __global__ __launch_bounds__(kDescWarps * 32, 8) void describe_kernel(const __gr
     if (lane == 0) {
         const float angle = __fmul_rn(fast_atan2_deg(static_cast<float>(m01), static_cast<float>(m10)),
                                       0x1.1df46ap-6f);
-        a = static_cast<float>(cos(static_cast<double>(angle)));
-        b = static_cast<float>(sin(static_cast<double>(angle)));
+        // one sincos for both: it equals cos() and sin() bit for bit on every
+        // float in [0, 6.2832] (all the angles this can produce; checked
+        // exhaustively by tests/test_gpu_sincos.py)
+        double sd, cd;
+        sincos(static_cast<double>(angle), &sd, &cd);
+        a = static_cast<float>(cd);
+        b = static_cast<float>(sd);
     }
     a = __shfl_sync(0xffffffffu, a, 0);
     b = __shfl_sync(0xffffffffu, b, 0);
