@@ -264,11 +264,12 @@ __device__ __forceinline__ std::uint32_t blur_byte(float acc) {
 //      reflected at the border otherwise (FAST never reads outside the
 //      image, the blur does);
 //   2. run the compass test on the tile plus a 1-pixel ring, 4 positions per
-//      thread with per-byte SIMD compares, and list the survivors so that
-//      full scores are computed on full warps;
+//      thread in 16-bit lanes, and list the survivors so that full scores are
+//      computed on full warps;
 //   3. score the survivors; keep strict 3x3 maxima inside the 31-pixel edge
-//      margin (4 pixels per thread, per-byte compares), write the maxima map
-//      and add their scores to the histogram.
+//      margin (only survivors can score, so only they are tested), write the
+//      maxima map from a shared-memory tile in 32-bit stores and add their
+//      scores to the histogram.
 // With j.blurred set the block also writes the tile of the S3 7x7 blur
 // (rows pass, then columns pass; per output the taps summed first to last
 // with each product and sum rounded on its own, then rounded half-to-even
@@ -279,6 +280,7 @@ __global__ __launch_bounds__(256, 6) void fast_nms_kernel(const __grid_constant_
     __shared__ __align__(16) std::uint8_t sc[kFastScH][kScStride];
     __shared__ std::uint16_t cand[kFastScH * kScGroups];
     __shared__ std::uint32_t hist[256];
+    __shared__ __align__(16) std::uint8_t mx[kFastTileH][kFastTileW];  // the tile's maxima map
     __shared__ __align__(16) float rows[kFastTileH + 6][kFastTileW];
     __shared__ int n_cand;
     __shared__ std::size_t row_at[kFastInH];  // reflected row offsets (border tiles)
@@ -291,6 +293,9 @@ __global__ __launch_bounds__(256, 6) void fast_nms_kernel(const __grid_constant_
     const int y0 = (local / j.tiles_x) * kFastTileH;
     const int x0 = (local % j.tiles_x) * kFastTileW;
     hist[tid] = 0;
+    static_assert(kFastTileH * kFastTileW == 8 * 256, "two maxima words per thread");
+    reinterpret_cast<std::uint32_t*>(&mx[0][0])[tid] = 0u;
+    reinterpret_cast<std::uint32_t*>(&mx[0][0])[tid + 256] = 0u;
     if (tid == 0) n_cand = 0;
     // 1. stage
     const bool vec = ((reinterpret_cast<std::uintptr_t>(j.image) | static_cast<std::uintptr_t>(j.pitch)) & 15) == 0 &&
@@ -431,27 +436,34 @@ __global__ __launch_bounds__(256, 6) void fast_nms_kernel(const __grid_constant_
         }
     }
     __syncthreads();
-    // 3. strict 3x3 maxima, 4 pixels (r, 4q .. 4q+3) per thread
+    // 3. strict 3x3 maxima inside the 31-pixel edge margin. A position
+    // scores above 0 only if it passed the compass test, so only the listed
+    // survivors can be maxima: each survivor of the tile compares its score
+    // with its 8 neighbours and a maximum goes into mx (zero elsewhere).
+    for (int i = tid; i < nc; i += 256) {
+        const int e = cand[i];
+        const int grp = e >> 4, r = grp / kScGroups, c0 = 4 * (grp - r * kScGroups);
+        if (r < 1 || r > kFastTileH) continue;  // the ring rows hold neighbours only
+        for (unsigned bits = e & 0xfu; bits; bits &= bits - 1) {
+            const int c = c0 + __ffs(bits) - 1;
+            if (c < 1 || c > kFastTileW) continue;
+            const int gy = y0 - 1 + r, gx = x0 - 1 + c;
+            if (gy < kEdge || gy >= H - kEdge || gx < kEdge || gx >= W - kEdge) continue;
+            const unsigned v = sc[r][c];
+            if (v && v > sc[r - 1][c - 1] && v > sc[r - 1][c] && v > sc[r - 1][c + 1] && v > sc[r][c - 1] &&
+                v > sc[r][c + 1] && v > sc[r + 1][c - 1] && v > sc[r + 1][c] && v > sc[r + 1][c + 1]) {
+                mx[r - 1][c - 1] = static_cast<std::uint8_t>(v);
+                atomicAdd(&hist[v], 1u);
+            }
+        }
+    }
+    __syncthreads();
+    // the tile's maxima rows, 4 pixels (r, 4q .. 4q+3) per store
     for (int g = tid; g < kFastTileH * (kFastTileW / 4); g += 256) {
         const int r = g / (kFastTileW / 4), q = g - r * (kFastTileW / 4);
         const int gy = y0 + r, gx = x0 + 4 * q;
         if (gy >= H || gx >= W) continue;
-        const auto* up = reinterpret_cast<const std::uint32_t*>(&sc[r][0]);
-        const auto* md = reinterpret_cast<const std::uint32_t*>(&sc[r + 1][0]);
-        const auto* dn = reinterpret_cast<const std::uint32_t*>(&sc[r + 2][0]);
-        const std::uint32_t u0 = up[q], u1 = up[q + 1], m0 = md[q], m1 = md[q + 1], d0 = dn[q], d1 = dn[q + 1];
-        const std::uint32_t sv = __funnelshift_r(m0, m1, 8);
-        std::uint32_t keep = __vcmpgtu4(sv, 0u);
-        keep &= __vcmpgtu4(sv, u0) & __vcmpgtu4(sv, __funnelshift_r(u0, u1, 8)) &
-                __vcmpgtu4(sv, __funnelshift_r(u0, u1, 16));
-        keep &= __vcmpgtu4(sv, m0) & __vcmpgtu4(sv, __funnelshift_r(m0, m1, 16));
-        keep &= __vcmpgtu4(sv, d0) & __vcmpgtu4(sv, __funnelshift_r(d0, d1, 8)) &
-                __vcmpgtu4(sv, __funnelshift_r(d0, d1, 16));
-        if (gy < kEdge || gy >= H - kEdge) keep = 0;
-#pragma unroll
-        for (int k = 0; k < 4; ++k)
-            if (gx + k < kEdge || gx + k >= W - kEdge) keep &= ~(0xffu << (8 * k));
-        const std::uint32_t out = sv & keep;
+        const std::uint32_t out = reinterpret_cast<const std::uint32_t*>(&mx[r][0])[q];
         std::uint8_t* dst = j.maxima + static_cast<std::size_t>(gy) * W + gx;
         if (gx + 3 < W && (reinterpret_cast<std::uintptr_t>(dst) & 3) == 0) {
             *reinterpret_cast<std::uint32_t*>(dst) = out;
@@ -459,13 +471,6 @@ __global__ __launch_bounds__(256, 6) void fast_nms_kernel(const __grid_constant_
 #pragma unroll
             for (int k = 0; k < 4; ++k)
                 if (gx + k < W) dst[k] = static_cast<std::uint8_t>(out >> (8 * k));
-        }
-        if (out) {
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const std::uint32_t b = (out >> (8 * k)) & 0xffu;
-                if (b) atomicAdd(&hist[b], 1u);
-            }
         }
     }
     __syncthreads();
