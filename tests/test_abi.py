@@ -137,3 +137,51 @@ def test_pyramid_workspace_and_validation():
     assert L.stitch_pyramid_detect_describe(C.byref(iv), C.byref(S2Config(20, 10, 0.04)),
                                             C.byref(_abi.PyramidConfig(8, 1.2)), C.byref(kp), C.byref(ds), None, 0,
                                             None) == Status.INVALID_ARGUMENT
+
+
+def test_server_request_bytes_is_host_only():
+    """The served form's footprint query (no device work): a request's arena
+    bytes grow with its images, K and a panorama buffer, and requests the
+    server would reject are rejected the same way."""
+    import numpy as np
+
+    from crossstage_stitch_b200._abi import Request
+    from crossstage_stitch_b200.stages import Knobs
+
+    L = _abi.load()
+    host = np.zeros((1080, 1920 * 3), np.uint8)
+
+    def request(w, h, rgb=False, k=1000, pano=0, mask=False):
+        r = Request()
+        r.host_a = r.host_b = host.ctypes.data
+        r.width_a = r.width_b = w
+        r.height_a = r.height_b = h
+        r.pitch_a = r.pitch_b = host.strides[0]
+        r.rgb = 1 if rgb else 0
+        r.scale = 1.0 if rgb else 0.0
+        kn = Knobs(max_keypoints=k, levels=8)
+        r.s2, r.s4, r.s5, r.pyramid = kn.s2(), kn.s4(), kn.s5(), kn.pyramid()
+        if pano:
+            r.host_panorama, r.panorama_capacity = host.ctypes.data, pano
+        if mask:
+            r.host_mask = host.ctypes.data
+        return r
+
+    def nbytes(r):
+        b = C.c_size_t(123)
+        st = L.stitch_server_request_bytes(C.byref(r), C.byref(b))
+        return st, b.value
+
+    st_small, small = nbytes(request(512, 512))
+    st_big, big = nbytes(request(1920, 1080))
+    st_k, more_k = nbytes(request(512, 512, k=8000))
+    assert st_small == st_big == st_k == Status.OK and 0 < small < big and small < more_k
+    st_rgb, rgb = nbytes(request(512, 512, rgb=True))
+    st_pano, pano = nbytes(request(512, 512, rgb=True, pano=1 << 20))
+    assert st_rgb == st_pano == Status.OK and rgb > small and pano >= rgb + 4 * (1 << 20)
+    assert nbytes(request(512, 512, pano=1 << 20))[0] == Status.INVALID_ARGUMENT   # panoramas need RGB
+    assert nbytes(request(512, 512, rgb=True, mask=True))[0] == Status.INVALID_ARGUMENT  # mask without panorama
+    bad = request(512, 512)
+    bad.host_a = None
+    assert nbytes(bad) == (Status.INVALID_ARGUMENT, 0)
+    assert L.stitch_server_request_bytes(None, None) == Status.INVALID_ARGUMENT
