@@ -216,9 +216,9 @@ def run_reference(args):
 # DRAM bytes (read + write) per launch of a kernel of the batched step, from
 # one ncu capture of this workload (dram__bytes_read.sum + dram__bytes_write.sum).
 NCU_TRAFFIC = {
-    "fast_nms": (274.42e6, "ncu, profiles/fast_nms_batch64_512_l8_ncu.md"),
-    "describe": (170.50e6, "ncu, profiles/fast_nms_batch64_512_l8_ncu.md"),
-    "search": (13.10e6, "ncu, profiles/fast_nms_batch64_512_l8_ncu.md (scoring kernel)"),
+    "fast_nms": (276.13e6, "ncu, profiles/fast_nms_batch64_512_l8_ncu.md"),
+    "describe": (171.29e6, "ncu, profiles/fast_nms_batch64_512_l8_ncu.md"),
+    "search": (13.09e6, "ncu, profiles/fast_nms_batch64_512_l8_ncu.md (scoring kernel)"),
 }
 
 N_MIXED = 256
