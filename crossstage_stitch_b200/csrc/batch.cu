@@ -12,7 +12,8 @@
 //                         L pyramid layer counts, zeroed every run
 //   hists    u32[J][256]  FAST histograms of the J detect jobs, zeroed every run
 //   results  HomographyResult[n]
-//   tables   job tables + prefixes, copied from pinned host staging
+//   tables   job tables + prefixes, copied from pinned host staging by every
+//            enqueue (a captured graph reads its own device copy instead)
 //   per pair: keypoints x/y/response, descriptors, S2 and S3 workspaces per
 //             image (or its pyramid workspace), matches, inlier mask, S4 and
 //             S5 workspaces
@@ -38,6 +39,16 @@ template <class T> T* at(void* base, std::size_t off) { return at_offset<T>(base
 
 const ImageView& view(const stitch_image_view& v) { return *reinterpret_cast<const ImageView*>(&v); }
 
+// Clears the counts and histograms at the start of the workspace. A kernel,
+// not a memset: a graph replay then holds no copy-engine work before its
+// first stage kernel, so it never queues behind an image upload running on
+// another stream.
+__global__ void zero_words_kernel(std::uint32_t* __restrict__ p, std::size_t words) {
+    for (std::size_t i = blockIdx.x * static_cast<std::size_t>(blockDim.x) + threadIdx.x; i < words;
+         i += static_cast<std::size_t>(gridDim.x) * blockDim.x)
+        p[i] = 0;
+}
+
 bool small_image(const stitch_image_view& v) { return v.width <= 2 * s2::kEdge || v.height <= 2 * s2::kEdge; }
 
 // Device job tables, in this order inside the table block.
@@ -62,6 +73,7 @@ void set_attributes_once() {
 
 Plan::~Plan() {
     if (graph_exec) cudaGraphExecDestroy(static_cast<cudaGraphExec_t>(graph_exec));
+    if (graph_tables) cudaFree(graph_tables);
     if (graph) cudaGraphDestroy(static_cast<cudaGraph_t>(graph));
     if (staging && owns_staging) cudaFreeHost(staging);
 }
@@ -409,16 +421,24 @@ Status Plan::stage_tables(void* ws) {
     return Status::OK;
 }
 
-Status Plan::enqueue(void* ws, std::size_t bytes, stitch_homography_result* host_results, cudaStream_t s) {
+Status Plan::enqueue(void* ws, std::size_t bytes, stitch_homography_result* host_results, cudaStream_t s,
+                     const unsigned char* device_tables) {
     if (!ws || !aligned(ws, kWorkspaceAlign)) return Status::INVALID_ARGUMENT;
     if (bytes < total) return Status::INSUFFICIENT_WORKSPACE;
     set_attributes_once();
     const Status st = stage_tables(ws);
     if (st != Status::OK) return st;
-    unsigned char* T = at<unsigned char>(ws, tables);
-    if (cudaMemcpyAsync(T, staging, table_bytes, cudaMemcpyHostToDevice, s) != cudaSuccess) return Status::CUDA_ERROR;
-    // counts and histograms: contiguous at the start, zeroed together
-    if (cudaMemsetAsync(ws, 0, zeroed, s) != cudaSuccess) return Status::CUDA_ERROR;
+    const unsigned char* T = device_tables;
+    if (!T) {
+        unsigned char* W = at<unsigned char>(ws, tables);
+        if (cudaMemcpyAsync(W, staging, table_bytes, cudaMemcpyHostToDevice, s) != cudaSuccess)
+            return Status::CUDA_ERROR;
+        T = W;
+    }
+    // counts and histograms: contiguous 32-bit words at the start, zeroed together
+    const std::size_t words = zeroed / sizeof(std::uint32_t);
+    const auto zero_blocks = static_cast<unsigned>(std::min<std::size_t>((words + 255) / 256, 148));
+    zero_words_kernel<<<zero_blocks, 256, 0, s>>>(static_cast<std::uint32_t*>(ws), words);
 
     using DetSrc = s2s3::JobTable<DetectJob>;
     using DesSrc = s2s3::JobTable<DescribeJob>;
@@ -429,7 +449,7 @@ Status Plan::enqueue(void* ws, std::size_t bytes, stitch_homography_result* host
                      reinterpret_cast<const int*>(T + offsets[kDesPrefix]), n_det};
     const RsSrc rs{reinterpret_cast<const ResizeJob*>(T + offsets[kRsJobs]),
                    reinterpret_cast<const int*>(T + offsets[kRsPrefix]), n_resize};
-    int launches = 0;
+    int launches = 1;  // zero_words_kernel
     int next_mark = 0;
     bool marks_ok = true;
     cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
@@ -578,14 +598,27 @@ int stitch_batch_capture(stitch_batch* b, void* ws, size_t bytes, stitch_homogra
         cudaGraphDestroy(static_cast<cudaGraph_t>(p.graph));
         p.graph = nullptr;
     }
-    // first enqueue outside capture sets kernel attributes; it is a full run
+    // The first enqueue, outside capture, sets kernel attributes and uploads
+    // the job tables into the workspace (it is a full run); they are then
+    // copied, device to device, into the plan's own table buffer. Replays read
+    // that buffer, so they start with a kernel rather than a host-to-device
+    // copy, which would wait behind any other upload in flight on the same
+    // copy engine, and depend on nothing left in the workspace.
+    if (!p.graph_tables && cudaMalloc(reinterpret_cast<void**>(&p.graph_tables), p.table_bytes) != cudaSuccess) {
+        p.graph_tables = nullptr;
+        return static_cast<int>(Status::CUDA_ERROR);
+    }
     const long long before = stitch_launch_count();
     Status st = p.enqueue(ws, bytes, results, s);
     if (st != Status::OK) return static_cast<int>(st);
     b->launches_per_run = static_cast<int>(stitch_launch_count() - before);
+    if (cudaMemcpyAsync(p.graph_tables, static_cast<unsigned char*>(ws) + p.tables, p.table_bytes, cudaMemcpyDeviceToDevice, s) !=
+        cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)  // replays may go to any stream
+        return static_cast<int>(Status::CUDA_ERROR);
     if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
         return static_cast<int>(Status::CUDA_ERROR);
-    st = p.enqueue(ws, bytes, results, s);
+    st = p.enqueue(ws, bytes, results, s, p.graph_tables);
     cudaGraph_t g = nullptr;
     const cudaError_t end = cudaStreamEndCapture(s, &g);
     if (st != Status::OK || end != cudaSuccess || !g) {

@@ -56,9 +56,10 @@ public:
     unsigned char* staging = nullptr;
     bool owns_staging = false;
     const void* staged_for = nullptr;
-    // captured graph
+    // captured graph, and the device copy of the tables its replays read
     void* graph = nullptr;       // cudaGraph_t
     void* graph_exec = nullptr;  // cudaGraphExec_t
+    unsigned char* graph_tables = nullptr;
     std::size_t offsets[16] = {};  // table offsets inside the table block
     cudaEvent_t marks[STITCH_BATCH_MARKS] = {};
     bool marked = false;
@@ -75,7 +76,10 @@ public:
         staged_for = nullptr;
     }
     Status stage_tables(void* ws);
-    Status enqueue(void* ws, std::size_t bytes, stitch_homography_result* host_results, cudaStream_t s);
+    // With device_tables (graph capture), the kernels read the job tables
+    // there, already uploaded for `ws`, instead of uploading them into `ws`.
+    Status enqueue(void* ws, std::size_t bytes, stitch_homography_result* host_results, cudaStream_t s,
+                   const unsigned char* device_tables = nullptr);
 };
 
 }  // namespace stitch::b200::batch

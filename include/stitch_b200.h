@@ -304,7 +304,8 @@ typedef struct stitch_pair_desc {
 } stitch_pair_desc;
 
 /* Opaque plan of a batch (host object; owns a pinned staging buffer for the
- * device job tables and, after stitch_batch_capture, a CUDA graph). */
+ * device job tables and, after stitch_batch_capture, a CUDA graph and the
+ * device copy of the job tables that the graph reads). */
 typedef struct stitch_batch stitch_batch;
 
 /* No reference counterpart (batched form). Validates every pair with the
@@ -321,7 +322,11 @@ int stitch_batch_enqueue(stitch_batch* plan, void* workspace, size_t workspace_b
                          stitch_homography_result* results_pinned, void* stream);
 /* No reference counterpart (batched form). Captures stitch_batch_enqueue with
  * these arguments into a CUDA graph held by the plan (the stream must not be
- * capturing already); stitch_batch_launch replays it. */
+ * capturing already); stitch_batch_launch replays it. The call runs the chain
+ * once uncaptured and keeps a device copy of the plan's job tables, which the
+ * replays read: a replay starts with a kernel, not a host-to-device copy (so
+ * it never waits for an image upload on another stream), and depends on
+ * nothing left in `workspace`. The call synchronises `stream`. */
 int stitch_batch_capture(stitch_batch* plan, void* workspace, size_t workspace_bytes,
                          stitch_homography_result* results_pinned, void* stream);
 int stitch_batch_launch(stitch_batch* plan, void* stream);
