@@ -54,13 +54,13 @@ bool small_image(const stitch_image_view& v) { return v.width <= 2 * s2::kEdge |
 // Device job tables, in this order inside the table block.
 enum Table {
     kDetJobs, kDetPrefix, kDesJobs, kDesPrefix, kKnnJobs, kKnnPrefix, kMergePrefix, kAccJobs, kAccPrefix,
-    kPairJobs, kPairPrefix, kSearchJobs, kSearchPrefix, kFitPrefix, kRsJobs, kRsPrefix, kTables
+    kPairJobs, kPairPrefix, kSearchJobs, kSearchPrefix, kFitPrefix, kRsJobs, kRsPrefix, kBlockMap, kTables
 };
 
 void set_attributes_once() {
     static std::once_flag flag;
     std::call_once(flag, [] {
-        static_assert(kTables <= 16, "table offsets");
+        static_assert(kTables <= 20, "table offsets");
         cudaFuncSetAttribute(s2s3::sort_topk_kernel<s2s3::JobTable<DetectJob>>,
                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                              s2s3::kSortCap * static_cast<int>(sizeof(std::uint64_t)));
@@ -215,6 +215,43 @@ Status Plan::build(int n_pairs, const stitch_pair_desc* p, int* bad_pair, bool a
         if (rounds_at >= 2 * kSmCount) break;
     }
     search_blocks = static_cast<int>(rounds_at);
+    // block totals of every detect, describe and resize kind, for the block
+    // -> job maps (the same per-job counts stage_tables lays out)
+    bool map_fits = alloc_staging && n_det < (1 << 16) && n_resize < (1 << 16);
+    for (int i = 0; i < n; ++i)
+        for (int s = 0; s < 2; ++s) {
+            const int L = off[i].pyramid[s] ? off[i].pyr[s].plan.levels : 1;
+            for (int l = 0; l < L; ++l) {
+                int db[s2s3::kDetectKinds], sb[s2s3::kDescribeKinds];
+                job_blocks(i, s, l, db, sb);
+                for (int kind = 0; kind < s2s3::kDetectKinds; ++kind) {
+                    det_total[kind] += db[kind];
+                    map_fits = map_fits && db[kind] < (1 << 16);
+                }
+                for (int kind = 0; kind < s2s3::kDescribeKinds; ++kind) {
+                    des_total[kind] += sb[kind];
+                    map_fits = map_fits && sb[kind] < (1 << 16);
+                }
+                if (l > 0) {
+                    rs_total[l - 1] += off[i].pyr[s].resize_tiles[l];
+                    map_fits = map_fits && off[i].pyr[s].resize_tiles[l] < (1 << 16);
+                }
+            }
+        }
+    std::size_t map_entries = 0;
+    for (int kind = 0; kind < s2s3::kDetectKinds; ++kind) {
+        det_first[kind] = map_entries;
+        map_entries += static_cast<std::size_t>(det_total[kind]);
+    }
+    for (int kind = 0; kind < s2s3::kDescribeKinds; ++kind) {
+        des_first[kind] = map_entries;
+        map_entries += static_cast<std::size_t>(des_total[kind]);
+    }
+    for (int kind = 0; kind < resize_kinds(); ++kind) {
+        rs_first[kind] = map_entries;
+        map_entries += static_cast<std::size_t>(rs_total[kind]);
+    }
+    block_map = map_fits;
     // 5. table block layout
     std::size_t cur = 0;
     auto put = [&](int t, std::size_t bytes) {
@@ -239,6 +276,7 @@ Status Plan::build(int n_pairs, const stitch_pair_desc* p, int* bad_pair, bool a
     put(kFitPrefix, (n + 1) * sizeof(int));
     put(kRsJobs, nr * sizeof(ResizeJob));
     put(kRsPrefix, static_cast<std::size_t>(resize_kinds()) * (nr + 1) * sizeof(int));
+    put(kBlockMap, block_map ? map_entries * sizeof(std::uint32_t) : 0);
     table_bytes = cur;
     tables = lay.take(table_bytes, 1);
     if (!lay.ok) return Status::INVALID_ARGUMENT;
@@ -251,6 +289,25 @@ Status Plan::build(int n_pairs, const stitch_pair_desc* p, int* bad_pair, bool a
     owns_staging = true;
     // Block counts of every launch are final once stage_tables has run.
     return Status::OK;
+}
+
+void Plan::job_blocks(int i, int s, int l, int (&db)[s2s3::kDetectKinds], int (&sb)[s2s3::kDescribeKinds]) const {
+    const auto& q = pairs[i];
+    const auto& o = off[i];
+    if (o.pyramid[s]) {
+        s2s3::pyramid_detect_blocks(o.pyr[s], l, db);
+        s2s3::pyramid_describe_blocks(o.pyr[s], l, sb);
+        return;
+    }
+    const stitch_image_view& im = s ? q.image_b : q.image_a;
+    const int k = q.s2.max_keypoints;
+    const bool active = k > 0 && !small_image(im);
+    db[s2s3::kFastKind] = active ? o.det[s].tiles : 0;
+    db[s2s3::kChunkKind] = active ? o.det[s].chunks : 0;
+    db[s2s3::kHarrisKind] = active ? ceil_div(o.det[s].candidates, s2s3::kHarrisThreads) : 0;
+    db[s2s3::kSortKind] = active ? 1 : 0;
+    sb[s2s3::kBlurKind] = 0;  // the FAST kernel writes the blur; no blur launch
+    sb[s2s3::kDescKind] = k > 0 ? ceil_div(k, s2s3::kDescWarps) : 0;
 }
 
 Status Plan::stage_tables(void* ws) {
@@ -278,16 +335,29 @@ Status Plan::stage_tables(void* ws) {
     int run_det[s2s3::kDetectKinds] = {}, run_des[s2s3::kDescribeKinds] = {};
     int run_rs[s2s3::kMaxLevels] = {};
     int rjob = 0;
+    std::uint32_t* bmap = block_map ? reinterpret_cast<std::uint32_t*>(T + offsets[kBlockMap]) : nullptr;
+    bool map_ok = true;  // every map entry lands inside its kind's range
+    auto fill_map = [&](std::size_t first, int run, int total, int job, int blocks) {
+        if (!bmap) return;
+        if (run + blocks > total) {
+            map_ok = false;
+            return;
+        }
+        for (int b = 0; b < blocks; ++b)
+            bmap[first + static_cast<std::size_t>(run + b)] = (static_cast<std::uint32_t>(job) << 16) | b;
+    };
     auto add_job = [&](int idx, const DetectJob& d, const DescribeJob& e, const int (&db)[s2s3::kDetectKinds],
                        const int (&sb)[s2s3::kDescribeKinds]) {
         dj[idx] = d;
         sj[idx] = e;
         for (int kind = 0; kind < s2s3::kDetectKinds; ++kind) {
             dp[kind * (nd + 1) + idx] = run_det[kind];
+            fill_map(det_first[kind], run_det[kind], det_total[kind], idx, db[kind]);
             run_det[kind] += db[kind];
         }
         for (int kind = 0; kind < s2s3::kDescribeKinds; ++kind) {
             sp[kind * (nd + 1) + idx] = run_des[kind];
+            fill_map(des_first[kind], run_des[kind], des_total[kind], idx, sb[kind]);
             run_des[kind] += sb[kind];
         }
     };
@@ -320,12 +390,12 @@ Status Plan::stage_tables(void* ws) {
                                         &pjobs);
                 for (int l = 0; l < pl.plan.levels; ++l) {
                     int db[s2s3::kDetectKinds], sb[s2s3::kDescribeKinds];
-                    s2s3::pyramid_detect_blocks(pl, l, db);
-                    s2s3::pyramid_describe_blocks(pl, l, sb);
+                    job_blocks(i, s, l, db, sb);
                     add_job(idx + l, pjobs.detect[l], pjobs.describe[l], db, sb);
                 }
                 for (int l = 1; l < pl.plan.levels; ++l, ++rjob) {
                     zj[rjob] = pjobs.resize[l];
+                    fill_map(rs_first[l - 1], run_rs[l - 1], rs_total[l - 1], rjob, pl.resize_tiles[l]);
                     for (int kind = 0; kind < rkinds; ++kind) {
                         zp[kind * (nr + 1) + rjob] = run_rs[kind];
                         run_rs[kind] += kind == l - 1 ? pl.resize_tiles[l] : 0;
@@ -335,12 +405,8 @@ Status Plan::stage_tables(void* ws) {
             }
             DetectJob d = s2s3::make_detect_job(view(im), c2, kps[s], at<void>(ws, o.s2ws[s]), o.det[s]);
             d.hist = hist_base + static_cast<std::size_t>(idx) * 256;
-            const bool active = k > 0 && !small_image(im);
-            const int db[s2s3::kDetectKinds] = {
-                active ? o.det[s].tiles : 0, active ? o.det[s].chunks : 0,
-                active ? ceil_div(o.det[s].candidates, s2s3::kHarrisThreads) : 0, active ? 1 : 0};
-            // the FAST kernel writes the blur; no blur launch
-            const int sb[s2s3::kDescribeKinds] = {0, k > 0 ? ceil_div(k, s2s3::kDescWarps) : 0};
+            int db[s2s3::kDetectKinds], sb[s2s3::kDescribeKinds];
+            job_blocks(i, s, 0, db, sb);
             const DescribeJob e =
                 s2s3::make_describe_job(view(im), kps[s], desc[s], at<void>(ws, o.s3ws[s]), o.des[s]);
             d.blurred = e.blurred;
@@ -401,6 +467,12 @@ Status Plan::stage_tables(void* ws) {
         fp[i] = run_fit;
         run_fit += io.search_blocks > 0 ? ceil_div(q.s5.hypotheses, s5k::kFitThreads) : 0;
     }
+    if (bmap) {  // the maps must cover exactly the blocks of every launch
+        for (int kind = 0; kind < s2s3::kDetectKinds; ++kind) map_ok = map_ok && run_det[kind] == det_total[kind];
+        for (int kind = 0; kind < s2s3::kDescribeKinds; ++kind) map_ok = map_ok && run_des[kind] == des_total[kind];
+        for (int kind = 0; kind < rkinds; ++kind) map_ok = map_ok && run_rs[kind] == rs_total[kind];
+        if (!map_ok) return Status::INVALID_ARGUMENT;
+    }
     for (int kind = 0; kind < s2s3::kDetectKinds; ++kind) dp[kind * (nd + 1) + nd] = run_det[kind];
     for (int kind = 0; kind < s2s3::kDescribeKinds; ++kind) sp[kind * (nd + 1) + nd] = run_des[kind];
     for (int kind = 0; kind < rkinds; ++kind) zp[kind * (nr + 1) + nr] = run_rs[kind];
@@ -443,12 +515,27 @@ Status Plan::enqueue(void* ws, std::size_t bytes, stitch_homography_result* host
     using DetSrc = s2s3::JobTable<DetectJob>;
     using DesSrc = s2s3::JobTable<DescribeJob>;
     using RsSrc = s2s3::JobTable<ResizeJob>;
-    const DetSrc det{reinterpret_cast<const DetectJob*>(T + offsets[kDetJobs]),
-                     reinterpret_cast<const int*>(T + offsets[kDetPrefix]), n_det};
-    const DesSrc des{reinterpret_cast<const DescribeJob*>(T + offsets[kDesJobs]),
-                     reinterpret_cast<const int*>(T + offsets[kDesPrefix]), n_det};
-    const RsSrc rs{reinterpret_cast<const ResizeJob*>(T + offsets[kRsJobs]),
-                   reinterpret_cast<const int*>(T + offsets[kRsPrefix]), n_resize};
+    DetSrc det{reinterpret_cast<const DetectJob*>(T + offsets[kDetJobs]),
+               reinterpret_cast<const int*>(T + offsets[kDetPrefix]), n_det};
+    DesSrc des{reinterpret_cast<const DescribeJob*>(T + offsets[kDesJobs]),
+               reinterpret_cast<const int*>(T + offsets[kDesPrefix]), n_det};
+    RsSrc rs{reinterpret_cast<const ResizeJob*>(T + offsets[kRsJobs]),
+             reinterpret_cast<const int*>(T + offsets[kRsPrefix]), n_resize};
+    if (block_map) {
+        const auto* M = reinterpret_cast<const std::uint32_t*>(T + offsets[kBlockMap]);
+        for (int kind = 0; kind < s2s3::kDetectKinds; ++kind) {
+            det.map[kind] = M + det_first[kind];
+            det.map_blocks[kind] = det_total[kind];
+        }
+        for (int kind = 0; kind < s2s3::kDescribeKinds; ++kind) {
+            des.map[kind] = M + des_first[kind];
+            des.map_blocks[kind] = des_total[kind];
+        }
+        for (int kind = 0; kind < resize_kinds(); ++kind) {
+            rs.map[kind] = M + rs_first[kind];
+            rs.map_blocks[kind] = rs_total[kind];
+        }
+    }
     int launches = 1;  // zero_words_kernel
     int next_mark = 0;
     bool marks_ok = true;

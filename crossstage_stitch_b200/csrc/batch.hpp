@@ -60,7 +60,14 @@ public:
     void* graph = nullptr;       // cudaGraph_t
     void* graph_exec = nullptr;  // cudaGraphExec_t
     unsigned char* graph_tables = nullptr;
-    std::size_t offsets[16] = {};  // table offsets inside the table block
+    std::size_t offsets[20] = {};  // table offsets inside the table block
+    // block -> job maps of the detect, describe and resize kinds (one table,
+    // kinds one after the other; see s2s3::JobTable), when every job index
+    // and block within a job fits 16 bits and the plan owns its staging
+    bool block_map = false;
+    int det_total[s2s3::kDetectKinds] = {}, des_total[s2s3::kDescribeKinds] = {}, rs_total[s2s3::kMaxLevels] = {};
+    std::size_t det_first[s2s3::kDetectKinds] = {}, des_first[s2s3::kDescribeKinds] = {},
+                rs_first[s2s3::kMaxLevels] = {};  // entry index of each kind's map
     cudaEvent_t marks[STITCH_BATCH_MARKS] = {};
     bool marked = false;
 
@@ -76,6 +83,8 @@ public:
         staged_for = nullptr;
     }
     Status stage_tables(void* ws);
+    // Blocks of the detect and describe kinds of job (pair i, side s, layer l).
+    void job_blocks(int i, int s, int l, int (&db)[s2s3::kDetectKinds], int (&sb)[s2s3::kDescribeKinds]) const;
     // With device_tables (graph capture), the kernels read the job tables
     // there, already uploaded for `ws`, instead of uploading them into `ws`.
     Status enqueue(void* ws, std::size_t bytes, stitch_homography_result* host_results, cudaStream_t s,

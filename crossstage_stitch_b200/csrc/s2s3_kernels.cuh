@@ -102,12 +102,25 @@ template <class Job> struct OneJob {
 };
 
 // Device table: prefix[kind * (n + 1) + i] is the first block of job i for
-// launch kind `kind`; blocks past the end are idle.
+// launch kind `kind`; blocks past the end are idle. With map[kind] set, entry
+// b of it is (job << 16 | block within the job) for block b of that kind, so
+// a block finds its job in one load instead of a binary search over the
+// prefix (each step of which waits on the previous one).
+constexpr int kMapKinds = 16;
 template <class Job> struct JobTable {
     const Job* jobs;
     const int* prefix;
     int n;
+    const std::uint32_t* map[kMapKinds] = {};
+    int map_blocks[kMapKinds] = {};
     __device__ bool find(int block, int kind, Job* j, int* local) const {
+        if (const std::uint32_t* m = map[kind]) {
+            if (block >= map_blocks[kind]) return false;
+            const std::uint32_t e = __ldg(m + block);
+            *j = jobs[e >> 16];
+            *local = static_cast<int>(e & 0xffffu);
+            return true;
+        }
         const int* p = prefix + kind * (n + 1);
         if (block >= p[n]) return false;
         int lo = 0, hi = n - 1;
@@ -151,8 +164,8 @@ constexpr int kBlurTileW = 64, kBlurTileH = 32;
 constexpr int kDescWarps = 8;
 constexpr int kEdge = 31;
 constexpr int kResizeTileW = 64, kResizeTileH = 64;  // widest tile; a job's tile_h may be smaller
-constexpr int kResizeSrcRows = 2 * kResizeTileH + 2;  // source rows a tile stages (layer ratio <= 2)
 constexpr int kMaxLevels = 16;
+static_assert(kMaxLevels <= kMapKinds && kDetectKinds <= kMapKinds, "block map kinds");
 
 // ------------------------------------------------------------- FAST + NMS
 
@@ -809,30 +822,83 @@ __device__ __forceinline__ int2 linear_exact_tap(int v, int src, double scale) {
     return make_int2(static_cast<int>(fl), static_cast<int>(rint((f - fl) * 256.0)));
 }
 
-// One block = one tile of 64 x kTileH (16..64) layer pixels, separable: per-column and per-row
-// taps once in shared memory; then the horizontal pass once per source row
-// the tile needs,
-//   h(r, c) = src[r][c0] * (256 - wx) + src[r][c1] * wx   (< 2^16),
-// kept as uint16 in shared memory; then the vertical pass, 4 horizontally
-// adjacent outputs per thread (one 32-bit store),
-//   (h(r0, c) * (256 - wy) + h(r1, c) * wy + 2^15) >> 16,
-// the integer form of the 8-bit fixed-point horizontal pass followed by the
-// vertical pass with one final rounding. Tiles whose source rows exceed the
-// shared buffer (layer ratios above 2) read the source bytes directly.
+// One block = one tile of 64 x kTileH (16..64) layer pixels:
+//   1. the tile's source window, bounded from float arithmetic with a pixel
+//      of slack per side, is staged in shared memory with 16-byte loads
+//      (while the taps are computed);
+//   2. per-column and per-row taps in shared memory (double, as above);
+//   3. each warp produces whole layer rows, each lane two adjacent outputs:
+//        h(r, c) = src[r][c0] * (256 - wx) + src[r][c1] * wx   (< 2^16)
+//        out = (h(r0, c) * (256 - wy) + h(r1, c) * wy + 2^15) >> 16,
+//      the integer form of the 8-bit fixed-point horizontal pass followed
+//      by the vertical pass with one final rounding.
+// The exact taps are checked against the staged window; a tile outside it
+// (source image not 16-byte aligned, or a layer ratio above about 1.45)
+// reads the source bytes from global memory instead, with the same result.
+constexpr int kRawStride = 112;  // bytes of a staged source row: 7 chunks of 16
+template <int kTileH> __host__ __device__ constexpr int resize_raw_rows() { return kTileH * 3 / 2 + 6; }
+
 template <class Src, int kTileH>
-__global__ __launch_bounds__(256) void resize_kernel(const __grid_constant__ Src src, int kind) {
+__global__ __launch_bounds__(256, 6) void resize_kernel(const __grid_constant__ Src src, int kind) {
     static_assert(kTileH >= 16 && kTileH <= kResizeTileH && kTileH % 16 == 0, "resize tile height");
+    constexpr int th = kTileH, kRows = resize_raw_rows<kTileH>(), kChunks = kRawStride / 16;
     __shared__ int2 xtap[kResizeTileW];
-    __shared__ int2 ytap[kResizeTileH];
-    __shared__ __align__(16) std::uint16_t hrow[kResizeSrcRows][kResizeTileW];
+    __shared__ int2 ytap[kTileH];
+    __shared__ __align__(16) std::uint8_t raw[kRows][kRawStride];
     __shared__ double scale[2];
     ResizeJob j;
     int local;
     if (!src.find(blockIdx.x, kind, &j, &local)) return;
-    constexpr int th = kTileH;
     const int y0 = (local / j.tiles_x) * th;
     const int x0 = (local % j.tiles_x) * kResizeTileW;
     const int t = threadIdx.x;
+    // 1. source window: rows ry0..ry1, 16-byte chunks from column rx0
+    const float fy = static_cast<float>(j.src_height) / static_cast<float>(j.height);
+    const float fx = static_cast<float>(j.src_width) / static_cast<float>(j.width);
+    const int last_y = min(y0 + th, j.height) - 1, last_x = min(x0 + kResizeTileW, j.width) - 1;
+    const int ry0 = max(__float2int_rd((y0 + 0.5f) * fy - 0.5f) - 1, 0);
+    const int ry1 = min(__float2int_rd((last_y + 0.5f) * fy - 0.5f) + 2, j.src_height - 1);
+    const int rx0 = max(__float2int_rd((x0 + 0.5f) * fx - 0.5f) - 1, 0) & ~15;
+    const int rx1 = min(__float2int_rd((last_x + 0.5f) * fx - 0.5f) + 2, j.src_width - 1);
+    const int nrow = ry1 - ry0 + 1;
+    const int nchunk = rx1 >= rx0 ? (rx1 - rx0) / 16 + 1 : 0;
+    const bool window = ((reinterpret_cast<std::uintptr_t>(j.src) | static_cast<std::uintptr_t>(j.src_pitch)) & 15) == 0 &&
+                        nrow > 0 && nrow <= kRows && nchunk > 0 && nchunk <= kChunks;  // block-uniform
+    if (window) {
+        // chunks start 16-byte aligned below src_width; one that reaches past
+        // the row's last pixel is read byte by byte (zeros beyond it)
+        const int n = nrow * nchunk;
+        for (int i0 = t; i0 < n; i0 += 2 * 256) {
+            uint4 v[2];
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const int i = i0 + 256 * k;
+                if (i < n) {
+                    const int r = i / nchunk, col = rx0 + 16 * (i - r * nchunk);
+                    const std::uint8_t* p = j.src + static_cast<std::size_t>(ry0 + r) * j.src_pitch + col;
+                    if (col + 16 <= j.src_width) {
+                        v[k] = __ldg(reinterpret_cast<const uint4*>(p));
+                    } else {
+                        std::uint32_t w[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+                        for (int b = 0; b < 16; ++b)
+                            if (col + b < j.src_width)
+                                w[b >> 2] |= static_cast<std::uint32_t>(__ldg(p + b)) << (8 * (b & 3));
+                        v[k] = make_uint4(w[0], w[1], w[2], w[3]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const int i = i0 + 256 * k;
+                if (i < n) {
+                    const int r = i / nchunk, c = i - r * nchunk;
+                    *reinterpret_cast<uint4*>(&raw[r][16 * c]) = v[k];
+                }
+            }
+        }
+    }
+    // 2. taps
     if (t == 0) scale[0] = linear_exact_scale(j.src_width, j.width);
     if (t == 32) scale[1] = linear_exact_scale(j.src_height, j.height);
     __syncthreads();
@@ -840,79 +906,46 @@ __global__ __launch_bounds__(256) void resize_kernel(const __grid_constant__ Src
     else if (t < kResizeTileW + th)
         ytap[t - kResizeTileW] = linear_exact_tap(min(y0 + t - kResizeTileW, j.height - 1), j.src_height, scale[1]);
     __syncthreads();
-    const int sy0 = ytap[0].x;                                              // taps are nondecreasing
-    const int sy1 = min(ytap[th - 1].x + 1, j.src_height - 1);
-    const int nsrc = sy1 - sy0 + 1;
-    const bool staged = nsrc <= kResizeSrcRows;                             // block-uniform
-    if (staged) {
-        // horizontal pass: item i = (source row sy0 + i / 64, output column
-        // i % 64); a thread's column is fixed (256 is a multiple of 64), and
-        // four of its rows are loaded before any is used
-        const int c = t & (kResizeTileW - 1);
-        const int2 tx = xtap[c];
-        const int xa = tx.x, xb = min(tx.x + 1, j.src_width - 1), wx = tx.y;
-        const int n = nsrc * kResizeTileW;
-        for (int i0 = t; i0 < n; i0 += 4 * 256) {
-            int pa[4], pb[4];
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const int i = i0 + 256 * k;
-                const std::uint8_t* row = j.src + static_cast<std::size_t>(sy0 + (i < n ? i / kResizeTileW : 0)) *
-                                                      j.src_pitch;
-                pa[k] = i < n ? __ldg(row + xa) : 0;
-                pb[k] = i < n ? __ldg(row + xb) : 0;
-            }
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const int i = i0 + 256 * k;
-                if (i < n) hrow[i / kResizeTileW][c] = static_cast<std::uint16_t>(pa[k] * (256 - wx) + pb[k] * wx);
-            }
-        }
-        __syncthreads();
-    }
-    // vertical pass: rows t/16 + 16 i, columns 4 (t % 16) .. +3
-    const int c = 4 * (t & 15);
-    const int x = x0 + c;
+    // taps are nondecreasing: the first and last give the tile's source span
+    const bool staged = window && ytap[0].x >= ry0 && min(ytap[th - 1].x + 1, j.src_height - 1) <= ry1 &&
+                        xtap[0].x >= rx0 && min(xtap[kResizeTileW - 1].x + 1, j.src_width - 1) < rx0 + 16 * nchunk;
+    // 3. warp w: rows w, w + 8, ...; lane l: columns 2l, 2l + 1
+    const int lane = t & 31;
+    const int c = 2 * lane, x = x0 + c;
     if (x >= j.width) return;
-    for (int rr = t >> 4; rr < th; rr += 16) {
+    const int2 t0 = xtap[c], t1 = xtap[c + 1];  // columns past the layer edge repeat the last tap
+    const int wx0 = t0.y, wx1 = t1.y;
+    int xa0 = t0.x, xb0 = min(t0.x + 1, j.src_width - 1), xa1 = t1.x, xb1 = min(t1.x + 1, j.src_width - 1);
+    if (staged) {
+        xa0 -= rx0; xb0 -= rx0; xa1 -= rx0; xb1 -= rx0;
+    }
+    for (int rr = t >> 5; rr < th; rr += 8) {
         const int y = y0 + rr;
         if (y >= j.height) break;
         const int2 ty = ytap[rr];
-        const int ra = ty.x, rb = min(ty.x + 1, j.src_height - 1);
-        std::uint32_t packed = 0;
+        const int ra = ty.x, rb = min(ty.x + 1, j.src_height - 1), wy = ty.y;
+        int pa[4], pb[4];  // rows ra, rb at xa0, xb0, xa1, xb1
         if (staged) {
-            const uint2 ha = *reinterpret_cast<const uint2*>(&hrow[ra - sy0][c]);
-            const uint2 hb = *reinterpret_cast<const uint2*>(&hrow[rb - sy0][c]);
-            const int hav[4] = {static_cast<int>(ha.x & 0xffffu), static_cast<int>(ha.x >> 16),
-                                static_cast<int>(ha.y & 0xffffu), static_cast<int>(ha.y >> 16)};
-            const int hbv[4] = {static_cast<int>(hb.x & 0xffffu), static_cast<int>(hb.x >> 16),
-                                static_cast<int>(hb.y & 0xffffu), static_cast<int>(hb.y >> 16)};
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const int v = hav[k] * (256 - ty.y) + hbv[k] * ty.y;
-                packed |= static_cast<std::uint32_t>((v + (1 << 15)) >> 16) << (8 * k);
-            }
+            const std::uint8_t* A = raw[ra - ry0];
+            const std::uint8_t* B = raw[rb - ry0];
+            pa[0] = A[xa0]; pa[1] = A[xb0]; pa[2] = A[xa1]; pa[3] = A[xb1];
+            pb[0] = B[xa0]; pb[1] = B[xb0]; pb[2] = B[xa1]; pb[3] = B[xb1];
         } else {
-            const std::uint8_t* pa = j.src + static_cast<std::size_t>(ra) * j.src_pitch;
-            const std::uint8_t* pb = j.src + static_cast<std::size_t>(rb) * j.src_pitch;
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const int2 tx = xtap[c + k];  // columns past the layer edge repeat the last tap
-                const int xa = tx.x, xb = min(tx.x + 1, j.src_width - 1);
-                const int wx1 = tx.y, wx0 = 256 - tx.y;
-                const int ha = __ldg(pa + xa) * wx0 + __ldg(pa + xb) * wx1;
-                const int hb = __ldg(pb + xa) * wx0 + __ldg(pb + xb) * wx1;
-                const int v = ha * (256 - ty.y) + hb * ty.y;
-                packed |= static_cast<std::uint32_t>((v + (1 << 15)) >> 16) << (8 * k);
-            }
+            const std::uint8_t* A = j.src + static_cast<std::size_t>(ra) * j.src_pitch;
+            const std::uint8_t* B = j.src + static_cast<std::size_t>(rb) * j.src_pitch;
+            pa[0] = __ldg(A + xa0); pa[1] = __ldg(A + xb0); pa[2] = __ldg(A + xa1); pa[3] = __ldg(A + xb1);
+            pb[0] = __ldg(B + xa0); pb[1] = __ldg(B + xb0); pb[2] = __ldg(B + xa1); pb[3] = __ldg(B + xb1);
         }
+        const int ha0 = pa[0] * (256 - wx0) + pa[1] * wx0, hb0 = pb[0] * (256 - wx0) + pb[1] * wx0;
+        const int ha1 = pa[2] * (256 - wx1) + pa[3] * wx1, hb1 = pb[2] * (256 - wx1) + pb[3] * wx1;
+        const unsigned v0 = static_cast<unsigned>(ha0 * (256 - wy) + hb0 * wy + (1 << 15)) >> 16;
+        const unsigned v1 = static_cast<unsigned>(ha1 * (256 - wy) + hb1 * wy + (1 << 15)) >> 16;
         std::uint8_t* dst = j.dst + static_cast<std::size_t>(y) * j.pitch + x;
-        if (x + 3 < j.width && (reinterpret_cast<std::uintptr_t>(dst) & 3) == 0) {
-            *reinterpret_cast<std::uint32_t*>(dst) = packed;
+        if (x + 1 < j.width && (reinterpret_cast<std::uintptr_t>(dst) & 1) == 0) {
+            *reinterpret_cast<std::uint16_t*>(dst) = static_cast<std::uint16_t>(v0 | (v1 << 8));
         } else {
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-                if (x + k < j.width) dst[k] = static_cast<std::uint8_t>(packed >> (8 * k));
+            dst[0] = static_cast<std::uint8_t>(v0);
+            if (x + 1 < j.width) dst[1] = static_cast<std::uint8_t>(v1);
         }
     }
 }
