@@ -196,14 +196,8 @@ Status Plan::build(int n_pairs, const stitch_pair_desc* p, int* bad_pair, bool a
     search_smem = s5k::search_smem_bytes(max_cap_m);
     // S4: one train partition per block unless the batch is too small to fill the GPU
     n_knn = 0;
-    int qtiles_total = 0;
-    for (int i = 0; i < n; ++i) {
-        const int k = pairs[i].s2.max_keypoints;
-        const int dirs = pairs[i].s4.cross_check ? 2 : 1;
-        n_knn += dirs;
-        qtiles_total += dirs * (k > 0 ? ceil_div(k, s4k::kQueryTile) : 0);
-    }
-    const int want_splits = std::max(1, ceil_div(2 * kSmCount, std::max(qtiles_total, 1)));
+    for (int i = 0; i < n; ++i) n_knn += pairs[i].s4.cross_check ? 2 : 1;
+    const int want_splits = knn_want_splits();
     knn_blocks = merge_blocks = 0;
     // S5: hypotheses per warp round, as large as still fills about two waves
     long long rounds_at = 0;
@@ -251,6 +245,25 @@ Status Plan::build(int n_pairs, const stitch_pair_desc* p, int* bad_pair, bool a
         rs_first[kind] = map_entries;
         map_entries += static_cast<std::size_t>(rs_total[kind]);
     }
+    map_fits = map_fits && n_knn < (1 << 16) && n < (1 << 16);
+    for (int i = 0; i < n; ++i) {
+        for (int dir = 0; dir < (pairs[i].s4.cross_check ? 2 : 1); ++dir) {
+            const KnnShape ks = knn_shape(i, dir, want_splits);
+            s45_total[kMapKnn] += ks.blocks;
+            s45_total[kMapMerge] += ks.merge_blocks;
+            map_fits = map_fits && ks.blocks < (1 << 16) && ks.merge_blocks < (1 << 16);
+        }
+        const int sb = s5k::plan_search(pairs[i].s5.hypotheses, hpw);
+        const int fb = sb > 0 ? ceil_div(pairs[i].s5.hypotheses, s5k::kFitThreads) : 0;
+        s45_total[kMapSearch] += sb;
+        s45_total[kMapFit] += fb;
+        map_fits = map_fits && sb < (1 << 16) && fb < (1 << 16);
+    }
+    s45_total[kMapAccept] = s45_total[kMapPair] = n;
+    for (int m = 0; m < kMapS45; ++m) {
+        s45_first[m] = map_entries;
+        map_entries += static_cast<std::size_t>(s45_total[m]);
+    }
     block_map = map_fits;
     // 5. table block layout
     std::size_t cur = 0;
@@ -289,6 +302,35 @@ Status Plan::build(int n_pairs, const stitch_pair_desc* p, int* bad_pair, bool a
     owns_staging = true;
     // Block counts of every launch are final once stage_tables has run.
     return Status::OK;
+}
+
+int Plan::knn_want_splits() const {
+    int qtiles_total = 0;
+    for (int i = 0; i < n; ++i) {
+        const int dirs = pairs[i].s4.cross_check ? 2 : 1;
+        const int k = pairs[i].s2.max_keypoints;
+        qtiles_total += dirs * (k > 0 ? ceil_div(k, s4k::kQueryTile) : 0);
+    }
+    return std::max(1, ceil_div(2 * kSmCount, std::max(qtiles_total, 1)));
+}
+
+Plan::KnnShape Plan::knn_shape(int i, int dir, int want_splits) const {
+    const int k = pairs[i].s2.max_keypoints;
+    const auto& match = off[i].match;
+    const int qt = k > 0 ? ceil_div(k, s4k::kQueryTile) : 0;
+    const int stages = std::max(1, ceil_div(std::max(k, 1), s4k::kTrainStage));
+    const int splits = std::min(want_splits, stages);
+    const int rows = ceil_div(stages, splits) * s4k::kTrainStage;
+    const int real_splits = ceil_div(std::max(k, 1), rows);
+    // the partial buffer of the match layout holds fsplits/rsplits entries;
+    // batch splits never exceed it (both come from the same capacities)
+    const bool fits = real_splits <= (dir ? match.rsplits : match.fsplits) || real_splits == 1;
+    KnnShape r;
+    r.splits = fits ? real_splits : 1;
+    r.rows = fits ? rows : std::max(s4k::kTrainStage, stages * s4k::kTrainStage);
+    r.blocks = qt * r.splits;
+    r.merge_blocks = (r.splits > 1 && k > 0) ? ceil_div(k, 256) : 0;
+    return r;
 }
 
 void Plan::job_blocks(int i, int s, int l, int (&db)[s2s3::kDetectKinds], int (&sb)[s2s3::kDescribeKinds]) const {
@@ -361,13 +403,7 @@ Status Plan::stage_tables(void* ws) {
             run_des[kind] += sb[kind];
         }
     };
-    int qtiles_total = 0;
-    for (int i = 0; i < n; ++i) {
-        const int dirs = pairs[i].s4.cross_check ? 2 : 1;
-        const int k = pairs[i].s2.max_keypoints;
-        qtiles_total += dirs * (k > 0 ? ceil_div(k, s4k::kQueryTile) : 0);
-    }
-    const int want_splits = std::max(1, ceil_div(2 * kSmCount, std::max(qtiles_total, 1)));
+    const int want_splits = knn_want_splits();
     int knn = 0, run_knn = 0, run_merge = 0, run_search = 0, run_fit = 0;
     for (int i = 0; i < n; ++i) {
         const auto& q = pairs[i];
@@ -420,22 +456,16 @@ Status Plan::stage_tables(void* ws) {
         for (int dir = 0; dir < dirs; ++dir) {
             const int qs = dir ? 1 : 0, ts = dir ? 0 : 1;
             const int qt = k > 0 ? ceil_div(k, s4k::kQueryTile) : 0;
-            const int stages = std::max(1, ceil_div(std::max(k, 1), s4k::kTrainStage));
-            const int splits = std::min(want_splits, stages);
-            const int rows = ceil_div(stages, splits) * s4k::kTrainStage;
-            const int real_splits = ceil_div(std::max(k, 1), rows);
-            // the partial buffer of the match layout holds fsplits/rsplits entries;
-            // batch splits never exceed it (both come from the same capacities)
+            const KnnShape sh = knn_shape(i, dir, want_splits);
             uint2* partial = at<uint2>(ws, o.s4ws + (dir ? o.match.rpartial : o.match.fpartial));
-            const bool fits = real_splits <= (dir ? o.match.rsplits : o.match.fsplits) || real_splits == 1;
-            const int use_splits = fits ? real_splits : 1;
-            const int use_rows = fits ? rows : std::max(s4k::kTrainStage, stages * s4k::kTrainStage);
-            kj[knn] = s4k::make_knn_job(kps[qs], desc[qs], kps[ts], desc[ts], std::max(qt, 1), use_splits, use_rows,
+            kj[knn] = s4k::make_knn_job(kps[qs], desc[qs], kps[ts], desc[ts], std::max(qt, 1), sh.splits, sh.rows,
                                         partial, dir ? rev : fwd);
             kp[knn] = run_knn;
             mp[knn] = run_merge;
-            run_knn += qt * use_splits;
-            run_merge += (use_splits > 1 && k > 0) ? ceil_div(k, 256) : 0;
+            fill_map(s45_first[kMapKnn], run_knn, s45_total[kMapKnn], knn, sh.blocks);
+            fill_map(s45_first[kMapMerge], run_merge, s45_total[kMapMerge], knn, sh.merge_blocks);
+            run_knn += sh.blocks;
+            run_merge += sh.merge_blocks;
             ++knn;
         }
         AcceptJob a{};
@@ -448,6 +478,8 @@ Status Plan::stage_tables(void* ws) {
                         at<int>(ws, o.mcount)};
         aj[i] = a;
         ap[i] = i;
+        fill_map(s45_first[kMapAccept], i, n, i, 1);
+        fill_map(s45_first[kMapPair], i, n, i, 1);
         // S5
         PairIO io;
         const Status st = s5k::check_and_build(
@@ -463,14 +495,19 @@ Status Plan::stage_tables(void* ws) {
         pp[i] = i;
         rj[i] = SearchJob{io, 0, q.s5.hypotheses, at<s5k::Model>(ws, o.models)};
         rp[i] = run_search;
+        const int fit_b = io.search_blocks > 0 ? ceil_div(q.s5.hypotheses, s5k::kFitThreads) : 0;
+        fill_map(s45_first[kMapSearch], run_search, s45_total[kMapSearch], i, io.search_blocks);
+        fill_map(s45_first[kMapFit], run_fit, s45_total[kMapFit], i, fit_b);
         run_search += io.search_blocks;
         fp[i] = run_fit;
-        run_fit += io.search_blocks > 0 ? ceil_div(q.s5.hypotheses, s5k::kFitThreads) : 0;
+        run_fit += fit_b;
     }
     if (bmap) {  // the maps must cover exactly the blocks of every launch
         for (int kind = 0; kind < s2s3::kDetectKinds; ++kind) map_ok = map_ok && run_det[kind] == det_total[kind];
         for (int kind = 0; kind < s2s3::kDescribeKinds; ++kind) map_ok = map_ok && run_des[kind] == des_total[kind];
         for (int kind = 0; kind < rkinds; ++kind) map_ok = map_ok && run_rs[kind] == rs_total[kind];
+        map_ok = map_ok && run_knn == s45_total[kMapKnn] && run_merge == s45_total[kMapMerge] &&
+                 run_search == s45_total[kMapSearch] && run_fit == s45_total[kMapFit];
         if (!map_ok) return Status::INVALID_ARGUMENT;
     }
     for (int kind = 0; kind < s2s3::kDetectKinds; ++kind) dp[kind * (nd + 1) + nd] = run_det[kind];
@@ -577,10 +614,19 @@ Status Plan::enqueue(void* ws, std::size_t bytes, stitch_homography_result* host
         s2s3::describe_kernel<DesSrc><<<des_blocks[s2s3::kDescKind], s2s3::kDescWarps * 32, 0, s>>>(des);
     mark();
 
+    // S4/S5 job tables, with their block maps when the plan has them
+    const auto* M = block_map ? reinterpret_cast<const std::uint32_t*>(T + offsets[kBlockMap]) : nullptr;
+    auto with_map = [&](auto src, int m) {
+        if (M) {
+            src.map = M + s45_first[m];
+            src.map_blocks = s45_total[m];
+        }
+        return src;
+    };
     using KnnSrc = s4k::JobTable<KnnJob>;
     const auto* kjobs = reinterpret_cast<const KnnJob*>(T + offsets[kKnnJobs]);
     if (go(knn_blocks)) {
-        const KnnSrc ks{kjobs, reinterpret_cast<const int*>(T + offsets[kKnnPrefix]), n_knn};
+        const KnnSrc ks = with_map(KnnSrc{kjobs, reinterpret_cast<const int*>(T + offsets[kKnnPrefix]), n_knn}, kMapKnn);
         if (s4k::matcher() == s4k::kMatcherTensor) {
             if (!s4k::enable_tc_smem<KnnSrc>()) return Status::CUDA_ERROR;
             s4k::knn_tc_kernel<KnnSrc><<<knn_blocks, s4k::kQueryThreads, s4k::kTcSmem, s>>>(ks);
@@ -591,28 +637,33 @@ Status Plan::enqueue(void* ws, std::size_t bytes, stitch_homography_result* host
     mark();
     if (go(merge_blocks))
         s4k::knn_merge_kernel<KnnSrc><<<merge_blocks, 256, 0, s>>>(
-            KnnSrc{kjobs, reinterpret_cast<const int*>(T + offsets[kMergePrefix]), n_knn});
+            with_map(KnnSrc{kjobs, reinterpret_cast<const int*>(T + offsets[kMergePrefix]), n_knn}, kMapMerge));
     mark();
     using AccSrc = s4k::JobTable<AcceptJob>;
     if (go(n))
-        s4k::accept_kernel<AccSrc><<<n, 1024, 0, s>>>(AccSrc{reinterpret_cast<const AcceptJob*>(T + offsets[kAccJobs]),
-                                                              reinterpret_cast<const int*>(T + offsets[kAccPrefix]), n});
+        s4k::accept_kernel<AccSrc><<<n, 1024, 0, s>>>(
+            with_map(AccSrc{reinterpret_cast<const AcceptJob*>(T + offsets[kAccJobs]),
+                            reinterpret_cast<const int*>(T + offsets[kAccPrefix]), n},
+                     kMapAccept));
     mark();
 
     using PairSrc = s5k::JobTable<PairIO>;
     using SearchSrc = s5k::JobTable<SearchJob>;
-    const PairSrc pairsrc{reinterpret_cast<const PairIO*>(T + offsets[kPairJobs]),
-                          reinterpret_cast<const int*>(T + offsets[kPairPrefix]), n};
+    const PairSrc pairsrc = with_map(PairSrc{reinterpret_cast<const PairIO*>(T + offsets[kPairJobs]),
+                                             reinterpret_cast<const int*>(T + offsets[kPairPrefix]), n},
+                                     kMapPair);
     if (go(n)) s5k::prepare_kernel<PairSrc><<<n, 256, 0, s>>>(pairsrc);
     mark();
     if (go(fit_blocks))
         s5k::fit_kernel<SearchSrc><<<fit_blocks, s5k::kFitThreads, 0, s>>>(
-            SearchSrc{reinterpret_cast<const SearchJob*>(T + offsets[kSearchJobs]),
-                      reinterpret_cast<const int*>(T + offsets[kFitPrefix]), n});
+            with_map(SearchSrc{reinterpret_cast<const SearchJob*>(T + offsets[kSearchJobs]),
+                               reinterpret_cast<const int*>(T + offsets[kFitPrefix]), n},
+                     kMapFit));
     if (go(search_blocks))
         s5k::search_kernel<SearchSrc, true><<<search_blocks, s5k::kSearchThreads, search_smem, s>>>(
-            SearchSrc{reinterpret_cast<const SearchJob*>(T + offsets[kSearchJobs]),
-                      reinterpret_cast<const int*>(T + offsets[kSearchPrefix]), n});
+            with_map(SearchSrc{reinterpret_cast<const SearchJob*>(T + offsets[kSearchJobs]),
+                               reinterpret_cast<const int*>(T + offsets[kSearchPrefix]), n},
+                     kMapSearch));
     mark();
     if (go(n)) s5k::finish_kernel<PairSrc><<<n, s5k::kFinishThreads, 0, s>>>(pairsrc);
     mark();

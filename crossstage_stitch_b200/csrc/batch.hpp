@@ -68,6 +68,11 @@ public:
     int det_total[s2s3::kDetectKinds] = {}, des_total[s2s3::kDescribeKinds] = {}, rs_total[s2s3::kMaxLevels] = {};
     std::size_t det_first[s2s3::kDetectKinds] = {}, des_first[s2s3::kDescribeKinds] = {},
                 rs_first[s2s3::kMaxLevels] = {};  // entry index of each kind's map
+    // and of the S4/S5 launches: knn, knn merge, accept, pair (prepare and
+    // finish), search, fit
+    enum { kMapKnn, kMapMerge, kMapAccept, kMapPair, kMapSearch, kMapFit, kMapS45 };
+    int s45_total[kMapS45] = {};
+    std::size_t s45_first[kMapS45] = {};
     cudaEvent_t marks[STITCH_BATCH_MARKS] = {};
     bool marked = false;
 
@@ -83,6 +88,12 @@ public:
         staged_for = nullptr;
     }
     Status stage_tables(void* ws);
+    // S4 train split of one matching direction of pair i.
+    struct KnnShape {
+        int splits, rows, blocks, merge_blocks;
+    };
+    int knn_want_splits() const;
+    KnnShape knn_shape(int i, int dir, int want_splits) const;
     // Blocks of the detect and describe kinds of job (pair i, side s, layer l).
     void job_blocks(int i, int s, int l, int (&db)[s2s3::kDetectKinds], int (&sb)[s2s3::kDescribeKinds]) const;
     // With device_tables (graph capture), the kernels read the job tables

@@ -68,7 +68,18 @@ template <class Job> struct JobTable {
     const Job* jobs;
     const int* prefix;
     int n;
+    // optional block -> (job << 16 | block within the job) map: one load
+    // instead of a binary search over the prefix
+    const std::uint32_t* map = nullptr;
+    int map_blocks = 0;
     __device__ bool find(int block, Job* j, int* local) const {
+        if (map) {
+            if (block >= map_blocks) return false;
+            const std::uint32_t e = __ldg(map + block);
+            *j = jobs[e >> 16];
+            *local = static_cast<int>(e & 0xffffu);
+            return true;
+        }
         if (block >= prefix[n]) return false;
         int lo = 0, hi = n - 1;
         while (lo < hi) {

@@ -100,7 +100,18 @@ template <class Job> struct JobTable {
     const Job* jobs;
     const int* prefix;
     int n;
+    // optional block -> (job << 16 | block within the job) map: one load
+    // instead of a binary search over the prefix
+    const std::uint32_t* map = nullptr;
+    int map_blocks = 0;
     __device__ bool find(int block, Job* j, int* local) const {
+        if (map) {
+            if (block >= map_blocks) return false;
+            const std::uint32_t e = __ldg(map + block);
+            *j = jobs[e >> 16];
+            *local = static_cast<int>(e & 0xffffu);
+            return true;
+        }
         if (block >= prefix[n]) return false;
         int lo = 0, hi = n - 1;
         while (lo < hi) {
@@ -621,7 +632,7 @@ __global__ __launch_bounds__(kFitThreads) void fit_kernel(const __grid_constant_
 // L1-backed local memory, but it is a small share of the work, and the
 // scoring loop gains the occupancy (1 block: 0.62 ms, 3 blocks: 0.43 ms for
 // 64 pairs x 2000 hypotheses x ~530 matches).
-constexpr int kPruneEvery = 256;  // points between the pruning checks of a model (multiple of 64)
+constexpr int kPruneEvery = 256;  // points between the pruning checks of a model (multiple of 128)
 
 // kPrefit: the models come from fit_kernel (sj.prefit) and the kernel only
 // scores (batched form: 0.387 -> 0.367 ms per step with the fit kernel
@@ -636,8 +647,11 @@ __global__ __launch_bounds__(kSearchThreads, 3) void search_kernel(const __grid_
     const PairIO& j = sj.io;
     const State* s = j.state;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    Model best{};
-    best.valid = 0;
+    // the warp's best model so far lives in shared memory, written by lane 0
+    // (registers stay with the scoring loop)
+    Model& best = warp_best[warp];
+    if (lane == 0) best.valid = 0;
+    __syncwarp();
     const bool ok = s->status == static_cast<int>(Status::OK);
     const int nm = ok ? s->nm : 0;
     const int staged = min(nm, kStagePoints);
@@ -693,30 +707,28 @@ __global__ __launch_bounds__(kSearchThreads, 3) void search_kernel(const __grid_
                 // nondecreasing in each operand, so the tree sum of the partial
                 // accumulators never exceeds the final loss. Once it is above
                 // the best loss the model cannot win (ties need equal losses).
-                const bool prune = __shfl_sync(0xffffffffu, best.valid, 0) != 0;
-                const double bound = __shfl_sync(0xffffffffu, best.loss, 0);
+                const bool prune = best.valid != 0;
+                const double bound = best.loss;
                 // Lane l accumulates the points l, l+32, l+64, l+96 (virtual
-                // lanes, slots 0..3) and every 128 after them in order; two
-                // points per step give two independent FP64 chains. A point
-                // past nm adds +0.0, which leaves a sum of nonnegative terms
+                // lanes, slots 0..3) and every 128 after them in order: four
+                // points per step, four independent FP64 chains. A point past
+                // nm adds +0.0, which leaves a sum of nonnegative terms
                 // (started at +0.0) bit for bit unchanged.
                 double acc0 = 0.0, acc1 = 0.0, acc2 = 0.0, acc3 = 0.0;
                 bool lost = false;
-                for (int base = 0; base < nm; base += 64) {  // warp-uniform trip count
-                    const int i0 = base + lane, i1 = base + 32 + lane;
+                for (int base = 0; base < nm; base += 128) {  // warp-uniform trip count
+                    const int i0 = base + lane, i1 = i0 + 32, i2 = i0 + 64, i3 = i0 + 96;
                     const Pt p0 = point_at(j, pts, min(i0, nm - 1));
                     const Pt p1 = point_at(j, pts, min(i1, nm - 1));
+                    const Pt p2 = point_at(j, pts, min(i2, nm - 1));
+                    const Pt p3 = point_at(j, pts, min(i3, nm - 1));
                     const double r0 = residual2(h, p0), r1 = residual2(h, p1);
-                    const double t0 = i0 < nm ? (r0 < thr2 ? r0 : thr2) : 0.0;
-                    const double t1 = i1 < nm ? (r1 < thr2 ? r1 : thr2) : 0.0;
-                    if ((base & 127) == 0) {
-                        acc0 += t0;
-                        acc1 += t1;
-                    } else {
-                        acc2 += t0;
-                        acc3 += t1;
-                    }
-                    if (prune && (base & (kPruneEvery - 1)) == kPruneEvery - 64 && base + 64 < nm) {
+                    const double r2 = residual2(h, p2), r3 = residual2(h, p3);
+                    acc0 += i0 < nm ? (r0 < thr2 ? r0 : thr2) : 0.0;
+                    acc1 += i1 < nm ? (r1 < thr2 ? r1 : thr2) : 0.0;
+                    acc2 += i2 < nm ? (r2 < thr2 ? r2 : thr2) : 0.0;
+                    acc3 += i3 < nm ? (r3 < thr2 ? r3 : thr2) : 0.0;
+                    if (prune && (base & (kPruneEvery - 1)) == kPruneEvery - 128 && base + 128 < nm) {
                         double part = (acc0 + acc2) + (acc1 + acc3);
 #pragma unroll
                         for (int o = 16; o > 0; o >>= 1) part += __shfl_down_sync(0xffffffffu, part, o);
@@ -740,10 +752,10 @@ __global__ __launch_bounds__(kSearchThreads, 3) void search_kernel(const __grid_
                     cand.valid = fin(v);
                     if (better(cand, best)) best = cand;
                 }
+                __syncwarp();
             }
         }
     }
-    if (lane == 0) warp_best[warp] = best;
     __syncthreads();
     if (threadIdx.x == 0) {
         Model b = warp_best[0];
