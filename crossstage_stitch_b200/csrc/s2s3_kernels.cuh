@@ -288,7 +288,7 @@ __device__ __forceinline__ std::uint32_t blur_byte(float acc) {
 // with each product and sum rounded on its own, then rounded half-to-even
 // and clamped), bit for bit the blur_kernel result.
 template <class Src>
-__global__ __launch_bounds__(256, 6) void fast_nms_kernel(const __grid_constant__ Src src) {
+__global__ __launch_bounds__(256, 8) void fast_nms_kernel(const __grid_constant__ Src src) {
     __shared__ __align__(16) std::uint8_t in[kFastInH][kInStride];
     __shared__ __align__(16) std::uint8_t sc[kFastScH][kScStride];
     __shared__ std::uint16_t cand[kFastScH * kScGroups];
@@ -390,20 +390,21 @@ __global__ __launch_bounds__(256, 6) void fast_nms_kernel(const __grid_constant_
             const auto* rb = reinterpret_cast<const std::uint32_t*>(&in[rr + 2][0]);
             const std::uint32_t a0 = ra[q + 3], a1 = ra[q + 4], a2 = ra[q + 5];  // bytes 4q+12 .. 4q+23
             const std::uint32_t b0 = rb[q + 3], b1 = rb[q + 4], b2 = rb[q + 5];
-            // output 4q+k reads halo columns 4q+k+1 .. 4q+k+7, i.e. x[1+k .. 7+k];
-            // lane x holds row rr, lane y row rr + 1
-            float2 x[11];
-            x[1] = byte_pair(a0, b0, 1); x[2] = byte_pair(a0, b0, 2); x[3] = byte_pair(a0, b0, 3);
-            x[4] = byte_pair(a1, b1, 0); x[5] = byte_pair(a1, b1, 1); x[6] = byte_pair(a1, b1, 2);
-            x[7] = byte_pair(a1, b1, 3); x[8] = byte_pair(a2, b2, 0); x[9] = byte_pair(a2, b2, 1);
-            x[10] = byte_pair(a2, b2, 2);
+            // output 4q+k reads halo columns 4q+k+1 .. 4q+k+7, i.e. x[1+k .. 7+k],
+            // tap t on x[1+k+t]; lane x holds row rr, lane y row rr + 1. The
+            // columns stream in once and every output adds its taps in order
+            // (0 + a nonnegative product is the product).
             float2 out[4];
 #pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                float2 acc = __fmul2_rn(tap_pair(0), x[1 + k]);  // 0 + a nonnegative product is the product
+            for (int m = 1; m <= 10; ++m) {
+                const std::uint32_t wa = m < 4 ? a0 : m < 8 ? a1 : a2, wb = m < 4 ? b0 : m < 8 ? b1 : b2;
+                const float2 xm = byte_pair(wa, wb, m & 3);
 #pragma unroll
-                for (int t = 1; t < 7; ++t) acc = __fadd2_rn(acc, __fmul2_rn(tap_pair(t), x[1 + k + t]));
-                out[k] = acc;
+                for (int k = 0; k < 4; ++k) {
+                    const int t = m - 1 - k;
+                    if (t == 0) out[k] = __fmul2_rn(tap_pair(0), xm);
+                    else if (t > 0 && t < 7) out[k] = __fadd2_rn(out[k], __fmul2_rn(tap_pair(t), xm));
+                }
             }
             *reinterpret_cast<float4*>(&rows[rr][4 * q]) = make_float4(out[0].x, out[1].x, out[2].x, out[3].x);
             *reinterpret_cast<float4*>(&rows[rr + 1][4 * q]) = make_float4(out[0].y, out[1].y, out[2].y, out[3].y);
@@ -421,20 +422,29 @@ __global__ __launch_bounds__(256, 6) void fast_nms_kernel(const __grid_constant_
     }
     if (j.blurred) {  // blur columns pass: rows 2p, 2p+1 and columns 4q .. 4q+3 per thread
         const int p = tid / (kFastTileW / 4), q = tid - p * (kFastTileW / 4);
-        float4 v[8];
+        // rows 2p .. 2p+7 stream in once: output row 2p + o adds tap t on
+        // row 2p + o + t, in order of t
+        float2 lo[2], hi[2];
 #pragma unroll
-        for (int t = 0; t < 8; ++t) v[t] = *reinterpret_cast<const float4*>(&rows[2 * p + t][4 * q]);
+        for (int r = 0; r < 8; ++r) {
+            const float4 v = *reinterpret_cast<const float4*>(&rows[2 * p + r][4 * q]);
+            const float2 vl = make_float2(v.x, v.y), vh = make_float2(v.z, v.w);
+#pragma unroll
+            for (int o = 0; o < 2; ++o) {
+                const int t = r - o;
+                if (t == 0) {
+                    lo[o] = __fmul2_rn(tap_pair(0), vl);
+                    hi[o] = __fmul2_rn(tap_pair(0), vh);
+                } else if (t > 0 && t < 7) {
+                    lo[o] = __fadd2_rn(lo[o], __fmul2_rn(tap_pair(t), vl));
+                    hi[o] = __fadd2_rn(hi[o], __fmul2_rn(tap_pair(t), vh));
+                }
+            }
+        }
 #pragma unroll
         for (int o = 0; o < 2; ++o) {
             const int gy = y0 + 2 * p + o, gx = x0 + 4 * q;
-            float2 lo = __fmul2_rn(tap_pair(0), make_float2(v[o].x, v[o].y));
-            float2 hi = __fmul2_rn(tap_pair(0), make_float2(v[o].z, v[o].w));
-#pragma unroll
-            for (int t = 1; t < 7; ++t) {
-                lo = __fadd2_rn(lo, __fmul2_rn(tap_pair(t), make_float2(v[o + t].x, v[o + t].y)));
-                hi = __fadd2_rn(hi, __fmul2_rn(tap_pair(t), make_float2(v[o + t].z, v[o + t].w)));
-            }
-            const float4 acc = make_float4(lo.x, lo.y, hi.x, hi.y);
+            const float4 acc = make_float4(lo[o].x, lo[o].y, hi[o].x, hi[o].y);
             if (gy >= H || gx >= W) continue;
             const std::uint32_t packed =
                 blur_byte(acc.x) | (blur_byte(acc.y) << 8) | (blur_byte(acc.z) << 16) | (blur_byte(acc.w) << 24);
