@@ -646,7 +646,7 @@ def main():
         e0.record(sb.copy_stream)
         prev = None
         for step in range(steps):
-            with torch.cuda.stream(sb.compute_stream):
+            with torch.cuda.stream(sb.streams[sb.next]):   # the stream of the slot this step takes
                 flush.zero_()
             slot = sb.step(hosts[step % 2])
             if prev is not None:
@@ -655,7 +655,9 @@ def main():
             prev = slot
         sb.wait(prev)
         _ = sb.result(prev, N_PAIRS - 1)["status"]
-        e1.record(sb.compute_stream)
+        for d in sb.done:
+            sb.copy_stream.wait_event(d)
+        e1.record(sb.copy_stream)
         e1.synchronize()
         return e0.elapsed_time(e1)
 

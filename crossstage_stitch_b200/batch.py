@@ -136,13 +136,15 @@ class StreamingBatches:
     All images of a step live in one contiguous buffer (image `side` of pair
     p at byte layout[p][side], rows of pitch_of(width) bytes), so a step's inputs
     move with one host-to-device copy. Two device slots, each with its own
-    captured graph, alternate: step() copies the pinned host buffer into the
-    free slot on a copy stream and launches that slot's graph on the compute
-    stream when the copy lands, so the copy of one step overlaps the
-    registration of the previous one. A slot's results stay valid until the
-    step after next is launched; wait(slot) then result(slot, i) reads them.
-    The host buffer of a step must not be refilled before that step's copy
-    has finished (use two host buffers, alternating)."""
+    captured graph and compute stream, alternate: step() copies the pinned
+    host buffer into the free slot on a copy stream and launches that slot's
+    graph on the slot's stream when the copy lands, so the copy of one step
+    overlaps the registration of the previous one, and a step's first kernels
+    may start on SMs that the previous step's last kernels leave idle. A
+    slot's results stay valid until the step after next is launched;
+    wait(slot) then result(slot, i) reads them. The host buffer of a step must
+    not be refilled before that step's copy has finished (use two host
+    buffers, alternating)."""
 
     def __init__(self, sizes: list[tuple[int, int, int, int]], knobs: list[Knobs], device=None):
         self.device = device or torch.device("cuda", torch.cuda.current_device())
@@ -157,9 +159,9 @@ class StreamingBatches:
         self.nbytes = max(cursor, 1)
         self.slots = [torch.empty(self.nbytes, dtype=torch.uint8, device=self.device) for _ in range(2)]
         self.copy_stream = torch.cuda.Stream(self.device)
-        self.compute_stream = torch.cuda.Stream(self.device)
+        self.streams = [torch.cuda.Stream(self.device) for _ in range(2)]  # compute stream of each slot
         self.batches = []
-        for buf in self.slots:
+        for buf, stream in zip(self.slots, self.streams):
             descs = []
             for (wa, ha, wb, hb), (oa, ob), k in zip(self.sizes, self.layout, knobs):
                 d = PairDesc()
@@ -169,12 +171,12 @@ class StreamingBatches:
                 d.pyramid = k.pyramid()
                 descs.append(d)
             b = Batch(descs, self.device)
-            b.capture(self.compute_stream)
+            b.capture(stream)
             self.batches.append(b)
         self.copied = [torch.cuda.Event() for _ in range(2)]
         self.done = [torch.cuda.Event() for _ in range(2)]
-        for e in self.done:
-            e.record(self.compute_stream)
+        for e, stream in zip(self.done, self.streams):
+            e.record(stream)
         self.next = 0
 
     @staticmethod
@@ -200,9 +202,9 @@ class StreamingBatches:
         with torch.cuda.stream(self.copy_stream):
             self.slots[s].copy_(host, non_blocking=True)
         self.copied[s].record(self.copy_stream)
-        self.compute_stream.wait_event(self.copied[s])
-        self.batches[s].launch(self.compute_stream)
-        self.done[s].record(self.compute_stream)
+        self.streams[s].wait_event(self.copied[s])
+        self.batches[s].launch(self.streams[s])
+        self.done[s].record(self.streams[s])
         return s
 
     def wait(self, slot: int) -> None:
