@@ -589,8 +589,8 @@ def main():
     flush = torch.empty(128 << 20, dtype=torch.int32, device=dev)  # 512 MB, written by a vectorised fill
 
     # ---- batched form: one graph for all pairs
-    # The timed graph carries no event marks (an event-record node costs about
-    # 2.6 us of graph time); a marked copy of it, on its own workspace, gives
+    # The timed graph carries no event marks (an event-record node between two
+    # kernels costs about 5 us of graph time); a marked copy of it, on its own workspace, gives
     # the per-kernel split.
     descs = [batch.pair_desc(ia, ib, k) for (ia, ib), k in zip(imgs, knobs)]
     b = batch.Batch(descs, device=dev)
