@@ -87,7 +87,7 @@ DetectJob make_detect_job(const ImageView& im, const s2::Config& c, const Keypoi
 
 int sort_smem_bytes(int candidates) {
     int n = candidates < kSortCap ? candidates : kSortCap;
-    int p = 1;
+    int p = kSortChunk;  // the kernel sorts at least one 64-key chunk
     while (p < n) p <<= 1;
     return p * static_cast<int>(sizeof(std::uint64_t));
 }

@@ -160,6 +160,7 @@ constexpr int kChunkPx = 8192;     // pixels per compaction block (256 threads x
 constexpr int kHarrisThreads = 256;
 constexpr int kSortCap = 16384;    // candidates sorted in shared memory by one block
 constexpr int kSortThreads = 1024;
+constexpr int kSortChunk = 64;      // keys a warp sorts in registers (2 per lane)
 constexpr int kBlurTileW = 64, kBlurTileH = 32;
 constexpr int kDescWarps = 8;
 constexpr int kEdge = 31;
@@ -766,22 +767,55 @@ __global__ __launch_bounds__(kSortThreads) void sort_topk_kernel(const __grid_co
     if (!src.find(blockIdx.x, kSortKind, &j, &local)) return;
     const int n = static_cast<int>(j.params->selected);
     if (n > kSortCap || n == 0) return;
-    int N = 1;
+    int N = kSortChunk;  // at least one 64-key chunk (zero keys pad and sort last)
     while (N < n) N <<= 1;
     for (int i = threadIdx.x; i < N; i += kSortThreads) sk[i] = i < n ? j.keys[i] : 0ull;
     __syncthreads();
-    for (int k = 2; k <= N; k <<= 1) {
-        for (int s = k >> 1; s > 0; s >>= 1) {
+    // Bitonic network, keys unique: a compare-exchange of i < q = i + s puts
+    // the larger key first where (i & k) == 0 (those runs end up descending).
+    // Exchanges closer than 64 keys run in registers, a warp holding keys
+    // c*64 + lane and c*64 + lane + 32 of chunk c; wider ones in shared memory.
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    auto chunk_pass = [&](int k_lo, int k_hi, int s_top) {
+        for (int c = warp; c < N / kSortChunk; c += kSortThreads / 32) {
+            const int e0 = c * kSortChunk + lane;
+            std::uint64_t v0 = sk[e0], v1 = sk[e0 + 32];
+            for (int k = k_lo; k <= k_hi; k <<= 1) {
+                for (int s = min(k >> 1, s_top); s > 0; s >>= 1) {
+                    if (s == 32) {  // v0 (key e0) is the lower of the pair
+                        const bool desc = (e0 & k) == 0;
+                        const std::uint64_t hi = v0 > v1 ? v0 : v1, lo = v0 > v1 ? v1 : v0;
+                        v0 = desc ? hi : lo;
+                        v1 = desc ? lo : hi;
+                    } else {
+                        const bool lower = (lane & s) == 0;
+                        const std::uint64_t p0 = __shfl_xor_sync(0xffffffffu, v0, s);
+                        const std::uint64_t p1 = __shfl_xor_sync(0xffffffffu, v1, s);
+                        const bool keep_hi0 = lower == ((e0 & k) == 0);
+                        const bool keep_hi1 = lower == (((e0 + 32) & k) == 0);
+                        v0 = keep_hi0 ? (v0 > p0 ? v0 : p0) : (v0 > p0 ? p0 : v0);
+                        v1 = keep_hi1 ? (v1 > p1 ? v1 : p1) : (v1 > p1 ? p1 : v1);
+                    }
+                }
+            }
+            sk[e0] = v0;
+            sk[e0 + 32] = v1;
+        }
+        __syncthreads();
+    };
+    chunk_pass(2, kSortChunk, kSortChunk / 2);  // runs up to 64 keys: registers only
+    for (int k = 2 * kSortChunk; k <= N; k <<= 1) {
+        for (int s = k >> 1; s >= kSortChunk; s >>= 1) {
             for (int t = threadIdx.x; t < (N >> 1); t += kSortThreads) {
                 const int i = (t / s) * (s << 1) + (t % s);
                 const int q = i + s;
                 const std::uint64_t a = sk[i], b = sk[q];
-                // Blocks with (i & k) == 0 end up descending.
                 const bool descending = (i & k) == 0;
                 if (descending ? (a < b) : (a > b)) { sk[i] = b; sk[q] = a; }
             }
             __syncthreads();
         }
+        chunk_pass(k, k, kSortChunk / 2);
     }
     const int limit = min(n, j.max_keypoints);
     for (int i = threadIdx.x; i < limit; i += kSortThreads) write_keypoint(j, i, sk[i]);
