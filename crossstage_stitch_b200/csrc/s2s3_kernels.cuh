@@ -413,12 +413,38 @@ __global__ __launch_bounds__(256, 8) void fast_nms_kernel(const __grid_constant_
     }
     __syncthreads();
     const int nc = n_cand;
-    for (int i = tid; i < nc; i += 256) {
-        const int e = cand[i];
-        const int grp = e >> 4, r = grp / kScGroups, c0 = 4 * (grp - r * kScGroups);
-        for (unsigned bits = e & 0xfu; bits; bits &= bits - 1) {
-            const int c = c0 + __ffs(bits) - 1;
-            sc[r][c] = static_cast<std::uint8_t>(fast_score(&in[r + 3][c + 3 + kInOff], kInStride, j.threshold));
+    {   // each warp expands its 32 survivor groups of a round into a warp-local
+        // position list (warp scan of the counts) and scores it 32 at a time,
+        // instead of looping over each group's survivors divergently
+        __shared__ std::uint16_t wpos[8][128];
+        const int warp = tid >> 5;
+        for (int base = 0; base < nc; base += 256) {
+            const int i = base + tid;
+            unsigned bits = 0;
+            int pos0 = 0;
+            if (i < nc) {
+                const int e = cand[i];
+                const int grp = e >> 4, r = grp / kScGroups, c0 = 4 * (grp - r * kScGroups);
+                bits = e & 0xfu;
+                pos0 = r * kScStride + c0;
+            }
+            const int cnt = __popc(bits);
+            int incl = cnt;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= o) incl += t;
+            }
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            int o = incl - cnt;
+            for (unsigned b = bits; b; b &= b - 1) wpos[warp][o++] = static_cast<std::uint16_t>(pos0 + __ffs(b) - 1);
+            __syncwarp();
+            for (int k = lane; k < total; k += 32) {
+                const int e2 = wpos[warp][k];
+                const int r = e2 / kScStride, c = e2 - r * kScStride;
+                sc[r][c] = static_cast<std::uint8_t>(fast_score(&in[r + 3][c + 3 + kInOff], kInStride, j.threshold));
+            }
+            __syncwarp();
         }
     }
     if (j.blurred) {  // blur columns pass: rows 2p, 2p+1 and columns 4q .. 4q+3 per thread
