@@ -216,8 +216,8 @@ def run_reference(args):
 # DRAM bytes (read + write) per launch of a kernel of the batched step, from
 # one ncu capture of this workload (dram__bytes_read.sum + dram__bytes_write.sum).
 NCU_TRAFFIC = {
-    "fast_nms": (284.56e6, "ncu, profiles/fast_nms_batch64_512_l8_ncu.md"),
-    "describe": (169.36e6, "ncu, profiles/fast_nms_batch64_512_l8_ncu.md"),
+    "fast_nms": (280.24e6, "ncu, profiles/fast_nms_batch64_512_l8_ncu.md"),
+    "describe": (169.51e6, "ncu, profiles/fast_nms_batch64_512_l8_ncu.md"),
     "search": (13.09e6, "ncu, profiles/fast_nms_batch64_512_l8_ncu.md (scoring kernel)"),
 }
 
