@@ -155,37 +155,11 @@ __device__ __forceinline__ bool h_normalize(double* h) {
 
 // Squared forward reprojection error of B -> A; DBL_MAX when the projective
 // denominator is not finite or too close to zero.
-// a / b rounded to nearest, given y = RN(1 / b). Markstein's theorem (P.
-// Markstein, "Computation of elementary functions on the IBM RISC System/6000
-// processor", IBM J. Res. Develop. 34(1), 1990): q0 = RN(a y) is within one
-// ulp of a / b, the FMA residual a - b q0 is exact, and RN(q0 + (a - b q0) y)
-// is RN(a / b), as long as nothing over- or underflows.
-__device__ __forceinline__ double div_by_recip(double a, double b, double y) {
-    const double q0 = __dmul_rn(a, y);
-    return __fma_rn(__fma_rn(-b, q0, a), y, q0);
-}
-
-// Squared reprojection distance of match p under h (B -> A). Both quotients
-// share one correctly rounded reciprocal of z; each equals the plain division
-// bit for bit (1/z is normal for 1e-15 <= |z| <= 1e300, where it is used; a
-// quotient that is subnormal or beyond DBL_MAX leaves r the same either way,
-// 0 or not finite).
 __device__ __forceinline__ double residual2(const double* h, const Pt& p) {
     const double z = h[6] * p.bx + h[7] * p.by + h[8];
     if (!fin(z) || fabs(z) < 1e-15) return DBL_MAX;
-    const double X = h[0] * p.bx + h[1] * p.by + h[2];
-    const double Y = h[3] * p.bx + h[4] * p.by + h[5];
-    double qx, qy;
-    if (fabs(z) <= 1e300) {
-        const double y = __drcp_rn(z);
-        qx = div_by_recip(X, z, y);
-        qy = div_by_recip(Y, z, y);
-    } else {
-        qx = X / z;
-        qy = Y / z;
-    }
-    const double dx = qx - p.ax;
-    const double dy = qy - p.ay;
+    const double dx = (h[0] * p.bx + h[1] * p.by + h[2]) / z - p.ax;
+    const double dy = (h[3] * p.bx + h[4] * p.by + h[5]) / z - p.ay;
     const double r = dx * dx + dy * dy;
     return fin(r) ? r : DBL_MAX;
 }

@@ -49,6 +49,17 @@ __global__ void check(unsigned long long n, unsigned long long* bad) {
         if (fabs(q) >= 0x1p-1022 && fabs(q) <= DBL_MAX &&
             __double_as_longlong(div_by_recip(a, b, __drcp_rn(b))) != __double_as_longlong(q))
             ++local;
+        // guarded division (any operands, zeros and extremes included): raw bits,
+        // so the sign of a zero counts
+        {
+            s = mix(s);
+            const int kind = static_cast<int>(s & 7);
+            const double ga = kind == 0 ? 0.0 : kind == 1 ? -0.0 : rnd(s, kind == 2 ? -1074 : -1022, kind == 3 ? 1023 : 200);
+            const double gb = rnd(s, kind == 4 ? -1074 : -1022, kind == 5 ? 1023 : 200);
+            if (__double_as_longlong(stitch::b200::s5k::div_guarded(ga, gb, stitch::b200::s5k::recip_or_nan(gb))) !=
+                __double_as_longlong(ga / gb))
+                ++local;
+        }
         // residuals: a homography near the identity or random, pixel or far-out points
         double h[9];
         s = mix(s);
