@@ -18,6 +18,7 @@
 //             image (or its pyramid workspace), matches, inlier mask, S4 and
 //             S5 workspaces
 #include <algorithm>
+#include <iterator>
 #include <cstring>
 #include <mutex>
 
@@ -211,6 +212,10 @@ Status Plan::build(int n_pairs, const stitch_pair_desc* p, int* bad_pair, bool a
     search_blocks = static_cast<int>(rounds_at);
     // block totals of every detect, describe and resize kind, for the block
     // -> job maps (the same per-job counts stage_tables lays out)
+    std::fill(std::begin(det_total), std::end(det_total), 0);
+    std::fill(std::begin(des_total), std::end(des_total), 0);
+    std::fill(std::begin(rs_total), std::end(rs_total), 0);
+    std::fill(std::begin(s45_total), std::end(s45_total), 0);
     bool map_fits = alloc_staging && n_det < (1 << 16) && n_resize < (1 << 16);
     for (int i = 0; i < n; ++i)
         for (int s = 0; s < 2; ++s) {
