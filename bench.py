@@ -216,9 +216,9 @@ def run_reference(args):
 # DRAM bytes (read + write) per launch of a kernel of the batched step, from
 # one ncu capture of this workload (dram__bytes_read.sum + dram__bytes_write.sum).
 NCU_TRAFFIC = {
-    "fast_nms": (280.24e6, "ncu, profiles/fast_nms_batch64_512_l8_ncu.md"),
-    "describe": (169.51e6, "ncu, profiles/fast_nms_batch64_512_l8_ncu.md"),
-    "search": (13.09e6, "ncu, profiles/fast_nms_batch64_512_l8_ncu.md (scoring kernel)"),
+    "fast_nms": (280.24e6, "ncu capture of this workload"),
+    "describe": (169.51e6, "ncu capture of this workload"),
+    "search": (13.09e6, "ncu capture of this workload (scoring kernel)"),
 }
 
 N_MIXED = 256

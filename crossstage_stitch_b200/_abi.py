@@ -194,6 +194,7 @@ PROTOTYPES: dict[str, tuple] = {
                                             P(Descriptors), P(Descriptors), P(Matches), P(C.c_void_p),
                                             P(C.c_void_p)]),
     "stitch_batch_destroy": (None, [C.c_void_p]),
+    "stitch_batch_set_matcher": (C.c_int, [C.c_void_p, C.c_int]),
     "stitch_batch_set_marks": (C.c_int, [C.c_void_p, P(C.c_void_p), C.c_int]),
     "stitch_server_create": (C.c_int, [P(ServerConfig), P(C.c_void_p)]),
     "stitch_server_request_bytes": (C.c_int, [P(Request), _size_p]),

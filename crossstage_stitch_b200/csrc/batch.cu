@@ -81,6 +81,7 @@ Plan::~Plan() {
 
 Status Plan::build(int n_pairs, const stitch_pair_desc* p, int* bad_pair, bool alloc_staging) {
     if (n_pairs <= 0 || !p) return Status::INVALID_ARGUMENT;
+    matcher = s4k::matcher();
     n = n_pairs;
     pairs.assign(p, p + n);
     off.assign(n, PairOffsets{});
@@ -632,7 +633,7 @@ Status Plan::enqueue(void* ws, std::size_t bytes, stitch_homography_result* host
     const auto* kjobs = reinterpret_cast<const KnnJob*>(T + offsets[kKnnJobs]);
     if (go(knn_blocks)) {
         const KnnSrc ks = with_map(KnnSrc{kjobs, reinterpret_cast<const int*>(T + offsets[kKnnPrefix]), n_knn}, kMapKnn);
-        if (s4k::matcher() == s4k::kMatcherTensor) {
+        if (matcher == s4k::kMatcherTensor) {
             if (!s4k::enable_tc_smem<KnnSrc>()) return Status::CUDA_ERROR;
             s4k::knn_tc_kernel<KnnSrc><<<knn_blocks, s4k::kQueryThreads, s4k::kTcSmem, s>>>(ks);
         } else {
@@ -812,6 +813,12 @@ int stitch_batch_pair_outputs(const stitch_batch* b, void* ws, int i, stitch_key
 }
 
 void stitch_batch_destroy(stitch_batch* b) { delete b; }
+
+int stitch_batch_set_matcher(stitch_batch* b, int kind) {
+    if (!b || !stitch::b200::s4k::valid_matcher(kind)) return static_cast<int>(Status::INVALID_ARGUMENT);
+    b->plan.matcher = kind;
+    return 0;
+}
 
 int stitch_batch_set_marks(stitch_batch* b, void* const* events, int count) {
     if (!b || (events && count != STITCH_BATCH_MARKS)) return static_cast<int>(Status::INVALID_ARGUMENT);

@@ -51,6 +51,9 @@ public:
     int sort_smem = 0, search_smem = 0;
     bool rank_fallback = false;
     int hpw = 8;
+    // binary matcher of this plan's S4 launches (s4k::kMatcherPopc or
+    // kMatcherTensor): the building thread's choice, or stitch_batch_set_matcher's
+    int matcher = s4k::kMatcherTensor;
     // host staging of the tables (pinned), filled for one workspace address;
     // either allocated by build() or lent by the caller (use_staging)
     unsigned char* staging = nullptr;
@@ -80,6 +83,10 @@ public:
     int resize_kinds() const { return max_levels > 1 ? max_levels - 1 : 1; }
     // Validates the pairs and lays out the workspace (host work only), then,
     // with alloc_staging, allocates the pinned staging of the job tables.
+    // Every count, total, offset and block-map total it derives is reset and
+    // recomputed, so calling it again on the same plan gives the layout of a
+    // fresh plan (tests/test_plan_rebuild.py builds one plan twice and
+    // compares).
     Status build(int n_pairs, const stitch_pair_desc* p, int* bad_pair, bool alloc_staging = true);
     // Lends a pinned buffer of at least table_bytes as the staging.
     void use_staging(unsigned char* buf) {

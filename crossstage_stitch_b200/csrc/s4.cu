@@ -6,7 +6,6 @@
 // Top2 array sits at offset 0 of the workspace, where s4_forward_neighbors
 // exposes it to later consumers.
 #include <algorithm>
-#include <atomic>
 #include <cmath>
 #include <limits>
 
@@ -96,11 +95,26 @@ KnnJob make_knn_job(const Keypoints& qk, const Descriptors& qd, const Keypoints&
 
 namespace {
 // The tensor-core matcher measured 2.7x faster than __popc on the batched
-// 64-pair workload (0.139 vs 0.375 ms per step), so it is the default.
-std::atomic<int> g_matcher{kMatcherTensor};
+// 64-pair workload (0.139 vs 0.375 ms per step), so it is the default. The
+// choice belongs to the calling host thread.
+thread_local int t_matcher = kMatcherTensor;
 }  // namespace
 
-int matcher() { return g_matcher.load(std::memory_order_relaxed); }
+int matcher() { return t_matcher; }
+
+Status check_match_args(const Keypoints& a, const Descriptors& da, const Keypoints& b, const Descriptors& db,
+                        const s4::Config& config, const Matches& output, std::size_t* required) {
+    *required = 0;
+    if (s4::s4_workspace_bytes(a.capacity, b.capacity, config, required) != Status::OK ||
+        !valid_pair(a, da, b, db) || output.capacity < a.capacity || !output.d_count ||
+        !aligned(output.d_count, alignof(int)) ||
+        (a.capacity && (!output.idx_a || !output.idx_b || !output.distance ||
+                        !aligned(output.idx_a, alignof(int32_t)) || !aligned(output.idx_b, alignof(int32_t)) ||
+                        !aligned(output.distance, alignof(float)))))
+        return Status::INVALID_ARGUMENT;
+    return Status::OK;
+}
+bool valid_matcher(int kind) { return kind == kMatcherPopc || kind == kMatcherTensor; }
 
 namespace {
 
@@ -182,13 +196,7 @@ Status s4_match(const Keypoints& a, const Descriptors& da, const Keypoints& b, c
                 const Config& config, Matches output, void* workspace, std::size_t workspace_bytes,
                 cudaStream_t stream) {
     std::size_t required = 0;
-    if (s4_workspace_bytes(a.capacity, b.capacity, config, &required) != Status::OK ||
-        !valid_pair(a, da, b, db) || output.capacity < a.capacity || !output.d_count ||
-        !aligned(output.d_count, alignof(int)) ||
-        (a.capacity && (!output.idx_a || !output.idx_b || !output.distance ||
-                        !aligned(output.idx_a, alignof(int32_t)) || !aligned(output.idx_b, alignof(int32_t)) ||
-                        !aligned(output.distance, alignof(float)))))
-        return Status::INVALID_ARGUMENT;
+    if (check_match_args(a, da, b, db, config, output, &required) != Status::OK) return Status::INVALID_ARGUMENT;
     if (workspace_bytes < required || (required && !workspace)) return Status::INSUFFICIENT_WORKSPACE;
     if (required && (!aligned(workspace, alignof(Top2)) ||
                      reinterpret_cast<std::uintptr_t>(workspace) >
@@ -237,8 +245,8 @@ extern "C" {
 
 int stitch_s4_set_matcher(int kind) {
     using namespace stitch::b200::s4k;
-    if (kind != kMatcherPopc && kind != kMatcherTensor) return static_cast<int>(stitch::Status::INVALID_ARGUMENT);
-    g_matcher.store(kind, std::memory_order_relaxed);
+    if (!valid_matcher(kind)) return static_cast<int>(stitch::Status::INVALID_ARGUMENT);
+    t_matcher = kind;
     return 0;
 }
 

@@ -17,11 +17,19 @@ bool valid_side(const Keypoints& k, const Descriptors& d);
 bool valid_pair(const Keypoints& a, const Descriptors& da, const Keypoints& b, const Descriptors& db);
 bool popc_eligible(const Descriptors& q, const Descriptors& t, int capacity_train);
 
-// Binary matcher used by every S4 launch of this process: kMatcherPopc (the
-// __popc tile kernel) or kMatcherTensor (tcgen05 kind::i8). Results are
-// identical; the choice only changes speed.
+// Binary matcher of an S4 launch: kMatcherPopc (the __popc tile kernel) or
+// kMatcherTensor (tcgen05 kind::i8). Results are identical; the choice only
+// changes speed. The stage calls use the calling host thread's choice
+// (stitch_s4_set_matcher), so threads never race on it; a batch plan and a
+// server take the creating thread's choice when they are made, and a plan can
+// be given its own (stitch_batch_set_matcher).
 constexpr int kMatcherPopc = 0, kMatcherTensor = 1;
 int matcher();
+bool valid_matcher(int kind);
+// Host-only argument checks of s4_match, in its order: INVALID_ARGUMENT or
+// OK, with *required the workspace bytes the call needs.
+Status check_match_args(const Keypoints& a, const Descriptors& da, const Keypoints& b, const Descriptors& db,
+                        const s4::Config& config, const Matches& output, std::size_t* required);
 // Opts the tensor-core kernel for a job source in to its shared memory
 // (once per device); false if the device refuses.
 template <class Src> bool enable_tc_smem() {

@@ -210,6 +210,7 @@ class Server {
 public:
     explicit Server(const stitch_server_config& c) : cfg_(c), arena_(c.arena_bytes) {
         t0_ = std::chrono::steady_clock::now();
+        matcher_ = s4k::matcher();  // the creating thread's choice; the dispatcher thread builds the plans
     }
     ~Server() { shutdown(); }
 
@@ -505,6 +506,7 @@ private:
                 return false;
             }
             plan->use_staging(s.staging);
+            plan->matcher = matcher_;
             s.reqs.assign(pending_.begin(), pending_.begin() + n);
             pending_.erase(pending_.begin(), pending_.begin() + n);
             s.offset = off;
@@ -608,6 +610,7 @@ private:
     }
 
     stitch_server_config cfg_;
+    int matcher_ = s4k::kMatcherTensor;  // S4 matcher of every plan this server builds
     Arena arena_;
     std::chrono::steady_clock::time_point t0_;
     std::vector<Slot> slots_;

@@ -198,11 +198,13 @@ int stitch_pyramid_detect_describe(const stitch_image_view* image, const stitch_
 
 /* ------------------------------------------------------------------- S4 */
 
-/* No reference counterpart. Chooses the exact binary matcher every later S4
- * launch of this process uses (stitch_s4_* calls and the batched and served
- * forms): 0 the __popc tile kernel, 1 (the default) the tcgen05 kind::i8
- * tensor-core kernel (descriptor bits as +-1 int8, Hamming = (256 - dot) /
- * 2). Results are identical. stitch_s4_tc_errors reads and clears the tensor-core
+/* No reference counterpart. Chooses the exact binary matcher of the calling
+ * host thread's later S4 launches (stitch_s4_* calls) and of the batch plans
+ * and servers it creates afterwards: 0 the __popc tile kernel, 1 (the
+ * default) the tcgen05 kind::i8 tensor-core kernel (descriptor bits as +-1
+ * int8, Hamming = (256 - dot) / 2). The choice is per thread, so threads
+ * never race on it; stitch_batch_set_matcher changes one plan's. Results
+ * are identical. stitch_s4_tc_errors reads and clears the tensor-core
  * kernel's error word (1: an MMA completion wait ran out; -1: read failed). */
 int stitch_s4_set_matcher(int kind);
 int stitch_s4_matcher(void);
@@ -336,6 +338,10 @@ int stitch_batch_pair_outputs(const stitch_batch* plan, void* workspace, int pai
                               stitch_keypoints* kp_b, stitch_descriptors* desc_a, stitch_descriptors* desc_b,
                               stitch_matches* matches, uint8_t** inlier_mask, stitch_homography_result** result);
 void stitch_batch_destroy(stitch_batch* plan);
+/* No reference counterpart (batched form). The S4 matcher of this plan's
+ * later enqueues and captures (0 __popc, 1 tensor cores; see
+ * stitch_s4_set_matcher, whose choice a plan takes when it is created). */
+int stitch_batch_set_matcher(stitch_batch* plan, int kind);
 /* Per-kernel timing hook of the batched form (like the reference's S2/S3
  * event marks, src/s2_s3/s2_s3_marks.hpp:16-34): `events` holds
  * STITCH_BATCH_MARKS cudaEvent_t recorded, in order, after the table upload,

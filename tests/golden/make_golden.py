@@ -1,7 +1,7 @@
 """Generates the S2/S3 golden fixtures from the reference's own NumPy path.
 
 Run here, where the reference tree is mounted:
-    python tests/golden/make_golden.py --reference /root/reference
+    python tests/golden/make_golden.py --reference <reference tree>
 
 It imports tools/s2_s3/reference.py and tools/s2_s3/fixtures.py from the
 reference tree and evaluates the nine cases that the reference's golden
@@ -45,7 +45,7 @@ def cases(fixtures):
 
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    ap.add_argument("--reference", type=Path, default=Path("/root/reference"))
+    ap.add_argument("--reference", type=Path, required=True, help="the reference source tree")
     ap.add_argument("--out", type=Path, default=HERE)
     args = ap.parse_args()
     sys.path.insert(0, str(args.reference))

@@ -1,7 +1,7 @@
 """Generates the S6 feather golden fixtures from the reference's FP64 NumPy path.
 
 Run here, where the reference tree is mounted:
-    python tests/golden/make_s6_golden.py --reference /root/reference
+    python tests/golden/make_s6_golden.py --reference <reference tree>
 
 It imports tools/s6_reference/reference.py from the reference tree and renders,
 in feather mode, the eight cases of the reference's own golden exporter
@@ -84,7 +84,7 @@ def cases():
 
 def main() -> None:
     ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
-    ap.add_argument("--reference", type=Path, default=Path("/root/reference"))
+    ap.add_argument("--reference", type=Path, required=True, help="the reference source tree")
     ap.add_argument("--out", type=Path, default=HERE)
     args = ap.parse_args()
     sys.path.insert(0, str(args.reference))

@@ -185,3 +185,51 @@ def test_server_request_bytes_is_host_only():
     bad.host_a = None
     assert nbytes(bad) == (Status.INVALID_ARGUMENT, 0)
     assert L.stitch_server_request_bytes(None, None) == Status.INVALID_ARGUMENT
+
+
+def test_static_match_reports_argument_errors_like_stitch_s4_match():
+    """stitch_s4_match_static runs stitch_s4_match's host checks first, so an
+    invalid request gets the same status from both (INVALID_ARGUMENT), and
+    only a valid request too large for the 4 MiB scratch gets
+    INSUFFICIENT_WORKSPACE; neither reaches the device."""
+    from crossstage_stitch_b200._abi import Descriptors, Keypoints, Matches
+    L = _abi.load()
+    cfg = S4Config()
+    cfg.ratio_threshold = 0.8
+    cfg.cross_check = 1
+    big = 200000
+    fake = 1 << 20   # aligned host-side stand-ins; nothing is dereferenced
+    kp = Keypoints(0, 0, 0, big, fake)
+    out = Matches(fake, fake, fake, big, fake)
+    bad_desc = Descriptors(0, 32, 0, fake)     # stride 0: invalid
+    good_desc = Descriptors(0, 32, 32, fake)
+    args = lambda d: (C.byref(kp), C.byref(d), C.byref(kp), C.byref(d), C.byref(cfg), C.byref(out))
+    assert L.stitch_s4_match_static(*args(bad_desc), None) == Status.INVALID_ARGUMENT
+    assert L.stitch_s4_match(*args(bad_desc), None, 0, None) == Status.INVALID_ARGUMENT
+    assert L.stitch_s4_match_static(*args(good_desc), None) == Status.INSUFFICIENT_WORKSPACE
+    assert L.stitch_s4_match(*args(good_desc), None, 0, None) == Status.INSUFFICIENT_WORKSPACE
+    short = Matches(fake, fake, fake, big - 1, fake)   # output capacity below the query capacity
+    assert L.stitch_s4_match_static(C.byref(kp), C.byref(good_desc), C.byref(kp), C.byref(good_desc),
+                                    C.byref(cfg), C.byref(short), None) == Status.INVALID_ARGUMENT
+
+
+def test_matcher_choice_is_per_thread():
+    """The S4 matcher is a property of the calling host thread: another
+    thread's choice does not change this one's."""
+    import threading
+    L = _abi.load()
+    mine = L.stitch_s4_matcher()
+    assert L.stitch_s4_set_matcher(7) == Status.INVALID_ARGUMENT
+    seen = {}
+
+    def other():
+        seen["default"] = L.stitch_s4_matcher()
+        seen["set"] = L.stitch_s4_set_matcher(1 - mine)
+        seen["after"] = L.stitch_s4_matcher()
+
+    t = threading.Thread(target=other)
+    t.start()
+    t.join()
+    assert seen == {"default": 1, "set": 0, "after": 1 - mine}
+    assert L.stitch_s4_matcher() == mine
+    assert L.stitch_batch_set_matcher(None, 0) == Status.INVALID_ARGUMENT
