@@ -122,7 +122,19 @@ def cpu_pair(args):
     return time.perf_counter() - t
 
 
-def cpu_baseline(sample_pairs: int, workers: int) -> dict:
+def cpu_model() -> str:
+    try:
+        for line in Path("/proc/cpuinfo").read_text().splitlines():
+            if line.startswith("model name"):
+                return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    import platform
+    return platform.processor() or "unknown"
+
+
+def cpu_baseline(sample_pairs: int, workers: int, one_core_pairs: int = 4) -> dict:
+    """The oracle chain on `workers` processes (all cores) and on one."""
     import multiprocessing as mp
     ctx = mp.get_context("spawn")
     with ctx.Pool(workers) as pool:
@@ -130,11 +142,20 @@ def cpu_baseline(sample_pairs: int, workers: int) -> dict:
         t = time.perf_counter()
         lat = pool.map(cpu_pair, [(i % N_PAIRS, 0) for i in range(sample_pairs)])
         wall = time.perf_counter() - t
-    lat = sorted(lat)
+    with ctx.Pool(1) as pool:
+        pool.map(cpu_pair, [(0, 0)])
+        t = time.perf_counter()
+        lat1 = pool.map(cpu_pair, [(i % N_PAIRS, 0) for i in range(one_core_pairs)])
+        wall1 = time.perf_counter() - t
+    lat, lat1 = sorted(lat), sorted(lat1)
     return {"value": sample_pairs / wall, "unit": "pairs/s", "cores": workers, "kind": "port",
+            "cpu_model": cpu_model(), "nproc": os.cpu_count(),
             "sample": f"{sample_pairs} pairs of the workload on {workers} processes "
                       f"(NumPy S2/S3 + C S4/S5 restatement of the reference)",
-            "p50_ms": 1e3 * lat[len(lat) // 2], "p99_ms": 1e3 * lat[int(0.99 * (len(lat) - 1))]}
+            "p50_ms": 1e3 * lat[len(lat) // 2], "p99_ms": 1e3 * lat[int(0.99 * (len(lat) - 1))],
+            "one_core": {"value": one_core_pairs / wall1, "unit": "pairs/s", "cores": 1,
+                         "sample": f"{one_core_pairs} pairs of the workload on one process",
+                         "p50_ms": 1e3 * lat1[len(lat1) // 2], "p99_ms": 1e3 * lat1[-1]}}
 
 
 def opencv_pair(i):
@@ -184,9 +205,63 @@ def opencv_baseline(n_pairs: int, workers: int) -> dict:
     return out
 
 
+REF_STAGES = ("s2_workspace_bytes", "s2_detect", "s3_workspace_bytes", "s3_describe", "s4_workspace_bytes",
+              "s4_match", "s5_workspace_bytes", "s5_estimate")
+
+
+def reference_gpu_per_pair(pairs: int = N_PAIRS, reps: int = 3) -> dict:
+    """The reference's own S2-S5 stage sources, built for sm_100a with the
+    reference's flags (oracle/_ref/libref_stages_stock.so), driven pair by
+    pair as its harness does (S2 A, S2 B, S3 A, S3 B, S4, S5 on one stream,
+    one synchronisation per pair; harness/pipeline_runner.cu:335-416) on the
+    workload's pairs and knobs, single level (the reference has no
+    pyramid). Wall time per pair, uploads excluded."""
+    import ctypes as C
+    import torch
+    from crossstage_stitch_b200 import _abi, stages, synth
+    path = ROOT / "oracle" / "_ref" / "libref_stages_stock.so"
+    if not path.exists():
+        return {"unavailable": "the reference's stage build (oracle/_ref/libref_stages_stock.so) is not present"}
+    if not torch.cuda.is_available():
+        return {"unavailable": "no CUDA device"}
+
+    class RefStages:
+        def __init__(self):
+            self.L = C.CDLL(str(path))
+            for name in REF_STAGES:
+                fn = getattr(self.L, "ref_" + name)
+                fn.restype = C.c_int
+                fn.argtypes = _abi.PROTOTYPES["stitch_" + name][1]
+                setattr(self, "stitch_" + name, fn)
+
+    torch.cuda.set_device(0)
+    knobs = [stages.Knobs(max_keypoints=K, hypotheses=R, seed=synth.BASE_SEED + i, threshold=3.0)
+             for i in range(pairs)]
+    ps = [synth.config0_pair(i) for i in range(pairs)]
+    runner = stages.PairRunner(SIZE, SIZE, K, max_r=R, stage_lib=RefStages())
+    stream = torch.cuda.current_stream()
+    lat = []
+    for rep in range(reps + 1):
+        for i, p in enumerate(ps):
+            runner.upload(p.gray_a, p.gray_b)
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            runner.enqueue(SIZE, SIZE, SIZE, SIZE, knobs[i])
+            stream.synchronize()
+            if rep:
+                lat.append(time.perf_counter() - t)
+    lat.sort()
+    return {"value": len(lat) / sum(lat), "unit": "pairs/s", "build": "reference sources, reference flags, sm_100a",
+            "workload": f"{pairs} pairs of the workload, single level, K={K}, FAST 20, R={R}, one "
+                        f"synchronisation per pair, {reps} passes",
+            "p50_ms": 1e3 * lat[len(lat) // 2], "p99_ms": 1e3 * lat[int(0.99 * (len(lat) - 1))]}
+
+
 def run_reference(args):
     """The reference arm: the oracle chain on every host core, one pool for
-    the whole run; a step is one pair per worker process."""
+    the whole run; a step registers the workload's 64 pairs, spread over the
+    worker processes. The line also carries the reference's own GPU kernels
+    per pair (reference_gpu_per_pair), measured after the timed CPU steps."""
     import multiprocessing as mp
     workers = min(os.cpu_count() or 1, 32)
     ctx = mp.get_context("spawn")
@@ -194,22 +269,28 @@ def run_reference(args):
     with ctx.Pool(workers) as pool:
         pool.map(cpu_pair, [(0, 0)] * workers)  # warm the workers (imports)
         for _ in range(args.warmup):
-            pool.map(cpu_pair, [(i % N_PAIRS, 0) for i in range(workers)])
-        for step in range(args.steps):
+            pool.map(cpu_pair, [(i, 0) for i in range(N_PAIRS)], chunksize=1)
+        for _ in range(args.steps):
             t = time.perf_counter()
-            lat += pool.map(cpu_pair, [((step * workers + i) % N_PAIRS, 0) for i in range(workers)])
+            lat += pool.map(cpu_pair, [(i, 0) for i in range(N_PAIRS)], chunksize=1)
             times.append(time.perf_counter() - t)
-    v = workers * args.steps / sum(times)
+    v = N_PAIRS * args.steps / sum(times)
     lat.sort()
-    sample = (f"{args.steps} steps of {workers} pairs of the workload, one per process on {workers} processes "
+    sample = (f"{args.steps} steps of the workload's {N_PAIRS} pairs on {workers} processes "
               f"(NumPy S2/S3 + C S4/S5 restatement of the reference)")
+    try:
+        gpu = reference_gpu_per_pair()
+    except Exception as e:  # the reference's GPU build is reported, never required
+        gpu = {"unavailable": f"{type(e).__name__}: {e}"}
     line = {"impl": "reference", "metric": "pairs/s", "value": v, "unit": "pairs/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/i32/f64",
-            "data": "synthetic", "config": {"workload": WORKLOAD, "pairs_per_step": workers},
+            "data": "synthetic", "config": {"workload": WORKLOAD, "pairs_per_step": N_PAIRS},
             "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": workers, "kind": "port", "sample": sample,
+                             "cpu_model": cpu_model(), "nproc": os.cpu_count(),
                              "p50_ms": 1e3 * lat[len(lat) // 2], "p99_ms": 1e3 * lat[int(0.99 * (len(lat) - 1))]},
-            "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+            "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+            "reference_gpu_per_pair": gpu}
     print(json.dumps(line), flush=True)
 
 
@@ -222,9 +303,10 @@ NCU_TRAFFIC = {
 }
 
 N_MIXED = 256
-SERVED_RATES = (500, 1000, 2000)
-SERVED_SECONDS = 3.0
-SERVED_POOL = 48
+SERVED_RATES = (200, 500, 1000, 2000)
+SERVED_SECONDS = 60.0       # per rate, served form
+PLAIN_SERVED_SECONDS = 10.0  # per rate, the plain per-pair comparison on the start of the same trace
+DEADLINE_MS = 25.0           # the latency target at 1000 pairs/s
 
 
 def mixed_pair_job(i):
@@ -273,7 +355,7 @@ def run_mixed(mixed, steps, warmup, dev, flush):
     H = max(max(a.shape[0], bb.shape[0]) for a, bb, _ in mixed)
     runner = stages.PairRunner(W, H, max(k.max_keypoints for k in knobs), max_r=max(k.hypotheses for k in knobs),
                                device=dev)
-    lat = []
+    lat, plain_results = [], []
 
     def plain(record):
         for (ia, ib), k in zip(imgs, knobs):
@@ -284,6 +366,7 @@ def run_mixed(mixed, steps, warmup, dev, flush):
             stream.synchronize()
             if record:
                 lat.append(f0.elapsed_time(f1))
+                plain_results.append(stages.result_dict(runner.result))
 
     plain(False)
     torch.cuda.synchronize()
@@ -295,6 +378,7 @@ def run_mixed(mixed, steps, warmup, dev, flush):
     lat.sort()
     n = len(mixed)
     mpx = sum(a.size + bb.size for a, bb, _ in mixed) / n / 1e6
+    parity = all(same_result(b.result(i), plain_results[i]) for i in range(n))
     del b
     return {"workload": f"{n} mixed pairs from {{640x480, 1280x720, 1920x1080, 3840x2160}}, K in {{500, 2000, 8000}}, "
                         f"FAST in {{10, 20, 40}}, R in {{500, 2000, 8000}}, 8 levels at 1.2, repeated-texture outliers",
@@ -302,7 +386,7 @@ def run_mixed(mixed, steps, warmup, dev, flush):
             "batched": {"value": n / (t_batch / 1e3), "unit": "pairs/s", "ms_per_step": t_batch},
             "plain_per_pair": {"value": n / (t_plain / 1e3), "unit": "pairs/s", "p50_ms": lat[len(lat) // 2],
                                "p99_ms": lat[int(0.99 * (len(lat) - 1))]},
-            "batched_over_plain": (n / (t_batch / 1e3)) / (n / (t_plain / 1e3))}
+            "batched_over_plain": (n / (t_batch / 1e3)) / (n / (t_plain / 1e3)), "parity": parity}
 
 
 def percentile(v, q):
@@ -310,16 +394,28 @@ def percentile(v, q):
     return v[min(len(v) - 1, int(q * (len(v) - 1) + 0.5))] if v else None
 
 
-def run_served(mixed, dev):
+def same_result(got: dict, want: dict) -> bool:
+    """A batched pair's result equals the plain per-pair result: status,
+    match and inlier counts, and every bit of H."""
+    import numpy as np
+    return (int(got["status"]) == int(want["status"]) and got["num_matches"] == want["num_matches"]
+            and got["num_inliers"] == want["num_inliers"]
+            and np.array_equal(np.asarray(got["H"]).view(np.uint64), np.asarray(want["H"]).view(np.uint64)))
+
+
+def run_served(mixed, dev, seconds: float, plain_seconds: float):
     """Open-loop Poisson arrivals of the mixed pairs (per-request seeds) at each
-    rate for SERVED_SECONDS: the served form (8 GB arena) against the plain
-    per-pair stages serving the same trace one request at a time. Latency runs
-    from submit (before the host-to-device copies) to the result on the host."""
+    rate for `seconds`: the served form (8 GB arena) against the plain
+    per-pair stages serving the same trace one request at a time for
+    `plain_seconds`. Latency runs from the arrival (submit, before the
+    host-to-device copies) to the result on the host. A request is dropped
+    when its result is not on the host within DEADLINE_MS of its arrival
+    (late, or refused at submit); drop_rate = dropped / arrivals."""
     import numpy as np
     import torch
     from crossstage_stitch_b200 import stages, synth
     from crossstage_stitch_b200.server import Server, pinned_image
-    pool = [(pinned_image(a), pinned_image(b), kn) for a, b, kn in mixed[:SERVED_POOL]]
+    pool = [(pinned_image(a), pinned_image(b), kn) for a, b, kn in mixed]
     W = max(max(a.shape[1], b.shape[1]) for a, b, _ in pool)
     H = max(max(a.shape[0], b.shape[0]) for a, b, _ in pool)
     runner = stages.PairRunner(W, H, 8000, max_r=8000, device=dev)
@@ -328,15 +424,15 @@ def run_served(mixed, dev):
     out = []
     for rate in SERVED_RATES:
         rng = np.random.default_rng(synth.BASE_SEED + rate)
-        arrivals = np.cumsum(rng.exponential(1.0 / rate, int(rate * SERVED_SECONDS * 1.2)))
-        arrivals = arrivals[arrivals < SERVED_SECONDS]
+        arrivals = np.cumsum(rng.exponential(1.0 / rate, int(rate * seconds * 1.2) + 16))
+        arrivals = arrivals[arrivals < seconds]
         picks = rng.integers(0, len(pool), len(arrivals))
         # served form
         srv = Server(arena_bytes=8 << 30, max_batch=64, streams=2, device=dev.index)
         for i in range(min(8, len(pool))):          # warm-up requests, not timed
             srv.submit(pool[i][0], pool[i][1], mixed_knobs(pool[i][2], 1), tag=1 << 40 | i)
         srv.drain()
-        res, t0 = [], time.perf_counter()
+        res, refused, t0 = [], 0, time.perf_counter()
         for n, (t, p) in enumerate(zip(arrivals, picks)):
             while True:
                 rem = t - (time.perf_counter() - t0)
@@ -346,18 +442,19 @@ def run_served(mixed, dev):
                 if rem > 5e-4:
                     time.sleep(2e-4)
             a, b, kn = pool[p]
-            assert srv.submit(a, b, mixed_knobs(kn, synth.BASE_SEED + 500000 + n), tag=n) == 0
-        res += srv.drain()
+            refused += srv.submit(a, b, mixed_knobs(kn, synth.BASE_SEED + 500000 + n), tag=n) != 0
+        res += srv.drain(timeout_s=max(120.0, seconds))
         span = max(r["done_ms"] for r in res) - min(r["submit_ms"] for r in res)
         srv.close()
         lat = [r["latency_ms"] for r in res]
-        # plain per-pair on the same trace, first come first served, within the same window + 2 s
+        late = sum(v > DEADLINE_MS for v in lat)
+        # plain per-pair on the same trace (its first plain_seconds), first come first served
+        plain_n = int(np.searchsorted(arrivals, plain_seconds))
         plat, t0 = [], time.perf_counter()
-        for n, (t, p) in enumerate(zip(arrivals, picks)):
+        for n in range(plain_n):
+            t, p = arrivals[n], picks[n]
             while time.perf_counter() - t0 < t:
                 pass
-            if time.perf_counter() - t0 > SERVED_SECONDS + 2.0:
-                break
             a, b, kn = pool[p]
             h, w = a.shape
             hb, wb = b.shape
@@ -366,14 +463,20 @@ def run_served(mixed, dev):
             runner.enqueue(w, h, wb, hb, mixed_knobs(kn, synth.BASE_SEED + 500000 + n), images=(dev_a, dev_b))
             torch.cuda.current_stream().synchronize()
             plat.append(1e3 * (time.perf_counter() - t0 - t))
-        out.append({"offered_pairs_s": rate, "requests": len(arrivals),
+        plain_span = time.perf_counter() - t0
+        out.append({"offered_pairs_s": rate, "seconds": seconds, "requests": len(arrivals),
+                    "completed": len(res), "refused": refused,
                     "throughput_pairs_s": len(res) / (span / 1e3), "p50_ms": percentile(lat, 0.5),
-                    "p99_ms": percentile(lat, 0.99), "drop_rate": 0.0,
-                    "mean_batch_pairs": sum(r["batch_pairs"] for r in res) / len(res),
-                    "plain_per_pair": {"p50_ms": percentile(plat, 0.5), "p99_ms": percentile(plat, 0.99),
-                                       "completed": len(plat),
-                                       "drop_rate": 1.0 - len(plat) / len(arrivals)}})
-    return {"arrivals": "open-loop Poisson", "seconds_per_rate": SERVED_SECONDS, "hbm_budget_bytes": 8 << 30,
+                    "p99_ms": percentile(lat, 0.99), "late": late,
+                    "drop_rate": (late + refused) / max(len(arrivals), 1),
+                    "mean_batch_pairs": sum(r["batch_pairs"] for r in res) / max(len(res), 1),
+                    "plain_per_pair": {"seconds": plain_seconds, "requests": plain_n,
+                                       "p50_ms": percentile(plat, 0.5), "p99_ms": percentile(plat, 0.99),
+                                       "throughput_pairs_s": plain_n / max(plain_span, 1e-9),
+                                       "drop_rate": sum(v > DEADLINE_MS for v in plat) / max(plain_n, 1)}})
+    return {"arrivals": "open-loop Poisson", "hbm_budget_bytes": 8 << 30, "deadline_ms": DEADLINE_MS,
+            "drop_rule": f"a request whose result is not on the host within {DEADLINE_MS} ms of its arrival "
+                         f"(late, or refused at submit) is dropped",
             "request_pool": f"{len(pool)} mixed-resolution pairs, per-request S5 seeds", "rates": out}
 
 
@@ -530,6 +633,8 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true", help="skip the mixed-resolution and served sections")
+    ap.add_argument("--served-seconds", type=float, default=SERVED_SECONDS,
+                    help="seconds of arrivals per rate in the served section")
     ap.add_argument("--only", choices=["matching", "render", "batched"], default=None,
                     help="run only the matching microbenchmark (popc vs tensor cores), the S6 feather "
                          "render microbenchmark, or the batched step with its kernel marks, and print its JSON")
@@ -655,23 +760,32 @@ def main():
         for i, p in enumerate(pairs):
             sb.fill(h, i, p.gray_a, p.gray_b)
 
-    def timed_e2e(steps):
+    step_latency_ms = []   # per step: submit of its image copy -> its results on the host
+
+    def timed_e2e(steps, record=False):
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(sb.copy_stream)
         prev = None
+        t_submit = {}
         for step in range(steps):
             with torch.cuda.stream(sb.streams[sb.next]):   # the stream of the slot this step takes
                 flush.zero_()
+            t0 = time.perf_counter()
             slot = sb.step(hosts[step % 2])
+            t_submit[slot] = t0
             if prev is not None:
                 sb.wait(prev)
                 _ = sb.result(prev, N_PAIRS - 1)["status"]   # the step's results on the host
+                if record:
+                    step_latency_ms.append(1e3 * (time.perf_counter() - t_submit[prev]))
             prev = slot
         sb.wait(prev)
         _ = sb.result(prev, N_PAIRS - 1)["status"]
+        if record:
+            step_latency_ms.append(1e3 * (time.perf_counter() - t_submit[prev]))
         for d in sb.done:
             sb.copy_stream.wait_event(d)
         e1.record(sb.copy_stream)
@@ -686,7 +800,7 @@ def main():
     l0 = L.stitch_launch_count()
     t_batch = timed_graph(args.steps)
     launches = L.stitch_launch_count() - l0
-    t_e2e = timed_e2e(args.steps)
+    t_e2e = timed_e2e(args.steps, record=True)
     clk = clocks.stop()
     per_kernel = kernel_split(args.steps)
     e2e_equal = all(bool((sb.result(sb.next ^ 1, i)["H"] == b.result(i)["H"]).all()) for i in range(N_PAIRS))
@@ -722,13 +836,15 @@ def main():
                 f.write(runs.row(runs.record_from_result(res, f"synthetic_{rank * N_PAIRS + i}", knobs[i], S=1.0,
                                                          run_id="bench", dataset="synthetic", t_e2e=ms)))
     lat.sort()
+    # the timed batched step against the plain per-pair stages, every pair
+    parity_config1 = all(same_result(b.result(i), plain_results[i]) for i in range(N_PAIRS))
 
     matching = run_matching(dev) if rank == 0 else None
     render_res = run_render(dev, flush) if rank == 0 else None
     mixed_res = served_res = None
     if mixed is not None:
         mixed_res = run_mixed(mixed, max(3, args.steps // 2), args.warmup, dev, flush)
-        served_res = run_served(mixed, dev)
+        served_res = run_served(mixed, dev, args.served_seconds, min(PLAIN_SERVED_SECONDS, args.served_seconds))
 
     counts = []
     for i in range(N_PAIRS):
@@ -769,7 +885,15 @@ def main():
                            "pairs_per_step": N_PAIRS, "pyramid_levels": LEVELS, "scale_factor": SCALE,
                            "l2": "512 MB flush between steps (inputs 33.5 MB < L2)",
                            "parallelism": f"replicas x{world}"},
-                "p50_pair_ms": t_batch / args.steps, "p99_pair_ms": t_batch / args.steps,
+                "latency": {"unit": "ms", "p50": percentile(step_latency_ms, 0.5),
+                            "p99": percentile(step_latency_ms, 0.99), "steps": len(step_latency_ms),
+                            "what": "per step of 64 pairs through the streaming API: host submit of the "
+                                    "step's image copy to its results on the host (every pair of a step "
+                                    "completes with it)"},
+                "parity": {"config1": parity_config1,
+                           "mixed": None if mixed_res is None else mixed_res.pop("parity"),
+                           "what": "batched results equal the plain per-pair stages for every pair of the "
+                                   "timed workloads (status, match and inlier counts, H bit for bit)"},
                 "e2e": {"value": pairs_total / (t_e2e / 1e3), "unit": "pairs/s",
                         "h2d_bytes_per_step": N_PAIRS * 2 * SIZE * SIZE,
                         "d2h_bytes_per_step": N_PAIRS * 184,

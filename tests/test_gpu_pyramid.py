@@ -170,3 +170,38 @@ def test_batch_mixed_levels_equals_per_pair(cuda):
             r = bt.result(i)
             assert r["status"] == res["status"] and r["num_inliers"] == res["num_inliers"]
             np.testing.assert_array_equal(r["H"], res["H"])
+
+
+@pytest.mark.parametrize("kind,k", [("c0a", 1000), ("c0b", 1000), ("c1", 2000)])
+def test_pyramid_layers_equal_reference_kernels(cuda, kind, k):
+    """Each pyramid layer runs the reference's single-level S2/S3 unchanged.
+    The reference's own S2/S3 kernels (src/s2_s3/s2.cu:333-385,
+    src/s2_s3/s3.cu:168-195, built for sm_100a into oracle/_ref as a
+    checker), run on each layer image of the pyramid oracle with that layer's
+    budget, give this library's pyramid output layer by layer: the same
+    counts, responses and descriptors bit for bit, and x and y equal to the
+    reference's layer coordinates times s_l in float32 (the one step the
+    pyramid adds)."""
+    from . import gpu_util as G
+    if not G.ref_available():
+        pytest.skip("reference stage build not present (oracle/_ref)")
+    gray = synth.config0_pair(2).gray_a if kind == "c1" else image(kind)
+    levels, factor, thr = 8, 1.2, 20
+    st, kp, desc = run_pyramid(gray, thr, k, levels, factor)
+    assert st == 0
+    budgets = pyramid.level_budgets(k, levels, factor)
+    scales = pyramid.layer_scales(levels, factor)
+    lib = G.Lib("ref")
+    off = 0
+    layers = pyramid.build_layers(gray, levels, factor)
+    assert len(layers) == levels
+    for l, layer in enumerate(layers):
+        rk, rd, _, (s2, s3, n) = G.detect_describe(lib, layer, thr, budgets[l])
+        assert (s2, s3) == (0, 0) and n == rk.shape[0] > 0, l
+        span = slice(off, off + n)
+        assert np.array_equal(kp[span, 0], rk[:, 0] * scales[l]), l
+        assert np.array_equal(kp[span, 1], rk[:, 1] * scales[l]), l
+        assert np.array_equal(kp[span, 2], rk[:, 2]), l
+        assert np.array_equal(desc[span], rd), l
+        off += n
+    assert off == kp.shape[0]
