@@ -135,11 +135,27 @@ Status Plan::build(int n_pairs, const stitch_pair_desc* p, int* bad_pair, bool a
             max_levels = std::max(max_levels, L);
         }
     }
-    // 3. layout
+    // 3. layout: blur-tile flags per image first (they sit in the zeroed head)
+    blur_total = 0;
+    for (int i = 0; i < n; ++i)
+        for (int s = 0; s < 2; ++s) {
+            auto& o = off[i];
+            const stitch_image_view& im = s ? pairs[i].image_b : pairs[i].image_a;
+            o.mark0[s] = blur_total;
+            if (o.pyramid[s]) {
+                blur_total += static_cast<std::size_t>(o.pyr[s].blur_first[o.pyr[s].plan.levels]);
+            } else {
+                blur_total += static_cast<std::size_t>(ceil_div(im.width, s2s3::kBlurTileW)) *
+                              static_cast<std::size_t>(ceil_div(im.height, s2s3::kBlurTileH));
+            }
+        }
     Layout lay;
     const std::size_t counts = lay.take(3 * static_cast<std::size_t>(n) + n_layers, sizeof(int));
-    hists = lay.take(static_cast<std::size_t>(std::max(n_det, 1)) * 256, sizeof(std::uint32_t));
+    hists = lay.take(static_cast<std::size_t>(std::max(n_det, 1)) * s2s3::kHistWords, sizeof(std::uint32_t));
+    queue = lay.take(2, sizeof(std::uint32_t));
+    blur_flags = lay.take(std::max<std::size_t>(blur_total, 1), sizeof(std::uint32_t));
     zeroed = lay.cursor;
+    blur_list = lay.take(std::max<std::size_t>(blur_total, 1), sizeof(uint2));
     results = lay.take(n, sizeof(HomographyResult));
     for (int i = 0; i < n; ++i) {
         auto& o = off[i];
@@ -351,10 +367,10 @@ void Plan::job_blocks(int i, int s, int l, int (&db)[s2s3::kDetectKinds], int (&
     const int k = q.s2.max_keypoints;
     const bool active = k > 0 && !small_image(im);
     db[s2s3::kFastKind] = active ? o.det[s].tiles : 0;
-    db[s2s3::kChunkKind] = active ? o.det[s].chunks : 0;
+    db[s2s3::kSelectKind] = active ? o.det[s].select_blocks : 0;
     db[s2s3::kHarrisKind] = active ? ceil_div(o.det[s].candidates, s2s3::kHarrisThreads) : 0;
     db[s2s3::kSortKind] = active ? 1 : 0;
-    sb[s2s3::kBlurKind] = 0;  // the FAST kernel writes the blur; no blur launch
+    sb[s2s3::kBlurKind] = 0;  // on demand: blur_tiles_kernel takes the flagged tiles from a list
     sb[s2s3::kDescKind] = k > 0 ? ceil_div(k, s2s3::kDescWarps) : 0;
 }
 
@@ -378,6 +394,9 @@ Status Plan::stage_tables(void* ws) {
     auto* zj = reinterpret_cast<ResizeJob*>(T + offsets[kRsJobs]);
     auto* zp = reinterpret_cast<int*>(T + offsets[kRsPrefix]);
     std::uint32_t* hist_base = at<std::uint32_t>(ws, hists);
+    std::uint32_t* mark_base = at<std::uint32_t>(ws, blur_flags);
+    uint2* list = at<uint2>(ws, blur_list);
+    std::uint32_t* list_count = at<std::uint32_t>(ws, queue) + 1;
     int* layer_counts = at<int>(ws, 0) + 3 * static_cast<std::size_t>(n);
     const int nd = n_det, nr = n_resize, rkinds = resize_kinds();
     int run_det[s2s3::kDetectKinds] = {}, run_des[s2s3::kDescribeKinds] = {};
@@ -427,9 +446,10 @@ Status Plan::stage_tables(void* ws) {
             if (o.pyramid[s]) {
                 const auto& pl = o.pyr[s];
                 s2s3::PyramidJobs pjobs;
-                s2s3::make_pyramid_jobs(view(im), c2, kps[s], desc[s], at<void>(ws, o.pyrws[s]), pl,
-                                        layer_counts + o.layer0[s], hist_base + static_cast<std::size_t>(idx) * 256,
-                                        &pjobs);
+                const s2s3::PyramidShared sh{layer_counts + o.layer0[s],
+                                             hist_base + static_cast<std::size_t>(idx) * s2s3::kHistWords,
+                                             mark_base + o.mark0[s], list, list_count, idx};
+                s2s3::make_pyramid_jobs(view(im), c2, kps[s], desc[s], at<void>(ws, o.pyrws[s]), pl, sh, &pjobs);
                 for (int l = 0; l < pl.plan.levels; ++l) {
                     int db[s2s3::kDetectKinds], sb[s2s3::kDescribeKinds];
                     job_blocks(i, s, l, db, sb);
@@ -446,13 +466,15 @@ Status Plan::stage_tables(void* ws) {
                 continue;
             }
             DetectJob d = s2s3::make_detect_job(view(im), c2, kps[s], at<void>(ws, o.s2ws[s]), o.det[s]);
-            d.hist = hist_base + static_cast<std::size_t>(idx) * 256;
+            d.hist = hist_base + static_cast<std::size_t>(idx) * s2s3::kHistWords;
+            d.blur_marks = mark_base + o.mark0[s];
+            d.blur_list = list;
+            d.blur_count = list_count;
+            d.job = idx;
             int db[s2s3::kDetectKinds], sb[s2s3::kDescribeKinds];
             job_blocks(i, s, 0, db, sb);
             const DescribeJob e =
                 s2s3::make_describe_job(view(im), kps[s], desc[s], at<void>(ws, o.s3ws[s]), o.des[s]);
-            d.blurred = e.blurred;
-            d.blur_pitch = e.blur_pitch;
             add_job(idx, d, e, db, sb);
         }
         // S4 (forward, then reverse when the mutual check is on)
@@ -598,11 +620,15 @@ Status Plan::enqueue(void* ws, std::size_t bytes, stitch_homography_result* host
     for (int kind = 0; kind + 1 < max_levels; ++kind)  // layer kind + 1 of every pyramid image
         if (go(rs_blocks[kind])) s2s3::resize_kernel<RsSrc, s2s3::kResizeTileH><<<rs_blocks[kind], 256, 0, s>>>(rs, kind);
     mark();
-    if (go(det_blocks[s2s3::kFastKind])) s2s3::fast_nms_kernel<DetSrc><<<det_blocks[s2s3::kFastKind], 256, 0, s>>>(det);
+    std::uint32_t* q = at<std::uint32_t>(ws, queue);  // FAST tile queue, then the blur-list count
+    const int tiles = det_blocks[s2s3::kFastKind];
+    if (go(tiles))
+        s2s3::fast_kernel<DetSrc><<<std::min(tiles, kSmCount * s2s3::kFastCtasPerSm), s2s3::kFastThreads, 0, s>>>(
+            det, q, tiles);
     mark();
-    if (go(det_blocks[s2s3::kChunkKind])) {
-        s2s3::select_count_kernel<DetSrc><<<det_blocks[s2s3::kChunkKind], 256, 0, s>>>(det);
-        s2s3::scatter_kernel<DetSrc><<<det_blocks[s2s3::kChunkKind], 256, 0, s>>>(det);
+    if (go(det_blocks[s2s3::kSelectKind])) {
+        s2s3::select_kernel<DetSrc><<<det_blocks[s2s3::kSelectKind], 256, 0, s>>>(det);
+        s2s3::ties_kernel<DetSrc><<<det_blocks[s2s3::kSortKind], s2s3::kTieThreads, 0, s>>>(det);
         ++launches;
     }
     mark();
@@ -614,7 +640,10 @@ Status Plan::enqueue(void* ws, std::size_t bytes, stitch_homography_result* host
     if (rank_fallback && go(det_blocks[s2s3::kHarrisKind]))
         s2s3::rank_topk_kernel<DetSrc><<<det_blocks[s2s3::kHarrisKind], s2s3::kHarrisThreads, 0, s>>>(det);
     mark();
-    if (go(des_blocks[s2s3::kBlurKind])) s2s3::blur_kernel<DesSrc><<<des_blocks[s2s3::kBlurKind], 256, 0, s>>>(des);
+    if (go(tiles > 0 && blur_total > 0 ? 1 : 0))
+        s2s3::blur_tiles_kernel<DesSrc>
+            <<<static_cast<int>(std::min<std::size_t>(blur_total, kSmCount * 8)), 256, 0, s>>>(des, at<uint2>(ws, blur_list),
+                                                                                                 q + 1);
     mark();
     if (go(des_blocks[s2s3::kDescKind]))
         s2s3::describe_kernel<DesSrc><<<des_blocks[s2s3::kDescKind], s2s3::kDescWarps * 32, 0, s>>>(des);

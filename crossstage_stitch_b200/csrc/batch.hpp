@@ -26,6 +26,7 @@ struct PairOffsets {
     s2s3::PyramidLayout pyr[2];
     std::size_t pyrws[2];
     int layer0[2], job0[2];
+    std::size_t mark0[2];  // first blur-tile flag of each image (all its layers)
 };
 
 class Plan {
@@ -42,7 +43,12 @@ public:
     int n_layers = 0;  // layer counts kept after the 3n image and match counts
     int n_resize = 0;  // resize jobs (layers 1.. of every pyramid image)
     int max_levels = 1;
-    std::size_t hists = 0, zeroed = 0;  // FAST histograms u32[n_det][256]; bytes zeroed per run
+    // zeroed head of the workspace: counts, then FAST histograms and counters
+    // u32[n_det][kHistWords], the FAST tile queue and blur-list count (2
+    // words), the blur-tile flags u32[blur_total]; `zeroed` bytes in all.
+    // The blur list uint2[blur_total] follows the head.
+    std::size_t hists = 0, queue = 0, blur_flags = 0, zeroed = 0, blur_list = 0;
+    std::size_t blur_total = 0;
     int det_blocks[s2s3::kDetectKinds] = {};
     int des_blocks[s2s3::kDescribeKinds] = {};
     int rs_blocks[s2s3::kMaxLevels] = {};  // resize launch of layer kind + 1

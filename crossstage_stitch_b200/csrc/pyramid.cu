@@ -9,6 +9,7 @@
 // here are OpenCV ORB's (modules/features2d/src/orb.cpp: getScale, layer
 // sizes, nfeaturesPerLevel, resize with INTER_LINEAR_EXACT, pt *= scale),
 // and each layer runs the reference's single-level S2/S3 unchanged.
+#include <algorithm>
 #include <cmath>
 #include <mutex>
 
@@ -66,10 +67,18 @@ bool pyramid_layout(int w, int h, int k, int levels, float sf, PyramidLayout* ou
     l.resize_tile_h = resize_tile_h;
     l.plan = level_plan(w, h, k, levels, sf);
     const int n = l.plan.levels;
+    // blur tiles of every layer (the describe layout's tile grid)
+    l.blur_first[0] = 0;
+    for (int i = 0; i < n; ++i)
+        l.blur_first[i + 1] = l.blur_first[i] + ceil_div(l.plan.width[i], kBlurTileW) * ceil_div(l.plan.height[i], kBlurTileH);
+    const std::size_t blur_total = static_cast<std::size_t>(std::max(l.blur_first[n], 1));
     Layout lay;
     l.counts = lay.take(static_cast<std::size_t>(n > 0 ? n : 1), sizeof(int));
-    l.hists = lay.take(static_cast<std::size_t>(n > 0 ? n : 1) * 256, sizeof(std::uint32_t));
+    l.hists = lay.take(static_cast<std::size_t>(n > 0 ? n : 1) * kHistWords, sizeof(std::uint32_t));
+    l.queue = lay.take(2, sizeof(std::uint32_t));  // FAST tile queue, blur-list count
+    l.marks = lay.take(blur_total, sizeof(std::uint32_t));
     l.zeroed_bytes = lay.cursor;
+    l.blur_list = lay.take(blur_total, sizeof(uint2));
     for (int i = 0; i < n; ++i) {
         const int lw = l.plan.width[i], lh = l.plan.height[i];
         const std::size_t kk = static_cast<std::size_t>(l.plan.budget[i] > 0 ? l.plan.budget[i] : 1);
@@ -90,7 +99,8 @@ bool pyramid_layout(int w, int h, int k, int levels, float sf, PyramidLayout* ou
 }
 
 void make_pyramid_jobs(const ImageView& im, const s2::Config& c, const Keypoints& out, const Descriptors& desc,
-                       void* ws, const PyramidLayout& l, int* counts, std::uint32_t* hists, PyramidJobs* jobs) {
+                       void* ws, const PyramidLayout& l, const PyramidShared& sh, PyramidJobs* jobs) {
+    int* counts = sh.counts;
     const LevelPlan& p = l.plan;
     for (int i = 0; i < p.levels; ++i) {
         ImageView layer = im;
@@ -117,7 +127,11 @@ void make_pyramid_jobs(const ImageView& im, const s2::Config& c, const Keypoints
         const Keypoints staged{at_offset<float>(ws, l.kx[i]), at_offset<float>(ws, l.ky[i]),
                                at_offset<float>(ws, l.kr[i]), p.budget[i], counts + i};
         DetectJob d = make_detect_job(layer, lc, staged, at_offset<void>(ws, l.detect[i]), l.det[i]);
-        d.hist = hists + static_cast<std::size_t>(i) * 256;
+        d.hist = sh.hists + static_cast<std::size_t>(i) * kHistWords;
+        d.blur_marks = sh.blur_marks + l.blur_first[i];
+        d.blur_list = sh.blur_list;
+        d.blur_count = sh.blur_count;
+        d.job = sh.job0 + i;
         jobs->detect[i] = d;
         DescribeJob s = make_describe_job(layer, staged, desc, at_offset<void>(ws, l.describe[i]), l.des[i]);
         s.response = staged.response;
@@ -129,8 +143,6 @@ void make_pyramid_jobs(const ImageView& im, const s2::Config& c, const Keypoints
         s.level = i;
         s.scale = p.scale[i];
         jobs->describe[i] = s;
-        jobs->detect[i].blurred = s.blurred;  // the FAST kernel writes the layer's blur
-        jobs->detect[i].blur_pitch = s.blur_pitch;
     }
 }
 
@@ -138,14 +150,14 @@ void pyramid_detect_blocks(const PyramidLayout& l, int i, int (&blocks)[kDetectK
     const bool active = i < l.plan.levels && l.plan.budget[i] > 0;
     const DetectLayout& d = l.det[i];
     blocks[kFastKind] = active ? d.tiles : 0;
-    blocks[kChunkKind] = active ? d.chunks : 0;
+    blocks[kSelectKind] = active ? d.select_blocks : 0;
     blocks[kHarrisKind] = active ? ceil_div(d.candidates, kHarrisThreads) : 0;
     blocks[kSortKind] = active ? 1 : 0;
 }
 
 void pyramid_describe_blocks(const PyramidLayout& l, int i, int (&blocks)[kDescribeKinds]) {
     const bool active = i < l.plan.levels && l.plan.budget[i] > 0;
-    blocks[kBlurKind] = 0;  // fused into the FAST kernel
+    blocks[kBlurKind] = 0;  // on demand: blur_tiles_kernel takes the flagged tiles from a list
     blocks[kDescKind] = active ? ceil_div(l.plan.budget[i], kDescWarps) : 0;
 }
 
@@ -200,8 +212,10 @@ Status pyramid_detect_describe(const ImageView& image, const s2::Config& c, int 
     if (n == 0 || c.max_keypoints == 0) return launch_status();
     if (!enable_pyramid_sort_smem()) return Status::CUDA_ERROR;
     PyramidJobs jobs;
-    make_pyramid_jobs(image, c, out, desc, ws, l, at_offset<int>(ws, l.counts),
-                      at_offset<std::uint32_t>(ws, l.hists), &jobs);
+    std::uint32_t* queue = at_offset<std::uint32_t>(ws, l.queue);
+    const PyramidShared sh{at_offset<int>(ws, l.counts), at_offset<std::uint32_t>(ws, l.hists),
+                           at_offset<std::uint32_t>(ws, l.marks), at_offset<uint2>(ws, l.blur_list), queue + 1, 0};
+    make_pyramid_jobs(image, c, out, desc, ws, l, sh, &jobs);
     int launches = 0;
     for (int i = 1; i < n; ++i) {
         resize_kernel<OneJob<ResizeJob>, kSingleResizeTileH>
@@ -224,9 +238,10 @@ Status pyramid_detect_describe(const ImageView& image, const s2::Config& c, int 
     }
     auto blocks = [&](int kind) { return det.first[kind][n]; };
     if (blocks(kFastKind)) {
-        fast_nms_kernel<DetSrc><<<blocks(kFastKind), 256, 0, stream>>>(det);
-        select_count_kernel<DetSrc><<<blocks(kChunkKind), 256, 0, stream>>>(det);
-        scatter_kernel<DetSrc><<<blocks(kChunkKind), 256, 0, stream>>>(det);
+        fast_kernel<DetSrc><<<std::min(blocks(kFastKind), kSmCount * kFastCtasPerSm), kFastThreads, 0, stream>>>(
+            det, queue, blocks(kFastKind));
+        select_kernel<DetSrc><<<blocks(kSelectKind), 256, 0, stream>>>(det);
+        ties_kernel<DetSrc><<<blocks(kSortKind), kTieThreads, 0, stream>>>(det);
         harris_kernel<DetSrc><<<blocks(kHarrisKind), kHarrisThreads, 0, stream>>>(det);
         sort_topk_kernel<DetSrc><<<blocks(kSortKind), kSortThreads, sort_smem_bytes(max_cand), stream>>>(det);
         launches += 5;
@@ -234,6 +249,9 @@ Status pyramid_detect_describe(const ImageView& image, const s2::Config& c, int 
             rank_topk_kernel<DetSrc><<<blocks(kHarrisKind), kHarrisThreads, 0, stream>>>(det);
             ++launches;
         }
+        blur_tiles_kernel<DesSrc><<<std::max(1, std::min(l.blur_first[n], kSmCount * 8)), 256, 0, stream>>>(
+            des, at_offset<uint2>(ws, l.blur_list), queue + 1);
+        ++launches;
     }
     if (des.first[kDescKind][n]) {
         describe_kernel<DesSrc><<<des.first[kDescKind][n], kDescWarps * 32, 0, stream>>>(des);

@@ -5,6 +5,7 @@
 // src/s2_s3/s3.cu:168-184; workspace queries follow
 // src/s2_s3/s2_s3_config.cpp:121-202 (sizes differ: this layout is the one
 // these kernels need).
+#include <algorithm>
 #include <cmath>
 #include <mutex>
 
@@ -29,16 +30,22 @@ bool detect_layout(int w, int h, int k, DetectLayout* out) {
     if (!out || !valid_image_shape(w, h) || k < 0 || k > INT_MAX / s2::kCandidateFactor) return false;
     DetectLayout l{};
     const std::size_t pixels = static_cast<std::size_t>(w) * static_cast<std::size_t>(h);
-    l.chunks = static_cast<int>((pixels + kChunkPx - 1) / kChunkPx);
+    // strict 3x3 maxima inside the edge margin: at most one per 2x2 cell
+    const std::size_t cells = (w > 2 * kEdge && h > 2 * kEdge)
+                                  ? static_cast<std::size_t>((w - 2 * kEdge + 1) / 2) *
+                                        static_cast<std::size_t>((h - 2 * kEdge + 1) / 2)
+                                  : 0;
+    if (cells > static_cast<std::size_t>(INT_MAX)) return false;
+    l.max_maxima = static_cast<int>(cells);
     l.candidates = s2::kCandidateFactor * k;
     l.tiles_x = ceil_div(w, kFastTileW);
     l.tiles = l.tiles_x * ceil_div(h, kFastTileH);
+    l.select_blocks = static_cast<int>(std::max<std::size_t>(1, (pixels + kSelectPx - 1) / kSelectPx));
     Layout lay;
-    l.maxima = lay.take(pixels, 1);
-    l.hist = lay.take(256, sizeof(std::uint32_t));
+    l.hist = lay.take(DetectLayout::hist_bytes, 1);
     l.params = lay.take(1, sizeof(SelectParams));
-    l.chunk_counts = lay.take(2 * static_cast<std::size_t>(l.chunks), sizeof(std::uint32_t));
     l.keys = lay.take(static_cast<std::size_t>(l.candidates), sizeof(std::uint64_t));
+    l.maxima = lay.take(std::max<std::size_t>(cells, 1), sizeof(std::uint64_t));
     if (!lay.ok) return false;
     l.total = lay.cursor;
     *out = l;
@@ -69,10 +76,10 @@ DetectJob make_detect_job(const ImageView& im, const s2::Config& c, const Keypoi
     j.threshold = c.fast_threshold;
     j.max_keypoints = c.max_keypoints;
     j.harris_k = c.harris_k;
-    j.maxima = at_offset<std::uint8_t>(ws, l.maxima);
+    j.maxima = at_offset<std::uint64_t>(ws, l.maxima);
+    j.max_maxima = l.max_maxima;
     j.hist = at_offset<std::uint32_t>(ws, l.hist);
     j.params = at_offset<SelectParams>(ws, l.params);
-    j.chunk_counts = at_offset<std::uint32_t>(ws, l.chunk_counts);
     j.keys = at_offset<std::uint64_t>(ws, l.keys);
     j.x = out.x;
     j.y = out.y;
@@ -80,7 +87,7 @@ DetectJob make_detect_job(const ImageView& im, const s2::Config& c, const Keypoi
     j.count = out.d_count;
     j.tiles_x = l.tiles_x;
     j.tiles = l.tiles;
-    j.chunks = l.chunks;
+    j.select_blocks = l.select_blocks;
     j.candidates = l.candidates;
     return j;
 }
@@ -132,12 +139,13 @@ Status detect(const ImageView& image, const s2::Config& config, const Keypoints&
     using Src = OneJob<DetectJob>;
     if (!enable_sort_smem<Src>()) return Status::CUDA_ERROR;
     const Src src{make_detect_job(image, config, output, ws, l)};
-    if (cudaMemsetAsync(src.job.hist, 0, 256 * sizeof(std::uint32_t), stream) != cudaSuccess)
+    if (cudaMemsetAsync(src.job.hist, 0, DetectLayout::hist_bytes, stream) != cudaSuccess)
         return Status::CUDA_ERROR;
-    fast_nms_kernel<Src><<<l.tiles, 256, 0, stream>>>(src);
+    const int fast_grid = std::min(l.tiles, kSmCount * kFastCtasPerSm);
+    fast_kernel<Src><<<fast_grid, kFastThreads, 0, stream>>>(src, src.job.counters() + kTileQueue, l.tiles);
     if (!record(e_fast, stream)) return Status::CUDA_ERROR;
-    select_count_kernel<Src><<<l.chunks, 256, 0, stream>>>(src);
-    scatter_kernel<Src><<<l.chunks, 256, 0, stream>>>(src);
+    select_kernel<Src><<<l.select_blocks, 256, 0, stream>>>(src);
+    ties_kernel<Src><<<1, kTieThreads, 0, stream>>>(src);
     if (!record(e_select, stream)) return Status::CUDA_ERROR;
     const int harris_blocks = ceil_div(l.candidates, kHarrisThreads);
     harris_kernel<Src><<<harris_blocks, kHarrisThreads, 0, stream>>>(src);
@@ -145,7 +153,7 @@ Status detect(const ImageView& image, const s2::Config& config, const Keypoints&
     sort_topk_kernel<Src><<<1, kSortThreads, sort_smem_bytes(l.candidates), stream>>>(src);
     if (l.candidates > kSortCap)
         rank_topk_kernel<Src><<<harris_blocks, kHarrisThreads, 0, stream>>>(src);
-    note_launches(l.candidates > kSortCap ? 6 : 5);
+    note_launches(l.candidates > kSortCap ? 7 : 6);
     return launch_status();
 }
 

@@ -6,9 +6,13 @@
 
 namespace stitch::b200::s2s3 {
 
+// S2 workspace of one image (or pyramid layer). `hist` holds the 256
+// histogram bins and then the kDetectCounters counters, zeroed together
+// (hist_bytes) before each run.
 struct DetectLayout {
-    std::size_t maxima, hist, params, chunk_counts, keys, total;
-    int chunks, candidates, tiles_x, tiles;
+    std::size_t maxima, hist, params, keys, total;
+    int max_maxima, candidates, tiles_x, tiles, select_blocks;
+    static constexpr std::size_t hist_bytes = kHistWords * sizeof(std::uint32_t);
 };
 
 struct DescribeLayout {
@@ -48,11 +52,14 @@ struct LevelPlan {
 bool valid_pyramid(int levels, float scale_factor);
 LevelPlan level_plan(int w, int h, int k, int levels, float scale_factor);
 
-// Workspace of one image's pyramid. `zeroed` (layer counts int[levels],
-// then FAST histograms u32[levels][256]) must be zero before each run.
+// Workspace of one image's pyramid. The head (layer counts int[levels],
+// FAST histograms and counters u32[levels][kHistWords], the FAST tile queue
+// and the blur-list count, the blur-tile flags u32[blur_total]) must be zero
+// before each run (zeroed_bytes); the blur list uint2[blur_total] follows.
 struct PyramidLayout {
     LevelPlan plan;
-    std::size_t counts, hists, zeroed_bytes;
+    std::size_t counts, hists, queue, marks, zeroed_bytes, blur_list;
+    int blur_first[kMaxLevels + 1];  // first flag of each layer's blur tiles; blur_first[levels] = blur_total
     std::size_t image[kMaxLevels];  // dense layer images, l >= 1
     std::size_t kx[kMaxLevels], ky[kMaxLevels], kr[kMaxLevels];  // layer keypoints
     std::size_t detect[kMaxLevels], describe[kMaxLevels];
@@ -75,11 +82,21 @@ struct PyramidJobs {
     DescribeJob describe[kMaxLevels];
 };
 
-// Jobs of every layer over the workspace `ws` laid out by `l`; the layer
-// counts and histograms are `counts` and `hists` (the layout's own unless
-// the caller keeps them elsewhere).
+// Buffers an image's layer jobs point into that are zeroed per run or shared
+// by a whole launch: the layout's own head for the per-image call, the
+// batch workspace's head in the batched chain.
+struct PyramidShared {
+    int* counts;               // [levels] layer keypoint counts
+    std::uint32_t* hists;      // [levels][kHistWords]
+    std::uint32_t* blur_marks; // [blur_first[levels]] this image's blur-tile flags
+    uint2* blur_list;          // the launch's blur list
+    std::uint32_t* blur_count; // and its length
+    int job0;                  // describe-table index of layer 0
+};
+
+// Jobs of every layer over the workspace `ws` laid out by `l`.
 void make_pyramid_jobs(const ImageView& im, const s2::Config& c, const Keypoints& out, const Descriptors& desc,
-                       void* ws, const PyramidLayout& l, int* counts, std::uint32_t* hists, PyramidJobs* jobs);
+                       void* ws, const PyramidLayout& l, const PyramidShared& sh, PyramidJobs* jobs);
 
 // Block count of each detect/describe kind for layer i (0 when inactive).
 void pyramid_detect_blocks(const PyramidLayout& l, int layer, int (&blocks)[kDetectKinds]);

@@ -30,28 +30,38 @@ struct SelectParams {
     std::uint32_t selected;   // above + ties
 };
 
+// Per-job counters of the detect kernels, after the 256 histogram bins.
+enum DetectCounter { kListed = 0, kAboveWritten = 1, kTiesWritten = 2, kTileQueue = 3, kDetectCounters = 4 };
+constexpr int kHistWords = 256 + kDetectCounters;  // one job's histogram and counters
+
 struct DetectJob {
     const std::uint8_t* image;
     int width, height, pitch;
     int threshold, max_keypoints;
     float harris_k;
     // workspace
-    std::uint8_t* maxima;          // width*height NMS-surviving scores
-    std::uint32_t* hist;           // [256], zeroed before the FAST launch
+    std::uint64_t* maxima;         // NMS maxima listed by the FAST kernel: (score << 32) | raster index
+    int max_maxima;                // capacity of `maxima`
+    std::uint32_t* hist;           // [256] scores of the listed maxima, then DetectCounter words;
+                                   // all zeroed before the FAST launch
     SelectParams* params;
-    std::uint32_t* chunk_counts;   // [2 * chunks] (above, tie) per chunk
     std::uint64_t* keys;           // [candidates]
     // output
     float* x;
     float* y;
     float* response;  // may be null
     int* count;
-    // optional: the S3 blur of the image (rows of blur_pitch bytes), written
-    // by the FAST kernel when set
-    std::uint8_t* blurred;
-    int blur_pitch;
+    // On-demand S3 blur (pyramid and batched paths; null elsewhere): the
+    // blur tiles that final keypoints sample are flagged in blur_marks
+    // (one word per tile, zeroed every run) and listed once each in
+    // blur_list as (describe job, tile) behind the launch-wide *blur_count.
+    std::uint32_t* blur_marks;
+    uint2* blur_list;
+    std::uint32_t* blur_count;
+    int job;  // this job's index in the describe table of the launch
     // launch bookkeeping
-    int tiles_x, tiles, chunks, candidates;
+    int tiles_x, tiles, select_blocks, candidates;
+    __host__ __device__ std::uint32_t* counters() const { return hist + 256; }
 };
 
 struct DescribeJob {
@@ -99,6 +109,7 @@ template <class Job> struct OneJob {
         *local = block;
         return true;
     }
+    __device__ Job at(int /*index*/) const { return job; }
 };
 
 // Device table: prefix[kind * (n + 1) + i] is the first block of job i for
@@ -132,6 +143,7 @@ template <class Job> struct JobTable {
         *local = block - p[lo];
         return true;
     }
+    __device__ Job at(int index) const { return jobs[index]; }
 };
 
 // A few jobs passed by value (the layers of one image's pyramid):
@@ -148,15 +160,29 @@ template <class Job, int kJobs, int kKinds> struct InlineTable {
         *local = block - first[kind][i];
         return true;
     }
+    __device__ Job at(int index) const { return jobs[index]; }
 };
 
-enum DetectKind { kFastKind = 0, kChunkKind = 1, kHarrisKind = 2, kSortKind = 3, kDetectKinds = 4 };
+// Launch kinds of the detect table: kFastKind entries are the FAST tiles of
+// each job (looked up by tile index from the persistent FAST kernel's
+// queue), kSelectKind blocks walk a job's maxima list, kSortKind is one
+// block per job (tie selection, then the top-K sort).
+enum DetectKind { kFastKind = 0, kSelectKind = 1, kHarrisKind = 2, kSortKind = 3, kDetectKinds = 4 };
 enum DescribeKind { kBlurKind = 0, kDescKind = 1, kDescribeKinds = 2 };
 
 constexpr int kFastTileW = 64, kFastTileH = 32;
 constexpr int kFastInW = kFastTileW + 8, kFastInH = kFastTileH + 8;  // halo 4 = FAST 3 + NMS 1
 constexpr int kFastScW = kFastTileW + 2, kFastScH = kFastTileH + 2;
-constexpr int kChunkPx = 8192;     // pixels per compaction block (256 threads x 32)
+constexpr int kSelectPx = 65536;   // image pixels per select block (a job's maxima list is walked
+                                   // by ceil(W * H / kSelectPx) blocks)
+constexpr int kFastThreads = 256;
+constexpr int kFastCtasPerSm = 8;  // resident FAST blocks per SM; the persistent grid is 148 x this
+constexpr int kTileMaxima = kFastTileW * kFastTileH / 4;  // strict 3x3 maxima: at most one per 2x2 cell
+constexpr int kTieThreads = 1024;
+// Largest offset of a rotated rBRIEF sample from its keypoint: the pattern's
+// coordinates lie within a radius of 18.39 px (|x|, |y| <= 13), so a rotated
+// coordinate rounds to at most 18.
+constexpr int kSampleRadius = 18;
 constexpr int kHarrisThreads = 256;
 constexpr int kSortCap = 16384;    // candidates sorted in shared memory by one block
 constexpr int kSortThreads = 1024;
@@ -225,23 +251,20 @@ __device__ __forceinline__ int fast_score(const std::uint8_t* p, int stride, int
 }
 
 // Compass test of two pixels in 16-bit lanes (values 0..255), a necessary
-// condition for a FAST-9 corner: a 9-pixel arc always holds two of the four
-// compass pixels, so two of them must be beyond the threshold on the same
-// side, i.e. the second largest is brighter than v + t or the second
-// smallest darker than v - t. A
-// min/max network gives both (a = max(s0, s4), b = min(s0, s4), likewise
-// c, d for s8, s12; p = min(a, c), q = max(b, d); second largest max(p, q),
-// second smallest min(p, q)); x >= y per lane is the top bit of
-// (x | 0x8000) - y, with no borrow between lanes for x, y < 0x8000.
+// condition for a FAST-9 corner: every 9-pixel arc of the circle holds one of
+// the compass pixels s0, s8 (3 below, 3 above) and one of s4, s12 (3 right,
+// 3 left), so an arc brighter than v + t needs
+// min(max(s0, s8), max(s4, s12)) >= v + t + 1 and one darker than v - t needs
+// max(min(s0, s8), min(s4, s12)) <= v - t - 1. x >= y per lane is the top bit
+// of (x | 0x8000) - y, with no borrow between lanes for x, y < 0x8000.
 // thr1 = (t + 1) in both lanes. Returns 0x8000 per passing lane.
 __device__ __forceinline__ std::uint32_t compass_pass2(std::uint32_t v, std::uint32_t s0, std::uint32_t s4,
                                                        std::uint32_t s8, std::uint32_t s12, std::uint32_t thr1) {
-    const std::uint32_t a = __vmaxu2(s0, s4), b = __vminu2(s0, s4);
-    const std::uint32_t c = __vmaxu2(s8, s12), d = __vminu2(s8, s12);
-    const std::uint32_t p = __vminu2(a, c), q = __vmaxu2(b, d);
+    const std::uint32_t hi = __vminu2(__vmaxu2(s0, s8), __vmaxu2(s4, s12));
+    const std::uint32_t lo = __vmaxu2(__vminu2(s0, s8), __vminu2(s4, s12));
     constexpr std::uint32_t kTop = 0x80008000u;
-    const std::uint32_t bright = ((__vmaxu2(p, q) | kTop) - (v + thr1)) & kTop;  // 2nd largest >= v + t + 1
-    const std::uint32_t dark = ((v | kTop) - (__vminu2(p, q) + thr1)) & kTop;    // v >= 2nd smallest + t + 1
+    const std::uint32_t bright = ((hi | kTop) - (v + thr1)) & kTop;  // min(...) >= v + t + 1
+    const std::uint32_t dark = ((v | kTop) - (lo + thr1)) & kTop;    // v >= max(...) + t + 1
     return bright | dark;
 }
 
@@ -272,152 +295,159 @@ __device__ __forceinline__ std::uint32_t blur_byte(float acc) {
     return static_cast<std::uint32_t>(__float2int_rn(fminf(fmaxf(acc, 0.0f), 255.0f)));
 }
 
-// One block = one 64x32 output tile:
-//   1. stage the tile with a 4-pixel halo in shared memory: one 16-byte load
-//      per thread for interior tiles of 16-byte aligned images, byte loads
-//      reflected at the border otherwise (FAST never reads outside the
-//      image, the blur does);
-//   2. run the compass test on the tile plus a 1-pixel ring, 4 positions per
-//      thread in 16-bit lanes, and list the survivors so that full scores are
-//      computed on full warps;
-//   3. score the survivors; keep strict 3x3 maxima inside the 31-pixel edge
-//      margin (only survivors can score, so only they are tested), write the
-//      maxima map from a shared-memory tile in 32-bit stores and add their
-//      scores to the histogram.
-// With j.blurred set the block also writes the tile of the S3 7x7 blur
-// (rows pass, then columns pass; per output the taps summed first to last
-// with each product and sum rounded on its own, then rounded half-to-even
-// and clamped), bit for bit the blur_kernel result.
-template <class Src>
-__global__ __launch_bounds__(256, 8) void fast_nms_kernel(const __grid_constant__ Src src) {
-    __shared__ __align__(16) std::uint8_t in[kFastInH][kInStride];
-    __shared__ __align__(16) std::uint8_t sc[kFastScH][kScStride];
-    __shared__ std::uint16_t cand[kFastScH * kScGroups];
-    __shared__ std::uint32_t hist[256];
-    __shared__ __align__(16) std::uint8_t mx[kFastTileH][kFastTileW];  // the tile's maxima map
-    __shared__ __align__(16) float rows[kFastTileH + 6][kFastTileW];
-    __shared__ int n_cand;
-    __shared__ std::size_t row_at[kFastInH];  // reflected row offsets (border tiles)
-    __shared__ int col_at[kInStride];          // reflected image columns (border tiles)
-    DetectJob j;
-    int local;
-    if (!src.find(blockIdx.x, kFastKind, &j, &local)) return;
-    const int tid = threadIdx.x, lane = tid & 31;
+// Asynchronous 16-byte copy, global to shared memory (both 16-byte aligned).
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Stages rows y0-4 .. y0+35 and columns x0-16 .. x0+79 of the job's image in
+// `in` (byte c of row r = image (y0-4+r, x0-16+c)). The FAST test never reads
+// a position outside the image, so rows are clamped into it and the bytes of
+// columns outside it are left as they are. With a 16-byte aligned image (base
+// and pitch) every 16-byte chunk within a row's pitch (within the width on
+// the last row) is one asynchronous copy, and a chunk that straddles the end
+// of the last row is copied byte by byte; other images are loaded byte by
+// byte with clamped columns. Asynchronous copies complete at the caller's
+// cp_async_wait_all.
+__device__ __forceinline__ void stage_fast_tile(const DetectJob& j, int local, std::uint8_t (*in)[kInStride]) {
+    const int tid = threadIdx.x;
     const int W = j.width, H = j.height;
-    const int y0 = (local / j.tiles_x) * kFastTileH;
-    const int x0 = (local % j.tiles_x) * kFastTileW;
-    hist[tid] = 0;
-    static_assert(kFastTileH * kFastTileW == 8 * 256, "two maxima words per thread");
-    reinterpret_cast<std::uint32_t*>(&mx[0][0])[tid] = 0u;
-    reinterpret_cast<std::uint32_t*>(&mx[0][0])[tid + 256] = 0u;
-    if (tid == 0) n_cand = 0;
-    // 1. stage
-    const bool vec = ((reinterpret_cast<std::uintptr_t>(j.image) | static_cast<std::uintptr_t>(j.pitch)) & 15) == 0 &&
-                     x0 >= 16 && x0 + 80 <= W && y0 >= 4 && y0 + kFastTileH + 4 <= H;
+    const int y0 = (local / j.tiles_x) * kFastTileH, x0 = (local % j.tiles_x) * kFastTileW;
+    const bool vec = ((reinterpret_cast<std::uintptr_t>(j.image) | static_cast<std::uintptr_t>(j.pitch)) & 15) == 0;
     if (vec) {
-        if (tid < kFastInH * (kInStride / 16)) {
-            const int r = tid / (kInStride / 16), q = tid - r * (kInStride / 16);
-            *reinterpret_cast<uint4*>(&in[r][16 * q]) = *reinterpret_cast<const uint4*>(
-                j.image + static_cast<std::size_t>(y0 - 4 + r) * j.pitch + (x0 - 16 + 16 * q));
+        constexpr int kChunks = kInStride / 16;  // 6 per row
+        if (tid < kFastInH * kChunks) {
+            const int r = tid / kChunks, q = tid - r * kChunks;
+            const int gy = min(max(y0 - 4 + r, 0), H - 1);
+            const int cx = x0 - 16 + 16 * q;
+            const int limit = gy == H - 1 ? W : j.pitch;  // bytes of the row that may be read
+            const std::uint8_t* row = j.image + static_cast<std::size_t>(gy) * j.pitch;
+            if (cx >= 0 && cx + 16 <= limit) {
+                cp_async16(&in[r][16 * q], row + cx);
+            } else if (cx >= 0 && cx < W) {
+                for (int b = 0; b < 16 && cx + b < W; ++b) in[r][16 * q + b] = row[cx + b];
+            }
         }
     } else {
-        if (tid < kFastInH) row_at[tid] = static_cast<std::size_t>(reflect101(y0 - 4 + tid, H)) * j.pitch;
-        else if (tid < kFastInH + kInStride) col_at[tid - kFastInH] = reflect101(x0 - 16 + (tid - kFastInH), W);
+        for (int i = tid; i < kFastInH * kInStride; i += kFastThreads) {
+            const int r = i / kInStride, c = i - r * kInStride;
+            const int gy = min(max(y0 - 4 + r, 0), H - 1), gx = min(max(x0 - 16 + c, 0), W - 1);
+            in[r][c] = j.image[static_cast<std::size_t>(gy) * j.pitch + gx];
+        }
+    }
+}
+
+// FAST-9 + strict 3x3 NMS, persistent: each block takes 64x32 tiles of
+// every job of the launch from a device queue (`*queue`, zero at launch; tile
+// t of `total` is looked up through the source's kFastKind entries), while
+// the next tile's bytes are copied into the other half of a double buffer.
+// The jobs of the current and the next tile sit in shared memory. Per tile:
+//   1. the compass test on the tile plus a 1-pixel ring, 4 positions per
+//      thread in 16-bit lanes; groups with a survivor are listed so that full
+//      scores are computed on full warps;
+//   2. the survivors are scored (every other position scores 0);
+//   3. each survivor of the tile inside the 31-pixel edge margin that is a
+//      strict 3x3 maximum goes into the job's maxima list as
+//      (score << 32) | raster index, its score into the job's histogram.
+// No maxima map and no blur are written.
+template <class Src>
+__global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(const __grid_constant__ Src src,
+                                                                          std::uint32_t* queue, int total) {
+    __shared__ __align__(16) std::uint8_t in[2][kFastInH][kInStride];
+    __shared__ __align__(16) std::uint8_t sc[kFastScH][kScStride];
+    __shared__ std::uint16_t cand[kFastScH * kScGroups];
+    __shared__ std::uint16_t wpos[8][128];
+    __shared__ std::uint32_t hist[256];
+    __shared__ std::uint64_t found[kTileMaxima];
+    __shared__ DetectJob jobs[2];  // jobs of the tiles in in[0] and in[1] (kept here, not in registers)
+    __shared__ int locals[2];
+    __shared__ int n_cand, n_found, next;
+    __shared__ std::uint32_t list_base;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    hist[tid] = 0;
+    if (tid == 0) {
+        n_cand = 0;
+        n_found = 0;
+        next = static_cast<int>(atomicAdd(queue, 1u));
+        if (next < total && !src.find(next, kFastKind, &jobs[0], &locals[0])) next = total;
+    }
+    __syncthreads();
+    int tile = next, buf = 0;
+    if (tile < total) stage_fast_tile(jobs[0], locals[0], in[0]);
+    cp_async_wait_all();
+    __syncthreads();
+    while (tile < total) {
+        const DetectJob& j = jobs[buf];
+        const int local = locals[buf];
+        const int W = j.width, H = j.height;
+        const int y0 = (local / j.tiles_x) * kFastTileH, x0 = (local % j.tiles_x) * kFastTileW;
+        std::uint8_t (*cur)[kInStride] = in[buf];
+        if (tid == 0) {
+            int t = static_cast<int>(atomicAdd(queue, 1u));
+            if (t < total && !src.find(t, kFastKind, &jobs[buf ^ 1], &locals[buf ^ 1])) t = total;
+            next = t;
+        }
+        // 1. compass test: thread (q, rb) takes positions 4q .. 4q+3 of rows rb,
+        // rb + 15, rb + 30; groups with a survivor are listed as
+        // (group << 4 | survivor bits)
+        const std::uint32_t thr1 = static_cast<std::uint32_t>(j.threshold + 1) * 0x00010001u;
+        {
+            constexpr int kRowSets = 256 / kScGroups;  // 15
+            const int q = tid % kScGroups, rb = tid / kScGroups, c = 4 * q;
+            unsigned colmask = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int gx = x0 - 1 + c + k;
+                if (c + k < kFastScW && gx >= 3 && gx < W - 3) colmask |= 1u << k;
+            }
+            for (int it = 0; it < (kFastScH + kRowSets - 1) / kRowSets; ++it) {  // same trip count everywhere
+                const int r = rb + it * kRowSets;
+                unsigned bits = 0;
+                if (rb < kRowSets && r < kFastScH) {
+                    *reinterpret_cast<std::uint32_t*>(&sc[r][c]) = 0u;
+                    const int gy = y0 - 1 + r;
+                    if (colmask && gy >= 3 && gy < H - 3) {
+                        const int w = q + 3;  // word holding halo columns c .. c+3 (bytes c+12 .. c+15)
+                        const auto* mid = reinterpret_cast<const std::uint32_t*>(&cur[r + 3][0]);
+                        const auto* bot = reinterpret_cast<const std::uint32_t*>(&cur[r + 6][0]);
+                        const auto* top = reinterpret_cast<const std::uint32_t*>(&cur[r][0]);
+                        const std::uint32_t a0 = mid[w], a1 = mid[w + 1], a2 = mid[w + 2];
+                        const std::uint32_t v = __funnelshift_r(a0, a1, 24);   // centres, halo columns c+3 .. c+6
+                        const std::uint32_t s12 = a0;                          // 3 left
+                        const std::uint32_t s4 = __funnelshift_r(a1, a2, 16);  // 3 right
+                        const std::uint32_t s0 = __funnelshift_r(bot[w], bot[w + 1], 24);  // 3 down
+                        const std::uint32_t s8 = __funnelshift_r(top[w], top[w + 1], 24);  // 3 up
+                        const std::uint32_t plo =
+                            compass_pass2(__byte_perm(v, 0, 0x4140), __byte_perm(s0, 0, 0x4140),
+                                          __byte_perm(s4, 0, 0x4140), __byte_perm(s8, 0, 0x4140),
+                                          __byte_perm(s12, 0, 0x4140), thr1);
+                        const std::uint32_t phi =
+                            compass_pass2(__byte_perm(v, 0, 0x4342), __byte_perm(s0, 0, 0x4342),
+                                          __byte_perm(s4, 0, 0x4342), __byte_perm(s8, 0, 0x4342),
+                                          __byte_perm(s12, 0, 0x4342), thr1);
+                        bits = (((plo >> 15) & 1u) | ((plo >> 30) & 2u) | ((phi >> 13) & 4u) | ((phi >> 28) & 8u)) &
+                               colmask;
+                    }
+                }
+                const unsigned m = __ballot_sync(0xffffffffu, bits != 0);
+                int base = 0;
+                if (lane == 0 && m) base = atomicAdd(&n_cand, __popc(m));
+                base = __shfl_sync(0xffffffffu, base, 0);
+                if (bits)
+                    cand[base + __popc(m & ((1u << lane) - 1u))] =
+                        static_cast<std::uint16_t>(((r * kScGroups + q) << 4) | bits);
+            }
+        }
         __syncthreads();
-        for (int i = tid; i < kFastInH * (kInStride / 4); i += 256) {
-            const int r = i / (kInStride / 4), b = 4 * (i - r * (kInStride / 4));
-            const std::uint8_t* row = j.image + row_at[r];
-            *reinterpret_cast<std::uint32_t*>(&in[r][b]) =
-                static_cast<std::uint32_t>(row[col_at[b]]) | (static_cast<std::uint32_t>(row[col_at[b + 1]]) << 8) |
-                (static_cast<std::uint32_t>(row[col_at[b + 2]]) << 16) |
-                (static_cast<std::uint32_t>(row[col_at[b + 3]]) << 24);
-        }
-    }
-    __syncthreads();
-    // 2. compass test: thread (q, rb) takes positions 4q .. 4q+3 of rows rb,
-    // rb + 15, rb + 30; groups with a survivor are listed as
-    // (group << 4 | survivor bits)
-    const std::uint32_t thr1 = static_cast<std::uint32_t>(j.threshold + 1) * 0x00010001u;
-    {
-        constexpr int kRowSets = 256 / kScGroups;  // 15
-        const int q = tid % kScGroups, rb = tid / kScGroups, c = 4 * q;
-        unsigned colmask = 0;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const int gx = x0 - 1 + c + k;
-            if (c + k < kFastScW && gx >= 3 && gx < W - 3) colmask |= 1u << k;
-        }
-        for (int it = 0; it < (kFastScH + kRowSets - 1) / kRowSets; ++it) {  // same trip count everywhere
-            const int r = rb + it * kRowSets;
-            unsigned bits = 0;
-            if (rb < kRowSets && r < kFastScH) {
-                *reinterpret_cast<std::uint32_t*>(&sc[r][c]) = 0u;
-                const int gy = y0 - 1 + r;
-                if (colmask && gy >= 3 && gy < H - 3) {
-                    const int w = q + 3;  // word holding halo columns c .. c+3 (bytes c+12 .. c+15)
-                    const auto* mid = reinterpret_cast<const std::uint32_t*>(&in[r + 3][0]);
-                    const auto* bot = reinterpret_cast<const std::uint32_t*>(&in[r + 6][0]);
-                    const auto* top = reinterpret_cast<const std::uint32_t*>(&in[r][0]);
-                    const std::uint32_t a0 = mid[w], a1 = mid[w + 1], a2 = mid[w + 2];
-                    const std::uint32_t v = __funnelshift_r(a0, a1, 24);   // centres, halo columns c+3 .. c+6
-                    const std::uint32_t s12 = a0;                          // 3 left
-                    const std::uint32_t s4 = __funnelshift_r(a1, a2, 16);  // 3 right
-                    const std::uint32_t s0 = __funnelshift_r(bot[w], bot[w + 1], 24);  // 3 down
-                    const std::uint32_t s8 = __funnelshift_r(top[w], top[w + 1], 24);  // 3 up
-                    const std::uint32_t plo = compass_pass2(__byte_perm(v, 0, 0x4140), __byte_perm(s0, 0, 0x4140),
-                                                            __byte_perm(s4, 0, 0x4140), __byte_perm(s8, 0, 0x4140),
-                                                            __byte_perm(s12, 0, 0x4140), thr1);
-                    const std::uint32_t phi = compass_pass2(__byte_perm(v, 0, 0x4342), __byte_perm(s0, 0, 0x4342),
-                                                            __byte_perm(s4, 0, 0x4342), __byte_perm(s8, 0, 0x4342),
-                                                            __byte_perm(s12, 0, 0x4342), thr1);
-                    bits = (((plo >> 15) & 1u) | ((plo >> 30) & 2u) | ((phi >> 13) & 4u) | ((phi >> 28) & 8u)) &
-                           colmask;
-                }
-            }
-            const unsigned m = __ballot_sync(0xffffffffu, bits != 0);
-            int base = 0;
-            if (lane == 0 && m) base = atomicAdd(&n_cand, __popc(m));
-            base = __shfl_sync(0xffffffffu, base, 0);
-            if (bits)
-                cand[base + __popc(m & ((1u << lane) - 1u))] =
-                    static_cast<std::uint16_t>(((r * kScGroups + q) << 4) | bits);
-        }
-    }
-    if (j.blurred) {  // blur rows pass: image rows y0-3 .. y0+34, two rows x 4 outputs per item
-        static_assert((kFastTileH + 6) % 2 == 0, "rows pass takes row pairs");
-        for (int g = tid; g < (kFastTileH + 6) / 2 * (kFastTileW / 4); g += 256) {
-            const int rp = g / (kFastTileW / 4), q = g - rp * (kFastTileW / 4), rr = 2 * rp;
-            const auto* ra = reinterpret_cast<const std::uint32_t*>(&in[rr + 1][0]);
-            const auto* rb = reinterpret_cast<const std::uint32_t*>(&in[rr + 2][0]);
-            const std::uint32_t a0 = ra[q + 3], a1 = ra[q + 4], a2 = ra[q + 5];  // bytes 4q+12 .. 4q+23
-            const std::uint32_t b0 = rb[q + 3], b1 = rb[q + 4], b2 = rb[q + 5];
-            // output 4q+k reads halo columns 4q+k+1 .. 4q+k+7, i.e. x[1+k .. 7+k],
-            // tap t on x[1+k+t]; lane x holds row rr, lane y row rr + 1. The
-            // columns stream in once and every output adds its taps in order
-            // (0 + a nonnegative product is the product).
-            float2 out[4];
-#pragma unroll
-            for (int m = 1; m <= 10; ++m) {
-                const std::uint32_t wa = m < 4 ? a0 : m < 8 ? a1 : a2, wb = m < 4 ? b0 : m < 8 ? b1 : b2;
-                const float2 xm = byte_pair(wa, wb, m & 3);
-#pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const int t = m - 1 - k;
-                    if (t == 0) out[k] = __fmul2_rn(tap_pair(0), xm);
-                    else if (t > 0 && t < 7) out[k] = __fadd2_rn(out[k], __fmul2_rn(tap_pair(t), xm));
-                }
-            }
-            *reinterpret_cast<float4*>(&rows[rr][4 * q]) = make_float4(out[0].x, out[1].x, out[2].x, out[3].x);
-            *reinterpret_cast<float4*>(&rows[rr + 1][4 * q]) = make_float4(out[0].y, out[1].y, out[2].y, out[3].y);
-        }
-    }
-    __syncthreads();
-    const int nc = n_cand;
-    {   // each warp expands its 32 survivor groups of a round into a warp-local
-        // position list (warp scan of the counts) and scores it 32 at a time,
-        // instead of looping over each group's survivors divergently
-        __shared__ std::uint16_t wpos[8][128];
-        const int warp = tid >> 5;
+        // the next tile's bytes travel while this one is scored
+        const int nt = next;
+        if (nt < total) stage_fast_tile(jobs[buf ^ 1], locals[buf ^ 1], in[buf ^ 1]);
+        const int nc = n_cand;
+        // 2. each warp expands its 32 survivor groups of a round into a
+        // warp-local position list (warp scan of the counts) and scores it
+        // 32 at a time
         for (int base = 0; base < nc; base += 256) {
             const int i = base + tid;
             unsigned bits = 0;
@@ -435,96 +465,60 @@ __global__ __launch_bounds__(256, 8) void fast_nms_kernel(const __grid_constant_
                 const int t = __shfl_up_sync(0xffffffffu, incl, o);
                 if (lane >= o) incl += t;
             }
-            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            const int total_w = __shfl_sync(0xffffffffu, incl, 31);
             int o = incl - cnt;
             for (unsigned b = bits; b; b &= b - 1) wpos[warp][o++] = static_cast<std::uint16_t>(pos0 + __ffs(b) - 1);
             __syncwarp();
-            for (int k = lane; k < total; k += 32) {
+            for (int k = lane; k < total_w; k += 32) {
                 const int e2 = wpos[warp][k];
                 const int r = e2 / kScStride, c = e2 - r * kScStride;
-                sc[r][c] = static_cast<std::uint8_t>(fast_score(&in[r + 3][c + 3 + kInOff], kInStride, j.threshold));
+                sc[r][c] = static_cast<std::uint8_t>(fast_score(&cur[r + 3][c + 3 + kInOff], kInStride, j.threshold));
             }
             __syncwarp();
         }
-    }
-    if (j.blurred) {  // blur columns pass: rows 2p, 2p+1 and columns 4q .. 4q+3 per thread
-        const int p = tid / (kFastTileW / 4), q = tid - p * (kFastTileW / 4);
-        // rows 2p .. 2p+7 stream in once: output row 2p + o adds tap t on
-        // row 2p + o + t, in order of t
-        float2 lo[2], hi[2];
-#pragma unroll
-        for (int r = 0; r < 8; ++r) {
-            const float4 v = *reinterpret_cast<const float4*>(&rows[2 * p + r][4 * q]);
-            const float2 vl = make_float2(v.x, v.y), vh = make_float2(v.z, v.w);
-#pragma unroll
-            for (int o = 0; o < 2; ++o) {
-                const int t = r - o;
-                if (t == 0) {
-                    lo[o] = __fmul2_rn(tap_pair(0), vl);
-                    hi[o] = __fmul2_rn(tap_pair(0), vh);
-                } else if (t > 0 && t < 7) {
-                    lo[o] = __fadd2_rn(lo[o], __fmul2_rn(tap_pair(t), vl));
-                    hi[o] = __fadd2_rn(hi[o], __fmul2_rn(tap_pair(t), vh));
+        __syncthreads();
+        // 3. strict 3x3 maxima inside the 31-pixel edge margin: only listed
+        // survivors can score above 0, so only they are tested
+        for (int i = tid; i < nc; i += kFastThreads) {
+            const int e = cand[i];
+            const int grp = e >> 4, r = grp / kScGroups, c0 = 4 * (grp - r * kScGroups);
+            if (r < 1 || r > kFastTileH) continue;  // the ring rows hold neighbours only
+            for (unsigned bits = e & 0xfu; bits; bits &= bits - 1) {
+                const int c = c0 + __ffs(bits) - 1;
+                if (c < 1 || c > kFastTileW) continue;
+                const int gy = y0 - 1 + r, gx = x0 - 1 + c;
+                if (gy < kEdge || gy >= H - kEdge || gx < kEdge || gx >= W - kEdge) continue;
+                const unsigned v = sc[r][c];
+                if (v && v > sc[r - 1][c - 1] && v > sc[r - 1][c] && v > sc[r - 1][c + 1] && v > sc[r][c - 1] &&
+                    v > sc[r][c + 1] && v > sc[r + 1][c - 1] && v > sc[r + 1][c] && v > sc[r + 1][c + 1]) {
+                    const std::uint32_t px = static_cast<std::uint32_t>(gy) * static_cast<std::uint32_t>(W) +
+                                             static_cast<std::uint32_t>(gx);
+                    found[atomicAdd(&n_found, 1)] = (static_cast<std::uint64_t>(v) << 32) | px;
+                    atomicAdd(&hist[v], 1u);
                 }
             }
         }
-#pragma unroll
-        for (int o = 0; o < 2; ++o) {
-            const int gy = y0 + 2 * p + o, gx = x0 + 4 * q;
-            const float4 acc = make_float4(lo[o].x, lo[o].y, hi[o].x, hi[o].y);
-            if (gy >= H || gx >= W) continue;
-            const std::uint32_t packed =
-                blur_byte(acc.x) | (blur_byte(acc.y) << 8) | (blur_byte(acc.z) << 16) | (blur_byte(acc.w) << 24);
-            std::uint8_t* dst = j.blurred + static_cast<std::size_t>(gy) * j.blur_pitch + gx;
-            if (gx + 3 < W && (reinterpret_cast<std::uintptr_t>(dst) & 3) == 0) {
-                *reinterpret_cast<std::uint32_t*>(dst) = packed;
-            } else {
-#pragma unroll
-                for (int k = 0; k < 4; ++k)
-                    if (gx + k < W) dst[k] = static_cast<std::uint8_t>(packed >> (8 * k));
-            }
+        __syncthreads();
+        // the tile's maxima and histogram into the job's list and histogram
+        const int nf = n_found;
+        if (tid == 0 && nf) list_base = atomicAdd(&j.counters()[kListed], static_cast<std::uint32_t>(nf));
+        __syncthreads();
+        for (int i = tid; i < nf; i += kFastThreads)
+            if (list_base + static_cast<std::uint32_t>(i) < static_cast<std::uint32_t>(j.max_maxima))
+                j.maxima[list_base + i] = found[i];
+        if (hist[tid]) {
+            atomicAdd(&j.hist[tid], hist[tid]);
+            hist[tid] = 0;
         }
-    }
-    __syncthreads();
-    // 3. strict 3x3 maxima inside the 31-pixel edge margin. A position
-    // scores above 0 only if it passed the compass test, so only the listed
-    // survivors can be maxima: each survivor of the tile compares its score
-    // with its 8 neighbours and a maximum goes into mx (zero elsewhere).
-    for (int i = tid; i < nc; i += 256) {
-        const int e = cand[i];
-        const int grp = e >> 4, r = grp / kScGroups, c0 = 4 * (grp - r * kScGroups);
-        if (r < 1 || r > kFastTileH) continue;  // the ring rows hold neighbours only
-        for (unsigned bits = e & 0xfu; bits; bits &= bits - 1) {
-            const int c = c0 + __ffs(bits) - 1;
-            if (c < 1 || c > kFastTileW) continue;
-            const int gy = y0 - 1 + r, gx = x0 - 1 + c;
-            if (gy < kEdge || gy >= H - kEdge || gx < kEdge || gx >= W - kEdge) continue;
-            const unsigned v = sc[r][c];
-            if (v && v > sc[r - 1][c - 1] && v > sc[r - 1][c] && v > sc[r - 1][c + 1] && v > sc[r][c - 1] &&
-                v > sc[r][c + 1] && v > sc[r + 1][c - 1] && v > sc[r + 1][c] && v > sc[r + 1][c + 1]) {
-                mx[r - 1][c - 1] = static_cast<std::uint8_t>(v);
-                atomicAdd(&hist[v], 1u);
-            }
+        if (tid == 0) {
+            n_cand = 0;
+            n_found = 0;
         }
+        cp_async_wait_all();
+        __syncthreads();
+        tile = nt;
+        buf ^= 1;
     }
-    __syncthreads();
-    // the tile's maxima rows, 4 pixels (r, 4q .. 4q+3) per store
-    for (int g = tid; g < kFastTileH * (kFastTileW / 4); g += 256) {
-        const int r = g / (kFastTileW / 4), q = g - r * (kFastTileW / 4);
-        const int gy = y0 + r, gx = x0 + 4 * q;
-        if (gy >= H || gx >= W) continue;
-        const std::uint32_t out = reinterpret_cast<const std::uint32_t*>(&mx[r][0])[q];
-        std::uint8_t* dst = j.maxima + static_cast<std::size_t>(gy) * W + gx;
-        if (gx + 3 < W && (reinterpret_cast<std::uintptr_t>(dst) & 3) == 0) {
-            *reinterpret_cast<std::uint32_t*>(dst) = out;
-        } else {
-#pragma unroll
-            for (int k = 0; k < 4; ++k)
-                if (gx + k < W) dst[k] = static_cast<std::uint8_t>(out >> (8 * k));
-        }
-    }
-    __syncthreads();
-    if (hist[tid]) atomicAdd(&j.hist[tid], hist[tid]);
 }
 
 // --------------------------------------------------------- 2K selection
@@ -560,154 +554,113 @@ __device__ __forceinline__ SelectParams select_params(const std::uint32_t* hist,
     return *out;
 }
 
-// Loads the 32 maxima bytes of one thread as 8 little-endian words (zero
-// past the image end).
-__device__ __forceinline__ void load32(const std::uint8_t* maxima, long long first, long long pixels,
-                                       std::uint32_t (&w)[8]) {
-    if (first + 32 <= pixels) {
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            const uint4 v = *reinterpret_cast<const uint4*>(maxima + first + 16 * q);
-            w[4 * q] = v.x;
-            w[4 * q + 1] = v.y;
-            w[4 * q + 2] = v.z;
-            w[4 * q + 3] = v.w;
-        }
-    } else {
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            std::uint32_t v = 0;
-#pragma unroll
-            for (int k = 0; k < 4; ++k) {
-                const long long i = first + 4 * q + k;
-                if (i < pixels) v |= static_cast<std::uint32_t>(maxima[i]) << (8 * k);
-            }
-            w[q] = v;
-        }
-    }
-}
-
-// (above << 16) + ties among the 4 maxima bytes of w (threshold >= 1, so a
-// byte equal to it is a maximum).
-__device__ __forceinline__ std::uint32_t count_word(std::uint32_t w, std::uint32_t thr) {
-    std::uint32_t packed = 0;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        const std::uint32_t b = (w >> (8 * k)) & 0xffu;
-        packed += (b > thr) ? (1u << 16) : 0u;
-        packed += (b == thr) ? 1u : 0u;
-    }
-    return packed;
-}
-
-// Counts of one thread's 32 pixels; most words of a maxima map are zero.
-__device__ __forceinline__ std::uint32_t count32(const std::uint32_t (&w)[8], std::uint32_t thr) {
-    std::uint32_t packed = 0;
-#pragma unroll
-    for (int q = 0; q < 8; ++q)
-        if (w[q]) packed += count_word(w[q], thr);
-    return packed;
-}
-
-// Block-wide exclusive scan of packed (above << 16 | tie) counts (block totals
-// stay below 2^16); returns the exclusive prefix, *total gets the block sum.
-__device__ __forceinline__ std::uint32_t block_scan_packed(std::uint32_t v, std::uint32_t* total) {
-    __shared__ std::uint32_t warp_sum[8];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    std::uint32_t inc = v;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const std::uint32_t n = __shfl_up_sync(0xffffffffu, inc, o);
-        if (lane >= o) inc += n;
-    }
-    if (lane == 31) warp_sum[warp] = inc;
-    __syncthreads();
-    std::uint32_t base = 0, all = 0;
-#pragma unroll
-    for (int w = 0; w < 8; ++w) {
-        base += w < warp ? warp_sum[w] : 0u;
-        all += warp_sum[w];
-    }
-    __syncthreads();
-    *total = all;
-    return base + inc - v;
-}
-
-// Per 8192-pixel chunk: the 2K threshold (every block derives the same
-// one), the chunk's (above, tie) counts; chunk 0 publishes the parameters and
-// the keypoint count min(selected, K).
+// Pre-selection over a job's maxima list: every block of the job derives the
+// same threshold from the histogram; block 0 publishes the parameters and
+// the keypoint count min(selected, K). The maxima above the threshold go to
+// keys[0, above), and when every maximum at the threshold is kept (selected
+// below the cap, or the cap falls exactly on a score boundary) those go to
+// keys[above, selected); otherwise the tie kernel picks them. The order
+// inside each range is not the raster order: the keys are sorted later by
+// (response, raster index), which no order of equal sets changes.
 template <class Src>
-__global__ __launch_bounds__(256) void select_count_kernel(const __grid_constant__ Src src) {
+__global__ __launch_bounds__(256) void select_kernel(const __grid_constant__ Src src) {
     __shared__ std::uint32_t suffix[257];
     __shared__ SelectParams sp;
     DetectJob j;
-    int chunk;
-    if (!src.find(blockIdx.x, kChunkKind, &j, &chunk)) return;
+    int local;
+    if (!src.find(blockIdx.x, kSelectKind, &j, &local)) return;
     const SelectParams p = select_params(j.hist, static_cast<std::uint32_t>(j.candidates), suffix, &sp);
-    if (chunk == 0 && threadIdx.x == 0) {
+    if (local == 0 && threadIdx.x == 0) {
         *j.params = p;
         *j.count = static_cast<int>(min(p.selected, static_cast<std::uint32_t>(j.max_keypoints)));
     }
-    const long long pixels = static_cast<long long>(j.width) * j.height;
-    const long long first = static_cast<long long>(chunk) * kChunkPx + threadIdx.x * 32;
-    std::uint32_t w[8];
-    load32(j.maxima, first, pixels, w);
-    std::uint32_t total;
-    block_scan_packed(count32(w, p.threshold), &total);
-    if (threadIdx.x == 0) {
-        j.chunk_counts[2 * chunk] = total >> 16;
-        j.chunk_counts[2 * chunk + 1] = total & 0xffffu;
+    const bool all_ties = p.ties == j.hist[p.threshold];
+    std::uint32_t* ctr = j.counters();
+    const std::uint32_t n = min(ctr[kListed], static_cast<std::uint32_t>(j.max_maxima));
+    const int lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
+    const std::uint32_t stride = static_cast<std::uint32_t>(j.select_blocks) * 256u;
+    for (std::uint32_t i0 = static_cast<std::uint32_t>(local) * 256u; i0 < n; i0 += stride) {  // block-uniform
+        const std::uint32_t i = i0 + threadIdx.x;
+        bool above = false, tie = false;
+        std::uint32_t px = 0;
+        if (i < n) {
+            const std::uint64_t e = j.maxima[i];
+            const auto score = static_cast<std::uint32_t>(e >> 32);
+            px = static_cast<std::uint32_t>(e);
+            above = score > p.threshold;
+            tie = all_ties && score == p.threshold;
+        }
+        const unsigned ma = __ballot_sync(0xffffffffu, above), mt = __ballot_sync(0xffffffffu, tie);
+        std::uint32_t ba = 0, bt = 0;
+        if (lane == 0) {
+            if (ma) ba = atomicAdd(&ctr[kAboveWritten], static_cast<std::uint32_t>(__popc(ma)));
+            if (mt) bt = atomicAdd(&ctr[kTiesWritten], static_cast<std::uint32_t>(__popc(mt)));
+        }
+        ba = __shfl_sync(0xffffffffu, ba, 0) + __popc(ma & below);
+        bt = __shfl_sync(0xffffffffu, bt, 0) + __popc(mt & below);
+        if (above && ba < p.above) j.keys[ba] = px;  // always true when list and histogram agree
+        if (tie && bt < p.ties) j.keys[p.above + bt] = px;
     }
 }
 
-// Writes the raster index of every pre-selected maximum: slots [0, above) get
-// the maxima above the threshold in raster order, slots [above, selected) the
-// first `ties` maxima at the threshold in raster order.
+// The first `ties` maxima at the threshold score in raster order, when the
+// select kernel could not take every tie: a most-significant-digit radix
+// select over their raster indices (unique) finds the ties-th smallest, P,
+// and every tie at or below P goes to keys[above, selected). One block per
+// job; the reference's equivalent is the raster-order scatter of the first
+// ties (src/s2_s3/s2.cu:182-235).
 template <class Src>
-__global__ __launch_bounds__(256) void scatter_kernel(const __grid_constant__ Src src) {
-    __shared__ std::uint32_t red[2][8];
+__global__ __launch_bounds__(kTieThreads) void ties_kernel(const __grid_constant__ Src src) {
+    __shared__ std::uint32_t bins[256];
+    __shared__ std::uint32_t pick[2];  // digit, maxima before it
     DetectJob j;
-    int chunk;
-    if (!src.find(blockIdx.x, kChunkKind, &j, &chunk)) return;
+    int local;
+    if (!src.find(blockIdx.x, kSortKind, &j, &local)) return;
     const SelectParams p = *j.params;
-    // Offsets of this chunk: totals of all earlier chunks of the image.
-    std::uint32_t pa = 0, pt = 0;
-    for (int i = threadIdx.x; i < chunk; i += 256) {
-        pa += j.chunk_counts[2 * i];
-        pt += j.chunk_counts[2 * i + 1];
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        pa += __shfl_xor_sync(0xffffffffu, pa, o);
-        pt += __shfl_xor_sync(0xffffffffu, pt, o);
-    }
-    if ((threadIdx.x & 31) == 0) { red[0][threadIdx.x >> 5] = pa; red[1][threadIdx.x >> 5] = pt; }
-    __syncthreads();
-    std::uint32_t off_above = 0, off_tie = 0;
-#pragma unroll
-    for (int w = 0; w < 8; ++w) { off_above += red[0][w]; off_tie += red[1][w]; }
-    const long long pixels = static_cast<long long>(j.width) * j.height;
-    const long long first = static_cast<long long>(chunk) * kChunkPx + threadIdx.x * 32;
-    std::uint32_t w[8];
-    load32(j.maxima, first, pixels, w);
-    std::uint32_t total;
-    const std::uint32_t excl = block_scan_packed(count32(w, p.threshold), &total);
-    std::uint32_t ra = off_above + (excl >> 16), rt = off_tie + (excl & 0xffffu);
-#pragma unroll
-    for (int q = 0; q < 8; ++q) {
-        if (!w[q]) continue;
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            const std::uint32_t b = (w[q] >> (8 * k)) & 0xffu;
-            const std::uint64_t px = static_cast<std::uint64_t>(first + 4 * q + k);
-            if (b > p.threshold) {
-                if (ra < p.above) j.keys[ra] = px;  // always true when map and histogram agree
-                ++ra;
-            } else if (b == p.threshold) {
-                if (rt < p.ties) j.keys[p.above + rt] = px;
-                ++rt;
-            }
+    if (p.selected == 0 || p.ties == j.hist[p.threshold]) return;  // nothing to pick, or all written
+    std::uint32_t* ctr = j.counters();
+    const std::uint32_t n = min(ctr[kListed], static_cast<std::uint32_t>(j.max_maxima));
+    const std::uint32_t T = p.threshold;
+    std::uint32_t prefix = 0, need = p.ties;
+    for (int shift = 24; shift >= 0; shift -= 8) {
+        const std::uint32_t high = shift == 24 ? 0u : (0xffffffffu << (shift + 8));
+        for (int b = threadIdx.x; b < 256; b += kTieThreads) bins[b] = 0;
+        __syncthreads();
+        for (std::uint32_t i = threadIdx.x; i < n; i += kTieThreads) {
+            const std::uint64_t e = j.maxima[i];
+            const auto px = static_cast<std::uint32_t>(e);
+            if (static_cast<std::uint32_t>(e >> 32) == T && (px & high) == prefix)
+                atomicAdd(&bins[(px >> shift) & 255u], 1u);
         }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            std::uint32_t run = 0, d = 0;
+            while (d < 255 && run + bins[d] < need) run += bins[d++];
+            pick[0] = d;
+            pick[1] = run;
+        }
+        __syncthreads();
+        prefix |= pick[0] << shift;
+        need -= pick[1];
+        __syncthreads();
+    }
+    const int lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
+    for (std::uint32_t i0 = 0; i0 < n; i0 += kTieThreads) {  // block-uniform
+        const std::uint32_t i = i0 + threadIdx.x;
+        bool keep = false;
+        std::uint32_t px = 0;
+        if (i < n) {
+            const std::uint64_t e = j.maxima[i];
+            px = static_cast<std::uint32_t>(e);
+            keep = static_cast<std::uint32_t>(e >> 32) == T && px <= prefix;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, keep);
+        std::uint32_t b = 0;
+        if (lane == 0 && m) b = atomicAdd(&ctr[kTiesWritten], static_cast<std::uint32_t>(__popc(m)));
+        b = __shfl_sync(0xffffffffu, b, 0) + __popc(m & below);
+        if (keep && b < p.ties) j.keys[p.above + b] = px;
     }
 }
 
@@ -776,11 +729,28 @@ __global__ __launch_bounds__(kHarrisThreads) void harris_kernel(const __grid_con
 
 // ------------------------------------------------------------- top-K
 
+// Flags the blur tiles within kSampleRadius of the keypoint at (x, y) (the
+// describe kernel samples nothing else of the blurred layer around it) and
+// lists each newly flagged tile once for blur_tiles_kernel.
+__device__ __forceinline__ void mark_blur_tiles(const DetectJob& j, int x, int y) {
+    const int tx0 = max(x - kSampleRadius, 0) / kBlurTileW, tx1 = min(x + kSampleRadius, j.width - 1) / kBlurTileW;
+    const int ty0 = max(y - kSampleRadius, 0) / kBlurTileH, ty1 = min(y + kSampleRadius, j.height - 1) / kBlurTileH;
+    const int tiles_x = (j.width + kBlurTileW - 1) / kBlurTileW;
+    for (int ty = ty0; ty <= ty1; ++ty)
+        for (int tx = tx0; tx <= tx1; ++tx) {
+            const int t = ty * tiles_x + tx;
+            if (atomicExch(&j.blur_marks[t], 1u) == 0u)
+                j.blur_list[atomicAdd(j.blur_count, 1u)] = make_uint2(static_cast<unsigned>(j.job), static_cast<unsigned>(t));
+        }
+}
+
 __device__ __forceinline__ void write_keypoint(const DetectJob& j, int rank, std::uint64_t key) {
     const std::uint32_t px = 0xffffffffu - static_cast<std::uint32_t>(key);
-    j.x[rank] = static_cast<float>(px % static_cast<std::uint32_t>(j.width));
-    j.y[rank] = static_cast<float>(px / static_cast<std::uint32_t>(j.width));
+    const std::uint32_t x = px % static_cast<std::uint32_t>(j.width), y = px / static_cast<std::uint32_t>(j.width);
+    j.x[rank] = static_cast<float>(x);
+    j.y[rank] = static_cast<float>(y);
     if (j.response) j.response[rank] = from_order_bits(static_cast<std::uint32_t>(key >> 32));
+    if (j.blur_marks) mark_blur_tiles(j, static_cast<int>(x), static_cast<int>(y));
 }
 
 // One block per image: bitonic sort (descending) of up to kSortCap keys in
@@ -1062,6 +1032,120 @@ __global__ __launch_bounds__(256) void blur_kernel(const __grid_constant__ Src s
         // finite acc, and keeps signed integer min/max out of this kernel.
         j.blurred[static_cast<std::size_t>(gy) * j.blur_pitch + gx] =
             static_cast<std::uint8_t>(__float2int_rn(fminf(fmaxf(acc, 0.0f), 255.0f)));
+    }
+}
+
+// The S3 blur of the 64x32 tiles listed by the keypoint writers (on-demand
+// blur of the pyramid and batched paths): the same bytes as blur_kernel
+// (per output the taps summed first to last, each product and sum rounded on
+// its own, then rounded half-to-even and clamped), with both passes on the
+// sm_100 packed FP32x2 add and multiply (two rows, or two columns, per
+// instruction, each lane rounded as the scalar op). Persistent: block b takes
+// list entries b, b + gridDim.x, ... (the list is complete when the kernel
+// starts). A tile is staged with its reflect-101 halo: 16-byte loads for
+// interior tiles of 16-byte aligned images, reflected byte loads otherwise.
+static_assert(kBlurTileW == kFastTileW && kBlurTileH == kFastTileH, "blur tiles share the FAST tile staging");
+template <class Src>
+__global__ __launch_bounds__(256, 8) void blur_tiles_kernel(const __grid_constant__ Src src, const uint2* list,
+                                                            const std::uint32_t* count) {
+    __shared__ __align__(16) std::uint8_t in[kFastInH][kInStride];  // rows y0-4 .., columns x0-16 ..
+    __shared__ __align__(16) float rows[kFastTileH + 6][kFastTileW];
+    __shared__ std::size_t row_at[kFastInH];
+    __shared__ int col_at[kInStride];
+    const int tid = threadIdx.x;
+    const int n = static_cast<int>(*count);
+    for (int i = blockIdx.x; i < n; i += gridDim.x) {
+        const uint2 e = list[i];
+        const DescribeJob j = src.at(static_cast<int>(e.x));
+        const int W = j.width, H = j.height;
+        const int tiles_x = (W + kBlurTileW - 1) / kBlurTileW;
+        const int y0 = (static_cast<int>(e.y) / tiles_x) * kBlurTileH, x0 = (static_cast<int>(e.y) % tiles_x) * kBlurTileW;
+        const bool vec = ((reinterpret_cast<std::uintptr_t>(j.image) | static_cast<std::uintptr_t>(j.pitch)) & 15) == 0 &&
+                         x0 >= 16 && x0 + 80 <= W && y0 >= 4 && y0 + kFastTileH + 4 <= H;
+        if (vec) {
+            if (tid < kFastInH * (kInStride / 16)) {
+                const int r = tid / (kInStride / 16), q = tid - r * (kInStride / 16);
+                *reinterpret_cast<uint4*>(&in[r][16 * q]) = *reinterpret_cast<const uint4*>(
+                    j.image + static_cast<std::size_t>(y0 - 4 + r) * j.pitch + (x0 - 16 + 16 * q));
+            }
+        } else {
+            if (tid < kFastInH) row_at[tid] = static_cast<std::size_t>(reflect101(y0 - 4 + tid, H)) * j.pitch;
+            else if (tid < kFastInH + kInStride) col_at[tid - kFastInH] = reflect101(x0 - 16 + (tid - kFastInH), W);
+            __syncthreads();
+            for (int k = tid; k < kFastInH * (kInStride / 4); k += 256) {
+                const int r = k / (kInStride / 4), b = 4 * (k - r * (kInStride / 4));
+                const std::uint8_t* row = j.image + row_at[r];
+                *reinterpret_cast<std::uint32_t*>(&in[r][b]) =
+                    static_cast<std::uint32_t>(row[col_at[b]]) | (static_cast<std::uint32_t>(row[col_at[b + 1]]) << 8) |
+                    (static_cast<std::uint32_t>(row[col_at[b + 2]]) << 16) |
+                    (static_cast<std::uint32_t>(row[col_at[b + 3]]) << 24);
+            }
+        }
+        __syncthreads();
+        // rows pass: image rows y0-3 .. y0+34, two rows x 4 outputs per item
+        static_assert((kFastTileH + 6) % 2 == 0, "rows pass takes row pairs");
+        for (int g = tid; g < (kFastTileH + 6) / 2 * (kFastTileW / 4); g += 256) {
+            const int rp = g / (kFastTileW / 4), q = g - rp * (kFastTileW / 4), rr = 2 * rp;
+            const auto* ra = reinterpret_cast<const std::uint32_t*>(&in[rr + 1][0]);
+            const auto* rb = reinterpret_cast<const std::uint32_t*>(&in[rr + 2][0]);
+            const std::uint32_t a0 = ra[q + 3], a1 = ra[q + 4], a2 = ra[q + 5];  // bytes 4q+12 .. 4q+23
+            const std::uint32_t b0 = rb[q + 3], b1 = rb[q + 4], b2 = rb[q + 5];
+            // output 4q+k reads halo columns 4q+k+1 .. 4q+k+7, tap t on column
+            // 4q+k+1+t; lane x holds row rr, lane y row rr + 1. The columns
+            // stream in once and every output adds its taps in order (0 + a
+            // nonnegative product is the product).
+            float2 out[4];
+#pragma unroll
+            for (int m = 1; m <= 10; ++m) {
+                const std::uint32_t wa = m < 4 ? a0 : m < 8 ? a1 : a2, wb = m < 4 ? b0 : m < 8 ? b1 : b2;
+                const float2 xm = byte_pair(wa, wb, m & 3);
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const int t = m - 1 - k;
+                    if (t == 0) out[k] = __fmul2_rn(tap_pair(0), xm);
+                    else if (t > 0 && t < 7) out[k] = __fadd2_rn(out[k], __fmul2_rn(tap_pair(t), xm));
+                }
+            }
+            *reinterpret_cast<float4*>(&rows[rr][4 * q]) = make_float4(out[0].x, out[1].x, out[2].x, out[3].x);
+            *reinterpret_cast<float4*>(&rows[rr + 1][4 * q]) = make_float4(out[0].y, out[1].y, out[2].y, out[3].y);
+        }
+        __syncthreads();
+        {   // columns pass: rows 2p, 2p+1 and columns 4q .. 4q+3 per thread
+            const int pr = tid / (kFastTileW / 4), q = tid - pr * (kFastTileW / 4);
+            float2 lo[2], hi[2];
+#pragma unroll
+            for (int r = 0; r < 8; ++r) {
+                const float4 v = *reinterpret_cast<const float4*>(&rows[2 * pr + r][4 * q]);
+                const float2 vl = make_float2(v.x, v.y), vh = make_float2(v.z, v.w);
+#pragma unroll
+                for (int o = 0; o < 2; ++o) {
+                    const int t = r - o;
+                    if (t == 0) {
+                        lo[o] = __fmul2_rn(tap_pair(0), vl);
+                        hi[o] = __fmul2_rn(tap_pair(0), vh);
+                    } else if (t > 0 && t < 7) {
+                        lo[o] = __fadd2_rn(lo[o], __fmul2_rn(tap_pair(t), vl));
+                        hi[o] = __fadd2_rn(hi[o], __fmul2_rn(tap_pair(t), vh));
+                    }
+                }
+            }
+#pragma unroll
+            for (int o = 0; o < 2; ++o) {
+                const int gy = y0 + 2 * pr + o, gx = x0 + 4 * q;
+                if (gy >= H || gx >= W) continue;
+                const std::uint32_t packed = blur_byte(lo[o].x) | (blur_byte(lo[o].y) << 8) |
+                                             (blur_byte(hi[o].x) << 16) | (blur_byte(hi[o].y) << 24);
+                std::uint8_t* dst = j.blurred + static_cast<std::size_t>(gy) * j.blur_pitch + gx;
+                if (gx + 3 < W && (reinterpret_cast<std::uintptr_t>(dst) & 3) == 0) {
+                    *reinterpret_cast<std::uint32_t*>(dst) = packed;
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+                        if (gx + k < W) dst[k] = static_cast<std::uint8_t>(packed >> (8 * k));
+                }
+            }
+        }
+        __syncthreads();  // before the next tile's staging
     }
 }
 
