@@ -662,9 +662,8 @@ Status Plan::enqueue(void* ws, std::size_t bytes, stitch_homography_result* host
     const auto* kjobs = reinterpret_cast<const KnnJob*>(T + offsets[kKnnJobs]);
     if (go(knn_blocks)) {
         const KnnSrc ks = with_map(KnnSrc{kjobs, reinterpret_cast<const int*>(T + offsets[kKnnPrefix]), n_knn}, kMapKnn);
-        if (matcher == s4k::kMatcherTensor) {
-            if (!s4k::enable_tc_smem<KnnSrc>()) return Status::CUDA_ERROR;
-            s4k::knn_tc_kernel<KnnSrc><<<knn_blocks, s4k::kQueryThreads, s4k::kTcSmem, s>>>(ks);
+        if (s4k::is_tensor(matcher)) {
+            if (!s4k::launch_tc(matcher, knn_blocks, ks, s)) return Status::CUDA_ERROR;
         } else {
             s4k::knn_popc_kernel<KnnSrc, s4k::kQueriesPerThread><<<knn_blocks, s4k::kQueryThreads, 0, s>>>(ks);
         }

@@ -220,31 +220,31 @@ __device__ __forceinline__ int reflect101(int i, int n) {
 // largest over the 16 arcs of both kinds, the pixel is a corner iff the raw
 // score exceeds the threshold, and it then scores raw - 1. Both kinds run
 // at once as unsigned 16-bit lanes q_k = (d_k + 256) | (256 - d_k) << 16
-// (all in [1, 511]); 9-wide arc minima come from 2-, 4- and 8-wide ones.
-// (CUDA 12.9 ptxas at -O1 and above miscompiles the signed
-// max(min(arc), -max(arc)) form of this score on sm_100; this unsigned
-// form is exact at every optimisation level.)
+// (all in [1, 511]), which is c + r_k * 0xffff for c = (v + 256) |
+// (256 - v) << 16: one multiply-add per ring pixel, no borrow between the
+// lanes. 9-wide arc minima come from 3-wide ones through the 3-input 16x2
+// minimum (min3(m3[k], m3[k+3], m3[k+6])), and the 16 arcs are folded with
+// the 3-input maximum. (CUDA 12.9 ptxas at -O1 and above miscompiles the
+// signed max(min(arc), -max(arc)) form of this score on sm_100; this
+// unsigned form is exact at every optimisation level.)
 __device__ __forceinline__ int fast_score(const std::uint8_t* p, int stride, int thr) {
-    const int v = p[0];
-    const int ring[16] = {p[3 * stride],      p[3 * stride + 1],  p[2 * stride + 2],  p[stride + 3],
-                          p[3],               p[-stride + 3],     p[-2 * stride + 2], p[-3 * stride + 1],
-                          p[-3 * stride],     p[-3 * stride - 1], p[-2 * stride - 2], p[-stride - 3],
-                          p[-3],              p[stride - 3],      p[2 * stride - 2],  p[3 * stride - 1]};
-    unsigned q[16], m2[16], m4[16], m8[16];
+    const unsigned v = p[0];
+    const unsigned c = (v + 256u) | ((256u - v) << 16);
+    const unsigned r[16] = {p[3 * stride],      p[3 * stride + 1],  p[2 * stride + 2],  p[stride + 3],
+                            p[3],               p[-stride + 3],     p[-2 * stride + 2], p[-3 * stride + 1],
+                            p[-3 * stride],     p[-3 * stride - 1], p[-2 * stride - 2], p[-stride - 3],
+                            p[-3],              p[stride - 3],      p[2 * stride - 2],  p[3 * stride - 1]};
+    unsigned q[16], m3[16], m9[16];
 #pragma unroll
-    for (int k = 0; k < 16; ++k) {
-        const int d = v - ring[k];
-        q[k] = static_cast<unsigned>(d + 256) | (static_cast<unsigned>(256 - d) << 16);
-    }
+    for (int k = 0; k < 16; ++k) q[k] = c + r[k] * 0xffffu;
 #pragma unroll
-    for (int k = 0; k < 16; ++k) m2[k] = __vminu2(q[k], q[(k + 1) & 15]);
+    for (int k = 0; k < 16; ++k) m3[k] = __vimin3_u16x2(q[k], q[(k + 1) & 15], q[(k + 2) & 15]);
 #pragma unroll
-    for (int k = 0; k < 16; ++k) m4[k] = __vminu2(m2[k], m2[(k + 2) & 15]);
-#pragma unroll
-    for (int k = 0; k < 16; ++k) m8[k] = __vminu2(m4[k], m4[(k + 4) & 15]);
-    unsigned best = 0;
-#pragma unroll
-    for (int k = 0; k < 16; ++k) best = __vmaxu2(best, __vminu2(m8[k], q[(k + 8) & 15]));
+    for (int k = 0; k < 16; ++k) m9[k] = __vimin3_u16x2(m3[k], m3[(k + 3) & 15], m3[(k + 6) & 15]);
+    const unsigned b0 = __vimax3_u16x2(m9[0], m9[1], m9[2]), b1 = __vimax3_u16x2(m9[3], m9[4], m9[5]);
+    const unsigned b2 = __vimax3_u16x2(m9[6], m9[7], m9[8]), b3 = __vimax3_u16x2(m9[9], m9[10], m9[11]);
+    const unsigned b4 = __vimax3_u16x2(m9[12], m9[13], m9[14]);
+    const unsigned best = __vmaxu2(__vimax3_u16x2(b0, b1, b2), __vimax3_u16x2(b3, b4, m9[15]));
     const unsigned lo = best & 0xffffu, hi = best >> 16;
     const int score = static_cast<int>(lo > hi ? lo : hi) - 256;
     return score > thr ? score - 1 : 0;

@@ -114,7 +114,7 @@ Status check_match_args(const Keypoints& a, const Descriptors& da, const Keypoin
         return Status::INVALID_ARGUMENT;
     return Status::OK;
 }
-bool valid_matcher(int kind) { return kind == kMatcherPopc || kind == kMatcherTensor; }
+bool valid_matcher(int kind) { return kind >= kMatcherPopc && kind <= kMatcherTensor64; }
 
 namespace {
 
@@ -127,18 +127,18 @@ Status launch_direction(const Keypoints& qk, const Descriptors& qd, const Keypoi
     if (popc_eligible(qd, td, tk.capacity)) {
         using Src = OneJob<KnnJob>;
         const Src src{make_knn_job(qk, qd, tk, td, q_tiles, splits, rows, partial, out)};
-        if (matcher() == kMatcherTensor) {
+        if (is_tensor(matcher())) {
             // Two tensor-core blocks fit on an SM (shared memory), so a grid
             // above 2 x 148 blocks leaves a second, mostly idle wave: use the
             // largest train partition count whose grid fits one wave (never
             // more partitions than the workspace plan holds).
             const int stages = ceil_div(std::max(tk.capacity, 1), kTrainStage);
-            const int want = std::min(splits, std::max(1, kTcBlocksPerSm * kSmCount / std::max(q_tiles, 1)));
+            const int want =
+                std::min(splits, std::max(1, tc_blocks_per_sm(matcher()) * kSmCount / std::max(q_tiles, 1)));
             const int tc_rows = ceil_div(stages, want) * kTrainStage;
             const int tc_splits = ceil_div(std::max(tk.capacity, 1), tc_rows);
             const Src tc{make_knn_job(qk, qd, tk, td, q_tiles, tc_splits, tc_rows, partial, out)};
-            if (!enable_tc_smem<Src>()) return Status::CUDA_ERROR;
-            knn_tc_kernel<Src><<<q_tiles * tc_splits, kQueryThreads, kTcSmem, stream>>>(tc);
+            if (!launch_tc(matcher(), q_tiles * tc_splits, tc, stream)) return Status::CUDA_ERROR;
             if (tc_splits > 1) knn_merge_kernel<Src><<<ceil_div(qk.capacity, 256), 256, 0, stream>>>(tc);
             note_launches(tc_splits > 1 ? 2 : 1);
         } else {

@@ -23,7 +23,10 @@ bool popc_eligible(const Descriptors& q, const Descriptors& t, int capacity_trai
 // (stitch_s4_set_matcher), so threads never race on it; a batch plan and a
 // server take the creating thread's choice when they are made, and a plan can
 // be given its own (stitch_batch_set_matcher).
-constexpr int kMatcherPopc = 0, kMatcherTensor = 1;
+constexpr int kMatcherPopc = 0, kMatcherTensor = 1, kMatcherTensor128 = 2, kMatcherTensor64 = 3;
+// Train rows per tensor-core stage of a tensor-core matcher kind.
+constexpr int tc_rows(int kind) { return kind == kMatcherTensor64 ? 64 : kind == kMatcherTensor128 ? 128 : 256; }
+constexpr bool is_tensor(int kind) { return kind != kMatcherPopc; }
 int matcher();
 bool valid_matcher(int kind);
 // Host-only argument checks of s4_match, in its order: INVALID_ARGUMENT or
@@ -32,16 +35,37 @@ Status check_match_args(const Keypoints& a, const Descriptors& da, const Keypoin
                         const s4::Config& config, const Matches& output, std::size_t* required);
 // Opts the tensor-core kernel for a job source in to its shared memory
 // (once per device); false if the device refuses.
-template <class Src> bool enable_tc_smem() {
+template <class Src, int kRowsB> bool enable_tc_smem() {
     static std::once_flag flags[64];
     static bool ok[64];
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return false;
     std::call_once(flags[dev], [&] {
-        ok[dev] = cudaFuncSetAttribute(knn_tc_kernel<Src>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTcSmem) ==
-                  cudaSuccess;
+        ok[dev] = cudaFuncSetAttribute(knn_tc_kernel<Src, kRowsB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       TcShape<kRowsB>::smem) == cudaSuccess;
     });
     return ok[dev];
+}
+// Launches the tensor-core matcher of `kind` over `blocks` blocks.
+template <class Src> bool launch_tc(int kind, int blocks, const Src& src, cudaStream_t s) {
+    switch (tc_rows(kind)) {
+        case 64:
+            if (!enable_tc_smem<Src, 64>()) return false;
+            knn_tc_kernel<Src, 64><<<blocks, kQueryThreads, TcShape<64>::smem, s>>>(src);
+            return true;
+        case 128:
+            if (!enable_tc_smem<Src, 128>()) return false;
+            knn_tc_kernel<Src, 128><<<blocks, kQueryThreads, TcShape<128>::smem, s>>>(src);
+            return true;
+        default:
+            if (!enable_tc_smem<Src, 256>()) return false;
+            knn_tc_kernel<Src, 256><<<blocks, kQueryThreads, TcShape<256>::smem, s>>>(src);
+            return true;
+    }
+}
+constexpr int tc_blocks_per_sm(int kind) {
+    return tc_rows(kind) == 64 ? TcShape<64>::blocks_per_sm
+                               : tc_rows(kind) == 128 ? TcShape<128>::blocks_per_sm : TcShape<256>::blocks_per_sm;
 }
 // Reads and clears the tensor-core error word of the batched chain's
 // translation unit (batch.cu).

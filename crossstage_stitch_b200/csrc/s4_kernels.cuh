@@ -187,15 +187,26 @@ __global__ __launch_bounds__(kQueryThreads) void knn_popc_kernel(const __grid_co
 // keys, so results equal knn_popc_kernel's bit for bit.
 //
 // Shared memory holds the expanded queries (128 rows x 256 bytes) and one
-// train stage (256 rows x 256 bytes) in the K-major 128-byte-swizzle layout
-// tcgen05 reads: per 128-byte K block, 8-row groups of 1024 bytes, 16-byte
-// chunk c of row r stored at chunk c ^ (r % 8).
+// train stage (kRowsB rows x 256 bytes: 256, 128 or 64) in the K-major
+// 128-byte-swizzle layout tcgen05 reads: per 128-byte K block, 8-row groups
+// of 1024 bytes, 16-byte chunk c of row r stored at chunk c ^ (r % 8). A
+// narrower stage halves the shared memory and TMEM of a block, so more
+// blocks share an SM and one block's staging and epilogue overlap another's
+// MMA (2, 3 or 4 blocks per SM).
 constexpr int kTcRowsA = kQueryThreads;       // 128 queries (MMA M)
-constexpr int kTcRowsB = kTrainStage;         // 256 train rows (MMA N)
-constexpr int kTcBytesA = kTcRowsA * 256, kTcBytesB = kTcRowsB * 256;
-constexpr int kTcBlocksPerSm = 2;  // resident tensor-core blocks per SM (shared memory bound)
-constexpr int kTcSmem = kTcBytesA + kTcBytesB + 1024 + 64;  // + alignment slack + barrier/slot
-static_assert(kTcBlocksPerSm * (kTcSmem + 1024) <= 228 * 1024, "tensor-core blocks per SM");
+constexpr int kTcBytesA = kTcRowsA * 256;
+template <int kRowsB> struct TcShape {
+    static_assert(kRowsB == 64 || kRowsB == 128 || kRowsB == 256, "MMA N and TMEM columns");
+    static constexpr int rows_b = kRowsB;                                  // MMA N, TMEM columns
+    static constexpr int bytes_b = kRowsB * 256;
+    static constexpr int smem = kTcBytesA + bytes_b + 1024 + 64;            // + alignment slack + barrier/slot
+    static constexpr int blocks_per_sm = (228 * 1024) / (smem + 1024);     // shared memory bound
+    // kind::i8 instruction descriptor: s32 accumulator, signed A and B, both
+    // K-major, N = kRowsB, M = 128
+    static constexpr std::uint32_t idesc =
+        (2u << 4) | (1u << 7) | (1u << 10) | ((kRowsB >> 3) << 17) | ((kTcRowsA >> 4) << 24);
+    static_assert(blocks_per_sm * kRowsB <= 512, "TMEM columns of the resident blocks");
+};
 constexpr long long kTcWaitLimit = 1ll << 26;  // mbarrier polls before giving up
 
 // Error word of the tensor-core matcher (one per translation unit): set when
@@ -243,12 +254,11 @@ __device__ __forceinline__ std::uint64_t sw128_desc(std::uint32_t addr) {
            (2ull << 61);
 }
 
-// kind::i8 instruction descriptor: s32 accumulator, signed A and B, both
-// K-major, N = 256, M = 128.
-constexpr std::uint32_t kTcIdesc = (2u << 4) | (1u << 7) | (1u << 10) | ((kTcRowsB >> 3) << 17) | ((kTcRowsA >> 4) << 24);
-
-template <class Src>
+template <class Src, int kRowsB>
 __global__ __launch_bounds__(kQueryThreads, 1) void knn_tc_kernel(const __grid_constant__ Src src) {
+    using Shape = TcShape<kRowsB>;
+    constexpr int kTcRowsB = Shape::rows_b;
+    constexpr int kTcBytesB = Shape::bytes_b;
     extern __shared__ std::uint8_t dyn[];
     KnnJob j;
     int local;
@@ -303,7 +313,7 @@ __global__ __launch_bounds__(kQueryThreads, 1) void knn_tc_kernel(const __grid_c
                 asm volatile(
                     "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
                     "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(tmem),
-                    "l"(da), "l"(db), "r"(kTcIdesc), "r"(s));
+                    "l"(da), "l"(db), "r"(Shape::idesc), "r"(s));
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
                              smem_u32(bar))

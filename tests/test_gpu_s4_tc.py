@@ -2,7 +2,9 @@
 (256 - dot) / 2 from tensor-core dot products) against the oracle, on the
 same cases as the __popc kernel: edges, ties across train tiles, planted
 partners at every shape including 8192 x 8192, counts below capacity, and
-the whole batched chain against the per-pair chain run with __popc."""
+the whole batched chain against the per-pair chain run with __popc. Every
+train-stage width runs (matcher kinds 1, 2, 3: 256, 128 and 64 train rows
+per MMA stage)."""
 import numpy as np
 import pytest
 import torch
@@ -14,13 +16,14 @@ from .test_gpu_s4 import check, planted, u8
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture
-def tc(cuda):
+@pytest.fixture(params=[1, 2, 3], ids=["stage256", "stage128", "stage64"])
+def tc(cuda, request):
     from .gpu_util import Lib
     lib = Lib("ours")
     L = _abi.load()
-    assert L.stitch_s4_set_matcher(1) == 0 and L.stitch_s4_matcher() == 1
+    assert L.stitch_s4_set_matcher(request.param) == 0 and L.stitch_s4_matcher() == request.param
     yield lib
+    L.stitch_s4_set_matcher(1)
     assert L.stitch_s4_tc_errors() == 0, "an MMA completion wait ran out"
 
 
@@ -51,7 +54,8 @@ def test_tc_full_microbenchmark_size(tc):
     assert ia.size > 0.2 * 8192
 
 
-def test_tc_batched_chain_equals_popc_per_pair(cuda):
+@pytest.mark.parametrize("kind", [1, 2, 3])
+def test_tc_batched_chain_equals_popc_per_pair(cuda, kind):
     L = _abi.load()
     cases = []
     for i in range(3):
@@ -64,7 +68,7 @@ def test_tc_batched_chain_equals_popc_per_pair(cuda):
     for a, b, k in cases:
         res = runner.run(a, b, k)
         want.append((res, runner.download()))
-    assert L.stitch_s4_set_matcher(1) == 0
+    assert L.stitch_s4_set_matcher(kind) == 0
     try:
         imgs = [(torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()) for a, b, _ in cases]
         bt = batch.Batch([batch.pair_desc(ia, ib, k) for (ia, ib), (_, _, k) in zip(imgs, cases)])
