@@ -351,6 +351,23 @@ def run_mixed(mixed, steps, warmup, dev, flush):
         if it >= warmup:
             times.append(e0.elapsed_time(e1))
     t_batch = sum(times) / len(times)
+    # per-kernel split from a copy of the graph with event marks (own workspace)
+    from crossstage_stitch_b200 import _abi
+    bm = batch.Batch([batch.pair_desc(ia, ib, k) for (ia, ib), k in zip(imgs, knobs)], device=dev)
+    marks = [torch.cuda.Event(enable_timing=True) for _ in _abi.BATCH_MARKS]
+    bm.set_marks(marks)
+    bm.capture()
+    split = [0.0] * len(marks)
+    for it in range(warmup + steps):
+        flush.zero_()
+        torch.cuda.synchronize()
+        bm.launch(stream)
+        torch.cuda.synchronize()
+        if it >= warmup:
+            for i in range(1, len(marks)):
+                split[i] += marks[i - 1].elapsed_time(marks[i]) / steps
+    del bm
+    kernel_ms = {_abi.BATCH_MARKS[i]: round(split[i], 4) for i in range(1, len(marks))}
     W = max(max(a.shape[1], bb.shape[1]) for a, bb, _ in mixed)
     H = max(max(a.shape[0], bb.shape[0]) for a, bb, _ in mixed)
     runner = stages.PairRunner(W, H, max(k.max_keypoints for k in knobs), max_r=max(k.hypotheses for k in knobs),
@@ -383,7 +400,8 @@ def run_mixed(mixed, steps, warmup, dev, flush):
     return {"workload": f"{n} mixed pairs from {{640x480, 1280x720, 1920x1080, 3840x2160}}, K in {{500, 2000, 8000}}, "
                         f"FAST in {{10, 20, 40}}, R in {{500, 2000, 8000}}, 8 levels at 1.2, repeated-texture outliers",
             "pairs": n, "mean_mpx_per_pair": round(mpx, 3),
-            "batched": {"value": n / (t_batch / 1e3), "unit": "pairs/s", "ms_per_step": t_batch},
+            "batched": {"value": n / (t_batch / 1e3), "unit": "pairs/s", "ms_per_step": t_batch,
+                        "kernel_ms": kernel_ms},
             "plain_per_pair": {"value": n / (t_plain / 1e3), "unit": "pairs/s", "p50_ms": lat[len(lat) // 2],
                                "p99_ms": lat[int(0.99 * (len(lat) - 1))]},
             "batched_over_plain": (n / (t_batch / 1e3)) / (n / (t_plain / 1e3)), "parity": parity}

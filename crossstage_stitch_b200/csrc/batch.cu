@@ -642,7 +642,7 @@ Status Plan::enqueue(void* ws, std::size_t bytes, stitch_homography_result* host
     mark();
     if (go(tiles > 0 && blur_total > 0 ? 1 : 0))
         s2s3::blur_tiles_kernel<DesSrc>
-            <<<static_cast<int>(std::min<std::size_t>(blur_total, kSmCount * 8)), 256, 0, s>>>(des, at<uint2>(ws, blur_list),
+            <<<static_cast<int>(std::min<std::size_t>(blur_total, kSmCount * s2s3::kBlurCtasPerSm)), 256, 0, s>>>(des, at<uint2>(ws, blur_list),
                                                                                                  q + 1);
     mark();
     if (go(des_blocks[s2s3::kDescKind]))

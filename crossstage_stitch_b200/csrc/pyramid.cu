@@ -249,7 +249,7 @@ Status pyramid_detect_describe(const ImageView& image, const s2::Config& c, int 
             rank_topk_kernel<DetSrc><<<blocks(kHarrisKind), kHarrisThreads, 0, stream>>>(det);
             ++launches;
         }
-        blur_tiles_kernel<DesSrc><<<std::max(1, std::min(l.blur_first[n], kSmCount * 8)), 256, 0, stream>>>(
+        blur_tiles_kernel<DesSrc><<<std::max(1, std::min(l.blur_first[n], kSmCount * kBlurCtasPerSm)), 256, 0, stream>>>(
             des, at_offset<uint2>(ws, l.blur_list), queue + 1);
         ++launches;
     }

@@ -1045,30 +1045,46 @@ __global__ __launch_bounds__(256) void blur_kernel(const __grid_constant__ Src s
 // starts). A tile is staged with its reflect-101 halo: 16-byte loads for
 // interior tiles of 16-byte aligned images, reflected byte loads otherwise.
 static_assert(kBlurTileW == kFastTileW && kBlurTileH == kFastTileH, "blur tiles share the FAST tile staging");
+
+// Tile origin of blur-list entry e and whether it is staged by 16-byte copies
+// (an interior tile of a 16-byte aligned image: no reflected halo needed).
+__device__ __forceinline__ bool blur_tile_vec(const DescribeJob& j, unsigned tile, int* x0, int* y0) {
+    const int tiles_x = (j.width + kBlurTileW - 1) / kBlurTileW;
+    *y0 = (static_cast<int>(tile) / tiles_x) * kBlurTileH;
+    *x0 = (static_cast<int>(tile) % tiles_x) * kBlurTileW;
+    return ((reinterpret_cast<std::uintptr_t>(j.image) | static_cast<std::uintptr_t>(j.pitch)) & 15) == 0 &&
+           *x0 >= 16 && *x0 + 80 <= j.width && *y0 >= 4 && *y0 + kFastTileH + 4 <= j.height;
+}
+
+constexpr int kBlurCtasPerSm = 6;  // resident blur blocks per SM; the persistent grid is 148 x this
 template <class Src>
-__global__ __launch_bounds__(256, 8) void blur_tiles_kernel(const __grid_constant__ Src src, const uint2* list,
+__global__ __launch_bounds__(256, kBlurCtasPerSm) void blur_tiles_kernel(const __grid_constant__ Src src, const uint2* list,
                                                             const std::uint32_t* count) {
-    __shared__ __align__(16) std::uint8_t in[kFastInH][kInStride];  // rows y0-4 .., columns x0-16 ..
+    __shared__ __align__(16) std::uint8_t in2[2][kFastInH][kInStride];  // rows y0-4 .., columns x0-16 ..
     __shared__ __align__(16) float rows[kFastTileH + 6][kFastTileW];
     __shared__ std::size_t row_at[kFastInH];
     __shared__ int col_at[kInStride];
     const int tid = threadIdx.x;
     const int n = static_cast<int>(*count);
-    for (int i = blockIdx.x; i < n; i += gridDim.x) {
+    // interior tiles are copied asynchronously, the next one while this one is blurred
+    auto prefetch = [&](int i, std::uint8_t (*dst)[kInStride]) {
+        const uint2 e = list[i];
+        const DescribeJob jn = src.at(static_cast<int>(e.x));
+        int x0, y0;
+        if (blur_tile_vec(jn, e.y, &x0, &y0) && tid < kFastInH * (kInStride / 16)) {
+            const int r = tid / (kInStride / 16), q = tid - r * (kInStride / 16);
+            cp_async16(&dst[r][16 * q], jn.image + static_cast<std::size_t>(y0 - 4 + r) * jn.pitch + (x0 - 16 + 16 * q));
+        }
+    };
+    int buf = 0;
+    if (static_cast<int>(blockIdx.x) < n) prefetch(blockIdx.x, in2[0]);
+    for (int i = blockIdx.x; i < n; i += gridDim.x, buf ^= 1) {
+        std::uint8_t (*in)[kInStride] = in2[buf];
         const uint2 e = list[i];
         const DescribeJob j = src.at(static_cast<int>(e.x));
         const int W = j.width, H = j.height;
-        const int tiles_x = (W + kBlurTileW - 1) / kBlurTileW;
-        const int y0 = (static_cast<int>(e.y) / tiles_x) * kBlurTileH, x0 = (static_cast<int>(e.y) % tiles_x) * kBlurTileW;
-        const bool vec = ((reinterpret_cast<std::uintptr_t>(j.image) | static_cast<std::uintptr_t>(j.pitch)) & 15) == 0 &&
-                         x0 >= 16 && x0 + 80 <= W && y0 >= 4 && y0 + kFastTileH + 4 <= H;
-        if (vec) {
-            if (tid < kFastInH * (kInStride / 16)) {
-                const int r = tid / (kInStride / 16), q = tid - r * (kInStride / 16);
-                *reinterpret_cast<uint4*>(&in[r][16 * q]) = *reinterpret_cast<const uint4*>(
-                    j.image + static_cast<std::size_t>(y0 - 4 + r) * j.pitch + (x0 - 16 + 16 * q));
-            }
-        } else {
+        int x0, y0;
+        if (!blur_tile_vec(j, e.y, &x0, &y0)) {  // border tile or unaligned image: reflected byte loads
             if (tid < kFastInH) row_at[tid] = static_cast<std::size_t>(reflect101(y0 - 4 + tid, H)) * j.pitch;
             else if (tid < kFastInH + kInStride) col_at[tid - kFastInH] = reflect101(x0 - 16 + (tid - kFastInH), W);
             __syncthreads();
@@ -1081,7 +1097,9 @@ __global__ __launch_bounds__(256, 8) void blur_tiles_kernel(const __grid_constan
                     (static_cast<std::uint32_t>(row[col_at[b + 3]]) << 24);
             }
         }
+        cp_async_wait_all();
         __syncthreads();
+        if (i + static_cast<int>(gridDim.x) < n) prefetch(i + gridDim.x, in2[buf ^ 1]);
         // rows pass: image rows y0-3 .. y0+34, two rows x 4 outputs per item
         static_assert((kFastTileH + 6) % 2 == 0, "rows pass takes row pairs");
         for (int g = tid; g < (kFastTileH + 6) / 2 * (kFastTileW / 4); g += 256) {
