@@ -59,6 +59,11 @@ struct DetectJob {
     uint2* blur_list;
     std::uint32_t* blur_count;
     int job;  // this job's index in the describe table of the launch
+    // The next pyramid layer (null for the last layer built, or a single
+    // level): the FAST tiles of this layer write its pixels, resized from
+    // this layer (cv::resize INTER_LINEAR_EXACT on 8-bit images).
+    std::uint8_t* next;
+    int next_width, next_height, next_pitch;
     // launch bookkeeping
     int tiles_x, tiles, select_blocks, candidates;
     __host__ __device__ std::uint32_t* counters() const { return hist + 256; }
@@ -89,16 +94,6 @@ struct DescribeJob {
     const int* level_counts;
     int level;
     float scale;
-};
-
-// One pyramid layer: `dst` (dense) resized from `src` by fixed-point
-// bilinear interpolation (cv::resize INTER_LINEAR_EXACT on 8-bit images).
-struct ResizeJob {
-    const std::uint8_t* src;
-    int src_width, src_height, src_pitch;
-    std::uint8_t* dst;
-    int width, height, pitch;
-    int tiles_x, tiles;
 };
 
 // Per-image job passed by value.
@@ -190,7 +185,6 @@ constexpr int kSortChunk = 64;      // keys a warp sorts in registers (2 per lan
 constexpr int kBlurTileW = 64, kBlurTileH = 32;
 constexpr int kDescWarps = 8;
 constexpr int kEdge = 31;
-constexpr int kResizeTileW = 64, kResizeTileH = 64;  // widest tile; a job's tile_h may be smaller
 constexpr int kMaxLevels = 16;
 static_assert(kMaxLevels <= kMapKinds && kDetectKinds <= kMapKinds, "block map kinds");
 
@@ -302,6 +296,35 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// Source index and 8-bit weight of the right neighbour for destination
+// index v of a src -> dst linear resize: f = (v + 0.5) * scale - 0.5 in
+// double with scale = 1 / (dst / src), weight rint((f - floor f) * 256).
+// Indices left of the source (every index when src == 1) read pixel 0 with
+// weight 0, indices past the last interval read pixel src - 1 with weight 0.
+__device__ __forceinline__ double linear_exact_scale(int src, int dst) {
+    return 1.0 / (static_cast<double>(dst) / static_cast<double>(src));
+}
+
+__device__ __forceinline__ int2 linear_exact_tap(int v, int src, double scale) {
+    const double f = scale * (static_cast<double>(v) + 0.5) - 0.5;
+    const double fl = floor(f);
+    if (src == 1 || fl < 0.0) return make_int2(0, 0);
+    if (fl >= static_cast<double>(src - 1)) return make_int2(src - 1, 0);
+    return make_int2(static_cast<int>(fl), static_cast<int>(rint((f - fl) * 256.0)));
+}
+
+// The first destination index whose source tap is at least s0 (dst when
+// none is): the taps never decrease, so the destination pixels of a source
+// span [s0, s1) are [first_dst_at(s0), first_dst_at(s1)).
+__device__ __forceinline__ int first_dst_at(int s0, int src, int dst, double scale) {
+    if (s0 <= 0) return 0;
+    int v = static_cast<int>(ceil((static_cast<double>(s0) + 0.5) / scale - 0.5));
+    v = min(max(v, 0), dst);
+    while (v > 0 && linear_exact_tap(v - 1, src, scale).x >= s0) --v;
+    while (v < dst && linear_exact_tap(v, src, scale).x < s0) ++v;
+    return v;
+}
+
 // Stages rows y0-4 .. y0+35 and columns x0-16 .. x0+79 of the job's image in
 // `in` (byte c of row r = image (y0-4+r, x0-16+c)). The FAST test never reads
 // a position outside the image, so rows are clamped into it and the bytes of
@@ -343,15 +366,26 @@ __device__ __forceinline__ void stage_fast_tile(const DetectJob& j, int local, s
 // every job of the launch from a device queue (`*queue`, zero at launch; tile
 // t of `total` is looked up through the source's kFastKind entries), while
 // the next tile's bytes are copied into the other half of a double buffer.
-// The jobs of the current and the next tile sit in shared memory. Per tile:
+// The jobs of the current and the next tile sit in shared memory. A job with
+// a next pyramid layer also resizes: every pixel of the next layer whose
+// top-left source tap lies in the tile's 64x32 core is computed from the
+// staged bytes (its right and lower source neighbours are in the halo), so
+// each next-layer pixel is written by exactly one tile and the layers of a
+// pyramid are built by one FAST launch per layer depth. Per tile:
 //   1. the compass test on the tile plus a 1-pixel ring, 4 positions per
 //      thread in 16-bit lanes; groups with a survivor are listed so that full
 //      scores are computed on full warps;
 //   2. the survivors are scored (every other position scores 0);
 //   3. each survivor of the tile inside the 31-pixel edge margin that is a
 //      strict 3x3 maximum goes into the job's maxima list as
-//      (score << 32) | raster index, its score into the job's histogram.
-// No maxima map and no blur are written.
+//      (score << 32) | raster index, its score into the job's histogram;
+//      the next layer's pixels of the tile are written, each
+//        h(r, c) = src[r][c0] * (256 - wx) + src[r][c1] * wx   (< 2^16)
+//        out = (h(r0, c) * (256 - wy) + h(r1, c) * wy + 2^15) >> 16,
+//      the integer form of INTER_LINEAR_EXACT's 8-bit fixed-point horizontal
+//      pass followed by the vertical pass with one final rounding.
+// A layer without keypoints of its own (budget 0) only resizes. No maxima
+// map and no blur are written.
 template <class Src>
 __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(const __grid_constant__ Src src,
                                                                           std::uint32_t* queue, int total) {
@@ -363,6 +397,8 @@ __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(cons
     __shared__ std::uint64_t found[kTileMaxima];
     __shared__ DetectJob jobs[2];  // jobs of the tiles in in[0] and in[1] (kept here, not in registers)
     __shared__ int locals[2];
+    __shared__ int2 xtap[kFastTileW], ytap[kFastTileH];  // next-layer taps of the tile's pixels
+    __shared__ int span[4];                               // first column, columns, first row, rows
     __shared__ int n_cand, n_found, next;
     __shared__ std::uint32_t list_base;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -389,10 +425,25 @@ __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(cons
             if (t < total && !src.find(t, kFastKind, &jobs[buf ^ 1], &locals[buf ^ 1])) t = total;
             next = t;
         }
+        // the next-layer pixels of this tile: columns and rows whose source tap
+        // falls in the core [x0, x0 + 64) x [y0, y0 + 32)
+        if (tid < 4) {
+            int v = 0;
+            if (j.next) {
+                const bool col = tid < 2;
+                const int src_n = col ? W : H, dst_n = col ? j.next_width : j.next_height;
+                const int s0 = col ? x0 : y0, len = col ? kFastTileW : kFastTileH;
+                const double sc = linear_exact_scale(src_n, dst_n);
+                const int a = first_dst_at(s0, src_n, dst_n, sc);
+                v = (tid & 1) ? first_dst_at(s0 + len, src_n, dst_n, sc) - a : a;
+            }
+            span[tid] = v;
+        }
         // 1. compass test: thread (q, rb) takes positions 4q .. 4q+3 of rows rb,
         // rb + 15, rb + 30; groups with a survivor are listed as
         // (group << 4 | survivor bits)
         const std::uint32_t thr1 = static_cast<std::uint32_t>(j.threshold + 1) * 0x00010001u;
+        const bool detect = j.max_keypoints > 0;
         {
             constexpr int kRowSets = 256 / kScGroups;  // 15
             const int q = tid % kScGroups, rb = tid / kScGroups, c = 4 * q;
@@ -408,7 +459,7 @@ __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(cons
                 if (rb < kRowSets && r < kFastScH) {
                     *reinterpret_cast<std::uint32_t*>(&sc[r][c]) = 0u;
                     const int gy = y0 - 1 + r;
-                    if (colmask && gy >= 3 && gy < H - 3) {
+                    if (detect && colmask && gy >= 3 && gy < H - 3) {
                         const int w = q + 3;  // word holding halo columns c .. c+3 (bytes c+12 .. c+15)
                         const auto* mid = reinterpret_cast<const std::uint32_t*>(&cur[r + 3][0]);
                         const auto* bot = reinterpret_cast<const std::uint32_t*>(&cur[r + 6][0]);
@@ -445,6 +496,12 @@ __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(cons
         const int nt = next;
         if (nt < total) stage_fast_tile(jobs[buf ^ 1], locals[buf ^ 1], in[buf ^ 1]);
         const int nc = n_cand;
+        const int rx0 = span[0], rnx = span[1], ry0 = span[2], rny = span[3];
+        if (tid < rnx) {
+            xtap[tid] = linear_exact_tap(rx0 + tid, W, linear_exact_scale(W, j.next_width));
+        } else if (tid >= kFastTileW && tid - kFastTileW < rny) {
+            ytap[tid - kFastTileW] = linear_exact_tap(ry0 + tid - kFastTileW, H, linear_exact_scale(H, j.next_height));
+        }
         // 2. each warp expands its 32 survivor groups of a round into a
         // warp-local position list (warp scan of the counts) and scores it
         // 32 at a time
@@ -497,6 +554,18 @@ __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(cons
                     atomicAdd(&hist[v], 1u);
                 }
             }
+        }
+        // the next layer's pixels of this tile (source (x, y) is staged at
+        // cur[y - y0 + 4][x - x0 + 16]; x + 1 <= x0 + 64 and y + 1 <= y0 + 32)
+        for (int k = tid; k < rnx * rny; k += kFastThreads) {
+            const int r = k / rnx, c = k - r * rnx;
+            const int2 tx = xtap[c], ty = ytap[r];
+            const int ca = tx.x - x0 + 16, cb = min(tx.x + 1, W - 1) - x0 + 16;
+            const std::uint8_t* ra = cur[ty.x - y0 + 4];
+            const std::uint8_t* rb2 = cur[min(ty.x + 1, H - 1) - y0 + 4];
+            const int ha = ra[ca] * (256 - tx.y) + ra[cb] * tx.y, hb = rb2[ca] * (256 - tx.y) + rb2[cb] * tx.y;
+            const unsigned out = static_cast<unsigned>(ha * (256 - ty.y) + hb * ty.y + (1 << 15)) >> 16;
+            j.next[static_cast<std::size_t>(ry0 + r) * j.next_pitch + (rx0 + c)] = static_cast<std::uint8_t>(out);
         }
         __syncthreads();
         // the tile's maxima and histogram into the job's list and histogram
@@ -841,153 +910,6 @@ __global__ __launch_bounds__(kHarrisThreads) void rank_topk_kernel(const __grid_
         __syncthreads();
     }
     if (slot < n && rank < j.max_keypoints) write_keypoint(j, rank, key);
-}
-
-// ------------------------------------------------------ pyramid layers
-
-// Source index and 8-bit weight of the right neighbour for destination
-// index v of a src -> dst linear resize: f = (v + 0.5) * scale - 0.5 in
-// double with scale = 1 / (dst / src), weight rint((f - floor f) * 256).
-// Indices left of the source (every index when src == 1) read pixel 0 with
-// weight 0, indices past the last interval read pixel src - 1 with weight 0.
-__device__ __forceinline__ double linear_exact_scale(int src, int dst) {
-    return 1.0 / (static_cast<double>(dst) / static_cast<double>(src));
-}
-
-__device__ __forceinline__ int2 linear_exact_tap(int v, int src, double scale) {
-    const double f = scale * (static_cast<double>(v) + 0.5) - 0.5;
-    const double fl = floor(f);
-    if (src == 1 || fl < 0.0) return make_int2(0, 0);
-    if (fl >= static_cast<double>(src - 1)) return make_int2(src - 1, 0);
-    return make_int2(static_cast<int>(fl), static_cast<int>(rint((f - fl) * 256.0)));
-}
-
-// One block = one tile of 64 x kTileH (16..64) layer pixels:
-//   1. the tile's source window, bounded from float arithmetic with a pixel
-//      of slack per side, is staged in shared memory with 16-byte loads
-//      (while the taps are computed);
-//   2. per-column and per-row taps in shared memory (double, as above);
-//   3. each warp produces whole layer rows, each lane two adjacent outputs:
-//        h(r, c) = src[r][c0] * (256 - wx) + src[r][c1] * wx   (< 2^16)
-//        out = (h(r0, c) * (256 - wy) + h(r1, c) * wy + 2^15) >> 16,
-//      the integer form of the 8-bit fixed-point horizontal pass followed
-//      by the vertical pass with one final rounding.
-// The exact taps are checked against the staged window; a tile outside it
-// (source image not 16-byte aligned, or a layer ratio above about 1.45)
-// reads the source bytes from global memory instead, with the same result.
-constexpr int kRawStride = 112;  // bytes of a staged source row: 7 chunks of 16
-template <int kTileH> __host__ __device__ constexpr int resize_raw_rows() { return kTileH * 3 / 2 + 6; }
-
-template <class Src, int kTileH>
-__global__ __launch_bounds__(256, 6) void resize_kernel(const __grid_constant__ Src src, int kind) {
-    static_assert(kTileH >= 16 && kTileH <= kResizeTileH && kTileH % 16 == 0, "resize tile height");
-    constexpr int th = kTileH, kRows = resize_raw_rows<kTileH>(), kChunks = kRawStride / 16;
-    __shared__ int2 xtap[kResizeTileW];
-    __shared__ int2 ytap[kTileH];
-    __shared__ __align__(16) std::uint8_t raw[kRows][kRawStride];
-    __shared__ double scale[2];
-    ResizeJob j;
-    int local;
-    if (!src.find(blockIdx.x, kind, &j, &local)) return;
-    const int y0 = (local / j.tiles_x) * th;
-    const int x0 = (local % j.tiles_x) * kResizeTileW;
-    const int t = threadIdx.x;
-    // 1. source window: rows ry0..ry1, 16-byte chunks from column rx0
-    const float fy = static_cast<float>(j.src_height) / static_cast<float>(j.height);
-    const float fx = static_cast<float>(j.src_width) / static_cast<float>(j.width);
-    const int last_y = min(y0 + th, j.height) - 1, last_x = min(x0 + kResizeTileW, j.width) - 1;
-    const int ry0 = max(__float2int_rd((y0 + 0.5f) * fy - 0.5f) - 1, 0);
-    const int ry1 = min(__float2int_rd((last_y + 0.5f) * fy - 0.5f) + 2, j.src_height - 1);
-    const int rx0 = max(__float2int_rd((x0 + 0.5f) * fx - 0.5f) - 1, 0) & ~15;
-    const int rx1 = min(__float2int_rd((last_x + 0.5f) * fx - 0.5f) + 2, j.src_width - 1);
-    const int nrow = ry1 - ry0 + 1;
-    const int nchunk = rx1 >= rx0 ? (rx1 - rx0) / 16 + 1 : 0;
-    const bool window = ((reinterpret_cast<std::uintptr_t>(j.src) | static_cast<std::uintptr_t>(j.src_pitch)) & 15) == 0 &&
-                        nrow > 0 && nrow <= kRows && nchunk > 0 && nchunk <= kChunks;  // block-uniform
-    if (window) {
-        // chunks start 16-byte aligned below src_width; one that reaches past
-        // the row's last pixel is read byte by byte (zeros beyond it)
-        const int n = nrow * nchunk;
-        for (int i0 = t; i0 < n; i0 += 2 * 256) {
-            uint4 v[2];
-#pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                const int i = i0 + 256 * k;
-                if (i < n) {
-                    const int r = i / nchunk, col = rx0 + 16 * (i - r * nchunk);
-                    const std::uint8_t* p = j.src + static_cast<std::size_t>(ry0 + r) * j.src_pitch + col;
-                    if (col + 16 <= j.src_width) {
-                        v[k] = __ldg(reinterpret_cast<const uint4*>(p));
-                    } else {
-                        std::uint32_t w[4] = {0u, 0u, 0u, 0u};
-#pragma unroll
-                        for (int b = 0; b < 16; ++b)
-                            if (col + b < j.src_width)
-                                w[b >> 2] |= static_cast<std::uint32_t>(__ldg(p + b)) << (8 * (b & 3));
-                        v[k] = make_uint4(w[0], w[1], w[2], w[3]);
-                    }
-                }
-            }
-#pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                const int i = i0 + 256 * k;
-                if (i < n) {
-                    const int r = i / nchunk, c = i - r * nchunk;
-                    *reinterpret_cast<uint4*>(&raw[r][16 * c]) = v[k];
-                }
-            }
-        }
-    }
-    // 2. taps
-    if (t == 0) scale[0] = linear_exact_scale(j.src_width, j.width);
-    if (t == 32) scale[1] = linear_exact_scale(j.src_height, j.height);
-    __syncthreads();
-    if (t < kResizeTileW) xtap[t] = linear_exact_tap(min(x0 + t, j.width - 1), j.src_width, scale[0]);
-    else if (t < kResizeTileW + th)
-        ytap[t - kResizeTileW] = linear_exact_tap(min(y0 + t - kResizeTileW, j.height - 1), j.src_height, scale[1]);
-    __syncthreads();
-    // taps are nondecreasing: the first and last give the tile's source span
-    const bool staged = window && ytap[0].x >= ry0 && min(ytap[th - 1].x + 1, j.src_height - 1) <= ry1 &&
-                        xtap[0].x >= rx0 && min(xtap[kResizeTileW - 1].x + 1, j.src_width - 1) < rx0 + 16 * nchunk;
-    // 3. warp w: rows w, w + 8, ...; lane l: columns 2l, 2l + 1
-    const int lane = t & 31;
-    const int c = 2 * lane, x = x0 + c;
-    if (x >= j.width) return;
-    const int2 t0 = xtap[c], t1 = xtap[c + 1];  // columns past the layer edge repeat the last tap
-    const int wx0 = t0.y, wx1 = t1.y;
-    int xa0 = t0.x, xb0 = min(t0.x + 1, j.src_width - 1), xa1 = t1.x, xb1 = min(t1.x + 1, j.src_width - 1);
-    if (staged) {
-        xa0 -= rx0; xb0 -= rx0; xa1 -= rx0; xb1 -= rx0;
-    }
-    for (int rr = t >> 5; rr < th; rr += 8) {
-        const int y = y0 + rr;
-        if (y >= j.height) break;
-        const int2 ty = ytap[rr];
-        const int ra = ty.x, rb = min(ty.x + 1, j.src_height - 1), wy = ty.y;
-        int pa[4], pb[4];  // rows ra, rb at xa0, xb0, xa1, xb1
-        if (staged) {
-            const std::uint8_t* A = raw[ra - ry0];
-            const std::uint8_t* B = raw[rb - ry0];
-            pa[0] = A[xa0]; pa[1] = A[xb0]; pa[2] = A[xa1]; pa[3] = A[xb1];
-            pb[0] = B[xa0]; pb[1] = B[xb0]; pb[2] = B[xa1]; pb[3] = B[xb1];
-        } else {
-            const std::uint8_t* A = j.src + static_cast<std::size_t>(ra) * j.src_pitch;
-            const std::uint8_t* B = j.src + static_cast<std::size_t>(rb) * j.src_pitch;
-            pa[0] = __ldg(A + xa0); pa[1] = __ldg(A + xb0); pa[2] = __ldg(A + xa1); pa[3] = __ldg(A + xb1);
-            pb[0] = __ldg(B + xa0); pb[1] = __ldg(B + xb0); pb[2] = __ldg(B + xa1); pb[3] = __ldg(B + xb1);
-        }
-        const int ha0 = pa[0] * (256 - wx0) + pa[1] * wx0, hb0 = pb[0] * (256 - wx0) + pb[1] * wx0;
-        const int ha1 = pa[2] * (256 - wx1) + pa[3] * wx1, hb1 = pb[2] * (256 - wx1) + pb[3] * wx1;
-        const unsigned v0 = static_cast<unsigned>(ha0 * (256 - wy) + hb0 * wy + (1 << 15)) >> 16;
-        const unsigned v1 = static_cast<unsigned>(ha1 * (256 - wy) + hb1 * wy + (1 << 15)) >> 16;
-        std::uint8_t* dst = j.dst + static_cast<std::size_t>(y) * j.pitch + x;
-        if (x + 1 < j.width && (reinterpret_cast<std::uintptr_t>(dst) & 1) == 0) {
-            *reinterpret_cast<std::uint16_t*>(dst) = static_cast<std::uint16_t>(v0 | (v1 << 8));
-        } else {
-            dst[0] = static_cast<std::uint8_t>(v0);
-            if (x + 1 < j.width) dst[1] = static_cast<std::uint8_t>(v1);
-        }
-    }
 }
 
 // ------------------------------------------------------------- S3 blur

@@ -25,7 +25,8 @@ def test_plan_build_twice_equals_fresh_plan():
         cmd = [nvcc, *native.ARCH, "-std=c++17", "-O1", "-I", str(native.CSRC), "-I", str(native.INCLUDE),
                str(ROOT / "tests" / "plan_rebuild_check.cu"), str(lib), "-o", str(exe),
                "-Xlinker", f"-rpath={lib.parent}"]
-        subprocess.run(cmd, check=True, capture_output=True, text=True)
+        built = subprocess.run(cmd, capture_output=True, text=True)
+        assert built.returncode == 0, built.stderr[-4000:]
         env = dict(os.environ, CUDA_VISIBLE_DEVICES="")
         out = subprocess.run([str(exe)], capture_output=True, text=True, env=env)
         assert out.returncode == 0, (out.returncode, out.stdout, out.stderr)
