@@ -129,6 +129,11 @@ void make_pyramid_jobs(const ImageView& im, const s2::Config& c, const Keypoints
             d.next_width = p.width[i + 1];
             d.next_height = p.height[i + 1];
             d.next_pitch = layer_pitch(p.width[i + 1]);
+            // the resize scale exactly as linear_exact_scale computes it
+            d.next_scale_x = 1.0 / (static_cast<double>(p.width[i + 1]) / static_cast<double>(p.width[i]));
+            d.next_scale_y = 1.0 / (static_cast<double>(p.height[i + 1]) / static_cast<double>(p.height[i]));
+            d.next_inv_x = static_cast<float>(p.width[i + 1]) / static_cast<float>(p.width[i]);
+            d.next_inv_y = static_cast<float>(p.height[i + 1]) / static_cast<float>(p.height[i]);
         }
         jobs->detect[i] = d;
         DescribeJob s = make_describe_job(layer, staged, desc, at_offset<void>(ws, l.describe[i]), l.des[i]);

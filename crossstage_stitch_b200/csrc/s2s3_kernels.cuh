@@ -64,6 +64,8 @@ struct DetectJob {
     // this layer (cv::resize INTER_LINEAR_EXACT on 8-bit images).
     std::uint8_t* next;
     int next_width, next_height, next_pitch;
+    double next_scale_x, next_scale_y;  // 1 / (next / this) per axis, as linear_exact_scale computes it
+    float next_inv_x, next_inv_y;       // next / this: estimates of a tile's first next-layer column and row
     // launch bookkeeping
     int tiles_x, tiles, select_blocks, candidates;
     __host__ __device__ std::uint32_t* counters() const { return hist + 256; }
@@ -313,18 +315,6 @@ __device__ __forceinline__ int2 linear_exact_tap(int v, int src, double scale) {
     return make_int2(static_cast<int>(fl), static_cast<int>(rint((f - fl) * 256.0)));
 }
 
-// The first destination index whose source tap is at least s0 (dst when
-// none is): the taps never decrease, so the destination pixels of a source
-// span [s0, s1) are [first_dst_at(s0), first_dst_at(s1)).
-__device__ __forceinline__ int first_dst_at(int s0, int src, int dst, double scale) {
-    if (s0 <= 0) return 0;
-    int v = static_cast<int>(ceil((static_cast<double>(s0) + 0.5) / scale - 0.5));
-    v = min(max(v, 0), dst);
-    while (v > 0 && linear_exact_tap(v - 1, src, scale).x >= s0) --v;
-    while (v < dst && linear_exact_tap(v, src, scale).x < s0) ++v;
-    return v;
-}
-
 // Stages rows y0-4 .. y0+35 and columns x0-16 .. x0+79 of the job's image in
 // `in` (byte c of row r = image (y0-4+r, x0-16+c)). The FAST test never reads
 // a position outside the image, so rows are clamped into it and the bytes of
@@ -386,6 +376,17 @@ __device__ __forceinline__ void stage_fast_tile(const DetectJob& j, int local, s
 //      pass followed by the vertical pass with one final rounding.
 // A layer without keypoints of its own (budget 0) only resizes. No maxima
 // map and no blur are written.
+// Candidate next-layer columns and rows of a tile: its owned ones lie within
+// [base, base + kNextCandX) x [base, base + kNextCandY), with base one below
+// the float estimate of the first one (at most 64 columns and 32 rows are
+// owned: the layer ratio is at least 1, so the taps of consecutive
+// destination indices differ).
+constexpr int kNextCandX = kFastTileW + 4, kNextCandY = kFastTileH + 4;
+constexpr int kCandYThread = 96;  // first thread computing row candidates
+__device__ __forceinline__ int next_base(int s0, float inv) {
+    return max(0, __float2int_rd((static_cast<float>(s0) + 0.5f) * inv - 0.5f) - 1);
+}
+
 template <class Src>
 __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(const __grid_constant__ Src src,
                                                                           std::uint32_t* queue, int total) {
@@ -397,10 +398,8 @@ __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(cons
     __shared__ std::uint64_t found[kTileMaxima];
     __shared__ DetectJob jobs[2];  // jobs of the tiles in in[0] and in[1] (kept here, not in registers)
     __shared__ int locals[2];
-    __shared__ int2 xtap[kFastTileW], ytap[kFastTileH];  // next-layer taps of the tile's pixels
-    __shared__ int span[4];                               // first column, columns, first row, rows
+    __shared__ int2 ctx[kNextCandX], cty[kNextCandY];  // candidate next-layer taps; x < 0: not this tile's
     __shared__ int n_cand, n_found, next;
-    __shared__ std::uint32_t list_base;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     hist[tid] = 0;
     if (tid == 0) {
@@ -420,24 +419,35 @@ __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(cons
         const int W = j.width, H = j.height;
         const int y0 = (local / j.tiles_x) * kFastTileH, x0 = (local % j.tiles_x) * kFastTileW;
         std::uint8_t (*cur)[kInStride] = in[buf];
+        // what the flush after the last barrier needs (jobs[buf] is refilled then)
+        std::uint32_t* const job_hist = j.hist;
+        std::uint64_t* const job_maxima = j.maxima;
+        const std::uint32_t job_max = static_cast<std::uint32_t>(j.max_maxima);
         if (tid == 0) {
             int t = static_cast<int>(atomicAdd(queue, 1u));
             if (t < total && !src.find(t, kFastKind, &jobs[buf ^ 1], &locals[buf ^ 1])) t = total;
             next = t;
         }
-        // the next-layer pixels of this tile: columns and rows whose source tap
-        // falls in the core [x0, x0 + 64) x [y0, y0 + 32)
-        if (tid < 4) {
-            int v = 0;
-            if (j.next) {
-                const bool col = tid < 2;
-                const int src_n = col ? W : H, dst_n = col ? j.next_width : j.next_height;
-                const int s0 = col ? x0 : y0, len = col ? kFastTileW : kFastTileH;
-                const double sc = linear_exact_scale(src_n, dst_n);
-                const int a = first_dst_at(s0, src_n, dst_n, sc);
-                v = (tid & 1) ? first_dst_at(s0 + len, src_n, dst_n, sc) - a : a;
+        // the tile's next-layer taps, one candidate column or row per thread
+        // (owned: the source tap lies in the core [x0, x0 + 64) x [y0, y0 + 32))
+        if (j.next) {
+            if (tid < kNextCandX) {
+                const int X = next_base(x0, j.next_inv_x) + tid;
+                int2 t = make_int2(-1, 0);
+                if (X < j.next_width) {
+                    const int2 tp = linear_exact_tap(X, W, j.next_scale_x);
+                    if (tp.x >= x0 && tp.x < x0 + kFastTileW) t = tp;
+                }
+                ctx[tid] = t;
+            } else if (tid >= kCandYThread && tid < kCandYThread + kNextCandY) {
+                const int Y = next_base(y0, j.next_inv_y) + (tid - kCandYThread);
+                int2 t = make_int2(-1, 0);
+                if (Y < j.next_height) {
+                    const int2 tp = linear_exact_tap(Y, H, j.next_scale_y);
+                    if (tp.x >= y0 && tp.x < y0 + kFastTileH) t = tp;
+                }
+                cty[tid - kCandYThread] = t;
             }
-            span[tid] = v;
         }
         // 1. compass test: thread (q, rb) takes positions 4q .. 4q+3 of rows rb,
         // rb + 15, rb + 30; groups with a survivor are listed as
@@ -491,17 +501,12 @@ __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(cons
                         static_cast<std::uint16_t>(((r * kScGroups + q) << 4) | bits);
             }
         }
-        __syncthreads();
+        __syncthreads();  // (1) survivors listed, next tile known
+        if (tid == 0) n_found = 0;  // every thread read the last tile's count before this barrier
         // the next tile's bytes travel while this one is scored
         const int nt = next;
         if (nt < total) stage_fast_tile(jobs[buf ^ 1], locals[buf ^ 1], in[buf ^ 1]);
         const int nc = n_cand;
-        const int rx0 = span[0], rnx = span[1], ry0 = span[2], rny = span[3];
-        if (tid < rnx) {
-            xtap[tid] = linear_exact_tap(rx0 + tid, W, linear_exact_scale(W, j.next_width));
-        } else if (tid >= kFastTileW && tid - kFastTileW < rny) {
-            ytap[tid - kFastTileW] = linear_exact_tap(ry0 + tid - kFastTileW, H, linear_exact_scale(H, j.next_height));
-        }
         // 2. each warp expands its 32 survivor groups of a round into a
         // warp-local position list (warp scan of the counts) and scores it
         // 32 at a time
@@ -533,7 +538,8 @@ __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(cons
             }
             __syncwarp();
         }
-        __syncthreads();
+        __syncthreads();  // (2) scores complete
+        if (tid == 0) n_cand = 0;  // every thread read it before barrier (1)
         // 3. strict 3x3 maxima inside the 31-pixel edge margin: only listed
         // survivors can score above 0, so only they are tested
         for (int i = tid; i < nc; i += kFastThreads) {
@@ -557,34 +563,39 @@ __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(cons
         }
         // the next layer's pixels of this tile (source (x, y) is staged at
         // cur[y - y0 + 4][x - x0 + 16]; x + 1 <= x0 + 64 and y + 1 <= y0 + 32)
-        for (int k = tid; k < rnx * rny; k += kFastThreads) {
-            const int r = k / rnx, c = k - r * rnx;
-            const int2 tx = xtap[c], ty = ytap[r];
-            const int ca = tx.x - x0 + 16, cb = min(tx.x + 1, W - 1) - x0 + 16;
-            const std::uint8_t* ra = cur[ty.x - y0 + 4];
-            const std::uint8_t* rb2 = cur[min(ty.x + 1, H - 1) - y0 + 4];
-            const int ha = ra[ca] * (256 - tx.y) + ra[cb] * tx.y, hb = rb2[ca] * (256 - tx.y) + rb2[cb] * tx.y;
-            const unsigned out = static_cast<unsigned>(ha * (256 - ty.y) + hb * ty.y + (1 << 15)) >> 16;
-            j.next[static_cast<std::size_t>(ry0 + r) * j.next_pitch + (rx0 + c)] = static_cast<std::uint8_t>(out);
-        }
-        __syncthreads();
-        // the tile's maxima and histogram into the job's list and histogram
-        const int nf = n_found;
-        if (tid == 0 && nf) list_base = atomicAdd(&j.counters()[kListed], static_cast<std::uint32_t>(nf));
-        __syncthreads();
-        for (int i = tid; i < nf; i += kFastThreads)
-            if (list_base + static_cast<std::uint32_t>(i) < static_cast<std::uint32_t>(j.max_maxima))
-                j.maxima[list_base + i] = found[i];
-        if (hist[tid]) {
-            atomicAdd(&j.hist[tid], hist[tid]);
-            hist[tid] = 0;
-        }
-        if (tid == 0) {
-            n_cand = 0;
-            n_found = 0;
+        if (j.next) {
+            const int bx = next_base(x0, j.next_inv_x), by = next_base(y0, j.next_inv_y);
+            for (int k = tid; k < kNextCandX * kNextCandY; k += kFastThreads) {
+                const int r = k / kNextCandX, c = k - r * kNextCandX;
+                const int2 tx = ctx[c], ty = cty[r];
+                if (tx.x < 0 || ty.x < 0) continue;
+                const int ca = tx.x - x0 + 16, cb = min(tx.x + 1, W - 1) - x0 + 16;
+                const std::uint8_t* ra = cur[ty.x - y0 + 4];
+                const std::uint8_t* rb2 = cur[min(ty.x + 1, H - 1) - y0 + 4];
+                const int ha = ra[ca] * (256 - tx.y) + ra[cb] * tx.y, hb = rb2[ca] * (256 - tx.y) + rb2[cb] * tx.y;
+                const unsigned out = static_cast<unsigned>(ha * (256 - ty.y) + hb * ty.y + (1 << 15)) >> 16;
+                j.next[static_cast<std::size_t>(by + r) * j.next_pitch + (bx + c)] = static_cast<std::uint8_t>(out);
+            }
         }
         cp_async_wait_all();
-        __syncthreads();
+        __syncthreads();  // (3) maxima listed, next tile staged
+        // the tile's maxima into the job's list, each warp one reservation
+        {
+            const int nf = n_found;
+            const int per = (nf + 7) >> 3, lo = min(nf, warp * per), hi = min(nf, lo + per);
+            if (lo < hi) {  // warp-uniform
+                std::uint32_t b = 0;
+                if (lane == 0) b = atomicAdd(job_hist + 256 + kListed, static_cast<std::uint32_t>(hi - lo));
+                b = __shfl_sync(0xffffffffu, b, 0);
+                for (int i = lo + lane; i < hi; i += 32)
+                    if (b + static_cast<std::uint32_t>(i - lo) < job_max) job_maxima[b + (i - lo)] = found[i];
+            }
+        }
+        // the histogram goes out when the next tile belongs to another job
+        if ((nt >= total || jobs[buf ^ 1].hist != job_hist) && hist[tid]) {
+            atomicAdd(job_hist + tid, hist[tid]);
+            hist[tid] = 0;
+        }
         tile = nt;
         buf ^= 1;
     }
