@@ -4,9 +4,8 @@
 // are unchanged, so results equal the per-pair calls bit for bit.
 //
 // With a scale pyramid (levels > 1) an image contributes one detect and one
-// describe job per layer. The FAST kernel runs once per layer depth over all
-// images; the tiles of layer l also write layer l + 1, so the layer chain
-// needs no launches of its own.
+// describe job per layer and one resize job per layer above the first; the
+// resize chain runs first, one launch per layer depth over all images.
 //
 // Workspace layout (one caller allocation, 256-byte aligned regions):
 //   counts   int[3n + L]  keypoint counts (2 per pair), match counts and the
@@ -31,6 +30,7 @@ namespace {
 
 using s2s3::DescribeJob;
 using s2s3::DetectJob;
+using s2s3::ResizeJob;
 using s4k::AcceptJob;
 using s4k::KnnJob;
 using s5k::PairIO;
@@ -55,7 +55,7 @@ bool small_image(const stitch_image_view& v) { return v.width <= 2 * s2::kEdge |
 // Device job tables, in this order inside the table block.
 enum Table {
     kDetJobs, kDetPrefix, kDesJobs, kDesPrefix, kKnnJobs, kKnnPrefix, kMergePrefix, kAccJobs, kAccPrefix,
-    kPairJobs, kPairPrefix, kSearchJobs, kSearchPrefix, kFitPrefix, kFastPrefix, kBlockMap, kTables
+    kPairJobs, kPairPrefix, kSearchJobs, kSearchPrefix, kFitPrefix, kRsJobs, kRsPrefix, kBlockMap, kTables
 };
 
 void set_attributes_once() {
@@ -109,7 +109,7 @@ Status Plan::build(int n_pairs, const stitch_pair_desc* p, int* bad_pair, bool a
         }
     }
     // 2. jobs per image: one single-level job, or one per pyramid layer
-    n_det = n_layers = 0;
+    n_det = n_layers = n_resize = 0;
     max_levels = 1;
     for (int i = 0; i < n; ++i) {
         auto& o = off[i];
@@ -131,6 +131,7 @@ Status Plan::build(int n_pairs, const stitch_pair_desc* p, int* bad_pair, bool a
             const int L = o.pyr[s].plan.levels;
             n_det += L;
             n_layers += L;
+            n_resize += L > 1 ? L - 1 : 0;
             max_levels = std::max(max_levels, L);
         }
     }
@@ -151,7 +152,7 @@ Status Plan::build(int n_pairs, const stitch_pair_desc* p, int* bad_pair, bool a
     Layout lay;
     const std::size_t counts = lay.take(3 * static_cast<std::size_t>(n) + n_layers, sizeof(int));
     hists = lay.take(static_cast<std::size_t>(std::max(n_det, 1)) * s2s3::kHistWords, sizeof(std::uint32_t));
-    queue = lay.take(s2s3::kMaxLevels + 1, sizeof(std::uint32_t));
+    queue = lay.take(2, sizeof(std::uint32_t));
     blur_flags = lay.take(std::max<std::size_t>(blur_total, 1), sizeof(std::uint32_t));
     zeroed = lay.cursor;
     blur_list = lay.take(std::max<std::size_t>(blur_total, 1), sizeof(uint2));
@@ -226,14 +227,13 @@ Status Plan::build(int n_pairs, const stitch_pair_desc* p, int* bad_pair, bool a
         if (rounds_at >= 2 * kSmCount) break;
     }
     search_blocks = static_cast<int>(rounds_at);
-    // block totals of every detect and describe kind, and the FAST tiles of
-    // every layer depth (kFastKind is mapped per depth), for the block -> job
-    // maps (the same per-job counts stage_tables lays out)
+    // block totals of every detect, describe and resize kind, for the block
+    // -> job maps (the same per-job counts stage_tables lays out)
     std::fill(std::begin(det_total), std::end(det_total), 0);
     std::fill(std::begin(des_total), std::end(des_total), 0);
-    std::fill(std::begin(fl_total), std::end(fl_total), 0);
+    std::fill(std::begin(rs_total), std::end(rs_total), 0);
     std::fill(std::begin(s45_total), std::end(s45_total), 0);
-    bool map_fits = alloc_staging && n_det < (1 << 16);
+    bool map_fits = alloc_staging && n_det < (1 << 16) && n_resize < (1 << 16);
     for (int i = 0; i < n; ++i)
         for (int s = 0; s < 2; ++s) {
             const int L = off[i].pyramid[s] ? off[i].pyr[s].plan.levels : 1;
@@ -241,12 +241,16 @@ Status Plan::build(int n_pairs, const stitch_pair_desc* p, int* bad_pair, bool a
                 int db[s2s3::kDetectKinds], sb[s2s3::kDescribeKinds];
                 job_blocks(i, s, l, db, sb);
                 for (int kind = 0; kind < s2s3::kDetectKinds; ++kind) {
-                    (kind == s2s3::kFastKind ? fl_total[l] : det_total[kind]) += db[kind];
+                    det_total[kind] += db[kind];
                     map_fits = map_fits && db[kind] < (1 << 16);
                 }
                 for (int kind = 0; kind < s2s3::kDescribeKinds; ++kind) {
                     des_total[kind] += sb[kind];
                     map_fits = map_fits && sb[kind] < (1 << 16);
+                }
+                if (l > 0) {
+                    rs_total[l - 1] += off[i].pyr[s].resize_tiles[l];
+                    map_fits = map_fits && off[i].pyr[s].resize_tiles[l] < (1 << 16);
                 }
             }
         }
@@ -259,9 +263,9 @@ Status Plan::build(int n_pairs, const stitch_pair_desc* p, int* bad_pair, bool a
         des_first[kind] = map_entries;
         map_entries += static_cast<std::size_t>(des_total[kind]);
     }
-    for (int l = 0; l < max_levels; ++l) {
-        fl_first[l] = map_entries;
-        map_entries += static_cast<std::size_t>(fl_total[l]);
+    for (int kind = 0; kind < resize_kinds(); ++kind) {
+        rs_first[kind] = map_entries;
+        map_entries += static_cast<std::size_t>(rs_total[kind]);
     }
     map_fits = map_fits && n_knn < (1 << 16) && n < (1 << 16);
     for (int i = 0; i < n; ++i) {
@@ -290,7 +294,7 @@ Status Plan::build(int n_pairs, const stitch_pair_desc* p, int* bad_pair, bool a
         offsets[t] = cur;
         cur += bytes;
     };
-    const std::size_t nd = static_cast<std::size_t>(n_det);
+    const std::size_t nd = static_cast<std::size_t>(n_det), nr = static_cast<std::size_t>(n_resize);
     put(kDetJobs, nd * sizeof(DetectJob));
     put(kDetPrefix, s2s3::kDetectKinds * (nd + 1) * sizeof(int));
     put(kDesJobs, nd * sizeof(DescribeJob));
@@ -305,7 +309,8 @@ Status Plan::build(int n_pairs, const stitch_pair_desc* p, int* bad_pair, bool a
     put(kSearchJobs, n * sizeof(SearchJob));
     put(kSearchPrefix, (n + 1) * sizeof(int));
     put(kFitPrefix, (n + 1) * sizeof(int));
-    put(kFastPrefix, static_cast<std::size_t>(max_levels) * (nd + 1) * sizeof(int));
+    put(kRsJobs, nr * sizeof(ResizeJob));
+    put(kRsPrefix, static_cast<std::size_t>(resize_kinds()) * (nr + 1) * sizeof(int));
     put(kBlockMap, block_map ? map_entries * sizeof(std::uint32_t) : 0);
     table_bytes = cur;
     tables = lay.take(table_bytes, 1);
@@ -386,15 +391,17 @@ Status Plan::stage_tables(void* ws) {
     auto* rj = reinterpret_cast<SearchJob*>(T + offsets[kSearchJobs]);
     auto* rp = reinterpret_cast<int*>(T + offsets[kSearchPrefix]);
     auto* fp = reinterpret_cast<int*>(T + offsets[kFitPrefix]);
-    auto* fl = reinterpret_cast<int*>(T + offsets[kFastPrefix]);  // FAST tile prefix of each layer depth
+    auto* zj = reinterpret_cast<ResizeJob*>(T + offsets[kRsJobs]);
+    auto* zp = reinterpret_cast<int*>(T + offsets[kRsPrefix]);
     std::uint32_t* hist_base = at<std::uint32_t>(ws, hists);
     std::uint32_t* mark_base = at<std::uint32_t>(ws, blur_flags);
     uint2* list = at<uint2>(ws, blur_list);
-    std::uint32_t* list_count = at<std::uint32_t>(ws, queue) + s2s3::kMaxLevels;
+    std::uint32_t* list_count = at<std::uint32_t>(ws, queue) + 1;
     int* layer_counts = at<int>(ws, 0) + 3 * static_cast<std::size_t>(n);
-    const int nd = n_det;
+    const int nd = n_det, nr = n_resize, rkinds = resize_kinds();
     int run_det[s2s3::kDetectKinds] = {}, run_des[s2s3::kDescribeKinds] = {};
-    int run_fl[s2s3::kMaxLevels] = {};
+    int run_rs[s2s3::kMaxLevels] = {};
+    int rjob = 0;
     std::uint32_t* bmap = block_map ? reinterpret_cast<std::uint32_t*>(T + offsets[kBlockMap]) : nullptr;
     bool map_ok = true;  // every map entry lands inside its kind's range
     auto fill_map = [&](std::size_t first, int run, int total, int job, int blocks) {
@@ -406,21 +413,15 @@ Status Plan::stage_tables(void* ws) {
         for (int b = 0; b < blocks; ++b)
             bmap[first + static_cast<std::size_t>(run + b)] = (static_cast<std::uint32_t>(job) << 16) | b;
     };
-    // job idx at layer depth `level`: its FAST tiles go to that depth's map and
-    // prefix (one FAST launch per depth), its other kinds to the detect ones
-    auto add_job = [&](int idx, int level, const DetectJob& d, const DescribeJob& e,
-                       const int (&db)[s2s3::kDetectKinds], const int (&sb)[s2s3::kDescribeKinds]) {
+    auto add_job = [&](int idx, const DetectJob& d, const DescribeJob& e, const int (&db)[s2s3::kDetectKinds],
+                       const int (&sb)[s2s3::kDescribeKinds]) {
         dj[idx] = d;
         sj[idx] = e;
         for (int kind = 0; kind < s2s3::kDetectKinds; ++kind) {
-            if (kind == s2s3::kFastKind) continue;
             dp[kind * (nd + 1) + idx] = run_det[kind];
             fill_map(det_first[kind], run_det[kind], det_total[kind], idx, db[kind]);
             run_det[kind] += db[kind];
         }
-        for (int l = 0; l < max_levels; ++l) fl[l * (nd + 1) + idx] = run_fl[l];
-        fill_map(fl_first[level], run_fl[level], fl_total[level], idx, db[s2s3::kFastKind]);
-        run_fl[level] += db[s2s3::kFastKind];
         for (int kind = 0; kind < s2s3::kDescribeKinds; ++kind) {
             sp[kind * (nd + 1) + idx] = run_des[kind];
             fill_map(des_first[kind], run_des[kind], des_total[kind], idx, sb[kind]);
@@ -452,7 +453,15 @@ Status Plan::stage_tables(void* ws) {
                 for (int l = 0; l < pl.plan.levels; ++l) {
                     int db[s2s3::kDetectKinds], sb[s2s3::kDescribeKinds];
                     job_blocks(i, s, l, db, sb);
-                    add_job(idx + l, l, pjobs.detect[l], pjobs.describe[l], db, sb);
+                    add_job(idx + l, pjobs.detect[l], pjobs.describe[l], db, sb);
+                }
+                for (int l = 1; l < pl.plan.levels; ++l, ++rjob) {
+                    zj[rjob] = pjobs.resize[l];
+                    fill_map(rs_first[l - 1], run_rs[l - 1], rs_total[l - 1], rjob, pl.resize_tiles[l]);
+                    for (int kind = 0; kind < rkinds; ++kind) {
+                        zp[kind * (nr + 1) + rjob] = run_rs[kind];
+                        run_rs[kind] += kind == l - 1 ? pl.resize_tiles[l] : 0;
+                    }
                 }
                 continue;
             }
@@ -466,7 +475,7 @@ Status Plan::stage_tables(void* ws) {
             job_blocks(i, s, 0, db, sb);
             const DescribeJob e =
                 s2s3::make_describe_job(view(im), kps[s], desc[s], at<void>(ws, o.s3ws[s]), o.des[s]);
-            add_job(idx, 0, d, e, db, sb);
+            add_job(idx, d, e, db, sb);
         }
         // S4 (forward, then reverse when the mutual check is on)
         auto* fwd = at<s4k::Top2>(ws, o.s4ws + o.match.forward);
@@ -524,15 +533,15 @@ Status Plan::stage_tables(void* ws) {
     if (bmap) {  // the maps must cover exactly the blocks of every launch
         for (int kind = 0; kind < s2s3::kDetectKinds; ++kind) map_ok = map_ok && run_det[kind] == det_total[kind];
         for (int kind = 0; kind < s2s3::kDescribeKinds; ++kind) map_ok = map_ok && run_des[kind] == des_total[kind];
-        for (int l = 0; l < max_levels; ++l) map_ok = map_ok && run_fl[l] == fl_total[l];
+        for (int kind = 0; kind < rkinds; ++kind) map_ok = map_ok && run_rs[kind] == rs_total[kind];
         map_ok = map_ok && run_knn == s45_total[kMapKnn] && run_merge == s45_total[kMapMerge] &&
                  run_search == s45_total[kMapSearch] && run_fit == s45_total[kMapFit];
         if (!map_ok) return Status::INVALID_ARGUMENT;
     }
     for (int kind = 0; kind < s2s3::kDetectKinds; ++kind) dp[kind * (nd + 1) + nd] = run_det[kind];
     for (int kind = 0; kind < s2s3::kDescribeKinds; ++kind) sp[kind * (nd + 1) + nd] = run_des[kind];
-    for (int l = 0; l < max_levels; ++l) fl[l * (nd + 1) + nd] = run_fl[l];
-    for (int l = 0; l < s2s3::kMaxLevels; ++l) fl_blocks[l] = l < max_levels ? run_fl[l] : 0;
+    for (int kind = 0; kind < rkinds; ++kind) zp[kind * (nr + 1) + nr] = run_rs[kind];
+    for (int kind = 0; kind < s2s3::kMaxLevels; ++kind) rs_blocks[kind] = kind < rkinds ? run_rs[kind] : 0;
     kp[n_knn] = run_knn;
     mp[n_knn] = run_merge;
     ap[n] = n;
@@ -570,10 +579,13 @@ Status Plan::enqueue(void* ws, std::size_t bytes, stitch_homography_result* host
 
     using DetSrc = s2s3::JobTable<DetectJob>;
     using DesSrc = s2s3::JobTable<DescribeJob>;
+    using RsSrc = s2s3::JobTable<ResizeJob>;
     DetSrc det{reinterpret_cast<const DetectJob*>(T + offsets[kDetJobs]),
                reinterpret_cast<const int*>(T + offsets[kDetPrefix]), n_det};
     DesSrc des{reinterpret_cast<const DescribeJob*>(T + offsets[kDesJobs]),
                reinterpret_cast<const int*>(T + offsets[kDesPrefix]), n_det};
+    RsSrc rs{reinterpret_cast<const ResizeJob*>(T + offsets[kRsJobs]),
+             reinterpret_cast<const int*>(T + offsets[kRsPrefix]), n_resize};
     if (block_map) {
         const auto* M = reinterpret_cast<const std::uint32_t*>(T + offsets[kBlockMap]);
         for (int kind = 0; kind < s2s3::kDetectKinds; ++kind) {
@@ -583,6 +595,10 @@ Status Plan::enqueue(void* ws, std::size_t bytes, stitch_homography_result* host
         for (int kind = 0; kind < s2s3::kDescribeKinds; ++kind) {
             des.map[kind] = M + des_first[kind];
             des.map_blocks[kind] = des_total[kind];
+        }
+        for (int kind = 0; kind < resize_kinds(); ++kind) {
+            rs.map[kind] = M + rs_first[kind];
+            rs.map_blocks[kind] = rs_total[kind];
         }
     }
     int launches = 1;  // zero_words_kernel
@@ -601,26 +617,14 @@ Status Plan::enqueue(void* ws, std::size_t bytes, stitch_homography_result* host
         ++next_mark;
     };
     mark();  // tables uploaded, counts cleared
-    mark();  // (the pyramid layers are built by the FAST launches)
-    // FAST, one persistent launch per layer depth over every image: the tiles
-    // of depth l also write layer l + 1. Each launch reads its depth's map
-    // (or prefix) as the kFastKind entries and takes tiles from its own queue.
-    static_assert(s2s3::kFastKind == 0, "the per-depth prefix stands in for the kind-0 prefix");
-    std::uint32_t* q = at<std::uint32_t>(ws, queue);  // FAST tile queue per depth, then the blur-list count
-    int tiles = 0;
-    for (int l = 0; l < max_levels; ++l) {
-        const int t = fl_blocks[l];
-        tiles += t;
-        if (!go(t)) continue;
-        DetSrc dl = det;
-        dl.prefix = reinterpret_cast<const int*>(T + offsets[kFastPrefix]) + static_cast<std::size_t>(l) * (n_det + 1);
-        if (block_map) {
-            dl.map[s2s3::kFastKind] = reinterpret_cast<const std::uint32_t*>(T + offsets[kBlockMap]) + fl_first[l];
-            dl.map_blocks[s2s3::kFastKind] = fl_total[l];
-        }
-        s2s3::fast_kernel<DetSrc><<<std::min(t, kSmCount * s2s3::kFastCtasPerSm), s2s3::kFastThreads, 0, s>>>(
-            dl, q + l, t);
-    }
+    for (int kind = 0; kind + 1 < max_levels; ++kind)  // layer kind + 1 of every pyramid image
+        if (go(rs_blocks[kind])) s2s3::resize_kernel<RsSrc, s2s3::kResizeTileH><<<rs_blocks[kind], 256, 0, s>>>(rs, kind);
+    mark();
+    std::uint32_t* q = at<std::uint32_t>(ws, queue);  // FAST tile queue, then the blur-list count
+    const int tiles = det_blocks[s2s3::kFastKind];
+    if (go(tiles))
+        s2s3::fast_kernel<DetSrc><<<std::min(tiles, kSmCount * s2s3::kFastCtasPerSm), s2s3::kFastThreads, 0, s>>>(
+            det, q, tiles);
     mark();
     if (go(det_blocks[s2s3::kSelectKind])) {
         s2s3::select_kernel<DetSrc><<<det_blocks[s2s3::kSelectKind], 256, 0, s>>>(det);
@@ -638,8 +642,8 @@ Status Plan::enqueue(void* ws, std::size_t bytes, stitch_homography_result* host
     mark();
     if (go(tiles > 0 && blur_total > 0 ? 1 : 0))
         s2s3::blur_tiles_kernel<DesSrc>
-            <<<static_cast<int>(std::min<std::size_t>(blur_total, kSmCount * s2s3::kBlurCtasPerSm)), 256, 0, s>>>(
-                des, at<uint2>(ws, blur_list), q + s2s3::kMaxLevels);
+            <<<static_cast<int>(std::min<std::size_t>(blur_total, kSmCount * s2s3::kBlurCtasPerSm)), 256, 0, s>>>(des, at<uint2>(ws, blur_list),
+                                                                                                 q + 1);
     mark();
     if (go(des_blocks[s2s3::kDescKind]))
         s2s3::describe_kernel<DesSrc><<<des_blocks[s2s3::kDescKind], s2s3::kDescWarps * 32, 0, s>>>(des);

@@ -41,17 +41,17 @@ public:
     // launch shapes
     int n_det = 0;     // detect/describe jobs: one per image, one per layer of a pyramid image
     int n_layers = 0;  // layer counts kept after the 3n image and match counts
+    int n_resize = 0;  // resize jobs (layers 1.. of every pyramid image)
     int max_levels = 1;
     // zeroed head of the workspace: counts, then FAST histograms and counters
-    // u32[n_det][kHistWords], the FAST tile queue of each layer depth and the
-    // blur-list count (kMaxLevels + 1 words), the blur-tile flags
-    // u32[blur_total]; `zeroed` bytes in all.
+    // u32[n_det][kHistWords], the FAST tile queue and blur-list count (2
+    // words), the blur-tile flags u32[blur_total]; `zeroed` bytes in all.
     // The blur list uint2[blur_total] follows the head.
     std::size_t hists = 0, queue = 0, blur_flags = 0, zeroed = 0, blur_list = 0;
     std::size_t blur_total = 0;
     int det_blocks[s2s3::kDetectKinds] = {};
     int des_blocks[s2s3::kDescribeKinds] = {};
-    int fl_blocks[s2s3::kMaxLevels] = {};  // FAST tiles of layer depth l (one persistent launch each)
+    int rs_blocks[s2s3::kMaxLevels] = {};  // resize launch of layer kind + 1
     int knn_blocks = 0, merge_blocks = 0, n_knn = 0;
     int search_blocks = 0, fit_blocks = 0;
     int sort_smem = 0, search_smem = 0;
@@ -70,13 +70,13 @@ public:
     void* graph_exec = nullptr;  // cudaGraphExec_t
     unsigned char* graph_tables = nullptr;
     std::size_t offsets[20] = {};  // table offsets inside the table block
-    // block -> job maps of the detect, describe and per-layer FAST kinds (one table,
+    // block -> job maps of the detect, describe and resize kinds (one table,
     // kinds one after the other; see s2s3::JobTable), when every job index
     // and block within a job fits 16 bits and the plan owns its staging
     bool block_map = false;
-    int det_total[s2s3::kDetectKinds] = {}, des_total[s2s3::kDescribeKinds] = {}, fl_total[s2s3::kMaxLevels] = {};
+    int det_total[s2s3::kDetectKinds] = {}, des_total[s2s3::kDescribeKinds] = {}, rs_total[s2s3::kMaxLevels] = {};
     std::size_t det_first[s2s3::kDetectKinds] = {}, des_first[s2s3::kDescribeKinds] = {},
-                fl_first[s2s3::kMaxLevels] = {};  // entry index of each kind's map
+                rs_first[s2s3::kMaxLevels] = {};  // entry index of each kind's map
     // and of the S4/S5 launches: knn, knn merge, accept, pair (prepare and
     // finish), search, fit
     enum { kMapKnn, kMapMerge, kMapAccept, kMapPair, kMapSearch, kMapFit, kMapS45 };
@@ -86,6 +86,7 @@ public:
     bool marked = false;
 
     ~Plan();
+    int resize_kinds() const { return max_levels > 1 ? max_levels - 1 : 1; }
     // Validates the pairs and lays out the workspace (host work only), then,
     // with alloc_staging, allocates the pinned staging of the job tables.
     // Every count, total, offset and block-map total it derives is reset and

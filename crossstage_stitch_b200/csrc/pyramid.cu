@@ -1,7 +1,6 @@
-// Scale-pyramid S2/S3 of one image: one FAST launch per layer, which also
-// writes the next layer (resized from the tiles it has staged), so the layer
-// chain costs no pass of its own; then the rest of S2 and S3 of every layer
-// in the same launches (the layers' jobs travel as kernel parameters), each
+// Scale-pyramid S2/S3 of one image: layers 1..L-1 resized in a chain, then
+// S2 and S3 of every layer in the same launches (the layers' jobs travel as
+// kernel parameters; the FAST kernel also writes each layer's blur), each
 // layer's keypoints and descriptors written by the describe kernel straight
 // into the image's concatenated outputs in level-0 coordinates.
 //
@@ -59,11 +58,13 @@ LevelPlan level_plan(int w, int h, int k, int levels, float sf) {
 // Rows of the layer images start on 16-byte boundaries.
 int layer_pitch(int width) { return (width + 15) / 16 * 16; }
 
-bool pyramid_layout(int w, int h, int k, int levels, float sf, PyramidLayout* out) {
+bool pyramid_layout(int w, int h, int k, int levels, float sf, PyramidLayout* out, int resize_tile_h) {
     if (!out || !valid_image_shape(w, h) || k < 0 || k > INT_MAX / s2::kCandidateFactor ||
         !valid_pyramid(levels, sf))
         return false;
     PyramidLayout l{};
+    if (resize_tile_h < 16 || resize_tile_h > kResizeTileH || resize_tile_h % 16) return false;
+    l.resize_tile_h = resize_tile_h;
     l.plan = level_plan(w, h, k, levels, sf);
     const int n = l.plan.levels;
     // blur tiles of every layer (the describe layout's tile grid)
@@ -74,7 +75,7 @@ bool pyramid_layout(int w, int h, int k, int levels, float sf, PyramidLayout* ou
     Layout lay;
     l.counts = lay.take(static_cast<std::size_t>(n > 0 ? n : 1), sizeof(int));
     l.hists = lay.take(static_cast<std::size_t>(n > 0 ? n : 1) * kHistWords, sizeof(std::uint32_t));
-    l.queue = lay.take(kMaxLevels + 1, sizeof(std::uint32_t));  // FAST tile queue per layer, blur-list count
+    l.queue = lay.take(2, sizeof(std::uint32_t));  // FAST tile queue, blur-list count
     l.marks = lay.take(blur_total, sizeof(std::uint32_t));
     l.zeroed_bytes = lay.cursor;
     l.blur_list = lay.take(blur_total, sizeof(uint2));
@@ -89,14 +90,9 @@ bool pyramid_layout(int w, int h, int k, int levels, float sf, PyramidLayout* ou
             return false;
         l.detect[i] = lay.take(l.det[i].total, 1);
         l.describe[i] = lay.take(l.des[i].total, 1);
-        l.fast_tiles[i] = 0;
+        l.resize_tiles[i] = i ? ceil_div(lw, kResizeTileW) * ceil_div(lh, resize_tile_h) : 0;
     }
     if (!lay.ok) return false;
-    bool later = false;  // some layer at or after i has keypoints
-    for (int i = n - 1; i >= 0; --i) {
-        later = later || l.plan.budget[i] > 0;
-        l.fast_tiles[i] = later ? l.det[i].tiles : 0;
-    }
     l.total = lay.cursor;
     *out = l;
     return true;
@@ -113,6 +109,18 @@ void make_pyramid_jobs(const ImageView& im, const s2::Config& c, const Keypoints
             layer.width = p.width[i];
             layer.height = p.height[i];
             layer.pitch_bytes = layer_pitch(p.width[i]);
+            ResizeJob r{};
+            r.src = i == 1 ? im.data : at_offset<std::uint8_t>(ws, l.image[i - 1]);
+            r.src_width = p.width[i - 1];
+            r.src_height = p.height[i - 1];
+            r.src_pitch = i == 1 ? im.pitch_bytes : layer_pitch(p.width[i - 1]);
+            r.dst = const_cast<std::uint8_t*>(layer.data);
+            r.width = p.width[i];
+            r.height = p.height[i];
+            r.pitch = layer.pitch_bytes;
+            r.tiles_x = ceil_div(p.width[i], kResizeTileW);
+            r.tiles = l.resize_tiles[i];
+            jobs->resize[i] = r;
         }
         s2::Config lc = c;
         lc.max_keypoints = p.budget[i];
@@ -124,17 +132,6 @@ void make_pyramid_jobs(const ImageView& im, const s2::Config& c, const Keypoints
         d.blur_list = sh.blur_list;
         d.blur_count = sh.blur_count;
         d.job = sh.job0 + i;
-        if (i + 1 < p.levels && l.fast_tiles[i + 1] > 0) {  // this layer's tiles build the next one
-            d.next = at_offset<std::uint8_t>(ws, l.image[i + 1]);
-            d.next_width = p.width[i + 1];
-            d.next_height = p.height[i + 1];
-            d.next_pitch = layer_pitch(p.width[i + 1]);
-            // the resize scale exactly as linear_exact_scale computes it
-            d.next_scale_x = 1.0 / (static_cast<double>(p.width[i + 1]) / static_cast<double>(p.width[i]));
-            d.next_scale_y = 1.0 / (static_cast<double>(p.height[i + 1]) / static_cast<double>(p.height[i]));
-            d.next_inv_x = static_cast<float>(p.width[i + 1]) / static_cast<float>(p.width[i]);
-            d.next_inv_y = static_cast<float>(p.height[i + 1]) / static_cast<float>(p.height[i]);
-        }
         jobs->detect[i] = d;
         DescribeJob s = make_describe_job(layer, staged, desc, at_offset<void>(ws, l.describe[i]), l.des[i]);
         s.response = staged.response;
@@ -152,7 +149,7 @@ void make_pyramid_jobs(const ImageView& im, const s2::Config& c, const Keypoints
 void pyramid_detect_blocks(const PyramidLayout& l, int i, int (&blocks)[kDetectKinds]) {
     const bool active = i < l.plan.levels && l.plan.budget[i] > 0;
     const DetectLayout& d = l.det[i];
-    blocks[kFastKind] = i < l.plan.levels ? l.fast_tiles[i] : 0;
+    blocks[kFastKind] = active ? d.tiles : 0;
     blocks[kSelectKind] = active ? d.select_blocks : 0;
     blocks[kHarrisKind] = active ? ceil_div(d.candidates, kHarrisThreads) : 0;
     blocks[kSortKind] = active ? 1 : 0;
@@ -190,7 +187,7 @@ Status pyramid_workspace_bytes(int w, int h, const s2::Config& c, int levels, fl
     if (!valid_detect_config(c) || !valid_image_shape(w, h) || !valid_pyramid(levels, sf))
         return Status::INVALID_ARGUMENT;
     PyramidLayout l;
-    if (!pyramid_layout(w, h, c.max_keypoints, levels, sf, &l)) return Status::INVALID_ARGUMENT;
+    if (!pyramid_layout(w, h, c.max_keypoints, levels, sf, &l, kSingleResizeTileH)) return Status::INVALID_ARGUMENT;
     *bytes = l.total;
     return Status::OK;
 }
@@ -204,7 +201,7 @@ Status pyramid_detect_describe(const ImageView& image, const s2::Config& c, int 
         desc.dim != s3::kDescriptorBytes || desc.row_stride_bytes < s3::kDescriptorBytes)
         return Status::INVALID_ARGUMENT;
     PyramidLayout l;
-    if (!pyramid_layout(image.width, image.height, c.max_keypoints, levels, sf, &l))
+    if (!pyramid_layout(image.width, image.height, c.max_keypoints, levels, sf, &l, kSingleResizeTileH))
         return Status::INVALID_ARGUMENT;
     if (!ws || !aligned(ws, kWorkspaceAlign)) return Status::INVALID_ARGUMENT;
     if (ws_bytes < l.total) return Status::INSUFFICIENT_WORKSPACE;
@@ -217,10 +214,14 @@ Status pyramid_detect_describe(const ImageView& image, const s2::Config& c, int 
     PyramidJobs jobs;
     std::uint32_t* queue = at_offset<std::uint32_t>(ws, l.queue);
     const PyramidShared sh{at_offset<int>(ws, l.counts), at_offset<std::uint32_t>(ws, l.hists),
-                           at_offset<std::uint32_t>(ws, l.marks), at_offset<uint2>(ws, l.blur_list),
-                           queue + kMaxLevels, 0};
+                           at_offset<std::uint32_t>(ws, l.marks), at_offset<uint2>(ws, l.blur_list), queue + 1, 0};
     make_pyramid_jobs(image, c, out, desc, ws, l, sh, &jobs);
     int launches = 0;
+    for (int i = 1; i < n; ++i) {
+        resize_kernel<OneJob<ResizeJob>, kSingleResizeTileH>
+            <<<l.resize_tiles[i], 256, 0, stream>>>(OneJob<ResizeJob>{jobs.resize[i]}, 0);
+        ++launches;
+    }
     DetSrc det{};
     DesSrc des{};
     det.n = des.n = n;
@@ -237,25 +238,19 @@ Status pyramid_detect_describe(const ImageView& image, const s2::Config& c, int 
     }
     auto blocks = [&](int kind) { return det.first[kind][n]; };
     if (blocks(kFastKind)) {
-        // one launch per layer, in order: layer i's tiles write layer i + 1
-        for (int i = 0; i < n; ++i) {
-            if (!l.fast_tiles[i]) continue;
-            fast_kernel<OneJob<DetectJob>>
-                <<<std::min(l.fast_tiles[i], kSmCount * kFastCtasPerSm), kFastThreads, 0, stream>>>(
-                    OneJob<DetectJob>{jobs.detect[i]}, queue + i, l.fast_tiles[i]);
-            ++launches;
-        }
+        fast_kernel<DetSrc><<<std::min(blocks(kFastKind), kSmCount * kFastCtasPerSm), kFastThreads, 0, stream>>>(
+            det, queue, blocks(kFastKind));
         select_kernel<DetSrc><<<blocks(kSelectKind), 256, 0, stream>>>(det);
         ties_kernel<DetSrc><<<blocks(kSortKind), kTieThreads, 0, stream>>>(det);
         harris_kernel<DetSrc><<<blocks(kHarrisKind), kHarrisThreads, 0, stream>>>(det);
         sort_topk_kernel<DetSrc><<<blocks(kSortKind), kSortThreads, sort_smem_bytes(max_cand), stream>>>(det);
-        launches += 4;
+        launches += 5;
         if (max_cand > kSortCap) {
             rank_topk_kernel<DetSrc><<<blocks(kHarrisKind), kHarrisThreads, 0, stream>>>(det);
             ++launches;
         }
         blur_tiles_kernel<DesSrc><<<std::max(1, std::min(l.blur_first[n], kSmCount * kBlurCtasPerSm)), 256, 0, stream>>>(
-            des, at_offset<uint2>(ws, l.blur_list), queue + kMaxLevels);
+            des, at_offset<uint2>(ws, l.blur_list), queue + 1);
         ++launches;
     }
     if (des.first[kDescKind][n]) {

@@ -65,13 +65,19 @@ struct PyramidLayout {
     std::size_t detect[kMaxLevels], describe[kMaxLevels];
     DetectLayout det[kMaxLevels];
     DescribeLayout des[kMaxLevels];
-    int fast_tiles[kMaxLevels];  // FAST tiles of layer l (0 when neither it nor a later layer has keypoints)
+    int resize_tiles[kMaxLevels];
+    int resize_tile_h;  // output rows per resize block
     std::size_t total;
 };
 
-bool pyramid_layout(int w, int h, int k, int levels, float scale_factor, PyramidLayout* out);
+// resize_tile_h: 64 rows per resize block when many images share a launch;
+// a single image's pyramid (kSingleResizeTileH) takes 16 to fill the GPU.
+constexpr int kSingleResizeTileH = 16;
+bool pyramid_layout(int w, int h, int k, int levels, float scale_factor, PyramidLayout* out,
+                    int resize_tile_h = kResizeTileH);
 
 struct PyramidJobs {
+    ResizeJob resize[kMaxLevels];  // entries 1 .. levels-1
     DetectJob detect[kMaxLevels];
     DescribeJob describe[kMaxLevels];
 };
@@ -92,9 +98,7 @@ struct PyramidShared {
 void make_pyramid_jobs(const ImageView& im, const s2::Config& c, const Keypoints& out, const Descriptors& desc,
                        void* ws, const PyramidLayout& l, const PyramidShared& sh, PyramidJobs* jobs);
 
-// Block count of each detect/describe kind for layer i (0 when inactive;
-// kFastKind also runs on a layer without keypoints when a later layer has
-// some, to build the next layer).
+// Block count of each detect/describe kind for layer i (0 when inactive).
 void pyramid_detect_blocks(const PyramidLayout& l, int layer, int (&blocks)[kDetectKinds]);
 void pyramid_describe_blocks(const PyramidLayout& l, int layer, int (&blocks)[kDescribeKinds]);
 

@@ -59,13 +59,6 @@ struct DetectJob {
     uint2* blur_list;
     std::uint32_t* blur_count;
     int job;  // this job's index in the describe table of the launch
-    // The next pyramid layer (null for the last layer built, or a single
-    // level): the FAST tiles of this layer write its pixels, resized from
-    // this layer (cv::resize INTER_LINEAR_EXACT on 8-bit images).
-    std::uint8_t* next;
-    int next_width, next_height, next_pitch;
-    double next_scale_x, next_scale_y;  // 1 / (next / this) per axis, as linear_exact_scale computes it
-    float next_inv_x, next_inv_y;       // next / this: estimates of a tile's first next-layer column and row
     // launch bookkeeping
     int tiles_x, tiles, select_blocks, candidates;
     __host__ __device__ std::uint32_t* counters() const { return hist + 256; }
@@ -96,6 +89,16 @@ struct DescribeJob {
     const int* level_counts;
     int level;
     float scale;
+};
+
+// One pyramid layer: `dst` (dense) resized from `src` by fixed-point
+// bilinear interpolation (cv::resize INTER_LINEAR_EXACT on 8-bit images).
+struct ResizeJob {
+    const std::uint8_t* src;
+    int src_width, src_height, src_pitch;
+    std::uint8_t* dst;
+    int width, height, pitch;
+    int tiles_x, tiles;
 };
 
 // Per-image job passed by value.
@@ -187,6 +190,7 @@ constexpr int kSortChunk = 64;      // keys a warp sorts in registers (2 per lan
 constexpr int kBlurTileW = 64, kBlurTileH = 32;
 constexpr int kDescWarps = 8;
 constexpr int kEdge = 31;
+constexpr int kResizeTileW = 64, kResizeTileH = 64;  // widest tile; a job's tile_h may be smaller
 constexpr int kMaxLevels = 16;
 static_assert(kMaxLevels <= kMapKinds && kDetectKinds <= kMapKinds, "block map kinds");
 
@@ -298,23 +302,6 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-// Source index and 8-bit weight of the right neighbour for destination
-// index v of a src -> dst linear resize: f = (v + 0.5) * scale - 0.5 in
-// double with scale = 1 / (dst / src), weight rint((f - floor f) * 256).
-// Indices left of the source (every index when src == 1) read pixel 0 with
-// weight 0, indices past the last interval read pixel src - 1 with weight 0.
-__device__ __forceinline__ double linear_exact_scale(int src, int dst) {
-    return 1.0 / (static_cast<double>(dst) / static_cast<double>(src));
-}
-
-__device__ __forceinline__ int2 linear_exact_tap(int v, int src, double scale) {
-    const double f = scale * (static_cast<double>(v) + 0.5) - 0.5;
-    const double fl = floor(f);
-    if (src == 1 || fl < 0.0) return make_int2(0, 0);
-    if (fl >= static_cast<double>(src - 1)) return make_int2(src - 1, 0);
-    return make_int2(static_cast<int>(fl), static_cast<int>(rint((f - fl) * 256.0)));
-}
-
 // Stages rows y0-4 .. y0+35 and columns x0-16 .. x0+79 of the job's image in
 // `in` (byte c of row r = image (y0-4+r, x0-16+c)). The FAST test never reads
 // a position outside the image, so rows are clamped into it and the bytes of
@@ -356,37 +343,15 @@ __device__ __forceinline__ void stage_fast_tile(const DetectJob& j, int local, s
 // every job of the launch from a device queue (`*queue`, zero at launch; tile
 // t of `total` is looked up through the source's kFastKind entries), while
 // the next tile's bytes are copied into the other half of a double buffer.
-// The jobs of the current and the next tile sit in shared memory. A job with
-// a next pyramid layer also resizes: every pixel of the next layer whose
-// top-left source tap lies in the tile's 64x32 core is computed from the
-// staged bytes (its right and lower source neighbours are in the halo), so
-// each next-layer pixel is written by exactly one tile and the layers of a
-// pyramid are built by one FAST launch per layer depth. Per tile:
+// The jobs of the current and the next tile sit in shared memory. Per tile:
 //   1. the compass test on the tile plus a 1-pixel ring, 4 positions per
 //      thread in 16-bit lanes; groups with a survivor are listed so that full
 //      scores are computed on full warps;
 //   2. the survivors are scored (every other position scores 0);
 //   3. each survivor of the tile inside the 31-pixel edge margin that is a
 //      strict 3x3 maximum goes into the job's maxima list as
-//      (score << 32) | raster index, its score into the job's histogram;
-//      the next layer's pixels of the tile are written, each
-//        h(r, c) = src[r][c0] * (256 - wx) + src[r][c1] * wx   (< 2^16)
-//        out = (h(r0, c) * (256 - wy) + h(r1, c) * wy + 2^15) >> 16,
-//      the integer form of INTER_LINEAR_EXACT's 8-bit fixed-point horizontal
-//      pass followed by the vertical pass with one final rounding.
-// A layer without keypoints of its own (budget 0) only resizes. No maxima
-// map and no blur are written.
-// Candidate next-layer columns and rows of a tile: its owned ones lie within
-// [base, base + kNextCandX) x [base, base + kNextCandY), with base one below
-// the float estimate of the first one (at most 64 columns and 32 rows are
-// owned: the layer ratio is at least 1, so the taps of consecutive
-// destination indices differ).
-constexpr int kNextCandX = kFastTileW + 4, kNextCandY = kFastTileH + 4;
-constexpr int kCandYThread = 96;  // first thread computing row candidates
-__device__ __forceinline__ int next_base(int s0, float inv) {
-    return max(0, __float2int_rd((static_cast<float>(s0) + 0.5f) * inv - 0.5f) - 1);
-}
-
+//      (score << 32) | raster index, its score into the job's histogram.
+// No maxima map and no blur are written.
 template <class Src>
 __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(const __grid_constant__ Src src,
                                                                           std::uint32_t* queue, int total) {
@@ -398,7 +363,6 @@ __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(cons
     __shared__ std::uint64_t found[kTileMaxima];
     __shared__ DetectJob jobs[2];  // jobs of the tiles in in[0] and in[1] (kept here, not in registers)
     __shared__ int locals[2];
-    __shared__ int2 ctx[kNextCandX], cty[kNextCandY];  // candidate next-layer taps; x < 0: not this tile's
     __shared__ int n_cand, n_found, next;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     hist[tid] = 0;
@@ -428,32 +392,10 @@ __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(cons
             if (t < total && !src.find(t, kFastKind, &jobs[buf ^ 1], &locals[buf ^ 1])) t = total;
             next = t;
         }
-        // the tile's next-layer taps, one candidate column or row per thread
-        // (owned: the source tap lies in the core [x0, x0 + 64) x [y0, y0 + 32))
-        if (j.next) {
-            if (tid < kNextCandX) {
-                const int X = next_base(x0, j.next_inv_x) + tid;
-                int2 t = make_int2(-1, 0);
-                if (X < j.next_width) {
-                    const int2 tp = linear_exact_tap(X, W, j.next_scale_x);
-                    if (tp.x >= x0 && tp.x < x0 + kFastTileW) t = tp;
-                }
-                ctx[tid] = t;
-            } else if (tid >= kCandYThread && tid < kCandYThread + kNextCandY) {
-                const int Y = next_base(y0, j.next_inv_y) + (tid - kCandYThread);
-                int2 t = make_int2(-1, 0);
-                if (Y < j.next_height) {
-                    const int2 tp = linear_exact_tap(Y, H, j.next_scale_y);
-                    if (tp.x >= y0 && tp.x < y0 + kFastTileH) t = tp;
-                }
-                cty[tid - kCandYThread] = t;
-            }
-        }
         // 1. compass test: thread (q, rb) takes positions 4q .. 4q+3 of rows rb,
         // rb + 15, rb + 30; groups with a survivor are listed as
         // (group << 4 | survivor bits)
         const std::uint32_t thr1 = static_cast<std::uint32_t>(j.threshold + 1) * 0x00010001u;
-        const bool detect = j.max_keypoints > 0;
         {
             constexpr int kRowSets = 256 / kScGroups;  // 15
             const int q = tid % kScGroups, rb = tid / kScGroups, c = 4 * q;
@@ -469,7 +411,7 @@ __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(cons
                 if (rb < kRowSets && r < kFastScH) {
                     *reinterpret_cast<std::uint32_t*>(&sc[r][c]) = 0u;
                     const int gy = y0 - 1 + r;
-                    if (detect && colmask && gy >= 3 && gy < H - 3) {
+                    if (colmask && gy >= 3 && gy < H - 3) {
                         const int w = q + 3;  // word holding halo columns c .. c+3 (bytes c+12 .. c+15)
                         const auto* mid = reinterpret_cast<const std::uint32_t*>(&cur[r + 3][0]);
                         const auto* bot = reinterpret_cast<const std::uint32_t*>(&cur[r + 6][0]);
@@ -559,22 +501,6 @@ __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(cons
                     found[atomicAdd(&n_found, 1)] = (static_cast<std::uint64_t>(v) << 32) | px;
                     atomicAdd(&hist[v], 1u);
                 }
-            }
-        }
-        // the next layer's pixels of this tile (source (x, y) is staged at
-        // cur[y - y0 + 4][x - x0 + 16]; x + 1 <= x0 + 64 and y + 1 <= y0 + 32)
-        if (j.next) {
-            const int bx = next_base(x0, j.next_inv_x), by = next_base(y0, j.next_inv_y);
-            for (int k = tid; k < kNextCandX * kNextCandY; k += kFastThreads) {
-                const int r = k / kNextCandX, c = k - r * kNextCandX;
-                const int2 tx = ctx[c], ty = cty[r];
-                if (tx.x < 0 || ty.x < 0) continue;
-                const int ca = tx.x - x0 + 16, cb = min(tx.x + 1, W - 1) - x0 + 16;
-                const std::uint8_t* ra = cur[ty.x - y0 + 4];
-                const std::uint8_t* rb2 = cur[min(ty.x + 1, H - 1) - y0 + 4];
-                const int ha = ra[ca] * (256 - tx.y) + ra[cb] * tx.y, hb = rb2[ca] * (256 - tx.y) + rb2[cb] * tx.y;
-                const unsigned out = static_cast<unsigned>(ha * (256 - ty.y) + hb * ty.y + (1 << 15)) >> 16;
-                j.next[static_cast<std::size_t>(by + r) * j.next_pitch + (bx + c)] = static_cast<std::uint8_t>(out);
             }
         }
         cp_async_wait_all();
@@ -923,6 +849,153 @@ __global__ __launch_bounds__(kHarrisThreads) void rank_topk_kernel(const __grid_
     if (slot < n && rank < j.max_keypoints) write_keypoint(j, rank, key);
 }
 
+// ------------------------------------------------------ pyramid layers
+
+// Source index and 8-bit weight of the right neighbour for destination
+// index v of a src -> dst linear resize: f = (v + 0.5) * scale - 0.5 in
+// double with scale = 1 / (dst / src), weight rint((f - floor f) * 256).
+// Indices left of the source (every index when src == 1) read pixel 0 with
+// weight 0, indices past the last interval read pixel src - 1 with weight 0.
+__device__ __forceinline__ double linear_exact_scale(int src, int dst) {
+    return 1.0 / (static_cast<double>(dst) / static_cast<double>(src));
+}
+
+__device__ __forceinline__ int2 linear_exact_tap(int v, int src, double scale) {
+    const double f = scale * (static_cast<double>(v) + 0.5) - 0.5;
+    const double fl = floor(f);
+    if (src == 1 || fl < 0.0) return make_int2(0, 0);
+    if (fl >= static_cast<double>(src - 1)) return make_int2(src - 1, 0);
+    return make_int2(static_cast<int>(fl), static_cast<int>(rint((f - fl) * 256.0)));
+}
+
+// One block = one tile of 64 x kTileH (16..64) layer pixels:
+//   1. the tile's source window, bounded from float arithmetic with a pixel
+//      of slack per side, is staged in shared memory with 16-byte loads
+//      (while the taps are computed);
+//   2. per-column and per-row taps in shared memory (double, as above);
+//   3. each warp produces whole layer rows, each lane two adjacent outputs:
+//        h(r, c) = src[r][c0] * (256 - wx) + src[r][c1] * wx   (< 2^16)
+//        out = (h(r0, c) * (256 - wy) + h(r1, c) * wy + 2^15) >> 16,
+//      the integer form of the 8-bit fixed-point horizontal pass followed
+//      by the vertical pass with one final rounding.
+// The exact taps are checked against the staged window; a tile outside it
+// (source image not 16-byte aligned, or a layer ratio above about 1.45)
+// reads the source bytes from global memory instead, with the same result.
+constexpr int kRawStride = 112;  // bytes of a staged source row: 7 chunks of 16
+template <int kTileH> __host__ __device__ constexpr int resize_raw_rows() { return kTileH * 3 / 2 + 6; }
+
+template <class Src, int kTileH>
+__global__ __launch_bounds__(256, 6) void resize_kernel(const __grid_constant__ Src src, int kind) {
+    static_assert(kTileH >= 16 && kTileH <= kResizeTileH && kTileH % 16 == 0, "resize tile height");
+    constexpr int th = kTileH, kRows = resize_raw_rows<kTileH>(), kChunks = kRawStride / 16;
+    __shared__ int2 xtap[kResizeTileW];
+    __shared__ int2 ytap[kTileH];
+    __shared__ __align__(16) std::uint8_t raw[kRows][kRawStride];
+    __shared__ double scale[2];
+    ResizeJob j;
+    int local;
+    if (!src.find(blockIdx.x, kind, &j, &local)) return;
+    const int y0 = (local / j.tiles_x) * th;
+    const int x0 = (local % j.tiles_x) * kResizeTileW;
+    const int t = threadIdx.x;
+    // 1. source window: rows ry0..ry1, 16-byte chunks from column rx0
+    const float fy = static_cast<float>(j.src_height) / static_cast<float>(j.height);
+    const float fx = static_cast<float>(j.src_width) / static_cast<float>(j.width);
+    const int last_y = min(y0 + th, j.height) - 1, last_x = min(x0 + kResizeTileW, j.width) - 1;
+    const int ry0 = max(__float2int_rd((y0 + 0.5f) * fy - 0.5f) - 1, 0);
+    const int ry1 = min(__float2int_rd((last_y + 0.5f) * fy - 0.5f) + 2, j.src_height - 1);
+    const int rx0 = max(__float2int_rd((x0 + 0.5f) * fx - 0.5f) - 1, 0) & ~15;
+    const int rx1 = min(__float2int_rd((last_x + 0.5f) * fx - 0.5f) + 2, j.src_width - 1);
+    const int nrow = ry1 - ry0 + 1;
+    const int nchunk = rx1 >= rx0 ? (rx1 - rx0) / 16 + 1 : 0;
+    const bool window = ((reinterpret_cast<std::uintptr_t>(j.src) | static_cast<std::uintptr_t>(j.src_pitch)) & 15) == 0 &&
+                        nrow > 0 && nrow <= kRows && nchunk > 0 && nchunk <= kChunks;  // block-uniform
+    if (window) {
+        // chunks start 16-byte aligned below src_width; one that reaches past
+        // the row's last pixel is read byte by byte (zeros beyond it)
+        const int n = nrow * nchunk;
+        for (int i0 = t; i0 < n; i0 += 2 * 256) {
+            uint4 v[2];
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const int i = i0 + 256 * k;
+                if (i < n) {
+                    const int r = i / nchunk, col = rx0 + 16 * (i - r * nchunk);
+                    const std::uint8_t* p = j.src + static_cast<std::size_t>(ry0 + r) * j.src_pitch + col;
+                    if (col + 16 <= j.src_width) {
+                        v[k] = __ldg(reinterpret_cast<const uint4*>(p));
+                    } else {
+                        std::uint32_t w[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+                        for (int b = 0; b < 16; ++b)
+                            if (col + b < j.src_width)
+                                w[b >> 2] |= static_cast<std::uint32_t>(__ldg(p + b)) << (8 * (b & 3));
+                        v[k] = make_uint4(w[0], w[1], w[2], w[3]);
+                    }
+                }
+            }
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const int i = i0 + 256 * k;
+                if (i < n) {
+                    const int r = i / nchunk, c = i - r * nchunk;
+                    *reinterpret_cast<uint4*>(&raw[r][16 * c]) = v[k];
+                }
+            }
+        }
+    }
+    // 2. taps
+    if (t == 0) scale[0] = linear_exact_scale(j.src_width, j.width);
+    if (t == 32) scale[1] = linear_exact_scale(j.src_height, j.height);
+    __syncthreads();
+    if (t < kResizeTileW) xtap[t] = linear_exact_tap(min(x0 + t, j.width - 1), j.src_width, scale[0]);
+    else if (t < kResizeTileW + th)
+        ytap[t - kResizeTileW] = linear_exact_tap(min(y0 + t - kResizeTileW, j.height - 1), j.src_height, scale[1]);
+    __syncthreads();
+    // taps are nondecreasing: the first and last give the tile's source span
+    const bool staged = window && ytap[0].x >= ry0 && min(ytap[th - 1].x + 1, j.src_height - 1) <= ry1 &&
+                        xtap[0].x >= rx0 && min(xtap[kResizeTileW - 1].x + 1, j.src_width - 1) < rx0 + 16 * nchunk;
+    // 3. warp w: rows w, w + 8, ...; lane l: columns 2l, 2l + 1
+    const int lane = t & 31;
+    const int c = 2 * lane, x = x0 + c;
+    if (x >= j.width) return;
+    const int2 t0 = xtap[c], t1 = xtap[c + 1];  // columns past the layer edge repeat the last tap
+    const int wx0 = t0.y, wx1 = t1.y;
+    int xa0 = t0.x, xb0 = min(t0.x + 1, j.src_width - 1), xa1 = t1.x, xb1 = min(t1.x + 1, j.src_width - 1);
+    if (staged) {
+        xa0 -= rx0; xb0 -= rx0; xa1 -= rx0; xb1 -= rx0;
+    }
+    for (int rr = t >> 5; rr < th; rr += 8) {
+        const int y = y0 + rr;
+        if (y >= j.height) break;
+        const int2 ty = ytap[rr];
+        const int ra = ty.x, rb = min(ty.x + 1, j.src_height - 1), wy = ty.y;
+        int pa[4], pb[4];  // rows ra, rb at xa0, xb0, xa1, xb1
+        if (staged) {
+            const std::uint8_t* A = raw[ra - ry0];
+            const std::uint8_t* B = raw[rb - ry0];
+            pa[0] = A[xa0]; pa[1] = A[xb0]; pa[2] = A[xa1]; pa[3] = A[xb1];
+            pb[0] = B[xa0]; pb[1] = B[xb0]; pb[2] = B[xa1]; pb[3] = B[xb1];
+        } else {
+            const std::uint8_t* A = j.src + static_cast<std::size_t>(ra) * j.src_pitch;
+            const std::uint8_t* B = j.src + static_cast<std::size_t>(rb) * j.src_pitch;
+            pa[0] = __ldg(A + xa0); pa[1] = __ldg(A + xb0); pa[2] = __ldg(A + xa1); pa[3] = __ldg(A + xb1);
+            pb[0] = __ldg(B + xa0); pb[1] = __ldg(B + xb0); pb[2] = __ldg(B + xa1); pb[3] = __ldg(B + xb1);
+        }
+        const int ha0 = pa[0] * (256 - wx0) + pa[1] * wx0, hb0 = pb[0] * (256 - wx0) + pb[1] * wx0;
+        const int ha1 = pa[2] * (256 - wx1) + pa[3] * wx1, hb1 = pb[2] * (256 - wx1) + pb[3] * wx1;
+        const unsigned v0 = static_cast<unsigned>(ha0 * (256 - wy) + hb0 * wy + (1 << 15)) >> 16;
+        const unsigned v1 = static_cast<unsigned>(ha1 * (256 - wy) + hb1 * wy + (1 << 15)) >> 16;
+        std::uint8_t* dst = j.dst + static_cast<std::size_t>(y) * j.pitch + x;
+        if (x + 1 < j.width && (reinterpret_cast<std::uintptr_t>(dst) & 1) == 0) {
+            *reinterpret_cast<std::uint16_t*>(dst) = static_cast<std::uint16_t>(v0 | (v1 << 8));
+        } else {
+            dst[0] = static_cast<std::uint8_t>(v0);
+            if (x + 1 < j.width) dst[1] = static_cast<std::uint8_t>(v1);
+        }
+    }
+}
+
 // ------------------------------------------------------------- S3 blur
 
 // One block = one 64x32 tile: rows pass into a float tile with a 3-row halo,
@@ -979,14 +1052,61 @@ __global__ __launch_bounds__(256) void blur_kernel(const __grid_constant__ Src s
 // interior tiles of 16-byte aligned images, reflected byte loads otherwise.
 static_assert(kBlurTileW == kFastTileW && kBlurTileH == kFastTileH, "blur tiles share the FAST tile staging");
 
-// Tile origin of blur-list entry e and whether it is staged by 16-byte copies
-// (an interior tile of a 16-byte aligned image: no reflected halo needed).
-__device__ __forceinline__ bool blur_tile_vec(const DescribeJob& j, unsigned tile, int* x0, int* y0) {
+// Origin of blur tile `tile` of job j.
+__device__ __forceinline__ void blur_tile_origin(const DescribeJob& j, unsigned tile, int* x0, int* y0) {
     const int tiles_x = (j.width + kBlurTileW - 1) / kBlurTileW;
     *y0 = (static_cast<int>(tile) / tiles_x) * kBlurTileH;
     *x0 = (static_cast<int>(tile) % tiles_x) * kBlurTileW;
-    return ((reinterpret_cast<std::uintptr_t>(j.image) | static_cast<std::uintptr_t>(j.pitch)) & 15) == 0 &&
-           *x0 >= 16 && *x0 + 80 <= j.width && *y0 >= 4 && *y0 + kFastTileH + 4 <= j.height;
+}
+
+__device__ __forceinline__ bool aligned16(const DescribeJob& j) {
+    return ((reinterpret_cast<std::uintptr_t>(j.image) | static_cast<std::uintptr_t>(j.pitch)) & 15) == 0;
+}
+
+// Asynchronous staging of a blur tile of a 16-byte aligned image: row r of
+// `in` is image row reflect101(y0 - 4 + r) (the reflected halo rows are whole
+// image rows), byte c is column x0 - 16 + c. Chunks inside a row's pitch
+// (inside the width on the last image row) are 16-byte copies, a chunk
+// straddling the end of the last row is copied byte by byte; the reflected
+// halo columns are filled by blur_fix_columns once the copies are complete.
+__device__ __forceinline__ void blur_stage_async(const DescribeJob& j, int x0, int y0, std::uint8_t (*in)[kInStride]) {
+    const int tid = threadIdx.x;
+    constexpr int kChunks = kInStride / 16;
+    if (tid < kFastInH * kChunks) {
+        const int r = tid / kChunks, q = tid - r * kChunks;
+        const int gy = reflect101(y0 - 4 + r, j.height);
+        const int cx = x0 - 16 + 16 * q;
+        const int limit = gy == j.height - 1 ? j.width : j.pitch;
+        const std::uint8_t* row = j.image + static_cast<std::size_t>(gy) * j.pitch;
+        if (cx >= 0 && cx + 16 <= limit) {
+            cp_async16(&in[r][16 * q], row + cx);
+        } else if (cx >= 0 && cx < j.width) {
+            for (int b = 0; b < 16 && cx + b < j.width; ++b) in[r][16 * q + b] = row[cx + b];
+        }
+    }
+}
+
+// Whether the 7x7 blur of the tile at x0 reads columns outside the image.
+__device__ __forceinline__ bool blur_needs_columns(int x0, int W) { return x0 < 3 || x0 + kBlurTileW + 3 > W; }
+
+// Reflect-101 halo columns of a staged tile: column -k is column k, column
+// W - 1 + k is column W - 1 - k (k = 1..3), copied inside `in`.
+__device__ __forceinline__ void blur_fix_columns(int x0, int W, std::uint8_t (*in)[kInStride]) {
+    const int tid = threadIdx.x;
+    if (tid >= kFastInH * 6) return;
+    const int r = tid / 6, k = tid % 6;
+    const int off = x0 - 16;  // column of byte 0
+    int dst, srcc;
+    if (k < 3) {  // left edge
+        dst = -(k + 1);
+        srcc = k + 1;
+    } else {      // right edge
+        dst = W - 1 + (k - 2);
+        srcc = W - 1 - (k - 2);
+    }
+    const int db = dst - off, sb = srcc - off;
+    if (db >= 0 && db < kInStride && sb >= 0 && sb < kInStride && dst >= x0 - 3 && dst <= x0 + kBlurTileW + 2)
+        in[r][db] = in[r][sb];
 }
 
 constexpr int kBlurCtasPerSm = 6;  // resident blur blocks per SM; the persistent grid is 148 x this
@@ -999,15 +1119,14 @@ __global__ __launch_bounds__(256, kBlurCtasPerSm) void blur_tiles_kernel(const _
     __shared__ int col_at[kInStride];
     const int tid = threadIdx.x;
     const int n = static_cast<int>(*count);
-    // interior tiles are copied asynchronously, the next one while this one is blurred
+    // tiles of aligned images are copied asynchronously, the next one while this one is blurred
     auto prefetch = [&](int i, std::uint8_t (*dst)[kInStride]) {
         const uint2 e = list[i];
         const DescribeJob jn = src.at(static_cast<int>(e.x));
+        if (!aligned16(jn)) return;
         int x0, y0;
-        if (blur_tile_vec(jn, e.y, &x0, &y0) && tid < kFastInH * (kInStride / 16)) {
-            const int r = tid / (kInStride / 16), q = tid - r * (kInStride / 16);
-            cp_async16(&dst[r][16 * q], jn.image + static_cast<std::size_t>(y0 - 4 + r) * jn.pitch + (x0 - 16 + 16 * q));
-        }
+        blur_tile_origin(jn, e.y, &x0, &y0);
+        blur_stage_async(jn, x0, y0, dst);
     };
     int buf = 0;
     if (static_cast<int>(blockIdx.x) < n) prefetch(blockIdx.x, in2[0]);
@@ -1017,7 +1136,8 @@ __global__ __launch_bounds__(256, kBlurCtasPerSm) void blur_tiles_kernel(const _
         const DescribeJob j = src.at(static_cast<int>(e.x));
         const int W = j.width, H = j.height;
         int x0, y0;
-        if (!blur_tile_vec(j, e.y, &x0, &y0)) {  // border tile or unaligned image: reflected byte loads
+        blur_tile_origin(j, e.y, &x0, &y0);
+        if (!aligned16(j)) {  // unaligned image: reflected byte loads
             if (tid < kFastInH) row_at[tid] = static_cast<std::size_t>(reflect101(y0 - 4 + tid, H)) * j.pitch;
             else if (tid < kFastInH + kInStride) col_at[tid - kFastInH] = reflect101(x0 - 16 + (tid - kFastInH), W);
             __syncthreads();
@@ -1032,6 +1152,10 @@ __global__ __launch_bounds__(256, kBlurCtasPerSm) void blur_tiles_kernel(const _
         }
         cp_async_wait_all();
         __syncthreads();
+        if (aligned16(j) && blur_needs_columns(x0, W)) {
+            blur_fix_columns(x0, W, in);
+            __syncthreads();
+        }
         if (i + static_cast<int>(gridDim.x) < n) prefetch(i + gridDim.x, in2[buf ^ 1]);
         // rows pass: image rows y0-3 .. y0+34, two rows x 4 outputs per item
         static_assert((kFastTileH + 6) % 2 == 0, "rows pass takes row pairs");

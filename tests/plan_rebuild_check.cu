@@ -28,18 +28,17 @@ stitch_pair_desc pair(int wa, int ha, int wb, int hb, int k, int r, int levels, 
 bool same(const Plan& a, const Plan& b) {
     bool ok = a.n == b.n && a.total == b.total && a.table_bytes == b.table_bytes && a.tables == b.tables &&
               a.results == b.results && a.n_det == b.n_det && a.n_layers == b.n_layers &&
-              a.max_levels == b.max_levels && a.hists == b.hists &&
+              a.n_resize == b.n_resize && a.max_levels == b.max_levels && a.hists == b.hists &&
               a.zeroed == b.zeroed && a.search_blocks == b.search_blocks && a.hpw == b.hpw &&
               a.sort_smem == b.sort_smem && a.search_smem == b.search_smem &&
               a.rank_fallback == b.rank_fallback && a.block_map == b.block_map;
     ok = ok && !std::memcmp(a.offsets, b.offsets, sizeof a.offsets) &&
          !std::memcmp(a.det_total, b.det_total, sizeof a.det_total) &&
          !std::memcmp(a.des_total, b.des_total, sizeof a.des_total) &&
-         !std::memcmp(a.fl_total, b.fl_total, sizeof a.fl_total) &&
+         !std::memcmp(a.rs_total, b.rs_total, sizeof a.rs_total) &&
          !std::memcmp(a.det_first, b.det_first, sizeof a.det_first) &&
          !std::memcmp(a.des_first, b.des_first, sizeof a.des_first) &&
-         !std::memcmp(a.fl_first, b.fl_first, sizeof a.fl_first) &&
-         a.blur_total == b.blur_total && a.blur_flags == b.blur_flags && a.blur_list == b.blur_list && a.queue == b.queue &&
+         !std::memcmp(a.rs_first, b.rs_first, sizeof a.rs_first) &&
          !std::memcmp(a.s45_total, b.s45_total, sizeof a.s45_total) &&
          !std::memcmp(a.s45_first, b.s45_first, sizeof a.s45_first);
     for (int i = 0; ok && i < a.n; ++i) {
