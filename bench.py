@@ -545,7 +545,7 @@ def run_matching(dev, reps=20):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     out, got = {}, {}
     before = L.stitch_s4_matcher()
-    for name, kind in (("popc", 0), ("tensor", 1), ("tensor128", 2), ("tensor64", 3)):
+    for name, kind in (("popc", 0), ("tensor", 1), ("tensor128", 2), ("tensor64", 3), ("tensor_pipe", 4)):
         assert L.stitch_s4_set_matcher(kind) == 0
         call = lambda: L.stitch_s4_match(C.byref(kq), C.byref(Dq), C.byref(kt), C.byref(Dt), C.byref(cfg),
                                          C.byref(m), C.c_void_p(ws.data_ptr()), nb.value,
@@ -569,12 +569,12 @@ def run_matching(dev, reps=20):
     out["popc"].update(achieved=24.0 * n * n / (out["popc"]["ms"] / 1e3) / 1e12, unit="Tops/s", peak=int_peak,
                        peak_source="nominal INT32 issue rate (64 lanes x 3 ops/clk/SM)")
     t_peak = 2 * peaks.get("bf16_tflops", 1590.0)
-    for name in ("tensor", "tensor128", "tensor64"):
+    for name in ("tensor", "tensor128", "tensor64", "tensor_pipe"):
         out[name].update(achieved=512.0 * n * n / (out[name]["ms"] / 1e3) / 1e12, unit="Tops/s", peak=t_peak,
                          peak_source="dense int8 = 2 x measured bf16 burst")
     for v in out.values():
         v["frac"] = v["achieved"] / v["peak"]
-    exact = all(torch.equal(a, b) for name in ("tensor", "tensor128", "tensor64")
+    exact = all(torch.equal(a, b) for name in ("tensor", "tensor128", "tensor64", "tensor_pipe")
                 for a, b in zip(got["popc"], got[name]))
     return {"workload": "8192 x 8192 planted 256-bit descriptors, kNN-2 + ratio 0.8 (s4_match, one direction)",
             "bit_exact": bool(exact), "tc_errors": errors,

@@ -114,7 +114,7 @@ Status check_match_args(const Keypoints& a, const Descriptors& da, const Keypoin
         return Status::INVALID_ARGUMENT;
     return Status::OK;
 }
-bool valid_matcher(int kind) { return kind >= kMatcherPopc && kind <= kMatcherTensor64; }
+bool valid_matcher(int kind) { return kind >= kMatcherPopc && kind <= kMatcherTensorPipe; }
 
 namespace {
 

@@ -23,7 +23,8 @@ bool popc_eligible(const Descriptors& q, const Descriptors& t, int capacity_trai
 // (stitch_s4_set_matcher), so threads never race on it; a batch plan and a
 // server take the creating thread's choice when they are made, and a plan can
 // be given its own (stitch_batch_set_matcher).
-constexpr int kMatcherPopc = 0, kMatcherTensor = 1, kMatcherTensor128 = 2, kMatcherTensor64 = 3;
+constexpr int kMatcherPopc = 0, kMatcherTensor = 1, kMatcherTensor128 = 2, kMatcherTensor64 = 3,
+              kMatcherTensorPipe = 4;
 // Train rows per tensor-core stage of a tensor-core matcher kind.
 constexpr int tc_rows(int kind) { return kind == kMatcherTensor64 ? 64 : kind == kMatcherTensor128 ? 128 : 256; }
 constexpr bool is_tensor(int kind) { return kind != kMatcherPopc; }
@@ -47,7 +48,23 @@ template <class Src, int kRowsB> bool enable_tc_smem() {
     return ok[dev];
 }
 // Launches the tensor-core matcher of `kind` over `blocks` blocks.
+template <class Src> bool enable_pipe_smem() {
+    static std::once_flag flags[64];
+    static bool ok[64];
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return false;
+    std::call_once(flags[dev], [&] {
+        ok[dev] = cudaFuncSetAttribute(knn_tc_pipe_kernel<Src>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       kPipeSmem) == cudaSuccess;
+    });
+    return ok[dev];
+}
 template <class Src> bool launch_tc(int kind, int blocks, const Src& src, cudaStream_t s) {
+    if (kind == kMatcherTensorPipe) {
+        if (!enable_pipe_smem<Src>()) return false;
+        knn_tc_pipe_kernel<Src><<<blocks, kPipeThreads, kPipeSmem, s>>>(src);
+        return true;
+    }
     switch (tc_rows(kind)) {
         case 64:
             if (!enable_tc_smem<Src, 64>()) return false;
@@ -64,7 +81,8 @@ template <class Src> bool launch_tc(int kind, int blocks, const Src& src, cudaSt
     }
 }
 constexpr int tc_blocks_per_sm(int kind) {
-    return tc_rows(kind) == 64 ? TcShape<64>::blocks_per_sm
+    return kind == kMatcherTensorPipe ? 1
+         : tc_rows(kind) == 64 ? TcShape<64>::blocks_per_sm
                                : tc_rows(kind) == 128 ? TcShape<128>::blocks_per_sm : TcShape<256>::blocks_per_sm;
 }
 // Reads and clears the tensor-core error word of the batched chain's

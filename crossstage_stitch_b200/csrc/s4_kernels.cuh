@@ -383,6 +383,215 @@ __global__ __launch_bounds__(kQueryThreads, 1) void knn_tc_kernel(const __grid_c
     if (warp == 0) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTcRowsB));
 }
 
+// ------------------------------------------------ pipelined tensor cores
+//
+// The same exact top-2 search as knn_tc_kernel, with the three kinds of work
+// of a stage overlapped instead of run one after the other. Warp roles:
+//   warps 0-7   epilogue: warp w reads TMEM lane quarter w % 4 (its 32
+//               queries) and column half w / 4 of an accumulator, keeping
+//               four top-2 key chains per thread;
+//   warps 8-11  producers: expand the queries once, then each train stage
+//               (256 rows) into one of two shared-memory stage buffers;
+//   warp 12     one thread issues the 8 MMAs of a stage into one of two TMEM
+//               accumulators (2 x 256 columns) and commits them.
+// Stage s uses buffer and accumulator s % 2. mbarriers order the roles:
+// full[b] (producers -> MMA), done[b] (MMA completion -> epilogue, and to
+// the producers: the buffer is free again), free[b] (epilogue -> MMA: the
+// accumulator was read). Every wait is bounded: when one runs out the block
+// sets the error word and a stop flag that ends every role, waits (bounded)
+// for its last MMA, frees its TMEM and leaves its outputs unwritten. The two
+// column halves of a query meet in shared memory at the end.
+constexpr int kPipeEpiWarps = 8, kPipeProdWarps = 4;
+constexpr int kPipeThreads = (kPipeEpiWarps + kPipeProdWarps + 1) * 32;
+constexpr int kPipeStage = 256;                                   // train rows per stage (MMA N)
+constexpr int kPipeBytesB = kPipeStage * 256;
+constexpr int kPipeSmem = kTcBytesA + 2 * kPipeBytesB + 1024 + 2048;  // + alignment + barriers and exchange
+constexpr std::uint32_t kPipeIdesc = TcShape<kPipeStage>::idesc;
+
+__device__ __forceinline__ void bar_init(std::uint64_t* bar, unsigned count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count));
+}
+__device__ __forceinline__ void bar_arrive(std::uint64_t* bar) {
+    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.shared::cta.b64 st, [%0];\n\t}" ::"r"(smem_u32(bar)) : "memory");
+}
+// Waits for the completion of the phase of `parity`; false when the wait ran
+// out (then the stop flag is set) or another role stopped the block.
+__device__ __forceinline__ bool bar_wait(std::uint64_t* bar, std::uint32_t parity, volatile int* stop) {
+    for (long long it = 0; it < kTcWaitLimit; ++it) {
+        std::uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(smem_u32(bar)), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if ((it & 255) == 255 && *stop) return false;
+    }
+    *stop = 1;
+    return false;
+}
+
+template <class Src>
+__global__ __launch_bounds__(kPipeThreads, 1) void knn_tc_pipe_kernel(const __grid_constant__ Src src) {
+    extern __shared__ std::uint8_t dyn[];
+    KnnJob j;
+    int local;
+    if (!src.find(blockIdx.x, &j, &local)) return;
+    std::uint8_t* tileA = reinterpret_cast<std::uint8_t*>((reinterpret_cast<std::uintptr_t>(dyn) + 1023) & ~std::uintptr_t(1023));
+    std::uint8_t* tileB[2] = {tileA + kTcBytesA, tileA + kTcBytesA + kPipeBytesB};
+    auto* full = reinterpret_cast<std::uint64_t*>(tileA + kTcBytesA + 2 * kPipeBytesB);
+    std::uint64_t* done = full + 2;
+    std::uint64_t* freeb = full + 4;
+    auto* tmem_slot = reinterpret_cast<std::uint32_t*>(full + 6);
+    auto* stop = reinterpret_cast<volatile int*>(tmem_slot + 1);
+    auto* last_issued = reinterpret_cast<int*>(tmem_slot + 2);
+    auto* xchg = reinterpret_cast<uint2*>(full + 8);  // [128] keys of column half 1
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int qt = local % j.q_tiles, split = local / j.q_tiles;
+    int nq, nt;
+    const bool ok = counts_valid(j, &nq, &nt);
+    const int t0 = split * j.rows_per_split;
+    const int t1 = ok ? min(nt, t0 + j.rows_per_split) : t0;
+    const int stages = t1 > t0 ? (t1 - t0 + kPipeStage - 1) / kPipeStage : 0;
+    if (warp == kPipeEpiWarps + kPipeProdWarps) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
+                     "r"(2 * kPipeStage));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        for (int b = 0; b < 2; ++b) {
+            bar_init(&full[b], kPipeProdWarps * 32);
+            bar_init(&done[b], 1);
+            bar_init(&freeb[b], kPipeEpiWarps * 32);
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        *stop = 0;
+        *last_issued = -1;
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const std::uint32_t tmem = *tmem_slot;
+    std::uint32_t k1[4] = {kEmptyKey, kEmptyKey, kEmptyKey, kEmptyKey};
+    std::uint32_t k2[4] = {kEmptyKey, kEmptyKey, kEmptyKey, kEmptyKey};
+    const int qrow = 32 * (warp & 3) + lane;  // epilogue: the query of this thread
+    if (warp < kPipeEpiWarps) {
+        const int half = warp >> 2;
+        for (int s = 0; s < stages; ++s) {
+            const int b = s & 1;
+            // the TMEM loads below are warp-collective: the warp goes on only together
+            if (!__all_sync(0xffffffffu, bar_wait(&done[b], (s >> 1) & 1, stop))) break;
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            const int base = t0 + s * kPipeStage + half * (kPipeStage / 2);
+#pragma unroll 1
+            for (int c = 0; c < kPipeStage / 2; c += 32) {
+                std::uint32_t v[32];
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, "
+                    "%13, %14, %15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, "
+                    "[%32];"
+                    : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+                      "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]),
+                      "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]),
+                      "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]),
+                      "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+                    : "r"(tmem + (static_cast<std::uint32_t>((warp & 3) * 32) << 16) +
+                          static_cast<std::uint32_t>(b * kPipeStage + half * (kPipeStage / 2) + c)));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                // (256 - dot) = 2 * Hamming, so (256 - dot) << 22 is the distance << 23
+                const std::uint32_t t = static_cast<std::uint32_t>(base + c);
+                if (base + c + 32 <= t1) {
+#pragma unroll
+                    for (int i = 0; i < 32; ++i) keep2(k1[i & 3], k2[i & 3], ((256u - v[i]) << 22) + (t + i));
+                } else {
+#pragma unroll
+                    for (int i = 0; i < 32; ++i)
+                        if (base + c + i < t1) keep2(k1[i & 3], k2[i & 3], ((256u - v[i]) << 22) + (t + i));
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;");
+            bar_arrive(&freeb[b]);
+        }
+    } else if (warp < kPipeEpiWarps + kPipeProdWarps) {
+        const int p = tid - kPipeEpiWarps * 32;  // 0 .. 127
+        const int q = qt * kTcRowsA + p;
+        stage_pm_row(tileA, kTcRowsA, p, ok && q < nq ? j.query.rows + static_cast<std::size_t>(q) * j.query.stride
+                                                      : nullptr);
+        for (int s = 0; s < stages; ++s) {
+            const int b = s & 1;
+            if (s >= 2 && !bar_wait(&done[b], ((s - 2) >> 1) & 1, stop)) break;
+            const int base = t0 + s * kPipeStage;
+            for (int r = p; r < kPipeStage; r += kPipeProdWarps * 32)
+                stage_pm_row(tileB[b], kPipeStage, r,
+                             base + r < t1 ? j.train.rows + static_cast<std::size_t>(base + r) * j.train.stride : nullptr);
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            bar_arrive(&full[b]);
+        }
+    } else if (lane == 0) {
+        const std::uint32_t a0 = smem_u32(tileA);
+        for (int s = 0; s < stages; ++s) {
+            const int b = s & 1;
+            if (!bar_wait(&full[b], (s >> 1) & 1, stop)) break;
+            if (s >= 2 && !bar_wait(&freeb[b], ((s - 2) >> 1) & 1, stop)) break;
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            const std::uint32_t b0 = smem_u32(tileB[b]);
+            const std::uint32_t d = tmem + static_cast<std::uint32_t>(b * kPipeStage);
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {  // K = 256 in slices of 32 bytes
+                const std::uint32_t koff = (k & 3) * 32;  // within the 128-byte swizzle atom
+                const std::uint64_t da = sw128_desc(a0 + (k >> 2) * kTcRowsA * 128 + koff);
+                const std::uint64_t db = sw128_desc(b0 + (k >> 2) * kPipeStage * 128 + koff);
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\tsetp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
+                    "l"(da), "l"(db), "r"(kPipeIdesc), "r"(k));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(
+                             smem_u32(&done[b]))
+                         : "memory");
+            *last_issued = s;
+        }
+    }
+    __syncthreads();
+    const bool failed = *stop != 0;
+    if (warp < kPipeEpiWarps) {
+#pragma unroll
+        for (int u = 1; u < 4; ++u) {
+            keep2(k1[0], k2[0], k1[u]);
+            keep2(k1[0], k2[0], k2[u]);
+        }
+        if (warp >= 4) xchg[qrow] = make_uint2(k1[0], k2[0]);
+    }
+    __syncthreads();
+    if (failed && tid == 0) atomicExch(&g_tc_error, 1);
+    if (!failed && warp < 4) {
+        const uint2 o = xchg[qrow];
+        keep2(k1[0], k2[0], o.x);
+        keep2(k1[0], k2[0], o.y);
+        const int q = qt * kTcRowsA + qrow;
+        if (q < j.query.capacity) {
+            const bool active = ok && q < nq;
+            const std::uint32_t a1 = active ? k1[0] : kEmptyKey, a2 = active ? k2[0] : kEmptyKey;
+            if (j.splits == 1) {
+                j.top2[q] = top2_from_keys(a1, a2);
+            } else {
+                j.partial[static_cast<std::size_t>(split) * j.query.capacity + q] = make_uint2(a1, a2);
+            }
+        }
+    }
+    if (warp == kPipeEpiWarps + kPipeProdWarps) {
+        // after a stop, MMAs may still be running: wait (bounded) for the last one
+        const int last = *last_issued;
+        if (failed && last >= 0) {
+            volatile int never = 0;
+            bar_wait(&done[last & 1], (last >> 1) & 1, &never);
+        }
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(2 * kPipeStage));
+    }
+}
+
 // Thread per query: the two smallest keys over all train partitions.
 template <class Src>
 __global__ __launch_bounds__(256) void knn_merge_kernel(const __grid_constant__ Src src) {

@@ -204,7 +204,9 @@ int stitch_pyramid_detect_describe(const stitch_image_view* image, const stitch_
  * default) the tcgen05 kind::i8 tensor-core kernel (descriptor bits as +-1
  * int8, Hamming = (256 - dot) / 2) with 256 train rows per MMA stage, 2 and
  * 3 the same kernel with 128 and 64 train rows per stage (smaller blocks,
- * more of them per SM). The choice is per thread, so threads never race on
+ * more of them per SM), 4 the pipelined tensor-core kernel (train-stage
+ * expansion, MMAs and the top-2 epilogue of consecutive stages overlapped by
+ * warp roles, two shared-memory stages and two TMEM accumulators). The choice is per thread, so threads never race on
  * it; stitch_batch_set_matcher changes one plan's. Results are identical. stitch_s4_tc_errors reads and clears the tensor-core
  * kernel's error word (1: an MMA completion wait ran out; -1: read failed). */
 int stitch_s4_set_matcher(int kind);

@@ -4,7 +4,7 @@ same cases as the __popc kernel: edges, ties across train tiles, planted
 partners at every shape including 8192 x 8192, counts below capacity, and
 the whole batched chain against the per-pair chain run with __popc. Every
 train-stage width runs (matcher kinds 1, 2, 3: 256, 128 and 64 train rows
-per MMA stage)."""
+per MMA stage), and the pipelined kernel (kind 4)."""
 import numpy as np
 import pytest
 import torch
@@ -16,7 +16,7 @@ from .test_gpu_s4 import check, planted, u8
 pytestmark = pytest.mark.gpu
 
 
-@pytest.fixture(params=[1, 2, 3], ids=["stage256", "stage128", "stage64"])
+@pytest.fixture(params=[1, 2, 3, 4], ids=["stage256", "stage128", "stage64", "pipelined"])
 def tc(cuda, request):
     from .gpu_util import Lib
     lib = Lib("ours")
@@ -54,7 +54,7 @@ def test_tc_full_microbenchmark_size(tc):
     assert ia.size > 0.2 * 8192
 
 
-@pytest.mark.parametrize("kind", [1, 2, 3])
+@pytest.mark.parametrize("kind", [1, 2, 3, 4])
 def test_tc_batched_chain_equals_popc_per_pair(cuda, kind):
     L = _abi.load()
     cases = []
