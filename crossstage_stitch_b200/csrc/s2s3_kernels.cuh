@@ -364,6 +364,7 @@ __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(cons
     __shared__ DetectJob jobs[2];  // jobs of the tiles in in[0] and in[1] (kept here, not in registers)
     __shared__ int locals[2];
     __shared__ int n_cand, n_found, next;
+    __shared__ std::uint32_t list_base;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     hist[tid] = 0;
     if (tid == 0) {
@@ -383,10 +384,6 @@ __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(cons
         const int W = j.width, H = j.height;
         const int y0 = (local / j.tiles_x) * kFastTileH, x0 = (local % j.tiles_x) * kFastTileW;
         std::uint8_t (*cur)[kInStride] = in[buf];
-        // what the flush after the last barrier needs (jobs[buf] is refilled then)
-        std::uint32_t* const job_hist = j.hist;
-        std::uint64_t* const job_maxima = j.maxima;
-        const std::uint32_t job_max = static_cast<std::uint32_t>(j.max_maxima);
         if (tid == 0) {
             int t = static_cast<int>(atomicAdd(queue, 1u));
             if (t < total && !src.find(t, kFastKind, &jobs[buf ^ 1], &locals[buf ^ 1])) t = total;
@@ -443,8 +440,7 @@ __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(cons
                         static_cast<std::uint16_t>(((r * kScGroups + q) << 4) | bits);
             }
         }
-        __syncthreads();  // (1) survivors listed, next tile known
-        if (tid == 0) n_found = 0;  // every thread read the last tile's count before this barrier
+        __syncthreads();
         // the next tile's bytes travel while this one is scored
         const int nt = next;
         if (nt < total) stage_fast_tile(jobs[buf ^ 1], locals[buf ^ 1], in[buf ^ 1]);
@@ -480,8 +476,7 @@ __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(cons
             }
             __syncwarp();
         }
-        __syncthreads();  // (2) scores complete
-        if (tid == 0) n_cand = 0;  // every thread read it before barrier (1)
+        __syncthreads();
         // 3. strict 3x3 maxima inside the 31-pixel edge margin: only listed
         // survivors can score above 0, so only they are tested
         for (int i = tid; i < nc; i += kFastThreads) {
@@ -503,25 +498,24 @@ __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(cons
                 }
             }
         }
-        cp_async_wait_all();
-        __syncthreads();  // (3) maxima listed, next tile staged
-        // the tile's maxima into the job's list, each warp one reservation
-        {
-            const int nf = n_found;
-            const int per = (nf + 7) >> 3, lo = min(nf, warp * per), hi = min(nf, lo + per);
-            if (lo < hi) {  // warp-uniform
-                std::uint32_t b = 0;
-                if (lane == 0) b = atomicAdd(job_hist + 256 + kListed, static_cast<std::uint32_t>(hi - lo));
-                b = __shfl_sync(0xffffffffu, b, 0);
-                for (int i = lo + lane; i < hi; i += 32)
-                    if (b + static_cast<std::uint32_t>(i - lo) < job_max) job_maxima[b + (i - lo)] = found[i];
-            }
-        }
-        // the histogram goes out when the next tile belongs to another job
-        if ((nt >= total || jobs[buf ^ 1].hist != job_hist) && hist[tid]) {
-            atomicAdd(job_hist + tid, hist[tid]);
+        __syncthreads();
+        // the tile's maxima and histogram into the job's list and histogram
+        const int nf = n_found;
+        if (tid == 0 && nf) list_base = atomicAdd(&j.counters()[kListed], static_cast<std::uint32_t>(nf));
+        __syncthreads();
+        for (int i = tid; i < nf; i += kFastThreads)
+            if (list_base + static_cast<std::uint32_t>(i) < static_cast<std::uint32_t>(j.max_maxima))
+                j.maxima[list_base + i] = found[i];
+        if (hist[tid]) {
+            atomicAdd(&j.hist[tid], hist[tid]);
             hist[tid] = 0;
         }
+        if (tid == 0) {
+            n_cand = 0;
+            n_found = 0;
+        }
+        cp_async_wait_all();
+        __syncthreads();
         tile = nt;
         buf ^= 1;
     }
