@@ -96,6 +96,12 @@ class PairDesc(C.Structure):
                 ("s2", S2Config), ("s4", S4Config), ("s5", S5Config), ("pyramid", PyramidConfig)]
 
 
+class BatchTuning(C.Structure):
+    """stitch_batch_tuning: launch shapes of a batch plan (0: default)."""
+    _fields_ = [("fast_ctas_per_sm", C.c_int), ("blur_ctas_per_sm", C.c_int), ("matcher", C.c_int),
+                ("search_hpw", C.c_int), ("resize_tile_h", C.c_int)]
+
+
 class ServerConfig(C.Structure):
     """stitch_server_config."""
     _fields_ = [("arena", C.c_void_p), ("arena_bytes", C.c_size_t), ("device", C.c_int), ("max_batch", C.c_int),
@@ -187,6 +193,8 @@ PROTOTYPES: dict[str, tuple] = {
     "stitch_s6_render": (C.c_int, [P(ImageView), P(ImageView), P(S6Geometry), C.c_int, P(ImageView), P(ImageView),
                                    C.c_void_p, C.c_size_t, C.c_void_p, P(C.c_uint64)]),
     "stitch_batch_create": (C.c_int, [C.c_int, P(PairDesc), P(C.c_void_p), _size_p, P(C.c_int)]),
+    "stitch_batch_create_tuned": (C.c_int, [C.c_int, P(PairDesc), P(BatchTuning), P(C.c_void_p), _size_p,
+                                            P(C.c_int)]),
     "stitch_batch_enqueue": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p]),
     "stitch_batch_capture": (C.c_int, [C.c_void_p, C.c_void_p, C.c_size_t, C.c_void_p, C.c_void_p]),
     "stitch_batch_launch": (C.c_int, [C.c_void_p, C.c_void_p]),

@@ -124,7 +124,8 @@ Status Plan::build(int n_pairs, const stitch_pair_desc* p, int* bad_pair, bool a
                 continue;
             }
             if (!s2s3::pyramid_layout(im.width, im.height, q.s2.max_keypoints, q.pyramid.levels,
-                                      q.pyramid.scale_factor, &o.pyr[s])) {
+                                      q.pyramid.scale_factor, &o.pyr[s],
+                                      tuning.resize_tile_h ? tuning.resize_tile_h : s2s3::kResizeTileH)) {
                 if (bad_pair) *bad_pair = i;
                 return Status::INVALID_ARGUMENT;
             }
@@ -221,10 +222,11 @@ Status Plan::build(int n_pairs, const stitch_pair_desc* p, int* bad_pair, bool a
     long long rounds_at = 0;
     hpw = 32;
     for (int h : {32, 16, 8, 4}) {
+        if (tuning.search_hpw && h != tuning.search_hpw) continue;
         hpw = h;
         rounds_at = 0;
         for (int i = 0; i < n; ++i) rounds_at += s5k::plan_search(pairs[i].s5.hypotheses, h);
-        if (rounds_at >= 2 * kSmCount) break;
+        if (tuning.search_hpw || rounds_at >= 2 * kSmCount) break;
     }
     search_blocks = static_cast<int>(rounds_at);
     // block totals of every detect, describe and resize kind, for the block
@@ -618,13 +620,20 @@ Status Plan::enqueue(void* ws, std::size_t bytes, stitch_homography_result* host
     };
     mark();  // tables uploaded, counts cleared
     for (int kind = 0; kind + 1 < max_levels; ++kind)  // layer kind + 1 of every pyramid image
-        if (go(rs_blocks[kind])) s2s3::resize_kernel<RsSrc, s2s3::kResizeTileH><<<rs_blocks[kind], 256, 0, s>>>(rs, kind);
+        if (go(rs_blocks[kind])) {
+            switch (tuning.resize_tile_h) {
+                case 16: s2s3::resize_kernel<RsSrc, 16><<<rs_blocks[kind], 256, 0, s>>>(rs, kind); break;
+                case 32: s2s3::resize_kernel<RsSrc, 32><<<rs_blocks[kind], 256, 0, s>>>(rs, kind); break;
+                default: s2s3::resize_kernel<RsSrc, s2s3::kResizeTileH><<<rs_blocks[kind], 256, 0, s>>>(rs, kind);
+            }
+        }
     mark();
     std::uint32_t* q = at<std::uint32_t>(ws, queue);  // FAST tile queue, then the blur-list count
     const int tiles = det_blocks[s2s3::kFastKind];
     if (go(tiles))
-        s2s3::fast_kernel<DetSrc><<<std::min(tiles, kSmCount * s2s3::kFastCtasPerSm), s2s3::kFastThreads, 0, s>>>(
-            det, q, tiles);
+        s2s3::fast_kernel<DetSrc><<<std::min(tiles, kSmCount * (tuning.fast_ctas_per_sm ? tuning.fast_ctas_per_sm
+                                                                                      : s2s3::kFastCtasPerSm)),
+                                    s2s3::kFastThreads, 0, s>>>(det, q, tiles);
     mark();
     if (go(det_blocks[s2s3::kSelectKind])) {
         s2s3::select_kernel<DetSrc><<<det_blocks[s2s3::kSelectKind], 256, 0, s>>>(det);
@@ -642,8 +651,9 @@ Status Plan::enqueue(void* ws, std::size_t bytes, stitch_homography_result* host
     mark();
     if (go(tiles > 0 && blur_total > 0 ? 1 : 0))
         s2s3::blur_tiles_kernel<DesSrc>
-            <<<static_cast<int>(std::min<std::size_t>(blur_total, kSmCount * s2s3::kBlurCtasPerSm)), 256, 0, s>>>(des, at<uint2>(ws, blur_list),
-                                                                                                 q + 1);
+            <<<static_cast<int>(std::min<std::size_t>(
+                   blur_total, kSmCount * (tuning.blur_ctas_per_sm ? tuning.blur_ctas_per_sm : s2s3::kBlurCtasPerSm))),
+               256, 0, s>>>(des, at<uint2>(ws, blur_list), q + 1);
     mark();
     if (go(des_blocks[s2s3::kDescKind]))
         s2s3::describe_kernel<DesSrc><<<des_blocks[s2s3::kDescKind], s2s3::kDescWarps * 32, 0, s>>>(des);
@@ -733,21 +743,39 @@ struct stitch_batch {
 
 extern "C" {
 
-int stitch_batch_create(int n_pairs, const stitch_pair_desc* pairs, stitch_batch** out, size_t* bytes,
-                        int* bad_pair) {
+int stitch_batch_create_tuned(int n_pairs, const stitch_pair_desc* pairs, const stitch_batch_tuning* tuning,
+                              stitch_batch** out, size_t* bytes, int* bad_pair) {
     if (!out || !bytes) return static_cast<int>(Status::INVALID_ARGUMENT);
     *out = nullptr;
     *bytes = 0;
+    if (tuning) {
+        const auto& t = *tuning;
+        const bool ok = t.fast_ctas_per_sm >= 0 && t.fast_ctas_per_sm <= stitch::b200::s2s3::kFastCtasPerSm &&
+                        t.blur_ctas_per_sm >= 0 && t.blur_ctas_per_sm <= stitch::b200::s2s3::kBlurCtasPerSm &&
+                        (t.matcher == 0 || stitch::b200::s4k::valid_matcher(t.matcher - 1)) &&
+                        (t.search_hpw == 0 || t.search_hpw == 4 || t.search_hpw == 8 || t.search_hpw == 16 ||
+                         t.search_hpw == 32) &&
+                        (t.resize_tile_h == 0 || t.resize_tile_h == 16 || t.resize_tile_h == 32 ||
+                         t.resize_tile_h == 64);
+        if (!ok) return static_cast<int>(Status::INVALID_ARGUMENT);
+    }
     auto* b = new (std::nothrow) stitch_batch;
     if (!b) return static_cast<int>(Status::CUDA_ERROR);
+    if (tuning) b->plan.tuning = *tuning;
     const Status st = b->plan.build(n_pairs, pairs, bad_pair);
     if (st != Status::OK) {
         delete b;
         return static_cast<int>(st);
     }
+    if (tuning && tuning->matcher > 0) b->plan.matcher = tuning->matcher - 1;
     *bytes = b->plan.total;
     *out = b;
     return 0;
+}
+
+int stitch_batch_create(int n_pairs, const stitch_pair_desc* pairs, stitch_batch** out, size_t* bytes,
+                        int* bad_pair) {
+    return stitch_batch_create_tuned(n_pairs, pairs, nullptr, out, bytes, bad_pair);
 }
 
 int stitch_batch_enqueue(stitch_batch* b, void* ws, size_t bytes, stitch_homography_result* results, void* stream) {

@@ -60,6 +60,7 @@ public:
     // binary matcher of this plan's S4 launches (s4k::kMatcherPopc or
     // kMatcherTensor): the building thread's choice, or stitch_batch_set_matcher's
     int matcher = s4k::kMatcherTensor;
+    stitch_batch_tuning tuning{};  // launch shapes (0: default)
     // host staging of the tables (pinned), filled for one workspace address;
     // either allocated by build() or lent by the caller (use_staging)
     unsigned char* staging = nullptr;

@@ -319,6 +319,27 @@ typedef struct stitch_batch stitch_batch;
  * offending pair. */
 int stitch_batch_create(int n_pairs, const stitch_pair_desc* pairs, stitch_batch** plan,
                         size_t* workspace_bytes, int* bad_pair);
+/* No reference counterpart (batched form). Launch shapes of a plan, chosen
+ * per plan by an autotuner (results never depend on them); 0 in a field
+ * keeps its default. fast_ctas_per_sm: resident FAST blocks per SM in the
+ * persistent FAST grid, 1..8 (default 8); blur_ctas_per_sm: the same for the
+ * on-demand blur, 1..6 (default 6); matcher: 1 + an S4 matcher kind (0..4,
+ * as for stitch_s4_set_matcher), or 0 for the creating thread's choice;
+ * search_hpw: MSAC hypotheses per warp round, 4, 8, 16 or 32 (default: the
+ * largest that still fills about two waves); resize_tile_h: pyramid rows per
+ * resize block, 16, 32 or 64 (default 64). */
+typedef struct stitch_batch_tuning {
+    int fast_ctas_per_sm;
+    int blur_ctas_per_sm;
+    int matcher;
+    int search_hpw;
+    int resize_tile_h;
+} stitch_batch_tuning;
+
+/* No reference counterpart (batched form). stitch_batch_create with a
+ * tuning (NULL: the defaults); INVALID_ARGUMENT for a field out of range. */
+int stitch_batch_create_tuned(int n_pairs, const stitch_pair_desc* pairs, const stitch_batch_tuning* tuning,
+                              stitch_batch** plan, size_t* workspace_bytes, int* bad_pair);
 /* No reference counterpart (batched form). Enqueues the whole chain for all
  * pairs on `stream`: results are identical, bit for bit, to calling the
  * stages pair by pair. results_pinned (n entries, may be NULL) receives the
