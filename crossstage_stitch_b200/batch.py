@@ -29,14 +29,20 @@ class Batch:
     """Plan + workspace of one batch. The images must stay alive (and at the
     same addresses) while the plan is used."""
 
-    def __init__(self, descs: list[PairDesc], device=None):
+    def __init__(self, descs: list[PairDesc], device=None, tuning: dict | None = None):
+        """tuning: launch shapes of the plan (the fields of
+        _abi.BatchTuning; missing or 0 fields keep their defaults)."""
         self.lib = _abi.load()
         self.n = len(descs)
         arr = (PairDesc * self.n)(*descs)
         plan = C.c_void_p()
         nbytes = C.c_size_t()
         bad = C.c_int(-1)
-        st = self.lib.stitch_batch_create(self.n, arr, C.byref(plan), C.byref(nbytes), C.byref(bad))
+        t = None
+        if tuning:
+            t = _abi.BatchTuning(**{k: int(v) for k, v in tuning.items()})
+        st = self.lib.stitch_batch_create_tuned(self.n, arr, C.byref(t) if t is not None else None, C.byref(plan),
+                                                C.byref(nbytes), C.byref(bad))
         if st != 0:
             raise StageError(f"stitch_batch_create (pair {bad.value})", st)
         self.plan = plan
