@@ -75,6 +75,8 @@ bool match_layout(int capacity_a, int capacity_b, bool cross, MatchLayout* out) 
     if (l.fsplits > 1) cursor += static_cast<std::size_t>(l.fsplits) * a * sizeof(uint2);
     l.rpartial = cursor;
     if (cross && l.rsplits > 1) cursor += static_cast<std::size_t>(l.rsplits) * b * sizeof(uint2);
+    l.accept_counts = cursor;
+    cursor += static_cast<std::size_t>((capacity_a + 1023) / 1024) * sizeof(int);
     l.total = cursor;
     *out = l;
     return true;
@@ -224,8 +226,16 @@ Status s4_match(const Keypoints& a, const Descriptors& da, const Keypoints& b, c
     aj.l2 = da.type == DescriptorType::FLOAT32;
     aj.ratio = aj.l2 ? config.ratio_threshold * config.ratio_threshold : config.ratio_threshold;
     aj.out = output;
-    accept_kernel<OneJob<AcceptJob>><<<1, 1024, 0, stream>>>(OneJob<AcceptJob>{aj});
-    note_launches(1);
+    if (a.capacity <= 1024) {
+        accept_kernel<OneJob<AcceptJob>><<<1, 1024, 0, stream>>>(OneJob<AcceptJob>{aj});
+        note_launches(1);
+    } else {  // many blocks: counts per 1024 queries, then offsets and the compaction
+        const int blocks = ceil_div(a.capacity, 1024);
+        int* counts = at_offset<int>(workspace, l.accept_counts);
+        accept_count_kernel<OneJob<AcceptJob>><<<blocks, 1024, 0, stream>>>(OneJob<AcceptJob>{aj}, counts);
+        accept_scatter_kernel<OneJob<AcceptJob>><<<blocks, 1024, 0, stream>>>(OneJob<AcceptJob>{aj}, counts);
+        note_launches(2);
+    }
     return launch_status();
 }
 

@@ -8,7 +8,7 @@
 namespace stitch::b200::s4k {
 
 struct MatchLayout {
-    std::size_t forward, reverse, fpartial, rpartial, total;
+    std::size_t forward, reverse, fpartial, rpartial, accept_counts, total;  // accept_counts: int per 1024 queries
     int fq_tiles, fsplits, frows;  // forward direction plan
     int rq_tiles, rsplits, rrows;  // reverse direction plan
 };

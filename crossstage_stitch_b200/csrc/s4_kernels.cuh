@@ -254,6 +254,65 @@ __device__ __forceinline__ std::uint64_t sw128_desc(std::uint32_t addr) {
            (2ull << 61);
 }
 
+// Packed top-2 of one stage's columns: in each 32-bit word the low 16-bit
+// lane holds a key of an even column and the high lane one of the next odd
+// column, key16 = (distance << 7) | (column - first) / 2 with distance =
+// (256 - dot) / 2 <= 256 (so key16 <= 32895; 0xffff is empty). Within a
+// lane, smaller key16 is exactly (smaller distance, then smaller column), so
+// one min/max.u16x2 updates two candidates. The even and odd lanes are
+// folded into the 32-bit (distance << 23 | train index) chains when the
+// stage ends (fold_stage), which keeps the top-2 exact.
+__device__ __forceinline__ void keep2x2(std::uint32_t& a1, std::uint32_t& a2, std::uint32_t x) {
+    a2 = __vminu2(a2, __vmaxu2(a1, x));
+    a1 = __vminu2(a1, x);
+}
+
+// 32 dot products v of columns first + c .. first + c + 31 (c even) into
+// the packed chains; columns at or past `limit` (train rows past the end)
+// are left out.
+__device__ __forceinline__ void stage_keys32(const std::uint32_t (&v)[32], int c, int first, int limit,
+                                             std::uint32_t (&p1)[4], std::uint32_t (&p2)[4]) {
+    const std::uint32_t m0 = static_cast<std::uint32_t>(c >> 1);
+    constexpr std::uint32_t kBias = (256u << 6) + (256u << 22);  // (256 - v) << 6 per lane, as one add
+    if (first + c + 32 <= limit) {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            const std::uint32_t m = m0 + static_cast<std::uint32_t>(i);
+            const std::uint32_t x = (kBias + (m | (m << 16))) - (v[2 * i] << 6) - (v[2 * i + 1] << 22);
+            keep2x2(p1[i & 3], p2[i & 3], x);
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            const std::uint32_t m = m0 + static_cast<std::uint32_t>(i);
+            std::uint32_t x = (kBias + (m | (m << 16))) - (v[2 * i] << 6) - (v[2 * i + 1] << 22);
+            if (first + c + 2 * i >= limit) x |= 0x0000ffffu;
+            if (first + c + 2 * i + 1 >= limit) x |= 0xffff0000u;
+            keep2x2(p1[i & 3], p2[i & 3], x);
+        }
+    }
+}
+
+// The packed chains of a stage whose first column is train row `first`
+// into the 32-bit key chains; the packed chains are emptied.
+__device__ __forceinline__ void fold_stage(std::uint32_t (&p1)[4], std::uint32_t (&p2)[4], std::uint32_t first,
+                                           std::uint32_t (&k1)[4], std::uint32_t (&k2)[4]) {
+#pragma unroll
+    for (int ch = 0; ch < 4; ++ch) {
+#pragma unroll
+        for (int r = 0; r < 2; ++r) {
+            const std::uint32_t w = r ? p2[ch] : p1[ch];
+#pragma unroll
+            for (int lane = 0; lane < 2; ++lane) {
+                const std::uint32_t key = (w >> (16 * lane)) & 0xffffu;
+                if (key != 0xffffu)
+                    keep2(k1[ch], k2[ch], ((key >> 7) << 23) + first + 2 * (key & 127u) + static_cast<std::uint32_t>(lane));
+            }
+        }
+        p1[ch] = p2[ch] = 0xffffffffu;
+    }
+}
+
 template <class Src, int kRowsB>
 __global__ __launch_bounds__(kQueryThreads, 1) void knn_tc_kernel(const __grid_constant__ Src src) {
     using Shape = TcShape<kRowsB>;
@@ -296,6 +355,7 @@ __global__ __launch_bounds__(kQueryThreads, 1) void knn_tc_kernel(const __grid_c
     std::uint32_t k1[4] = {kEmptyKey, kEmptyKey, kEmptyKey, kEmptyKey};
     std::uint32_t k2[4] = {kEmptyKey, kEmptyKey, kEmptyKey, kEmptyKey};
     std::uint32_t phase = 0;
+    std::uint32_t p1[4] = {~0u, ~0u, ~0u, ~0u}, p2[4] = {~0u, ~0u, ~0u, ~0u};  // packed chains of a stage
     for (int base = t0; base < t1; base += kTcRowsB) {
         for (int r = tid; r < kTcRowsB; r += kQueryThreads)
             stage_pm_row(tileB, kTcRowsB, r,
@@ -349,17 +409,9 @@ __global__ __launch_bounds__(kQueryThreads, 1) void knn_tc_kernel(const __grid_c
                   "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
                 : "r"(tmem + (static_cast<std::uint32_t>(warp * 32) << 16) + static_cast<std::uint32_t>(c)));
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            // (256 - dot) = 2 * Hamming, so (256 - dot) << 22 is the distance << 23
-            const std::uint32_t t = static_cast<std::uint32_t>(base + c);
-            if (base + c + 32 <= t1) {
-#pragma unroll
-                for (int i = 0; i < 32; ++i) keep2(k1[i & 3], k2[i & 3], ((256u - v[i]) << 22) + (t + i));
-            } else {
-#pragma unroll
-                for (int i = 0; i < 32; ++i)
-                    if (base + c + i < t1) keep2(k1[i & 3], k2[i & 3], ((256u - v[i]) << 22) + (t + i));
-            }
+            stage_keys32(v, c, base, t1, p1, p2);
         }
+        fold_stage(p1, p2, static_cast<std::uint32_t>(base), k1, k2);
         asm volatile("tcgen05.fence::before_thread_sync;");
         __syncthreads();  // TMEM and the train stage are free for the next stage
     }
@@ -478,6 +530,7 @@ __global__ __launch_bounds__(kPipeThreads, 1) void knn_tc_pipe_kernel(const __gr
     const int qrow = 32 * (warp & 3) + lane;  // epilogue: the query of this thread
     if (warp < kPipeEpiWarps) {
         const int half = warp >> 2;
+        std::uint32_t p1[4] = {~0u, ~0u, ~0u, ~0u}, p2[4] = {~0u, ~0u, ~0u, ~0u};  // packed chains of a stage
         for (int s = 0; s < stages; ++s) {
             const int b = s & 1;
             // the TMEM loads below are warp-collective: the warp goes on only together
@@ -499,19 +552,11 @@ __global__ __launch_bounds__(kPipeThreads, 1) void knn_tc_pipe_kernel(const __gr
                     : "r"(tmem + (static_cast<std::uint32_t>((warp & 3) * 32) << 16) +
                           static_cast<std::uint32_t>(b * kPipeStage + half * (kPipeStage / 2) + c)));
                 asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                // (256 - dot) = 2 * Hamming, so (256 - dot) << 22 is the distance << 23
-                const std::uint32_t t = static_cast<std::uint32_t>(base + c);
-                if (base + c + 32 <= t1) {
-#pragma unroll
-                    for (int i = 0; i < 32; ++i) keep2(k1[i & 3], k2[i & 3], ((256u - v[i]) << 22) + (t + i));
-                } else {
-#pragma unroll
-                    for (int i = 0; i < 32; ++i)
-                        if (base + c + i < t1) keep2(k1[i & 3], k2[i & 3], ((256u - v[i]) << 22) + (t + i));
-                }
+                stage_keys32(v, c, base, t1, p1, p2);
             }
             asm volatile("tcgen05.fence::before_thread_sync;");
             bar_arrive(&freeb[b]);
+            fold_stage(p1, p2, static_cast<std::uint32_t>(base), k1, k2);
         }
     } else if (warp < kPipeEpiWarps + kPipeProdWarps) {
         const int p = tid - kPipeEpiWarps * 32;  // 0 .. 127
@@ -683,6 +728,68 @@ struct AcceptJob {
     int l2;
     ::stitch::Matches out;
 };
+
+// Whether query q's forward neighbours pass the ratio test (and the mutual
+// check when there is a reverse direction); *p gets its Top2.
+__device__ __forceinline__ bool accepted(const AcceptJob& j, int q, Top2* p) {
+    *p = j.forward[q];
+    bool accept = p->second_index >= 0 &&
+                  (p->first_distance == 0 ? p->second_distance > 0 : p->first_distance < j.ratio * p->second_distance);
+    if (accept && j.reverse) accept = j.reverse[p->first_index].first_index == q;
+    return accept;
+}
+
+__device__ __forceinline__ void write_match(const AcceptJob& j, int at, int q, const Top2& p) {
+    j.out.idx_a[at] = q;
+    j.out.idx_b[at] = p.first_index;
+    const double d = j.l2 ? sqrt(p.first_distance) : p.first_distance;
+    j.out.distance[at] = d > FLT_MAX ? CUDART_INF_F : static_cast<float>(d);
+}
+
+// The accept step of one large query set over many blocks: block b counts
+// the accepted queries among b * 1024 .. b * 1024 + 1023 ...
+template <class Src>
+__global__ __launch_bounds__(1024) void accept_count_kernel(const __grid_constant__ Src src, int* counts) {
+    AcceptJob j;
+    int local;
+    if (!src.find(0, &j, &local)) return;
+    const int q = blockIdx.x * 1024 + threadIdx.x;
+    Top2 p;
+    const int n = __syncthreads_count(q < j.capacity && accepted(j, q, &p));
+    if (threadIdx.x == 0) counts[blockIdx.x] = n;
+}
+
+// ... and then writes them after the accepted queries of all earlier
+// blocks, in query order; the last block writes the match count.
+template <class Src>
+__global__ __launch_bounds__(1024) void accept_scatter_kernel(const __grid_constant__ Src src, const int* counts) {
+    __shared__ int warp_sum[32];
+    __shared__ int offset;
+    AcceptJob j;
+    int local;
+    if (!src.find(0, &j, &local)) return;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    if (warp == 0) {
+        int s = 0;
+        for (int b = lane; b < static_cast<int>(blockIdx.x); b += 32) s += counts[b];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+        if (lane == 0) offset = s;
+    }
+    const int q = blockIdx.x * 1024 + threadIdx.x;
+    Top2 p{};
+    const bool accept = q < j.capacity && accepted(j, q, &p);
+    const unsigned ballot = __ballot_sync(0xffffffffu, accept);
+    if (lane == 0) warp_sum[warp] = __popc(ballot);
+    __syncthreads();
+    int before = 0, total = 0;
+    for (int w = 0; w < 32; ++w) {
+        before += w < warp ? warp_sum[w] : 0;
+        total += warp_sum[w];
+    }
+    if (accept) write_match(j, offset + before + __popc(ballot & ((1u << lane) - 1u)), q, p);
+    if (blockIdx.x == gridDim.x - 1 && threadIdx.x == 0) *j.out.d_count = offset + total;
+}
 
 // One block per query set: ratio test (+ mutual check) and a stable
 // compaction in query order; writes the match count.

@@ -228,8 +228,8 @@ int stitch_s4_match(const stitch_keypoints* a, const stitch_descriptors* da, con
  * device allocations, or a loop that cannot afford cudaMalloc's implicit
  * device synchronisation). The workspace is a 4 MiB array in the library's
  * own device memory, held by every GPU that loads the library until exit;
- * requests needing more fail with INSUFFICIENT_WORKSPACE (up to 87381 query
- * and train rows each fit with the mutual check, 174762 without, at the
+ * requests needing more fail with INSUFFICIENT_WORKSPACE (up to 87374 query
+ * and train rows each fit with the mutual check, 174734 without, at the
  * current workspace layout). The first call on a device
  * looks the array up (make it before any stream capture); all calls on a
  * device share the array, so calls that overlap on the GPU race. */
