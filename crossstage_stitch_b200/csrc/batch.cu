@@ -620,12 +620,11 @@ Status Plan::enqueue(void* ws, std::size_t bytes, stitch_homography_result* host
     };
     mark();  // tables uploaded, counts cleared
     for (int kind = 0; kind + 1 < max_levels; ++kind)  // layer kind + 1 of every pyramid image
-        if (go(rs_blocks[kind])) {  // persistent: at most 6 blocks per SM walk the layer's tiles
-            const int tiles = rs_blocks[kind], grid = std::min(tiles, kSmCount * 6);
+        if (go(rs_blocks[kind])) {
             switch (tuning.resize_tile_h) {
-                case 16: s2s3::resize_kernel<RsSrc, 16><<<grid, 256, 0, s>>>(rs, kind, tiles); break;
-                case 32: s2s3::resize_kernel<RsSrc, 32><<<grid, 256, 0, s>>>(rs, kind, tiles); break;
-                default: s2s3::resize_kernel<RsSrc, s2s3::kResizeTileH><<<grid, 256, 0, s>>>(rs, kind, tiles);
+                case 16: s2s3::resize_kernel<RsSrc, 16><<<rs_blocks[kind], 256, 0, s>>>(rs, kind); break;
+                case 32: s2s3::resize_kernel<RsSrc, 32><<<rs_blocks[kind], 256, 0, s>>>(rs, kind); break;
+                default: s2s3::resize_kernel<RsSrc, s2s3::kResizeTileH><<<rs_blocks[kind], 256, 0, s>>>(rs, kind);
             }
         }
     mark();

@@ -219,8 +219,7 @@ Status pyramid_detect_describe(const ImageView& image, const s2::Config& c, int 
     int launches = 0;
     for (int i = 1; i < n; ++i) {
         resize_kernel<OneJob<ResizeJob>, kSingleResizeTileH>
-            <<<std::min(l.resize_tiles[i], kSmCount * 6), 256, 0, stream>>>(OneJob<ResizeJob>{jobs.resize[i]}, 0,
-                                                                              l.resize_tiles[i]);
+            <<<l.resize_tiles[i], 256, 0, stream>>>(OneJob<ResizeJob>{jobs.resize[i]}, 0);
         ++launches;
     }
     DetSrc det{};

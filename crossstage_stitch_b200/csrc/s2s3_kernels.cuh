@@ -878,151 +878,116 @@ __device__ __forceinline__ int2 linear_exact_tap(int v, int src, double scale) {
 constexpr int kRawStride = 112;  // bytes of a staged source row: 7 chunks of 16
 template <int kTileH> __host__ __device__ constexpr int resize_raw_rows() { return kTileH * 3 / 2 + 6; }
 
-// Source window of resize tile (x0, y0): rows ry0 .. ry1 and nchunk 16-byte
-// chunks from column rx0 (bounded in float with a pixel of slack per side;
-// the exact taps are checked against it before it is used). `window` is false
-// when the source is not 16-byte aligned or the window does not fit.
-struct ResizeWindow {
-    int ry0, ry1, rx0, nchunk;
-    bool window;
-};
-template <int kTileH>
-__device__ __forceinline__ ResizeWindow resize_window(const ResizeJob& j, int x0, int y0) {
-    constexpr int kRows = resize_raw_rows<kTileH>(), kChunks = kRawStride / 16;
-    const float fy = static_cast<float>(j.src_height) / static_cast<float>(j.height);
-    const float fx = static_cast<float>(j.src_width) / static_cast<float>(j.width);
-    const int last_y = min(y0 + kTileH, j.height) - 1, last_x = min(x0 + kResizeTileW, j.width) - 1;
-    ResizeWindow w;
-    w.ry0 = max(__float2int_rd((y0 + 0.5f) * fy - 0.5f) - 1, 0);
-    w.ry1 = min(__float2int_rd((last_y + 0.5f) * fy - 0.5f) + 2, j.src_height - 1);
-    w.rx0 = max(__float2int_rd((x0 + 0.5f) * fx - 0.5f) - 1, 0) & ~15;
-    const int rx1 = min(__float2int_rd((last_x + 0.5f) * fx - 0.5f) + 2, j.src_width - 1);
-    const int nrow = w.ry1 - w.ry0 + 1;
-    w.nchunk = rx1 >= w.rx0 ? (rx1 - w.rx0) / 16 + 1 : 0;
-    w.window = ((reinterpret_cast<std::uintptr_t>(j.src) | static_cast<std::uintptr_t>(j.src_pitch)) & 15) == 0 &&
-               nrow > 0 && nrow <= kRows && w.nchunk > 0 && w.nchunk <= kChunks;
-    return w;
-}
-
-// Copies the window into `raw` (chunks start 16-byte aligned below the
-// source width; one that reaches past a row's last pixel is copied byte by
-// byte, zeros beyond it): asynchronous 16-byte copies, complete at the
-// caller's cp_async_wait_all.
-template <int kTileH>
-__device__ __forceinline__ void resize_stage(const ResizeJob& j, const ResizeWindow& w,
-                                             std::uint8_t (*raw)[kRawStride]) {
-    if (!w.window) return;
-    const int n = (w.ry1 - w.ry0 + 1) * w.nchunk;
-    for (int i = threadIdx.x; i < n; i += 256) {
-        const int r = i / w.nchunk, c = i - r * w.nchunk, col = w.rx0 + 16 * c;
-        const std::uint8_t* p = j.src + static_cast<std::size_t>(w.ry0 + r) * j.src_pitch + col;
-        if (col + 16 <= j.src_width) {
-            cp_async16(&raw[r][16 * c], p);
-        } else {
-            for (int b = 0; b < 16; ++b) raw[r][16 * c + b] = col + b < j.src_width ? p[b] : 0;
-        }
-    }
-}
-
-// Pyramid layer kind + 1 of every job of the launch, 64 x kTileH output
-// tiles, persistent: block b takes tiles b, b + gridDim.x, ... of `total`
-// (looked up through the source's entries of `kind`), and copies the next
-// tile's source window into the other half of a double buffer while it
-// computes the current one:
-//   1. per-tile column and row taps in shared memory (double, as above);
-//   2. each warp produces whole layer rows, each lane two adjacent outputs:
-//        h(r, c) = src[r][c0] * (256 - wx) + src[r][c1] * wx   (< 2^16)
-//        out = (h(r0, c) * (256 - wy) + h(r1, c) * wy + 2^15) >> 16,
-//      the integer form of the 8-bit fixed-point horizontal pass followed
-//      by the vertical pass with one final rounding.
-// A tile whose exact taps leave the staged window (source not 16-byte
-// aligned, or a layer ratio above about 1.45) reads the source bytes from
-// global memory instead, with the same result.
 template <class Src, int kTileH>
-__global__ __launch_bounds__(256, 6) void resize_kernel(const __grid_constant__ Src src, int kind, int total) {
+__global__ __launch_bounds__(256, 6) void resize_kernel(const __grid_constant__ Src src, int kind) {
     static_assert(kTileH >= 16 && kTileH <= kResizeTileH && kTileH % 16 == 0, "resize tile height");
-    constexpr int th = kTileH, kRows = resize_raw_rows<kTileH>();
+    constexpr int th = kTileH, kRows = resize_raw_rows<kTileH>(), kChunks = kRawStride / 16;
     __shared__ int2 xtap[kResizeTileW];
     __shared__ int2 ytap[kTileH];
-    __shared__ __align__(16) std::uint8_t raw2[2][kRows][kRawStride];
+    __shared__ __align__(16) std::uint8_t raw[kRows][kRawStride];
     __shared__ double scale[2];
-    const int t = threadIdx.x, lane = t & 31;
-    int tile = blockIdx.x, buf = 0;
-    {
-        ResizeJob j0;
-        int l0;
-        if (tile < total && src.find(tile, kind, &j0, &l0))
-            resize_stage<kTileH>(j0, resize_window<kTileH>(j0, (l0 % j0.tiles_x) * kResizeTileW, (l0 / j0.tiles_x) * th),
-                                 raw2[0]);
-    }
-    for (; tile < total; tile += gridDim.x, buf ^= 1) {
-        ResizeJob j;
-        int local;
-        if (!src.find(tile, kind, &j, &local)) break;  // block-uniform
-        std::uint8_t (*raw)[kRawStride] = raw2[buf];
-        const int y0 = (local / j.tiles_x) * th, x0 = (local % j.tiles_x) * kResizeTileW;
-        const ResizeWindow w = resize_window<kTileH>(j, x0, y0);
-        if (t == 0) scale[0] = linear_exact_scale(j.src_width, j.width);
-        if (t == 32) scale[1] = linear_exact_scale(j.src_height, j.height);
-        cp_async_wait_all();
-        __syncthreads();  // window staged, scales known
-        if (t < kResizeTileW) xtap[t] = linear_exact_tap(min(x0 + t, j.width - 1), j.src_width, scale[0]);
-        else if (t < kResizeTileW + th)
-            ytap[t - kResizeTileW] = linear_exact_tap(min(y0 + t - kResizeTileW, j.height - 1), j.src_height, scale[1]);
-        __syncthreads();  // taps known
-        {   // the next tile's window travels while this one is computed
-            const int nt = tile + static_cast<int>(gridDim.x);
-            ResizeJob jn;
-            int ln;
-            if (nt < total && src.find(nt, kind, &jn, &ln))
-                resize_stage<kTileH>(jn, resize_window<kTileH>(jn, (ln % jn.tiles_x) * kResizeTileW, (ln / jn.tiles_x) * th),
-                                     raw2[buf ^ 1]);
-        }
-        // taps are nondecreasing: the first and last give the tile's source span
-        const bool staged = w.window && ytap[0].x >= w.ry0 && min(ytap[th - 1].x + 1, j.src_height - 1) <= w.ry1 &&
-                            xtap[0].x >= w.rx0 && min(xtap[kResizeTileW - 1].x + 1, j.src_width - 1) < w.rx0 + 16 * w.nchunk;
-        // warp w: rows w, w + 8, ...; lane l: columns 2l, 2l + 1
-        const int c = 2 * lane, x = x0 + c;
-        if (x < j.width) {
-            const int2 t0 = xtap[c], t1 = xtap[c + 1];  // columns past the layer edge repeat the last tap
-            const int wx0 = t0.y, wx1 = t1.y;
-            int xa0 = t0.x, xb0 = min(t0.x + 1, j.src_width - 1), xa1 = t1.x, xb1 = min(t1.x + 1, j.src_width - 1);
-            if (staged) {
-                xa0 -= w.rx0; xb0 -= w.rx0; xa1 -= w.rx0; xb1 -= w.rx0;
-            }
-            for (int rr = t >> 5; rr < th; rr += 8) {
-                const int y = y0 + rr;
-                if (y >= j.height) break;
-                const int2 ty = ytap[rr];
-                const int ra = ty.x, rb = min(ty.x + 1, j.src_height - 1), wy = ty.y;
-                int pa[4], pb[4];  // rows ra, rb at xa0, xb0, xa1, xb1
-                if (staged) {
-                    const std::uint8_t* A = raw[ra - w.ry0];
-                    const std::uint8_t* B = raw[rb - w.ry0];
-                    pa[0] = A[xa0]; pa[1] = A[xb0]; pa[2] = A[xa1]; pa[3] = A[xb1];
-                    pb[0] = B[xa0]; pb[1] = B[xb0]; pb[2] = B[xa1]; pb[3] = B[xb1];
-                } else {
-                    const std::uint8_t* A = j.src + static_cast<std::size_t>(ra) * j.src_pitch;
-                    const std::uint8_t* B = j.src + static_cast<std::size_t>(rb) * j.src_pitch;
-                    pa[0] = __ldg(A + xa0); pa[1] = __ldg(A + xb0); pa[2] = __ldg(A + xa1); pa[3] = __ldg(A + xb1);
-                    pb[0] = __ldg(B + xa0); pb[1] = __ldg(B + xb0); pb[2] = __ldg(B + xa1); pb[3] = __ldg(B + xb1);
+    ResizeJob j;
+    int local;
+    if (!src.find(blockIdx.x, kind, &j, &local)) return;
+    const int y0 = (local / j.tiles_x) * th;
+    const int x0 = (local % j.tiles_x) * kResizeTileW;
+    const int t = threadIdx.x;
+    // 1. source window: rows ry0..ry1, 16-byte chunks from column rx0
+    const float fy = static_cast<float>(j.src_height) / static_cast<float>(j.height);
+    const float fx = static_cast<float>(j.src_width) / static_cast<float>(j.width);
+    const int last_y = min(y0 + th, j.height) - 1, last_x = min(x0 + kResizeTileW, j.width) - 1;
+    const int ry0 = max(__float2int_rd((y0 + 0.5f) * fy - 0.5f) - 1, 0);
+    const int ry1 = min(__float2int_rd((last_y + 0.5f) * fy - 0.5f) + 2, j.src_height - 1);
+    const int rx0 = max(__float2int_rd((x0 + 0.5f) * fx - 0.5f) - 1, 0) & ~15;
+    const int rx1 = min(__float2int_rd((last_x + 0.5f) * fx - 0.5f) + 2, j.src_width - 1);
+    const int nrow = ry1 - ry0 + 1;
+    const int nchunk = rx1 >= rx0 ? (rx1 - rx0) / 16 + 1 : 0;
+    const bool window = ((reinterpret_cast<std::uintptr_t>(j.src) | static_cast<std::uintptr_t>(j.src_pitch)) & 15) == 0 &&
+                        nrow > 0 && nrow <= kRows && nchunk > 0 && nchunk <= kChunks;  // block-uniform
+    if (window) {
+        // chunks start 16-byte aligned below src_width; one that reaches past
+        // the row's last pixel is read byte by byte (zeros beyond it)
+        const int n = nrow * nchunk;
+        for (int i0 = t; i0 < n; i0 += 2 * 256) {
+            uint4 v[2];
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const int i = i0 + 256 * k;
+                if (i < n) {
+                    const int r = i / nchunk, col = rx0 + 16 * (i - r * nchunk);
+                    const std::uint8_t* p = j.src + static_cast<std::size_t>(ry0 + r) * j.src_pitch + col;
+                    if (col + 16 <= j.src_width) {
+                        v[k] = __ldg(reinterpret_cast<const uint4*>(p));
+                    } else {
+                        std::uint32_t w[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+                        for (int b = 0; b < 16; ++b)
+                            if (col + b < j.src_width)
+                                w[b >> 2] |= static_cast<std::uint32_t>(__ldg(p + b)) << (8 * (b & 3));
+                        v[k] = make_uint4(w[0], w[1], w[2], w[3]);
+                    }
                 }
-                const int ha0 = pa[0] * (256 - wx0) + pa[1] * wx0, hb0 = pb[0] * (256 - wx0) + pb[1] * wx0;
-                const int ha1 = pa[2] * (256 - wx1) + pa[3] * wx1, hb1 = pb[2] * (256 - wx1) + pb[3] * wx1;
-                const unsigned v0 = static_cast<unsigned>(ha0 * (256 - wy) + hb0 * wy + (1 << 15)) >> 16;
-                const unsigned v1 = static_cast<unsigned>(ha1 * (256 - wy) + hb1 * wy + (1 << 15)) >> 16;
-                std::uint8_t* dst = j.dst + static_cast<std::size_t>(y) * j.pitch + x;
-                if (x + 1 < j.width && (reinterpret_cast<std::uintptr_t>(dst) & 1) == 0) {
-                    *reinterpret_cast<std::uint16_t*>(dst) = static_cast<std::uint16_t>(v0 | (v1 << 8));
-                } else {
-                    dst[0] = static_cast<std::uint8_t>(v0);
-                    if (x + 1 < j.width) dst[1] = static_cast<std::uint8_t>(v1);
+            }
+#pragma unroll
+            for (int k = 0; k < 2; ++k) {
+                const int i = i0 + 256 * k;
+                if (i < n) {
+                    const int r = i / nchunk, c = i - r * nchunk;
+                    *reinterpret_cast<uint4*>(&raw[r][16 * c]) = v[k];
                 }
             }
         }
-        __syncthreads();  // the taps and this buffer are free for later tiles
     }
-    cp_async_wait_all();  // nothing in flight when the block leaves
+    // 2. taps
+    if (t == 0) scale[0] = linear_exact_scale(j.src_width, j.width);
+    if (t == 32) scale[1] = linear_exact_scale(j.src_height, j.height);
+    __syncthreads();
+    if (t < kResizeTileW) xtap[t] = linear_exact_tap(min(x0 + t, j.width - 1), j.src_width, scale[0]);
+    else if (t < kResizeTileW + th)
+        ytap[t - kResizeTileW] = linear_exact_tap(min(y0 + t - kResizeTileW, j.height - 1), j.src_height, scale[1]);
+    __syncthreads();
+    // taps are nondecreasing: the first and last give the tile's source span
+    const bool staged = window && ytap[0].x >= ry0 && min(ytap[th - 1].x + 1, j.src_height - 1) <= ry1 &&
+                        xtap[0].x >= rx0 && min(xtap[kResizeTileW - 1].x + 1, j.src_width - 1) < rx0 + 16 * nchunk;
+    // 3. warp w: rows w, w + 8, ...; lane l: columns 2l, 2l + 1
+    const int lane = t & 31;
+    const int c = 2 * lane, x = x0 + c;
+    if (x >= j.width) return;
+    const int2 t0 = xtap[c], t1 = xtap[c + 1];  // columns past the layer edge repeat the last tap
+    const int wx0 = t0.y, wx1 = t1.y;
+    int xa0 = t0.x, xb0 = min(t0.x + 1, j.src_width - 1), xa1 = t1.x, xb1 = min(t1.x + 1, j.src_width - 1);
+    if (staged) {
+        xa0 -= rx0; xb0 -= rx0; xa1 -= rx0; xb1 -= rx0;
+    }
+    for (int rr = t >> 5; rr < th; rr += 8) {
+        const int y = y0 + rr;
+        if (y >= j.height) break;
+        const int2 ty = ytap[rr];
+        const int ra = ty.x, rb = min(ty.x + 1, j.src_height - 1), wy = ty.y;
+        int pa[4], pb[4];  // rows ra, rb at xa0, xb0, xa1, xb1
+        if (staged) {
+            const std::uint8_t* A = raw[ra - ry0];
+            const std::uint8_t* B = raw[rb - ry0];
+            pa[0] = A[xa0]; pa[1] = A[xb0]; pa[2] = A[xa1]; pa[3] = A[xb1];
+            pb[0] = B[xa0]; pb[1] = B[xb0]; pb[2] = B[xa1]; pb[3] = B[xb1];
+        } else {
+            const std::uint8_t* A = j.src + static_cast<std::size_t>(ra) * j.src_pitch;
+            const std::uint8_t* B = j.src + static_cast<std::size_t>(rb) * j.src_pitch;
+            pa[0] = __ldg(A + xa0); pa[1] = __ldg(A + xb0); pa[2] = __ldg(A + xa1); pa[3] = __ldg(A + xb1);
+            pb[0] = __ldg(B + xa0); pb[1] = __ldg(B + xb0); pb[2] = __ldg(B + xa1); pb[3] = __ldg(B + xb1);
+        }
+        const int ha0 = pa[0] * (256 - wx0) + pa[1] * wx0, hb0 = pb[0] * (256 - wx0) + pb[1] * wx0;
+        const int ha1 = pa[2] * (256 - wx1) + pa[3] * wx1, hb1 = pb[2] * (256 - wx1) + pb[3] * wx1;
+        const unsigned v0 = static_cast<unsigned>(ha0 * (256 - wy) + hb0 * wy + (1 << 15)) >> 16;
+        const unsigned v1 = static_cast<unsigned>(ha1 * (256 - wy) + hb1 * wy + (1 << 15)) >> 16;
+        std::uint8_t* dst = j.dst + static_cast<std::size_t>(y) * j.pitch + x;
+        if (x + 1 < j.width && (reinterpret_cast<std::uintptr_t>(dst) & 1) == 0) {
+            *reinterpret_cast<std::uint16_t*>(dst) = static_cast<std::uint16_t>(v0 | (v1 << 8));
+        } else {
+            dst[0] = static_cast<std::uint8_t>(v0);
+            if (x + 1 < j.width) dst[1] = static_cast<std::uint8_t>(v1);
+        }
+    }
 }
 
 // ------------------------------------------------------------- S3 blur
