@@ -268,15 +268,21 @@ def run_reference(args):
     times, lat = [], []
     with ctx.Pool(workers) as pool:
         pool.map(cpu_pair, [(0, 0)] * workers)  # warm the workers (imports)
+        t = time.perf_counter()
+        pool.map(cpu_pair, [(i, 0) for i in range(workers)], chunksize=1)
+        rate = workers / (time.perf_counter() - t)
+        # a step is the workload's 64 pairs, or its first `per_step` pairs
+        # when 64 would take the whole run past REFERENCE_SECONDS
+        per_step = min(N_PAIRS, max(workers, int(rate * REFERENCE_SECONDS / max(1, args.steps + args.warmup))))
         for _ in range(args.warmup):
-            pool.map(cpu_pair, [(i, 0) for i in range(N_PAIRS)], chunksize=1)
+            pool.map(cpu_pair, [(i, 0) for i in range(per_step)], chunksize=1)
         for _ in range(args.steps):
             t = time.perf_counter()
-            lat += pool.map(cpu_pair, [(i, 0) for i in range(N_PAIRS)], chunksize=1)
+            lat += pool.map(cpu_pair, [(i, 0) for i in range(per_step)], chunksize=1)
             times.append(time.perf_counter() - t)
-    v = N_PAIRS * args.steps / sum(times)
+    v = per_step * args.steps / sum(times)
     lat.sort()
-    sample = (f"{args.steps} steps of the workload's {N_PAIRS} pairs on {workers} processes "
+    sample = (f"{args.steps} steps of {per_step} of the workload's {N_PAIRS} pairs on {workers} processes "
               f"(NumPy S2/S3 + C S4/S5 restatement of the reference)")
     try:
         gpu = reference_gpu_per_pair()
@@ -285,7 +291,7 @@ def run_reference(args):
     line = {"impl": "reference", "metric": "pairs/s", "value": v, "unit": "pairs/s", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "u8/i32/f64",
-            "data": "synthetic", "config": {"workload": WORKLOAD, "pairs_per_step": N_PAIRS},
+            "data": "synthetic", "config": {"workload": WORKLOAD, "pairs_per_step": per_step},
             "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": workers, "kind": "port", "sample": sample,
                              "cpu_model": cpu_model(), "nproc": os.cpu_count(),
                              "p50_ms": 1e3 * lat[len(lat) // 2], "p99_ms": 1e3 * lat[int(0.99 * (len(lat) - 1))]},
@@ -297,12 +303,14 @@ def run_reference(args):
 # DRAM bytes (read + write) per launch of a kernel of the batched step, from
 # one ncu capture of this workload (dram__bytes_read.sum + dram__bytes_write.sum).
 NCU_TRAFFIC = {
-    "fast_nms": (280.24e6, "ncu capture of this workload"),
-    "describe": (169.51e6, "ncu capture of this workload"),
+    "fast_nms": (111.19e6, "ncu capture of this workload (fast_kernel, one launch)"),
+    "blur": (183.90e6, "ncu capture of this workload (blur_tiles_kernel, one launch)"),
+    "describe": (169.82e6, "ncu capture of this workload (describe_kernel, one launch)"),
     "search": (13.09e6, "ncu capture of this workload (scoring kernel)"),
 }
 
 N_MIXED = 256
+REFERENCE_SECONDS = 150.0   # bound on the reference arm's CPU steps (warm-up and timed)
 SERVED_RATES = (200, 500, 1000, 2000)
 SERVED_SECONDS = 60.0       # per rate, served form
 PLAIN_SERVED_SECONDS = 10.0  # per rate, the plain per-pair comparison on the start of the same trace
