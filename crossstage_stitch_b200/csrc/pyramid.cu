@@ -120,6 +120,8 @@ void make_pyramid_jobs(const ImageView& im, const s2::Config& c, const Keypoints
             r.pitch = layer.pitch_bytes;
             r.tiles_x = ceil_div(p.width[i], kResizeTileW);
             r.tiles = l.resize_tiles[i];
+            r.scale_x = linear_exact_scale(r.src_width, r.width);
+            r.scale_y = linear_exact_scale(r.src_height, r.height);
             jobs->resize[i] = r;
         }
         s2::Config lc = c;

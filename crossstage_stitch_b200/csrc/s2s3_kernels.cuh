@@ -99,6 +99,7 @@ struct ResizeJob {
     std::uint8_t* dst;
     int width, height, pitch;
     int tiles_x, tiles;
+    double scale_x, scale_y;  // linear_exact_scale of each axis, computed by the host
 };
 
 // Per-image job passed by value.
@@ -190,7 +191,7 @@ constexpr int kSortChunk = 64;      // keys a warp sorts in registers (2 per lan
 constexpr int kBlurTileW = 64, kBlurTileH = 32;
 constexpr int kDescWarps = 8;
 constexpr int kEdge = 31;
-constexpr int kResizeTileW = 64, kResizeTileH = 64;  // widest tile; a job's tile_h may be smaller
+constexpr int kResizeTileW = 128, kResizeTileH = 64;  // tallest tile; a job's tile_h may be smaller
 constexpr int kMaxLevels = 16;
 static_assert(kMaxLevels <= kMapKinds && kDetectKinds <= kMapKinds, "block map kinds");
 
@@ -850,7 +851,7 @@ __global__ __launch_bounds__(kHarrisThreads) void rank_topk_kernel(const __grid_
 // double with scale = 1 / (dst / src), weight rint((f - floor f) * 256).
 // Indices left of the source (every index when src == 1) read pixel 0 with
 // weight 0, indices past the last interval read pixel src - 1 with weight 0.
-__device__ __forceinline__ double linear_exact_scale(int src, int dst) {
+__host__ __device__ inline double linear_exact_scale(int src, int dst) {
     return 1.0 / (static_cast<double>(dst) / static_cast<double>(src));
 }
 
@@ -862,131 +863,152 @@ __device__ __forceinline__ int2 linear_exact_tap(int v, int src, double scale) {
     return make_int2(static_cast<int>(fl), static_cast<int>(rint((f - fl) * 256.0)));
 }
 
-// One block = one tile of 64 x kTileH (16..64) layer pixels:
-//   1. the tile's source window, bounded from float arithmetic with a pixel
-//      of slack per side, is staged in shared memory with 16-byte loads
-//      (while the taps are computed);
-//   2. per-column and per-row taps in shared memory (double, as above);
-//   3. each warp produces whole layer rows, each lane two adjacent outputs:
-//        h(r, c) = src[r][c0] * (256 - wx) + src[r][c1] * wx   (< 2^16)
-//        out = (h(r0, c) * (256 - wy) + h(r1, c) * wy + 2^15) >> 16,
-//      the integer form of the 8-bit fixed-point horizontal pass followed
-//      by the vertical pass with one final rounding.
-// The exact taps are checked against the staged window; a tile outside it
-// (source image not 16-byte aligned, or a layer ratio above about 1.45)
-// reads the source bytes from global memory instead, with the same result.
-constexpr int kRawStride = 112;  // bytes of a staged source row: 7 chunks of 16
+// One block = one tile of 128 x kTileH (16..64) layer pixels:
+//   1. per-column and per-row taps in shared memory (double, as above);
+//   2. the tile's exact source window (rows of the first and last row taps,
+//      columns from the first column tap rounded down to 16 bytes) is
+//      staged in shared memory with 16-byte asynchronous copies;
+//   3. warp w makes the band of kTileH / 8 consecutive rows starting at row
+//      w * kTileH / 8, lane l columns 4l .. 4l + 3:
+//        h(r, c) = src[r][c0] * (256 - wx) + src[r][c0 + 1] * wx   (< 2^16)
+//        out = (h(ra, c) * (256 - wy) + h(rb, c) * wy + 2^15) >> 16,
+//      the integer form of the 8-bit fixed-point horizontal pass followed by
+//      the vertical pass with one final rounding. The band's source rows are
+//      walked once, top to bottom: a row's h comes from two byte permutes of
+//      aligned shared-memory words and one 16x8-bit dot product per column,
+//      and every output row whose lower source row it is goes out with the
+//      previous source row's h. A whole warp shares one band, so its lanes
+//      take the same branches.
+// Blocks whose source is not 16-byte aligned or whose window exceeds the
+// staging buffer (layer ratios above about 1.45), and lanes whose bytes do
+// not fit two 8-byte pools, read the source bytes from global memory per
+// output row instead, with the same result.
+constexpr int kRawStride = 256;  // bytes of a staged source row: 16 chunks of 16
 template <int kTileH> __host__ __device__ constexpr int resize_raw_rows() { return kTileH * 3 / 2 + 6; }
 
+__device__ __forceinline__ std::uint32_t resize_out(std::uint32_t ha, std::uint32_t hb, std::uint32_t wy) {
+    return (ha * (256u - wy) + hb * wy + 32768u) >> 16;
+}
+
 template <class Src, int kTileH>
-__global__ __launch_bounds__(256, 6) void resize_kernel(const __grid_constant__ Src src, int kind) {
+__global__ __launch_bounds__(256, 5) void resize_kernel(const __grid_constant__ Src src, int kind) {
     static_assert(kTileH >= 16 && kTileH <= kResizeTileH && kTileH % 16 == 0, "resize tile height");
-    constexpr int th = kTileH, kRows = resize_raw_rows<kTileH>(), kChunks = kRawStride / 16;
+    constexpr int kBand = kTileH / 8, kRows = resize_raw_rows<kTileH>();
     __shared__ int2 xtap[kResizeTileW];
     __shared__ int2 ytap[kTileH];
     __shared__ __align__(16) std::uint8_t raw[kRows][kRawStride];
-    __shared__ double scale[2];
     ResizeJob j;
     int local;
     if (!src.find(blockIdx.x, kind, &j, &local)) return;
-    const int y0 = (local / j.tiles_x) * th;
+    const int y0 = (local / j.tiles_x) * kTileH;
     const int x0 = (local % j.tiles_x) * kResizeTileW;
     const int t = threadIdx.x;
-    // 1. source window: rows ry0..ry1, 16-byte chunks from column rx0
-    const float fy = static_cast<float>(j.src_height) / static_cast<float>(j.height);
-    const float fx = static_cast<float>(j.src_width) / static_cast<float>(j.width);
-    const int last_y = min(y0 + th, j.height) - 1, last_x = min(x0 + kResizeTileW, j.width) - 1;
-    const int ry0 = max(__float2int_rd((y0 + 0.5f) * fy - 0.5f) - 1, 0);
-    const int ry1 = min(__float2int_rd((last_y + 0.5f) * fy - 0.5f) + 2, j.src_height - 1);
-    const int rx0 = max(__float2int_rd((x0 + 0.5f) * fx - 0.5f) - 1, 0) & ~15;
-    const int rx1 = min(__float2int_rd((last_x + 0.5f) * fx - 0.5f) + 2, j.src_width - 1);
-    const int nrow = ry1 - ry0 + 1;
-    const int nchunk = rx1 >= rx0 ? (rx1 - rx0) / 16 + 1 : 0;
-    const bool window = ((reinterpret_cast<std::uintptr_t>(j.src) | static_cast<std::uintptr_t>(j.src_pitch)) & 15) == 0 &&
-                        nrow > 0 && nrow <= kRows && nchunk > 0 && nchunk <= kChunks;  // block-uniform
-    if (window) {
-        // chunks start 16-byte aligned below src_width; one that reaches past
-        // the row's last pixel is read byte by byte (zeros beyond it)
-        const int n = nrow * nchunk;
-        for (int i0 = t; i0 < n; i0 += 2 * 256) {
-            uint4 v[2];
-#pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                const int i = i0 + 256 * k;
-                if (i < n) {
-                    const int r = i / nchunk, col = rx0 + 16 * (i - r * nchunk);
-                    const std::uint8_t* p = j.src + static_cast<std::size_t>(ry0 + r) * j.src_pitch + col;
-                    if (col + 16 <= j.src_width) {
-                        v[k] = __ldg(reinterpret_cast<const uint4*>(p));
-                    } else {
-                        std::uint32_t w[4] = {0u, 0u, 0u, 0u};
-#pragma unroll
-                        for (int b = 0; b < 16; ++b)
-                            if (col + b < j.src_width)
-                                w[b >> 2] |= static_cast<std::uint32_t>(__ldg(p + b)) << (8 * (b & 3));
-                        v[k] = make_uint4(w[0], w[1], w[2], w[3]);
-                    }
-                }
-            }
-#pragma unroll
-            for (int k = 0; k < 2; ++k) {
-                const int i = i0 + 256 * k;
-                if (i < n) {
-                    const int r = i / nchunk, c = i - r * nchunk;
-                    *reinterpret_cast<uint4*>(&raw[r][16 * c]) = v[k];
-                }
-            }
-        }
-    }
-    // 2. taps
-    if (t == 0) scale[0] = linear_exact_scale(j.src_width, j.width);
-    if (t == 32) scale[1] = linear_exact_scale(j.src_height, j.height);
+    // 1. taps (columns and rows past the layer edge repeat the last one)
+    if (t < kResizeTileW) xtap[t] = linear_exact_tap(min(x0 + t, j.width - 1), j.src_width, j.scale_x);
+    else if (t < kResizeTileW + kTileH)
+        ytap[t - kResizeTileW] = linear_exact_tap(min(y0 + t - kResizeTileW, j.height - 1), j.src_height, j.scale_y);
     __syncthreads();
-    if (t < kResizeTileW) xtap[t] = linear_exact_tap(min(x0 + t, j.width - 1), j.src_width, scale[0]);
-    else if (t < kResizeTileW + th)
-        ytap[t - kResizeTileW] = linear_exact_tap(min(y0 + t - kResizeTileW, j.height - 1), j.src_height, scale[1]);
-    __syncthreads();
-    // taps are nondecreasing: the first and last give the tile's source span
-    const bool staged = window && ytap[0].x >= ry0 && min(ytap[th - 1].x + 1, j.src_height - 1) <= ry1 &&
-                        xtap[0].x >= rx0 && min(xtap[kResizeTileW - 1].x + 1, j.src_width - 1) < rx0 + 16 * nchunk;
-    // 3. warp w: rows w, w + 8, ...; lane l: columns 2l, 2l + 1
-    const int lane = t & 31;
-    const int c = 2 * lane, x = x0 + c;
-    if (x >= j.width) return;
-    const int2 t0 = xtap[c], t1 = xtap[c + 1];  // columns past the layer edge repeat the last tap
-    const int wx0 = t0.y, wx1 = t1.y;
-    int xa0 = t0.x, xb0 = min(t0.x + 1, j.src_width - 1), xa1 = t1.x, xb1 = min(t1.x + 1, j.src_width - 1);
+    // 2. source window: rows ry0 .. ry1, 16-byte chunks from column rx0
+    const int ry0 = ytap[0].x, ry1 = min(ytap[kTileH - 1].x + 1, j.src_height - 1);
+    const int rx0 = xtap[0].x & ~15, rx1 = min(xtap[kResizeTileW - 1].x + 1, j.src_width - 1);
+    const int nrow = ry1 - ry0 + 1, nchunk = (rx1 - rx0) / 16 + 1;
+    const bool staged = ((reinterpret_cast<std::uintptr_t>(j.src) | static_cast<std::uintptr_t>(j.src_pitch)) & 15) == 0 &&
+                        nrow <= kRows && nchunk <= kRawStride / 16;  // block-uniform
     if (staged) {
-        xa0 -= rx0; xb0 -= rx0; xa1 -= rx0; xb1 -= rx0;
+        const int q = t & 15, col = rx0 + 16 * q;
+        if (q < nchunk) {
+            for (int r = t >> 4; r < nrow; r += 16) {
+                const int gy = ry0 + r;
+                const std::uint8_t* p = j.src + static_cast<std::size_t>(gy) * j.src_pitch + col;
+                // bytes of the row that may be read: the pitch, the width on the last row
+                if (col + 16 <= (gy < j.src_height - 1 ? j.src_pitch : j.src_width)) {
+                    cp_async16(&raw[r][16 * q], p);
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 16; ++k) raw[r][16 * q + k] = col + k < j.src_width ? p[k] : 0;
+                }
+            }
+        }
+        cp_async_wait_all();
     }
-    for (int rr = t >> 5; rr < th; rr += 8) {
-        const int y = y0 + rr;
-        if (y >= j.height) break;
-        const int2 ty = ytap[rr];
-        const int ra = ty.x, rb = min(ty.x + 1, j.src_height - 1), wy = ty.y;
-        int pa[4], pb[4];  // rows ra, rb at xa0, xb0, xa1, xb1
-        if (staged) {
-            const std::uint8_t* A = raw[ra - ry0];
-            const std::uint8_t* B = raw[rb - ry0];
-            pa[0] = A[xa0]; pa[1] = A[xb0]; pa[2] = A[xa1]; pa[3] = A[xb1];
-            pb[0] = B[xa0]; pb[1] = B[xb0]; pb[2] = B[xa1]; pb[3] = B[xb1];
+    __syncthreads();
+    // 3. bands
+    const int r0 = (t >> 5) * kBand;
+    const int r_end = r0 + min(kBand, j.height - y0 - r0);  // band rows inside the layer
+    const int c = 4 * (t & 31), x = x0 + c;
+    if (r_end <= r0 || x >= j.width) return;
+    int2 tx[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) tx[k] = xtap[c + k];
+    std::uint32_t wx[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) wx[k] = (256u - tx[k].y) | (static_cast<std::uint32_t>(tx[k].y) << 16);
+    const int nx = min(4, j.width - x);
+    std::uint8_t* dst = j.dst + static_cast<std::size_t>(y0 + r0) * j.pitch + x;
+    const bool word_store = nx == 4 && ((reinterpret_cast<std::uintptr_t>(j.dst) | static_cast<std::uintptr_t>(j.pitch)) & 3) == 0;
+    auto emit = [&](const std::uint32_t (&ha)[4], const std::uint32_t (&hb)[4], std::uint32_t wy) {
+        std::uint32_t v[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) v[k] = resize_out(ha[k], hb[k], wy);
+        if (word_store) {
+            *reinterpret_cast<std::uint32_t*>(dst) = __byte_perm(__byte_perm(v[0], v[1], 0x0040), __byte_perm(v[2], v[3], 0x0040), 0x5410);
         } else {
-            const std::uint8_t* A = j.src + static_cast<std::size_t>(ra) * j.src_pitch;
-            const std::uint8_t* B = j.src + static_cast<std::size_t>(rb) * j.src_pitch;
-            pa[0] = __ldg(A + xa0); pa[1] = __ldg(A + xb0); pa[2] = __ldg(A + xa1); pa[3] = __ldg(A + xb1);
-            pb[0] = __ldg(B + xa0); pb[1] = __ldg(B + xb0); pb[2] = __ldg(B + xa1); pb[3] = __ldg(B + xb1);
+#pragma unroll
+            for (int k = 0; k < 4; ++k)
+                if (k < nx) dst[k] = static_cast<std::uint8_t>(v[k]);
         }
-        const int ha0 = pa[0] * (256 - wx0) + pa[1] * wx0, hb0 = pb[0] * (256 - wx0) + pb[1] * wx0;
-        const int ha1 = pa[2] * (256 - wx1) + pa[3] * wx1, hb1 = pb[2] * (256 - wx1) + pb[3] * wx1;
-        const unsigned v0 = static_cast<unsigned>(ha0 * (256 - wy) + hb0 * wy + (1 << 15)) >> 16;
-        const unsigned v1 = static_cast<unsigned>(ha1 * (256 - wy) + hb1 * wy + (1 << 15)) >> 16;
-        std::uint8_t* dst = j.dst + static_cast<std::size_t>(y) * j.pitch + x;
-        if (x + 1 < j.width && (reinterpret_cast<std::uintptr_t>(dst) & 1) == 0) {
-            *reinterpret_cast<std::uint16_t*>(dst) = static_cast<std::uint16_t>(v0 | (v1 << 8));
-        } else {
-            dst[0] = static_cast<std::uint8_t>(v0);
-            if (x + 1 < j.width) dst[1] = static_cast<std::uint8_t>(v1);
+        dst += j.pitch;
+    };
+    // the lane's bytes: pool A = 8 bytes at column `base` (columns 0, 1),
+    // pool B = 8 bytes at base + 4 * kb (columns 2, 3)
+    const int base = tx[0].x & ~3;
+    const int o0 = tx[0].x - base, o1 = tx[1].x - base;
+    const int kb = (tx[2].x - base) >> 2;
+    const int o2 = tx[2].x - base - 4 * kb, o3 = tx[3].x - base - 4 * kb;
+    const bool fits = staged && o1 + 1 <= 7 && o3 + 1 <= 7 && base - rx0 + 4 * kb + 8 <= kRawStride;
+    if (!fits) {
+        int xb[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) xb[k] = min(tx[k].x + 1, j.src_width - 1);
+        for (int rr = r0; rr < r_end; ++rr) {
+            const int2 ty = ytap[rr];
+            const std::uint8_t* A = j.src + static_cast<std::size_t>(ty.x) * j.src_pitch;
+            const std::uint8_t* B = j.src + static_cast<std::size_t>(min(ty.x + 1, j.src_height - 1)) * j.src_pitch;
+            std::uint32_t ha[4], hb[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const std::uint32_t wa = __ldg(A + tx[k].x) | (static_cast<std::uint32_t>(__ldg(A + xb[k])) << 8);
+                const std::uint32_t wb = __ldg(B + tx[k].x) | (static_cast<std::uint32_t>(__ldg(B + xb[k])) << 8);
+                ha[k] = __dp2a_lo(wx[k], wa, 0u);
+                hb[k] = __dp2a_lo(wx[k], wb, 0u);
+            }
+            emit(ha, hb, static_cast<std::uint32_t>(ty.y));
         }
+        return;
+    }
+    const std::uint32_t sel_a = static_cast<std::uint32_t>(o0 | ((o0 + 1) << 4) | (o1 << 8) | ((o1 + 1) << 12));
+    const std::uint32_t sel_b = static_cast<std::uint32_t>(o2 | ((o2 + 1) << 4) | (o3 << 8) | ((o3 + 1) << 12));
+    const std::uint8_t* lane_bytes = &raw[0][0] + (base - rx0);
+    const int s_last = min(ytap[r_end - 1].x + 1, j.src_height - 1);
+    int rr = r0;
+    int2 ty = ytap[rr];
+    int s = ty.x;
+    std::uint32_t pa[4] = {0u, 0u, 0u, 0u};  // h of source row s - 1
+    while (rr < r_end && s <= s_last) {  // s <= rb of row rr throughout (monotone taps)
+        s = max(s, ty.x);  // skips source rows no output row reads (layer ratios above 2)
+        const auto* w = reinterpret_cast<const std::uint32_t*>(lane_bytes + (s - ry0) * kRawStride);
+        const std::uint32_t pool_a = __byte_perm(w[0], w[1], sel_a), pool_b = __byte_perm(w[kb], w[kb + 1], sel_b);
+        const std::uint32_t h[4] = {__dp2a_lo(wx[0], pool_a, 0u), __dp2a_hi(wx[1], pool_a, 0u),
+                                    __dp2a_lo(wx[2], pool_b, 0u), __dp2a_hi(wx[3], pool_b, 0u)};
+        // every row whose lower source row is s (ra = s - 1, or ra = s at the bottom edge)
+        while (rr < r_end && min(ty.x + 1, j.src_height - 1) == s) {
+            if (ty.x == s) emit(h, h, static_cast<std::uint32_t>(ty.y));
+            else emit(pa, h, static_cast<std::uint32_t>(ty.y));
+            if (++rr < r_end) ty = ytap[rr];
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) pa[k] = h[k];
+        ++s;
     }
 }
 
