@@ -62,7 +62,13 @@ struct State {
     std::uint64_t seed, generation;
     ScaleInfo scale_a, scale_b;
     int status;
+    // bits of the smallest loss of a fully scored model of this search (or
+    // of the previous winner), +inf when none: a pruning bound shared by
+    // every warp of the pair (nonnegative doubles order like their bits)
+    unsigned long long bound;
 };
+
+constexpr unsigned long long kInfBits = 0x7ff0000000000000ull;  // +inf
 
 constexpr int kSearchThreads = 256;
 constexpr int kSearchWarps = kSearchThreads / 32;
@@ -562,6 +568,8 @@ __global__ __launch_bounds__(256) void prepare_kernel(const __grid_constant__ Sr
                    s->nm != nm || !same_scale(s->scale_a, j.sa) || !same_scale(s->scale_b, j.sb)) {
             s->status = static_cast<int>(Status::INVALID_ARGUMENT);
         }
+        s->bound = s->best.valid && fin(s->best.loss) ? static_cast<unsigned long long>(__double_as_longlong(s->best.loss))
+                                                      : kInfBits;
         int g = s->status == static_cast<int>(Status::OK);
         if (g && (na < 0 || na > j.a.capacity || nb < 0 || nb > j.b.capacity || nm < 0 || nm > j.m.capacity)) {
             s->status = static_cast<int>(Status::INVALID_ARGUMENT);
@@ -632,7 +640,7 @@ __global__ __launch_bounds__(kFitThreads) void fit_kernel(const __grid_constant_
 // L1-backed local memory, but it is a small share of the work, and the
 // scoring loop gains the occupancy (1 block: 0.62 ms, 3 blocks: 0.43 ms for
 // 64 pairs x 2000 hypotheses x ~530 matches).
-constexpr int kPruneEvery = 256;  // points between the pruning checks of a model (multiple of 128)
+constexpr int kPruneEvery = 128;  // points between the pruning checks of a model (multiple of 128)
 
 // kPrefit: the models come from fit_kernel (sj.prefit) and the kernel only
 // scores (batched form: 0.387 -> 0.367 ms per step with the fit kernel
@@ -702,13 +710,17 @@ __global__ __launch_bounds__(kSearchThreads, 3) void search_kernel(const __grid_
 #pragma unroll
                     for (int e = 0; e < 9; ++e) h[e] = __shfl_sync(0xffffffffu, hm[e], k);
                 }
-                // Exact pruning against this warp's best so far: every term is
-                // >= 0 and a correctly rounded sum of nonnegative values is
-                // nondecreasing in each operand, so the tree sum of the partial
-                // accumulators never exceeds the final loss. Once it is above
-                // the best loss the model cannot win (ties need equal losses).
-                const bool prune = best.valid != 0;
-                const double bound = best.loss;
+                // Exact pruning against the smallest loss of a fully scored
+                // model so far (this warp's best, or the pair's bound that
+                // every warp publishes to): every term is >= 0 and a
+                // correctly rounded sum of nonnegative values is nondecreasing
+                // in each operand, so the tree sum of the partial accumulators
+                // never exceeds the final loss. Once it is above that loss the
+                // model cannot win (ties need equal losses).
+                const double shared_bound =
+                    __longlong_as_double(static_cast<long long>(*reinterpret_cast<volatile unsigned long long*>(&j.state->bound)));
+                const double bound = best.valid && best.loss < shared_bound ? best.loss : shared_bound;
+                const bool prune = bound <= DBL_MAX;
                 // Lane l accumulates the points l, l+32, l+64, l+96 (virtual
                 // lanes, slots 0..3) and every 128 after them in order: four
                 // points per step, four independent FP64 chains. A point past
@@ -751,6 +763,7 @@ __global__ __launch_bounds__(kSearchThreads, 3) void search_kernel(const __grid_
                     cand.hypothesis = h0 + k;
                     cand.valid = fin(v);
                     if (better(cand, best)) best = cand;
+                    if (cand.valid) atomicMin(&j.state->bound, static_cast<unsigned long long>(__double_as_longlong(v)));
                 }
                 __syncwarp();
             }
