@@ -34,7 +34,7 @@ struct SelectParams {
 enum DetectCounter { kListed = 0, kAboveWritten = 1, kTiesWritten = 2, kTileQueue = 3, kDetectCounters = 4 };
 constexpr int kHistWords = 256 + kDetectCounters;  // one job's histogram and counters
 
-struct DetectJob {
+struct alignas(16) DetectJob {  // 16-byte multiple: copied into shared memory in 16-byte chunks
     const std::uint8_t* image;
     int width, height, pitch;
     int threshold, max_keypoints;
@@ -302,6 +302,21 @@ __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
     asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(gmem) : "memory");
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+    const unsigned dst = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(dst), "l"(gmem) : "memory");
+}
+
+// The FAST kernel's block map and job array where its source has them
+// (tables staged by a plan); elsewhere the job is looked up in place.
+template <class S> __device__ __forceinline__ const std::uint32_t* fast_map(const S&) { return nullptr; }
+template <class S> __device__ __forceinline__ const DetectJob* fast_jobs(const S&) { return nullptr; }
+template <> __device__ __forceinline__ const std::uint32_t* fast_map(const JobTable<DetectJob>& s) {
+    return s.map[kFastKind];
+}
+template <class S> __device__ __forceinline__ int fast_map_tiles(const S&) { return 0; }
+template <> __device__ __forceinline__ int fast_map_tiles(const JobTable<DetectJob>& s) { return s.map_blocks[kFastKind]; }
+template <> __device__ __forceinline__ const DetectJob* fast_jobs(const JobTable<DetectJob>& s) { return s.jobs; }
 
 // Stages rows y0-4 .. y0+35 and columns x0-16 .. x0+79 of the job's image in
 // `in` (byte c of row r = image (y0-4+r, x0-16+c)). The FAST test never reads
@@ -356,6 +371,7 @@ __device__ __forceinline__ void stage_fast_tile(const DetectJob& j, int local, s
 template <class Src>
 __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(const __grid_constant__ Src src,
                                                                           std::uint32_t* queue, int total) {
+    static_assert(sizeof(DetectJob) % 16 == 0, "jobs are copied in 16-byte chunks");
     __shared__ __align__(16) std::uint8_t in[2][kFastInH][kInStride];
     __shared__ __align__(16) std::uint8_t sc[kFastScH][kScStride];
     __shared__ std::uint16_t cand[kFastScH * kScGroups];
@@ -366,13 +382,26 @@ __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(cons
     __shared__ int locals[2];
     __shared__ int n_cand, n_found, next;
     __shared__ std::uint32_t list_base;
+    __shared__ int ahead_tile;          // with a block map: the tile after `next`, taken from the queue
+    __shared__ std::uint32_t ahead_entry;  // and its block-map entry (job << 16 | tile within the job)
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    // With a block map, total is capped by the map; the job of the tile after
+    // the current one is copied into shared memory asynchronously while the
+    // current tile is tested, and the queue index and map entry of the tile
+    // after that are fetched a tile ahead, so no thread waits on the lookup.
+    const std::uint32_t* map = fast_map(src);
+    if (map) total = min(total, fast_map_tiles(src));
     hist[tid] = 0;
     if (tid == 0) {
         n_cand = 0;
         n_found = 0;
         next = static_cast<int>(atomicAdd(queue, 1u));
         if (next < total && !src.find(next, kFastKind, &jobs[0], &locals[0])) next = total;
+        if (map) {
+            const int t = static_cast<int>(atomicAdd(queue, 1u));
+            ahead_tile = t;
+            if (t < total) cp_async4(&ahead_entry, map + t);
+        }
     }
     __syncthreads();
     int tile = next, buf = 0;
@@ -385,10 +414,25 @@ __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(cons
         const int W = j.width, H = j.height;
         const int y0 = (local / j.tiles_x) * kFastTileH, x0 = (local % j.tiles_x) * kFastTileW;
         std::uint8_t (*cur)[kInStride] = in[buf];
+        int ahead = total;  // thread 0 with a block map: the queue index of the tile after next
         if (tid == 0) {
-            int t = static_cast<int>(atomicAdd(queue, 1u));
-            if (t < total && !src.find(t, kFastKind, &jobs[buf ^ 1], &locals[buf ^ 1])) t = total;
-            next = t;
+            if (map) {
+                const int t = ahead_tile;
+                next = t;
+                if (t < total) {
+                    const std::uint32_t e = ahead_entry;
+                    locals[buf ^ 1] = static_cast<int>(e & 0xffffu);
+                    const auto* g = reinterpret_cast<const char*>(fast_jobs(src) + (e >> 16));
+                    auto* d = reinterpret_cast<char*>(&jobs[buf ^ 1]);
+#pragma unroll
+                    for (int k = 0; k < static_cast<int>(sizeof(DetectJob) / 16); ++k) cp_async16(d + 16 * k, g + 16 * k);
+                    ahead = static_cast<int>(atomicAdd(queue, 1u));
+                }
+            } else {
+                int t = static_cast<int>(atomicAdd(queue, 1u));
+                if (t < total && !src.find(t, kFastKind, &jobs[buf ^ 1], &locals[buf ^ 1])) t = total;
+                next = t;
+            }
         }
         // 1. compass test: thread (q, rb) takes positions 4q .. 4q+3 of rows rb,
         // rb + 15, rb + 30; groups with a survivor are listed as
@@ -441,9 +485,14 @@ __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(cons
                         static_cast<std::uint16_t>(((r * kScGroups + q) << 4) | bits);
             }
         }
+        if (tid == 0 && map) cp_async_wait_all();  // the next tile's job
         __syncthreads();
         // the next tile's bytes travel while this one is scored
         const int nt = next;
+        if (tid == 0 && map) {
+            ahead_tile = ahead;
+            if (ahead < total) cp_async4(&ahead_entry, map + ahead);
+        }
         if (nt < total) stage_fast_tile(jobs[buf ^ 1], locals[buf ^ 1], in[buf ^ 1]);
         const int nc = n_cand;
         // 2. each warp expands its 32 survivor groups of a round into a
