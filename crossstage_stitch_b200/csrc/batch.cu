@@ -373,7 +373,7 @@ void Plan::job_blocks(int i, int s, int l, int (&db)[s2s3::kDetectKinds], int (&
     db[s2s3::kHarrisKind] = active ? ceil_div(o.det[s].candidates, s2s3::kHarrisThreads) : 0;
     db[s2s3::kSortKind] = active ? 1 : 0;
     sb[s2s3::kBlurKind] = 0;  // on demand: blur_tiles_kernel takes the flagged tiles from a list
-    sb[s2s3::kDescKind] = k > 0 ? ceil_div(k, s2s3::kDescWarps) : 0;
+    sb[s2s3::kDescKind] = k > 0 ? ceil_div(k, s2s3::kDescKeys) : 0;
 }
 
 Status Plan::stage_tables(void* ws) {

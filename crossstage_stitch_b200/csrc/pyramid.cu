@@ -160,7 +160,7 @@ void pyramid_detect_blocks(const PyramidLayout& l, int i, int (&blocks)[kDetectK
 void pyramid_describe_blocks(const PyramidLayout& l, int i, int (&blocks)[kDescribeKinds]) {
     const bool active = i < l.plan.levels && l.plan.budget[i] > 0;
     blocks[kBlurKind] = 0;  // on demand: blur_tiles_kernel takes the flagged tiles from a list
-    blocks[kDescKind] = active ? ceil_div(l.plan.budget[i], kDescWarps) : 0;
+    blocks[kDescKind] = active ? ceil_div(l.plan.budget[i], kDescKeys) : 0;
 }
 
 namespace {

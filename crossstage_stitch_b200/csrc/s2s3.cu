@@ -173,7 +173,7 @@ Status describe(const ImageView& image, const Keypoints& kp, const Descriptors& 
     const Src src{make_describe_job(image, kp, out, ws, l)};
     blur_kernel<Src><<<l.tiles, 256, 0, stream>>>(src);
     if (!record(e_blur, stream)) return Status::CUDA_ERROR;
-    describe_kernel<Src><<<ceil_div(kp.capacity, kDescWarps), kDescWarps * 32, 0, stream>>>(src);
+    describe_kernel<Src><<<ceil_div(kp.capacity, kDescKeys), kDescWarps * 32, 0, stream>>>(src);
     note_launches(2);
     return launch_status();
 }

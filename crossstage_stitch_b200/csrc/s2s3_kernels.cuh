@@ -190,6 +190,8 @@ constexpr int kSortThreads = 1024;
 constexpr int kSortChunk = 64;      // keys a warp sorts in registers (2 per lane)
 constexpr int kBlurTileW = 64, kBlurTileH = 32;
 constexpr int kDescWarps = 8;
+constexpr int kDescRounds = 4;                        // keypoints per warp of a describe block
+constexpr int kDescKeys = kDescWarps * kDescRounds;  // keypoints per describe block
 constexpr int kEdge = 31;
 constexpr int kResizeTileW = 128, kResizeTileH = 64;  // tallest tile; a job's tile_h may be smaller
 constexpr int kMaxLevels = 16;
@@ -1324,23 +1326,24 @@ __device__ __forceinline__ float fast_atan2_deg(float y, float x) {
     return a;
 }
 
-__device__ __forceinline__ int rotated_sample(const std::uint8_t* centre, int stride, int px, int py,
+__device__ __forceinline__ int rotated_sample(const std::uint8_t* centre, int stride, float fx, float fy,
                                               float a, float b) {
-    const float fx = static_cast<float>(px), fy = static_cast<float>(py);
     const int ix = __float2int_rn(__fsub_rn(__fmul_rn(fx, a), __fmul_rn(fy, b)));
     const int iy = __float2int_rn(__fadd_rn(__fmul_rn(fx, b), __fmul_rn(fy, a)));
     return centre[iy * stride + ix];
 }
 
-// One warp per keypoint: intensity-centroid moments over the radius-15 disc
-// of the unblurred image (lane v sums rows +-v), the angle on lane 0 (float
-// fastAtan2, cos/sin evaluated in double then rounded to float), then lane l
-// packs pattern pairs 8l..8l+7 of the blurred image into descriptor byte l.
+// One warp per keypoint, kDescRounds keypoints per warp (the block stages
+// the pattern once for its kDescKeys keypoints): intensity-centroid moments
+// over the radius-15 disc of the unblurred image (lane l sums column l - 15),
+// the angle on lane 0 (float fastAtan2, cos/sin evaluated in double then
+// rounded to float), then lane l packs pattern pairs 8l..8l+7 of the blurred
+// image into descriptor byte l.
 // 8 blocks per SM (32 registers): the kernel waits on scattered patch loads,
 // so resident warps matter more than the few registers it spills.
 template <class Src>
 __global__ __launch_bounds__(kDescWarps * 32, 8) void describe_kernel(const __grid_constant__ Src src) {
-    __shared__ std::uint32_t pat[8][32];  // pat[j][l] = pair 8l + j as 4 packed int8
+    __shared__ float4 pat[8][32];  // pat[k][l] = pair 8l + k as floats (x0, y0, x1, y1)
     DescribeJob j;
     int local;
     if (!src.find(blockIdx.x, kDescKind, &j, &local)) return;
@@ -1351,39 +1354,37 @@ __global__ __launch_bounds__(kDescWarps * 32, 8) void describe_kernel(const __gr
         if (local == 0 && threadIdx.x == 0) atomicAdd(j.out_count, count);
         for (int m = 0; m < j.level; ++m) base += j.level_counts[m];
     }
-    if (local * kDescWarps >= count) return;
+    if (local * kDescKeys >= count) return;
     {
         const int p = threadIdx.x;  // 256 threads, one pattern pair each
         const int4 q = kOrbPattern[p];
-        pat[p & 7][p >> 3] = (static_cast<std::uint32_t>(q.x & 0xff)) |
-                             (static_cast<std::uint32_t>(q.y & 0xff) << 8) |
-                             (static_cast<std::uint32_t>(q.z & 0xff) << 16) |
-                             (static_cast<std::uint32_t>(q.w & 0xff) << 24);
+        pat[p & 7][p >> 3] = make_float4(static_cast<float>(q.x), static_cast<float>(q.y), static_cast<float>(q.z),
+                                         static_cast<float>(q.w));
     }
     __syncthreads();
     const int lane = threadIdx.x & 31;
-    const int index = local * kDescWarps + (threadIdx.x >> 5);
-    if (index >= count) return;
-    std::uint8_t* row = j.out + static_cast<std::size_t>(base + index) * j.row_stride;
-    const int x = __float2int_rn(j.x[index]);
-    const int y = __float2int_rn(j.y[index]);
-    if (j.level_counts && lane == 0) {
-        j.out_x[base + index] = __fmul_rn(j.x[index], j.scale);
-        j.out_y[base + index] = __fmul_rn(j.y[index], j.scale);
-        if (j.out_response) j.out_response[base + index] = j.response[index];
-    }
-    if (x < kEdge || x >= j.width - kEdge || y < kEdge || y >= j.height - kEdge) {
-        row[lane] = 0;
-        return;
-    }
-    const int pitch = j.pitch;
-    const std::uint8_t* centre = j.image + static_cast<std::size_t>(y) * pitch + x;
-    // Moments as exact integer sums over the disc: lane l owns column
-    // u = l - 15 and walks the 31 rows, one coalesced row segment per step.
-    int m10 = 0, m01 = 0;
-    {
-        const int u = lane - 15;
-        const int au = u < 0 ? -u : u;
+    const int u = lane - 15, au = u < 0 ? -u : u;
+    const int pitch = j.pitch, blur_pitch = j.blur_pitch;
+    for (int r = 0; r < kDescRounds; ++r) {
+        const int index = local * kDescKeys + r * kDescWarps + (threadIdx.x >> 5);
+        if (index >= count) break;
+        std::uint8_t* row = j.out + static_cast<std::size_t>(base + index) * j.row_stride;
+        const float fx = j.x[index], fy = j.y[index];
+        const int x = __float2int_rn(fx);
+        const int y = __float2int_rn(fy);
+        if (j.level_counts && lane == 0) {
+            j.out_x[base + index] = __fmul_rn(fx, j.scale);
+            j.out_y[base + index] = __fmul_rn(fy, j.scale);
+            if (j.out_response) j.out_response[base + index] = j.response[index];
+        }
+        if (x < kEdge || x >= j.width - kEdge || y < kEdge || y >= j.height - kEdge) {
+            row[lane] = 0;
+            continue;
+        }
+        // Moments as exact integer sums over the disc: lane l owns column
+        // u = l - 15 and walks the 31 rows, one coalesced row segment per step.
+        const std::uint8_t* centre = j.image + static_cast<std::size_t>(y) * pitch + x;
+        int m10 = 0, m01 = 0;
 #pragma unroll
         for (int v = -15; v <= 15; ++v) {
             const int av = v < 0 ? -v : v;
@@ -1393,40 +1394,36 @@ __global__ __launch_bounds__(kDescWarps * 32, 8) void describe_kernel(const __gr
                 m01 += v * val;
             }
         }
-    }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        m10 += __shfl_xor_sync(0xffffffffu, m10, o);
-        m01 += __shfl_xor_sync(0xffffffffu, m01, o);
-    }
-    float a = 0.0f, b = 0.0f;
-    if (lane == 0) {
-        const float angle = __fmul_rn(fast_atan2_deg(static_cast<float>(m01), static_cast<float>(m10)),
-                                      0x1.1df46ap-6f);
-        // one sincos for both: it equals cos() and sin() bit for bit on every
-        // float in [0, 6.2832] (all the angles this can produce; checked
-        // exhaustively by tests/test_gpu_sincos.py)
-        double sd, cd;
-        sincos(static_cast<double>(angle), &sd, &cd);
-        a = static_cast<float>(cd);
-        b = static_cast<float>(sd);
-    }
-    a = __shfl_sync(0xffffffffu, a, 0);
-    b = __shfl_sync(0xffffffffu, b, 0);
-    const std::uint8_t* smooth = j.blurred + static_cast<std::size_t>(y) * j.blur_pitch + x;
-    int value = 0;
+        for (int o = 16; o > 0; o >>= 1) {
+            m10 += __shfl_xor_sync(0xffffffffu, m10, o);
+            m01 += __shfl_xor_sync(0xffffffffu, m01, o);
+        }
+        float a = 0.0f, b = 0.0f;
+        if (lane == 0) {
+            const float angle = __fmul_rn(fast_atan2_deg(static_cast<float>(m01), static_cast<float>(m10)),
+                                          0x1.1df46ap-6f);
+            // one sincos for both: it equals cos() and sin() bit for bit on every
+            // float in [0, 6.2832] (all the angles this can produce; checked
+            // exhaustively by tests/test_gpu_sincos.py)
+            double sd, cd;
+            sincos(static_cast<double>(angle), &sd, &cd);
+            a = static_cast<float>(cd);
+            b = static_cast<float>(sd);
+        }
+        a = __shfl_sync(0xffffffffu, a, 0);
+        b = __shfl_sync(0xffffffffu, b, 0);
+        const std::uint8_t* smooth = j.blurred + static_cast<std::size_t>(y) * blur_pitch + x;
+        int value = 0;
 #pragma unroll
-    for (int jj = 0; jj < 8; ++jj) {
-        const std::uint32_t pk = pat[jj][lane];
-        const int x0 = static_cast<int>(static_cast<std::int8_t>(pk & 0xff));
-        const int y0 = static_cast<int>(static_cast<std::int8_t>((pk >> 8) & 0xff));
-        const int x1 = static_cast<int>(static_cast<std::int8_t>((pk >> 16) & 0xff));
-        const int y1 = static_cast<int>(static_cast<std::int8_t>((pk >> 24) & 0xff));
-        const int t0 = rotated_sample(smooth, j.blur_pitch, x0, y0, a, b);
-        const int t1 = rotated_sample(smooth, j.blur_pitch, x1, y1, a, b);
-        value |= (t0 < t1) << jj;
+        for (int k = 0; k < 8; ++k) {
+            const float4 q = pat[k][lane];
+            const int t0 = rotated_sample(smooth, blur_pitch, q.x, q.y, a, b);
+            const int t1 = rotated_sample(smooth, blur_pitch, q.z, q.w, a, b);
+            value |= (t0 < t1) << k;
+        }
+        row[lane] = static_cast<std::uint8_t>(value);
     }
-    row[lane] = static_cast<std::uint8_t>(value);
 }
 
 }  // namespace stitch::b200::s2s3
