@@ -86,6 +86,9 @@ DetectJob make_detect_job(const ImageView& im, const s2::Config& c, const Keypoi
     j.response = out.response;
     j.count = out.d_count;
     j.tiles_x = l.tiles_x;
+    j.tiles_x_magic = l.tiles_x > 1 ? static_cast<std::uint32_t>((0x100000000ull + static_cast<std::uint64_t>(l.tiles_x) - 1) /
+                                                                 static_cast<std::uint64_t>(l.tiles_x))
+                                    : 0u;
     j.tiles = l.tiles;
     j.select_blocks = l.select_blocks;
     j.candidates = l.candidates;

@@ -61,6 +61,7 @@ struct alignas(16) DetectJob {  // 16-byte multiple: copied into shared memory i
     int job;  // this job's index in the describe table of the launch
     // launch bookkeeping
     int tiles_x, tiles, select_blocks, candidates;
+    std::uint32_t tiles_x_magic;  // ceil(2^32 / tiles_x), 0 for one tile column (see fast_origin)
     __host__ __device__ std::uint32_t* counters() const { return hist + 256; }
 };
 
@@ -172,6 +173,16 @@ enum DetectKind { kFastKind = 0, kSelectKind = 1, kHarrisKind = 2, kSortKind = 3
 enum DescribeKind { kBlurKind = 0, kDescKind = 1, kDescribeKinds = 2 };
 
 constexpr int kFastTileW = 64, kFastTileH = 32;
+
+// Origin (x0, y0) of FAST tile `local` of a job: local / tiles_x by a
+// multiply-high with ceil(2^32 / tiles_x), which is the quotient or one
+// above it (the error term local * (magic - 2^32 / tiles_x) / 2^32 is below
+// 1), then corrected.
+__device__ __forceinline__ int2 fast_origin(const DetectJob& j, int local) {
+    int ty = j.tiles_x_magic ? static_cast<int>(__umulhi(static_cast<std::uint32_t>(local), j.tiles_x_magic)) : local;
+    if (ty * j.tiles_x > local) --ty;
+    return make_int2((local - ty * j.tiles_x) * kFastTileW, ty * kFastTileH);
+}
 constexpr int kFastInW = kFastTileW + 8, kFastInH = kFastTileH + 8;  // halo 4 = FAST 3 + NMS 1
 constexpr int kFastScW = kFastTileW + 2, kFastScH = kFastTileH + 2;
 constexpr int kSelectPx = 65536;   // image pixels per select block (a job's maxima list is walked
@@ -332,7 +343,8 @@ template <> __device__ __forceinline__ const DetectJob* fast_jobs(const JobTable
 __device__ __forceinline__ void stage_fast_tile(const DetectJob& j, int local, std::uint8_t (*in)[kInStride]) {
     const int tid = threadIdx.x;
     const int W = j.width, H = j.height;
-    const int y0 = (local / j.tiles_x) * kFastTileH, x0 = (local % j.tiles_x) * kFastTileW;
+    const int2 org = fast_origin(j, local);
+    const int y0 = org.y, x0 = org.x;
     const bool vec = ((reinterpret_cast<std::uintptr_t>(j.image) | static_cast<std::uintptr_t>(j.pitch)) & 15) == 0;
     if (vec) {
         constexpr int kChunks = kInStride / 16;  // 6 per row
@@ -363,9 +375,9 @@ __device__ __forceinline__ void stage_fast_tile(const DetectJob& j, int local, s
 // the next tile's bytes are copied into the other half of a double buffer.
 // The jobs of the current and the next tile sit in shared memory. Per tile:
 //   1. the compass test on the tile plus a 1-pixel ring, 4 positions per
-//      thread in 16-bit lanes; groups with a survivor are listed so that full
-//      scores are computed on full warps;
-//   2. the survivors are scored (every other position scores 0);
+//      thread in 16-bit lanes; groups with a survivor are listed;
+//   2. the groups are expanded into one list of survivor positions, scored
+//      on full warps (every other position scores 0);
 //   3. each survivor of the tile inside the 31-pixel edge margin that is a
 //      strict 3x3 maximum goes into the job's maxima list as
 //      (score << 32) | raster index, its score into the job's histogram.
@@ -377,16 +389,16 @@ __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(cons
     __shared__ __align__(16) std::uint8_t in[2][kFastInH][kInStride];
     __shared__ __align__(16) std::uint8_t sc[kFastScH][kScStride];
     __shared__ std::uint16_t cand[kFastScH * kScGroups];
-    __shared__ std::uint16_t wpos[8][128];
+    __shared__ std::uint16_t pos[kFastScH * kFastScW];  // survivor positions r * kScStride + c
     __shared__ std::uint32_t hist[256];
     __shared__ std::uint64_t found[kTileMaxima];
     __shared__ DetectJob jobs[2];  // jobs of the tiles in in[0] and in[1] (kept here, not in registers)
     __shared__ int locals[2];
-    __shared__ int n_cand, n_found, next;
+    __shared__ int n_cand, n_found, n_pos, next;
     __shared__ std::uint32_t list_base;
     __shared__ int ahead_tile;          // with a block map: the tile after `next`, taken from the queue
     __shared__ std::uint32_t ahead_entry;  // and its block-map entry (job << 16 | tile within the job)
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int tid = threadIdx.x, lane = tid & 31;
     // With a block map, total is capped by the map; the job of the tile after
     // the current one is copied into shared memory asynchronously while the
     // current tile is tested, and the queue index and map entry of the tile
@@ -397,6 +409,7 @@ __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(cons
     if (tid == 0) {
         n_cand = 0;
         n_found = 0;
+        n_pos = 0;
         next = static_cast<int>(atomicAdd(queue, 1u));
         if (next < total && !src.find(next, kFastKind, &jobs[0], &locals[0])) next = total;
         if (map) {
@@ -414,7 +427,8 @@ __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(cons
         const DetectJob& j = jobs[buf];
         const int local = locals[buf];
         const int W = j.width, H = j.height;
-        const int y0 = (local / j.tiles_x) * kFastTileH, x0 = (local % j.tiles_x) * kFastTileW;
+        const int2 org = fast_origin(j, local);
+        const int y0 = org.y, x0 = org.x;
         std::uint8_t (*cur)[kInStride] = in[buf];
         int ahead = total;  // thread 0 with a block map: the queue index of the tile after next
         if (tid == 0) {
@@ -497,10 +511,9 @@ __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(cons
         }
         if (nt < total) stage_fast_tile(jobs[buf ^ 1], locals[buf ^ 1], in[buf ^ 1]);
         const int nc = n_cand;
-        // 2. each warp expands its 32 survivor groups of a round into a
-        // warp-local position list (warp scan of the counts) and scores it
-        // 32 at a time
-        for (int base = 0; base < nc; base += 256) {
+        // 2. the survivor groups expanded into one position list (each warp
+        // reserves its share with one shared atomic), then scored on full warps
+        for (int base = 0; base < nc; base += kFastThreads) {  // block-uniform trip count
             const int i = base + tid;
             unsigned bits = 0;
             int pos0 = 0;
@@ -517,37 +530,36 @@ __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(cons
                 const int t = __shfl_up_sync(0xffffffffu, incl, o);
                 if (lane >= o) incl += t;
             }
-            const int total_w = __shfl_sync(0xffffffffu, incl, 31);
-            int o = incl - cnt;
-            for (unsigned b = bits; b; b &= b - 1) wpos[warp][o++] = static_cast<std::uint16_t>(pos0 + __ffs(b) - 1);
-            __syncwarp();
-            for (int k = lane; k < total_w; k += 32) {
-                const int e2 = wpos[warp][k];
-                const int r = e2 / kScStride, c = e2 - r * kScStride;
-                sc[r][c] = static_cast<std::uint8_t>(fast_score(&cur[r + 3][c + 3 + kInOff], kInStride, j.threshold));
-            }
-            __syncwarp();
+            int first = 0;
+            if (lane == 31 && incl) first = atomicAdd(&n_pos, incl);
+            first = __shfl_sync(0xffffffffu, first, 31);
+            int o = first + incl - cnt;
+            for (unsigned b = bits; b; b &= b - 1) pos[o++] = static_cast<std::uint16_t>(pos0 + __ffs(b) - 1);
+        }
+        __syncthreads();
+        const int np = n_pos;
+        for (int k = tid; k < np; k += kFastThreads) {
+            const int e = pos[k];
+            const int r = e / kScStride, c = e - r * kScStride;
+            sc[r][c] = static_cast<std::uint8_t>(fast_score(&cur[r + 3][c + 3 + kInOff], kInStride, j.threshold));
         }
         __syncthreads();
         // 3. strict 3x3 maxima inside the 31-pixel edge margin: only listed
-        // survivors can score above 0, so only they are tested
-        for (int i = tid; i < nc; i += kFastThreads) {
-            const int e = cand[i];
-            const int grp = e >> 4, r = grp / kScGroups, c0 = 4 * (grp - r * kScGroups);
-            if (r < 1 || r > kFastTileH) continue;  // the ring rows hold neighbours only
-            for (unsigned bits = e & 0xfu; bits; bits &= bits - 1) {
-                const int c = c0 + __ffs(bits) - 1;
-                if (c < 1 || c > kFastTileW) continue;
-                const int gy = y0 - 1 + r, gx = x0 - 1 + c;
-                if (gy < kEdge || gy >= H - kEdge || gx < kEdge || gx >= W - kEdge) continue;
-                const unsigned v = sc[r][c];
-                if (v && v > sc[r - 1][c - 1] && v > sc[r - 1][c] && v > sc[r - 1][c + 1] && v > sc[r][c - 1] &&
-                    v > sc[r][c + 1] && v > sc[r + 1][c - 1] && v > sc[r + 1][c] && v > sc[r + 1][c + 1]) {
-                    const std::uint32_t px = static_cast<std::uint32_t>(gy) * static_cast<std::uint32_t>(W) +
-                                             static_cast<std::uint32_t>(gx);
-                    found[atomicAdd(&n_found, 1)] = (static_cast<std::uint64_t>(v) << 32) | px;
-                    atomicAdd(&hist[v], 1u);
-                }
+        // survivors can score above 0, so only they are tested (the ring
+        // rows and columns hold neighbours only)
+        for (int k = tid; k < np; k += kFastThreads) {
+            const int e = pos[k];
+            const int r = e / kScStride, c = e - r * kScStride;
+            if (r < 1 || r > kFastTileH || c < 1 || c > kFastTileW) continue;
+            const int gy = y0 - 1 + r, gx = x0 - 1 + c;
+            if (gy < kEdge || gy >= H - kEdge || gx < kEdge || gx >= W - kEdge) continue;
+            const unsigned v = sc[r][c];
+            if (v && v > sc[r - 1][c - 1] && v > sc[r - 1][c] && v > sc[r - 1][c + 1] && v > sc[r][c - 1] &&
+                v > sc[r][c + 1] && v > sc[r + 1][c - 1] && v > sc[r + 1][c] && v > sc[r + 1][c + 1]) {
+                const std::uint32_t px = static_cast<std::uint32_t>(gy) * static_cast<std::uint32_t>(W) +
+                                         static_cast<std::uint32_t>(gx);
+                found[atomicAdd(&n_found, 1)] = (static_cast<std::uint64_t>(v) << 32) | px;
+                atomicAdd(&hist[v], 1u);
             }
         }
         __syncthreads();
@@ -565,6 +577,7 @@ __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(cons
         if (tid == 0) {
             n_cand = 0;
             n_found = 0;
+            n_pos = 0;
         }
         cp_async_wait_all();
         __syncthreads();
