@@ -172,7 +172,7 @@ template <class Job, int kJobs, int kKinds> struct InlineTable {
 enum DetectKind { kFastKind = 0, kSelectKind = 1, kHarrisKind = 2, kSortKind = 3, kDetectKinds = 4 };
 enum DescribeKind { kBlurKind = 0, kDescKind = 1, kDescribeKinds = 2 };
 
-constexpr int kFastTileW = 64, kFastTileH = 32;
+constexpr int kFastTileW = 64, kFastTileH = 64;
 
 // Origin (x0, y0) of FAST tile `local` of a job: local / tiles_x by a
 // multiply-high with ceil(2^32 / tiles_x), which is the quotient or one
@@ -188,8 +188,7 @@ constexpr int kFastScW = kFastTileW + 2, kFastScH = kFastTileH + 2;
 constexpr int kSelectPx = 65536;   // image pixels per select block (a job's maxima list is walked
                                    // by ceil(W * H / kSelectPx) blocks)
 constexpr int kFastThreads = 256;
-constexpr int kFastCtasPerSm = 8;  // resident FAST blocks per SM; the persistent grid is 148 x this
-constexpr int kTileMaxima = kFastTileW * kFastTileH / 4;  // strict 3x3 maxima: at most one per 2x2 cell
+constexpr int kFastCtasPerSm = 7;  // resident FAST blocks per SM (shared memory); the persistent grid is 148 x this
 constexpr int kTieThreads = 1024;
 // Largest offset of a rotated rBRIEF sample from its keypoint: the pattern's
 // coordinates lie within a radius of 18.39 px (|x|, |y| <= 13), so a rotated
@@ -348,8 +347,8 @@ __device__ __forceinline__ void stage_fast_tile(const DetectJob& j, int local, s
     const bool vec = ((reinterpret_cast<std::uintptr_t>(j.image) | static_cast<std::uintptr_t>(j.pitch)) & 15) == 0;
     if (vec) {
         constexpr int kChunks = kInStride / 16;  // 6 per row
-        if (tid < kFastInH * kChunks) {
-            const int r = tid / kChunks, q = tid - r * kChunks;
+        for (int i = tid; i < kFastInH * kChunks; i += kFastThreads) {
+            const int r = i / kChunks, q = i - r * kChunks;
             const int gy = min(max(y0 - 4 + r, 0), H - 1);
             const int cx = x0 - 16 + 16 * q;
             const int limit = gy == H - 1 ? W : j.pitch;  // bytes of the row that may be read
@@ -369,7 +368,7 @@ __device__ __forceinline__ void stage_fast_tile(const DetectJob& j, int local, s
     }
 }
 
-// FAST-9 + strict 3x3 NMS, persistent: each block takes 64x32 tiles of
+// FAST-9 + strict 3x3 NMS, persistent: each block takes 64x64 tiles of
 // every job of the launch from a device queue (`*queue`, zero at launch; tile
 // t of `total` is looked up through the source's kFastKind entries), while
 // the next tile's bytes are copied into the other half of a double buffer.
@@ -380,7 +379,8 @@ __device__ __forceinline__ void stage_fast_tile(const DetectJob& j, int local, s
 //      on full warps (every other position scores 0);
 //   3. each survivor of the tile inside the 31-pixel edge margin that is a
 //      strict 3x3 maximum goes into the job's maxima list as
-//      (score << 32) | raster index, its score into the job's histogram.
+//      (score << 32) | raster index (one atomic per warp), its score into the
+//      tile's histogram, which is added to the job's at the end of the tile.
 // No maxima map and no blur are written.
 template <class Src>
 __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(const __grid_constant__ Src src,
@@ -391,11 +391,9 @@ __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(cons
     __shared__ std::uint16_t cand[kFastScH * kScGroups];
     __shared__ std::uint16_t pos[kFastScH * kFastScW];  // survivor positions r * kScStride + c
     __shared__ std::uint32_t hist[256];
-    __shared__ std::uint64_t found[kTileMaxima];
     __shared__ DetectJob jobs[2];  // jobs of the tiles in in[0] and in[1] (kept here, not in registers)
     __shared__ int locals[2];
-    __shared__ int n_cand, n_found, n_pos, next;
-    __shared__ std::uint32_t list_base;
+    __shared__ int n_cand, n_pos, next;
     __shared__ int ahead_tile;          // with a block map: the tile after `next`, taken from the queue
     __shared__ std::uint32_t ahead_entry;  // and its block-map entry (job << 16 | tile within the job)
     const int tid = threadIdx.x, lane = tid & 31;
@@ -408,7 +406,6 @@ __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(cons
     hist[tid] = 0;
     if (tid == 0) {
         n_cand = 0;
-        n_found = 0;
         n_pos = 0;
         next = static_cast<int>(atomicAdd(queue, 1u));
         if (next < total && !src.find(next, kFastKind, &jobs[0], &locals[0])) next = total;
@@ -451,7 +448,7 @@ __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(cons
             }
         }
         // 1. compass test: thread (q, rb) takes positions 4q .. 4q+3 of rows rb,
-        // rb + 15, rb + 30; groups with a survivor are listed as
+        // rb + 15, rb + 30, ...; groups with a survivor are listed as
         // (group << 4 | survivor bits)
         const std::uint32_t thr1 = static_cast<std::uint32_t>(j.threshold + 1) * 0x00010001u;
         {
@@ -546,37 +543,50 @@ __global__ __launch_bounds__(kFastThreads, kFastCtasPerSm) void fast_kernel(cons
         __syncthreads();
         // 3. strict 3x3 maxima inside the 31-pixel edge margin: only listed
         // survivors can score above 0, so only they are tested (the ring
-        // rows and columns hold neighbours only)
-        for (int k = tid; k < np; k += kFastThreads) {
-            const int e = pos[k];
-            const int r = e / kScStride, c = e - r * kScStride;
-            if (r < 1 || r > kFastTileH || c < 1 || c > kFastTileW) continue;
-            const int gy = y0 - 1 + r, gx = x0 - 1 + c;
-            if (gy < kEdge || gy >= H - kEdge || gx < kEdge || gx >= W - kEdge) continue;
-            const unsigned v = sc[r][c];
-            if (v && v > sc[r - 1][c - 1] && v > sc[r - 1][c] && v > sc[r - 1][c + 1] && v > sc[r][c - 1] &&
-                v > sc[r][c + 1] && v > sc[r + 1][c - 1] && v > sc[r + 1][c] && v > sc[r + 1][c + 1]) {
-                const std::uint32_t px = static_cast<std::uint32_t>(gy) * static_cast<std::uint32_t>(W) +
-                                         static_cast<std::uint32_t>(gx);
-                found[atomicAdd(&n_found, 1)] = (static_cast<std::uint64_t>(v) << 32) | px;
-                atomicAdd(&hist[v], 1u);
+        // rows and columns hold neighbours only). Each warp appends its maxima
+        // to the job's list with one atomic, and their scores to the tile's
+        // histogram.
+        for (int k0 = 0; k0 < np; k0 += kFastThreads) {  // block-uniform trip count
+            const int k = k0 + tid;
+            unsigned v = 0;
+            std::uint32_t px = 0;
+            if (k < np) {
+                const int e = pos[k];
+                const int r = e / kScStride, c = e - r * kScStride;
+                const int gy = y0 - 1 + r, gx = x0 - 1 + c;
+                if (r >= 1 && r <= kFastTileH && c >= 1 && c <= kFastTileW && gy >= kEdge && gy < H - kEdge &&
+                    gx >= kEdge && gx < W - kEdge) {
+                    const unsigned s0 = sc[r][c];
+                    if (s0 && s0 > sc[r - 1][c - 1] && s0 > sc[r - 1][c] && s0 > sc[r - 1][c + 1] &&
+                        s0 > sc[r][c - 1] && s0 > sc[r][c + 1] && s0 > sc[r + 1][c - 1] && s0 > sc[r + 1][c] &&
+                        s0 > sc[r + 1][c + 1]) {
+                        v = s0;
+                        px = static_cast<std::uint32_t>(gy) * static_cast<std::uint32_t>(W) + static_cast<std::uint32_t>(gx);
+                    }
+                }
+            }
+            const unsigned m = __ballot_sync(0xffffffffu, v != 0);
+            if (m) {
+                const int leader = __ffs(m) - 1;
+                std::uint32_t first = 0;
+                if (lane == leader) first = atomicAdd(&j.counters()[kListed], static_cast<std::uint32_t>(__popc(m)));
+                first = __shfl_sync(0xffffffffu, first, leader);
+                if (v) {
+                    const std::uint32_t slot = first + static_cast<std::uint32_t>(__popc(m & ((1u << lane) - 1u)));
+                    if (slot < static_cast<std::uint32_t>(j.max_maxima))
+                        j.maxima[slot] = (static_cast<std::uint64_t>(v) << 32) | px;
+                    atomicAdd(&hist[v], 1u);
+                }
             }
         }
         __syncthreads();
-        // the tile's maxima and histogram into the job's list and histogram
-        const int nf = n_found;
-        if (tid == 0 && nf) list_base = atomicAdd(&j.counters()[kListed], static_cast<std::uint32_t>(nf));
-        __syncthreads();
-        for (int i = tid; i < nf; i += kFastThreads)
-            if (list_base + static_cast<std::uint32_t>(i) < static_cast<std::uint32_t>(j.max_maxima))
-                j.maxima[list_base + i] = found[i];
+        // the tile's histogram into the job's
         if (hist[tid]) {
             atomicAdd(&j.hist[tid], hist[tid]);
             hist[tid] = 0;
         }
         if (tid == 0) {
             n_cand = 0;
-            n_found = 0;
             n_pos = 0;
         }
         cp_async_wait_all();
@@ -1130,7 +1140,7 @@ __global__ __launch_bounds__(256) void blur_kernel(const __grid_constant__ Src s
 // list entries b, b + gridDim.x, ... (the list is complete when the kernel
 // starts). A tile is staged with its reflect-101 halo: 16-byte loads for
 // interior tiles of 16-byte aligned images, reflected byte loads otherwise.
-static_assert(kBlurTileW == kFastTileW && kBlurTileH == kFastTileH, "blur tiles share the FAST tile staging");
+constexpr int kBlurInH = kBlurTileH + 8;  // staged rows of a blur tile: rows y0-4 .. y0+35 (halo 3, rounded to 4)
 
 // Origin of blur tile `tile` of job j.
 __device__ __forceinline__ void blur_tile_origin(const DescribeJob& j, unsigned tile, int* x0, int* y0) {
@@ -1152,7 +1162,7 @@ __device__ __forceinline__ bool aligned16(const DescribeJob& j) {
 __device__ __forceinline__ void blur_stage_async(const DescribeJob& j, int x0, int y0, std::uint8_t (*in)[kInStride]) {
     const int tid = threadIdx.x;
     constexpr int kChunks = kInStride / 16;
-    if (tid < kFastInH * kChunks) {
+    if (tid < kBlurInH * kChunks) {
         const int r = tid / kChunks, q = tid - r * kChunks;
         const int gy = reflect101(y0 - 4 + r, j.height);
         const int cx = x0 - 16 + 16 * q;
@@ -1173,7 +1183,7 @@ __device__ __forceinline__ bool blur_needs_columns(int x0, int W) { return x0 < 
 // W - 1 + k is column W - 1 - k (k = 1..3), copied inside `in`.
 __device__ __forceinline__ void blur_fix_columns(int x0, int W, std::uint8_t (*in)[kInStride]) {
     const int tid = threadIdx.x;
-    if (tid >= kFastInH * 6) return;
+    if (tid >= kBlurInH * 6) return;
     const int r = tid / 6, k = tid % 6;
     const int off = x0 - 16;  // column of byte 0
     int dst, srcc;
@@ -1193,9 +1203,9 @@ constexpr int kBlurCtasPerSm = 6;  // resident blur blocks per SM; the persisten
 template <class Src>
 __global__ __launch_bounds__(256, kBlurCtasPerSm) void blur_tiles_kernel(const __grid_constant__ Src src, const uint2* list,
                                                             const std::uint32_t* count) {
-    __shared__ __align__(16) std::uint8_t in2[2][kFastInH][kInStride];  // rows y0-4 .., columns x0-16 ..
-    __shared__ __align__(16) float rows[kFastTileH + 6][kFastTileW];
-    __shared__ std::size_t row_at[kFastInH];
+    __shared__ __align__(16) std::uint8_t in2[2][kBlurInH][kInStride];  // rows y0-4 .., columns x0-16 ..
+    __shared__ __align__(16) float rows[kBlurTileH + 6][kBlurTileW];
+    __shared__ std::size_t row_at[kBlurInH];
     __shared__ int col_at[kInStride];
     const int tid = threadIdx.x;
     const int n = static_cast<int>(*count);
@@ -1218,10 +1228,10 @@ __global__ __launch_bounds__(256, kBlurCtasPerSm) void blur_tiles_kernel(const _
         int x0, y0;
         blur_tile_origin(j, e.y, &x0, &y0);
         if (!aligned16(j)) {  // unaligned image: reflected byte loads
-            if (tid < kFastInH) row_at[tid] = static_cast<std::size_t>(reflect101(y0 - 4 + tid, H)) * j.pitch;
-            else if (tid < kFastInH + kInStride) col_at[tid - kFastInH] = reflect101(x0 - 16 + (tid - kFastInH), W);
+            if (tid < kBlurInH) row_at[tid] = static_cast<std::size_t>(reflect101(y0 - 4 + tid, H)) * j.pitch;
+            else if (tid < kBlurInH + kInStride) col_at[tid - kBlurInH] = reflect101(x0 - 16 + (tid - kBlurInH), W);
             __syncthreads();
-            for (int k = tid; k < kFastInH * (kInStride / 4); k += 256) {
+            for (int k = tid; k < kBlurInH * (kInStride / 4); k += 256) {
                 const int r = k / (kInStride / 4), b = 4 * (k - r * (kInStride / 4));
                 const std::uint8_t* row = j.image + row_at[r];
                 *reinterpret_cast<std::uint32_t*>(&in[r][b]) =
@@ -1238,9 +1248,9 @@ __global__ __launch_bounds__(256, kBlurCtasPerSm) void blur_tiles_kernel(const _
         }
         if (i + static_cast<int>(gridDim.x) < n) prefetch(i + gridDim.x, in2[buf ^ 1]);
         // rows pass: image rows y0-3 .. y0+34, two rows x 4 outputs per item
-        static_assert((kFastTileH + 6) % 2 == 0, "rows pass takes row pairs");
-        for (int g = tid; g < (kFastTileH + 6) / 2 * (kFastTileW / 4); g += 256) {
-            const int rp = g / (kFastTileW / 4), q = g - rp * (kFastTileW / 4), rr = 2 * rp;
+        static_assert((kBlurTileH + 6) % 2 == 0, "rows pass takes row pairs");
+        for (int g = tid; g < (kBlurTileH + 6) / 2 * (kBlurTileW / 4); g += 256) {
+            const int rp = g / (kBlurTileW / 4), q = g - rp * (kBlurTileW / 4), rr = 2 * rp;
             const auto* ra = reinterpret_cast<const std::uint32_t*>(&in[rr + 1][0]);
             const auto* rb = reinterpret_cast<const std::uint32_t*>(&in[rr + 2][0]);
             const std::uint32_t a0 = ra[q + 3], a1 = ra[q + 4], a2 = ra[q + 5];  // bytes 4q+12 .. 4q+23
@@ -1266,7 +1276,7 @@ __global__ __launch_bounds__(256, kBlurCtasPerSm) void blur_tiles_kernel(const _
         }
         __syncthreads();
         {   // columns pass: rows 2p, 2p+1 and columns 4q .. 4q+3 per thread
-            const int pr = tid / (kFastTileW / 4), q = tid - pr * (kFastTileW / 4);
+            const int pr = tid / (kBlurTileW / 4), q = tid - pr * (kBlurTileW / 4);
             float2 lo[2], hi[2];
 #pragma unroll
             for (int r = 0; r < 8; ++r) {

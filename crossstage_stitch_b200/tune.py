@@ -31,7 +31,7 @@ BUCKETS = (("vga", 640 * 480), ("720p", 1280 * 720), ("1080p", 1920 * 1080), ("4
 K_CLASSES = (("k500", 1000), ("k2000", 4000), ("k8000", 1 << 30))
 # candidate values of each tuning field, the default first
 SPACE = {
-    "fast_ctas_per_sm": (8, 6, 4),
+    "fast_ctas_per_sm": (7, 6, 4),
     "resize_tile_h": (64, 32, 16),
     "blur_ctas_per_sm": (6, 4),
     "matcher": (2, 5),          # 1 + matcher kind: tensor cores, pipelined tensor cores

@@ -322,7 +322,7 @@ int stitch_batch_create(int n_pairs, const stitch_pair_desc* pairs, stitch_batch
 /* No reference counterpart (batched form). Launch shapes of a plan, chosen
  * per plan by an autotuner (results never depend on them); 0 in a field
  * keeps its default. fast_ctas_per_sm: resident FAST blocks per SM in the
- * persistent FAST grid, 1..8 (default 8); blur_ctas_per_sm: the same for the
+ * persistent FAST grid, 1..7 (default 7); blur_ctas_per_sm: the same for the
  * on-demand blur, 1..6 (default 6); matcher: 1 + an S4 matcher kind (0..4,
  * as for stitch_s4_set_matcher), or 0 for the creating thread's choice;
  * search_hpw: MSAC hypotheses per warp round, 4, 8, 16 or 32 (default: the

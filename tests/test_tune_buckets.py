@@ -11,5 +11,5 @@ def test_buckets_and_k_classes():
     assert [tune.k_class(k) for k in (1, 500, 1000, 2000, 4000, 8000, 20000)] == \
         ["k500", "k500", "k500", "k2000", "k2000", "k8000", "k8000"]
     # every tuning field has its default first and valid values only
-    assert tune.SPACE["fast_ctas_per_sm"][0] == 8 and tune.SPACE["resize_tile_h"][0] == 64
+    assert tune.SPACE["fast_ctas_per_sm"][0] == 7 and tune.SPACE["resize_tile_h"][0] == 64
     assert all(1 <= m <= 5 for m in tune.SPACE["matcher"])
