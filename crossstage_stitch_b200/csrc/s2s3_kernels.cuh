@@ -198,7 +198,7 @@ constexpr int kHarrisThreads = 256;
 constexpr int kSortCap = 16384;    // candidates sorted in shared memory by one block
 constexpr int kSortThreads = 1024;
 constexpr int kSortChunk = 64;      // keys a warp sorts in registers (2 per lane)
-constexpr int kBlurTileW = 64, kBlurTileH = 32;
+constexpr int kBlurTileW = 64, kBlurTileH = 64;
 constexpr int kDescWarps = 8;
 constexpr int kDescRounds = 4;                        // keypoints per warp of a describe block
 constexpr int kDescKeys = kDescWarps * kDescRounds;  // keypoints per describe block
@@ -330,7 +330,7 @@ template <class S> __device__ __forceinline__ int fast_map_tiles(const S&) { ret
 template <> __device__ __forceinline__ int fast_map_tiles(const JobTable<DetectJob>& s) { return s.map_blocks[kFastKind]; }
 template <> __device__ __forceinline__ const DetectJob* fast_jobs(const JobTable<DetectJob>& s) { return s.jobs; }
 
-// Stages rows y0-4 .. y0+35 and columns x0-16 .. x0+79 of the job's image in
+// Stages rows y0-4 .. y0+67 and columns x0-16 .. x0+79 of the job's image in
 // `in` (byte c of row r = image (y0-4+r, x0-16+c)). The FAST test never reads
 // a position outside the image, so rows are clamped into it and the bytes of
 // columns outside it are left as they are. With a 16-byte aligned image (base
@@ -1088,7 +1088,7 @@ __global__ __launch_bounds__(256, 5) void resize_kernel(const __grid_constant__ 
 
 // ------------------------------------------------------------- S3 blur
 
-// One block = one 64x32 tile: rows pass into a float tile with a 3-row halo,
+// One block = one 64x64 tile: rows pass into a float tile with a 3-row halo,
 // then the columns pass; per output the taps are summed first to last with
 // each product and sum rounded separately, then rounded half-to-even and
 // clamped to [0, 255].
@@ -1131,7 +1131,7 @@ __global__ __launch_bounds__(256) void blur_kernel(const __grid_constant__ Src s
     }
 }
 
-// The S3 blur of the 64x32 tiles listed by the keypoint writers (on-demand
+// The S3 blur of the 64x64 tiles listed by the keypoint writers (on-demand
 // blur of the pyramid and batched paths): the same bytes as blur_kernel
 // (per output the taps summed first to last, each product and sum rounded on
 // its own, then rounded half-to-even and clamped), with both passes on the
@@ -1140,7 +1140,7 @@ __global__ __launch_bounds__(256) void blur_kernel(const __grid_constant__ Src s
 // list entries b, b + gridDim.x, ... (the list is complete when the kernel
 // starts). A tile is staged with its reflect-101 halo: 16-byte loads for
 // interior tiles of 16-byte aligned images, reflected byte loads otherwise.
-constexpr int kBlurInH = kBlurTileH + 8;  // staged rows of a blur tile: rows y0-4 .. y0+35 (halo 3, rounded to 4)
+constexpr int kBlurInH = kBlurTileH + 8;  // staged rows of a blur tile: rows y0-4 .. y0+kBlurTileH+3 (halo 3, rounded to 4)
 
 // Origin of blur tile `tile` of job j.
 __device__ __forceinline__ void blur_tile_origin(const DescribeJob& j, unsigned tile, int* x0, int* y0) {
@@ -1162,8 +1162,8 @@ __device__ __forceinline__ bool aligned16(const DescribeJob& j) {
 __device__ __forceinline__ void blur_stage_async(const DescribeJob& j, int x0, int y0, std::uint8_t (*in)[kInStride]) {
     const int tid = threadIdx.x;
     constexpr int kChunks = kInStride / 16;
-    if (tid < kBlurInH * kChunks) {
-        const int r = tid / kChunks, q = tid - r * kChunks;
+    for (int i = tid; i < kBlurInH * kChunks; i += 256) {
+        const int r = i / kChunks, q = i - r * kChunks;
         const int gy = reflect101(y0 - 4 + r, j.height);
         const int cx = x0 - 16 + 16 * q;
         const int limit = gy == j.height - 1 ? j.width : j.pitch;
@@ -1182,21 +1182,21 @@ __device__ __forceinline__ bool blur_needs_columns(int x0, int W) { return x0 < 
 // Reflect-101 halo columns of a staged tile: column -k is column k, column
 // W - 1 + k is column W - 1 - k (k = 1..3), copied inside `in`.
 __device__ __forceinline__ void blur_fix_columns(int x0, int W, std::uint8_t (*in)[kInStride]) {
-    const int tid = threadIdx.x;
-    if (tid >= kBlurInH * 6) return;
-    const int r = tid / 6, k = tid % 6;
-    const int off = x0 - 16;  // column of byte 0
-    int dst, srcc;
-    if (k < 3) {  // left edge
-        dst = -(k + 1);
-        srcc = k + 1;
-    } else {      // right edge
-        dst = W - 1 + (k - 2);
-        srcc = W - 1 - (k - 2);
+    for (int i = threadIdx.x; i < kBlurInH * 6; i += 256) {  // sources are interior columns, never written here
+        const int r = i / 6, k = i % 6;
+        const int off = x0 - 16;  // column of byte 0
+        int dst, srcc;
+        if (k < 3) {  // left edge
+            dst = -(k + 1);
+            srcc = k + 1;
+        } else {      // right edge
+            dst = W - 1 + (k - 2);
+            srcc = W - 1 - (k - 2);
+        }
+        const int db = dst - off, sb = srcc - off;
+        if (db >= 0 && db < kInStride && sb >= 0 && sb < kInStride && dst >= x0 - 3 && dst <= x0 + kBlurTileW + 2)
+            in[r][db] = in[r][sb];
     }
-    const int db = dst - off, sb = srcc - off;
-    if (db >= 0 && db < kInStride && sb >= 0 && sb < kInStride && dst >= x0 - 3 && dst <= x0 + kBlurTileW + 2)
-        in[r][db] = in[r][sb];
 }
 
 constexpr int kBlurCtasPerSm = 6;  // resident blur blocks per SM; the persistent grid is 148 x this
@@ -1275,8 +1275,9 @@ __global__ __launch_bounds__(256, kBlurCtasPerSm) void blur_tiles_kernel(const _
             *reinterpret_cast<float4*>(&rows[rr + 1][4 * q]) = make_float4(out[0].y, out[1].y, out[2].y, out[3].y);
         }
         __syncthreads();
-        {   // columns pass: rows 2p, 2p+1 and columns 4q .. 4q+3 per thread
-            const int pr = tid / (kBlurTileW / 4), q = tid - pr * (kBlurTileW / 4);
+        // columns pass: rows 2p, 2p+1 and columns 4q .. 4q+3 per thread and step
+        for (int pr = tid / (kBlurTileW / 4), q = tid % (kBlurTileW / 4); pr < kBlurTileH / 2;
+             pr += 256 / (kBlurTileW / 4)) {
             float2 lo[2], hi[2];
 #pragma unroll
             for (int r = 0; r < 8; ++r) {
