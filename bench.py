@@ -303,9 +303,9 @@ def run_reference(args):
 # DRAM bytes (read + write) per launch of a kernel of the batched step, from
 # one ncu capture of this workload (dram__bytes_read.sum + dram__bytes_write.sum).
 NCU_TRAFFIC = {
-    "fast_nms": (111.13e6, "ncu capture of this workload (fast_kernel, one launch)"),
-    "blur": (183.90e6, "ncu capture of this workload (blur_tiles_kernel, one launch)"),
-    "describe": (169.82e6, "ncu capture of this workload (describe_kernel, one launch)"),
+    "fast_nms": (110.70e6, "ncu capture of this workload (fast_kernel, one launch)"),
+    "blur": (192.09e6, "ncu capture of this workload (blur_tiles_kernel, one launch)"),
+    "describe": (170.39e6, "ncu capture of this workload (describe_kernel, one launch)"),
     "search": (13.09e6, "ncu capture of this workload (scoring kernel)"),
 }
 
@@ -936,7 +936,7 @@ def main():
                     "traffic_source": NCU_TRAFFIC.get(dominant, (None, None))[1],
                     "ms_per_launch": kern[dominant]}
             if dominant == "fast_nms":
-                roof["note"] = ("ALU-issue bound: about 86 thread-instructions per layer pixel (ncu), so its HBM "
+                roof["note"] = ("ALU-issue bound: about 68 thread-instructions per layer pixel (ncu), so its HBM "
                                 "fraction is set by the instruction count, not by wasted traffic")
         roof_fp64 = None
         if "search" in kern and "search" in work:
