@@ -20,10 +20,10 @@ pytestmark = pytest.mark.gpu
 ref = C.byref
 
 
-def run_pyramid(gray, thr, k, levels, factor, stride=48, capacity=None):
+def run_pyramid(gray, thr, k, levels, factor, stride=48, capacity=None, pad=None):
     L = _abi.load()
     h, w = gray.shape
-    img = pitched(gray)
+    img = pitched(gray) if pad is None else pitched(gray, pad)
     iv = ImageView(img.data_ptr(), w, h, img.stride(0), 1)
     cap = k if capacity is None else capacity
     n = max(cap, 1)
@@ -83,6 +83,29 @@ def test_pyramid_vs_oracle(cuda, case):
     assert st == 0
     want_kp, want_desc = pyramid.detect_and_describe(gray, thr, k, levels, factor)
     assert kp.shape == want_kp.shape
+    assert np.array_equal(kp, want_kp)
+    assert np.array_equal(desc, want_desc)
+
+
+# The resize of layer 1 reads the caller's image: a 16-byte aligned pitch
+# takes the staged-window path, the default odd pitch the byte path; layer
+# ratios of 3 and 4 leave lanes whose four columns do not fit two 8-byte
+# pools (per-lane byte path) and windows beyond the staging buffer.
+RESIZE_CASES = [
+    ("odd", 1.2), ("odd", 1.45), ("vga", 2.0), ("odd", 3.0), ("vga", 4.0),
+]
+
+
+@pytest.mark.parametrize("case", RESIZE_CASES, ids=[f"{c[0]}-s{c[1]}" for c in RESIZE_CASES])
+@pytest.mark.parametrize("aligned", [True, False], ids=["pitch16", "pitch-odd"])
+def test_pyramid_resize_paths_vs_oracle(cuda, case, aligned):
+    kind, factor = case
+    gray = image(kind)
+    w = gray.shape[1]
+    pad = (-w) % 16 + 16 if aligned else None
+    st, kp, desc = run_pyramid(gray, 20, 800, 4, factor, pad=pad)
+    assert st == 0
+    want_kp, want_desc = pyramid.detect_and_describe(gray, 20, 800, 4, factor)
     assert np.array_equal(kp, want_kp)
     assert np.array_equal(desc, want_desc)
 
