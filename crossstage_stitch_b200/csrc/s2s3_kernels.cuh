@@ -1332,6 +1332,37 @@ __device__ __forceinline__ int disc_half_width(int v) {
                  : static_cast<int>((hi >> (8 * (v - 8))) & 0xff);
 }
 
+// Weights of the orientation disc for 4-byte loads: the disc's 31 rows are
+// read as 9 aligned words each (279 (row, word) slots, slot = 9 row + word),
+// the first word starting a = (x - 15) & 3 bytes left of column x - 15. Byte
+// k of word w is column u = 4w + k - a - 15 of row v = row - 15; inside the
+// disc its weights are u (for m10) and v (for m01) as signed bytes, outside 0.
+constexpr int kDiscSlots = 288;  // 9 rounds of 32 lanes over the 279 slots
+__device__ __forceinline__ uint2 disc_weights(int a, int slot) {
+    const int row = slot / 9, word = slot - 9 * row;
+    const int v = row - 15, av = v < 0 ? -v : v;
+    std::uint32_t wu = 0, wv = 0;
+    if (row < 31) {
+        const int hw = disc_half_width(av);
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int u = 4 * word + k - a - 15;
+            if ((u < 0 ? -u : u) <= hw) {
+                wu |= (static_cast<std::uint32_t>(u) & 0xffu) << (8 * k);
+                wv |= (static_cast<std::uint32_t>(v) & 0xffu) << (8 * k);
+            }
+        }
+    }
+    return make_uint2(wu, wv);
+}
+
+// acc + sum of the four unsigned bytes of `bytes` times the four signed bytes of `w`
+__device__ __forceinline__ int dot4_us(std::uint32_t bytes, std::uint32_t w, int acc) {
+    int d;
+    asm("dp4a.u32.s32 %0, %1, %2, %3;" : "=r"(d) : "r"(bytes), "r"(w), "r"(acc));
+    return d;
+}
+
 // cv::fastAtan2 in degrees [0, 360): odd polynomial of the smaller/larger
 // magnitude ratio, every step rounded in float32.
 __device__ __forceinline__ float fast_atan2_deg(float y, float x) {
@@ -1368,6 +1399,7 @@ __device__ __forceinline__ int rotated_sample(const std::uint8_t* centre, int st
 template <class Src>
 __global__ __launch_bounds__(kDescWarps * 32, 8) void describe_kernel(const __grid_constant__ Src src) {
     __shared__ float4 pat[8][32];  // pat[k][l] = pair 8l + k as floats (x0, y0, x1, y1)
+    __shared__ uint2 disc_w[4][kDiscSlots];  // disc_weights(a, slot)
     DescribeJob j;
     int local;
     if (!src.find(blockIdx.x, kDescKind, &j, &local)) return;
@@ -1385,6 +1417,11 @@ __global__ __launch_bounds__(kDescWarps * 32, 8) void describe_kernel(const __gr
         pat[p & 7][p >> 3] = make_float4(static_cast<float>(q.x), static_cast<float>(q.y), static_cast<float>(q.z),
                                          static_cast<float>(q.w));
     }
+    // word loads of the disc need 4-byte aligned rows (block-uniform)
+    const bool words = ((reinterpret_cast<std::uintptr_t>(j.image) | static_cast<std::uintptr_t>(j.pitch)) & 3) == 0;
+    if (words)
+        for (int e = threadIdx.x; e < 4 * kDiscSlots; e += kDescWarps * 32)
+            disc_w[e / kDiscSlots][e % kDiscSlots] = disc_weights(e / kDiscSlots, e % kDiscSlots);
     __syncthreads();
     const int lane = threadIdx.x & 31;
     const int u = lane - 15, au = u < 0 ? -u : u;
@@ -1405,17 +1442,36 @@ __global__ __launch_bounds__(kDescWarps * 32, 8) void describe_kernel(const __gr
             row[lane] = 0;
             continue;
         }
-        // Moments as exact integer sums over the disc: lane l owns column
-        // u = l - 15 and walks the 31 rows, one coalesced row segment per step.
-        const std::uint8_t* centre = j.image + static_cast<std::size_t>(y) * pitch + x;
+        // Moments as exact integer sums over the disc. With aligned rows each
+        // lane takes slots lane, lane + 32, ... of the disc's words (four
+        // pixels per load, weighted by two byte dot products); otherwise lane
+        // l owns column u = l - 15 and walks the 31 rows.
         int m10 = 0, m01 = 0;
+        if (words) {
+            const int xs = x - 15, a = xs & 3;
+            const std::uint8_t* top = j.image + static_cast<std::size_t>(y - 15) * pitch + (xs - a);
 #pragma unroll
-        for (int v = -15; v <= 15; ++v) {
-            const int av = v < 0 ? -v : v;
-            if (lane < 31 && au <= disc_half_width(av)) {
-                const int val = centre[v * pitch + u];
-                m10 += u * val;
-                m01 += v * val;
+            for (int k = 0; k < kDiscSlots / 32; ++k) {
+                const int slot = 32 * k + lane;
+                if (slot < 279) {
+                    const int row = (slot * 57) >> 9, word = slot - 9 * row;  // slot / 9 for slot < 288
+                    const std::uint32_t d =
+                        __ldg(reinterpret_cast<const unsigned int*>(top + static_cast<std::size_t>(row) * pitch + 4 * word));
+                    const uint2 w = disc_w[a][slot];
+                    m10 = dot4_us(d, w.x, m10);
+                    m01 = dot4_us(d, w.y, m01);
+                }
+            }
+        } else {
+            const std::uint8_t* centre = j.image + static_cast<std::size_t>(y) * pitch + x;
+#pragma unroll
+            for (int v = -15; v <= 15; ++v) {
+                const int av = v < 0 ? -v : v;
+                if (lane < 31 && au <= disc_half_width(av)) {
+                    const int val = centre[v * pitch + u];
+                    m10 += u * val;
+                    m01 += v * val;
+                }
             }
         }
 #pragma unroll
