@@ -730,16 +730,34 @@ __global__ __launch_bounds__(kSearchThreads, 3) void search_kernel(const __grid_
                 bool lost = false;
                 for (int base = 0; base < nm; base += 128) {  // warp-uniform trip count
                     const int i0 = base + lane, i1 = i0 + 32, i2 = i0 + 64, i3 = i0 + 96;
-                    const Pt p0 = point_at(j, pts, min(i0, nm - 1));
-                    const Pt p1 = point_at(j, pts, min(i1, nm - 1));
-                    const Pt p2 = point_at(j, pts, min(i2, nm - 1));
-                    const Pt p3 = point_at(j, pts, min(i3, nm - 1));
-                    const double r0 = residual2(h, p0), r1 = residual2(h, p1);
-                    const double r2 = residual2(h, p2), r3 = residual2(h, p3);
-                    acc0 += i0 < nm ? (r0 < thr2 ? r0 : thr2) : 0.0;
-                    acc1 += i1 < nm ? (r1 < thr2 ? r1 : thr2) : 0.0;
-                    acc2 += i2 < nm ? (r2 < thr2 ? r2 : thr2) : 0.0;
-                    acc3 += i3 < nm ? (r3 < thr2 ? r3 : thr2) : 0.0;
+                    if (base + 128 <= nm) {  // every slot of the step holds a point
+                        const Pt p0 = point_at(j, pts, i0), p1 = point_at(j, pts, i1);
+                        const Pt p2 = point_at(j, pts, i2), p3 = point_at(j, pts, i3);
+                        const double r0 = residual2(h, p0), r1 = residual2(h, p1);
+                        const double r2 = residual2(h, p2), r3 = residual2(h, p3);
+                        acc0 += r0 < thr2 ? r0 : thr2;
+                        acc1 += r1 < thr2 ? r1 : thr2;
+                        acc2 += r2 < thr2 ? r2 : thr2;
+                        acc3 += r3 < thr2 ? r3 : thr2;
+                    } else {
+                        // the last, partial step: a virtual lane past nm adds
+                        // +0.0, a no-op on a sum of nonnegative terms, so the
+                        // chains with no point left (warp-uniform) are skipped
+                        const double r0 = residual2(h, point_at(j, pts, min(i0, nm - 1)));
+                        acc0 += i0 < nm ? (r0 < thr2 ? r0 : thr2) : 0.0;
+                        if (base + 32 < nm) {
+                            const double r1 = residual2(h, point_at(j, pts, min(i1, nm - 1)));
+                            acc1 += i1 < nm ? (r1 < thr2 ? r1 : thr2) : 0.0;
+                        }
+                        if (base + 64 < nm) {
+                            const double r2 = residual2(h, point_at(j, pts, min(i2, nm - 1)));
+                            acc2 += i2 < nm ? (r2 < thr2 ? r2 : thr2) : 0.0;
+                        }
+                        if (base + 96 < nm) {
+                            const double r3 = residual2(h, point_at(j, pts, min(i3, nm - 1)));
+                            acc3 += i3 < nm ? (r3 < thr2 ? r3 : thr2) : 0.0;
+                        }
+                    }
                     if (prune && (base & (kPruneEvery - 1)) == kPruneEvery - 128 && base + 128 < nm) {
                         double part = (acc0 + acc2) + (acc1 + acc3);
 #pragma unroll
